@@ -1,0 +1,142 @@
+"""lpmcxx_b200 -- B200-native (sm_100a) DirectSum / TreeSum hot path of lpmCxx.
+
+Python-side convenience layer over the C ABI in include/lpm_b200.h (liblpm_b200.so).  The
+reference-facing C++ drop-in classes live in lpmcxx_b200/host/; this module is what tests and
+bench.py use.  Every compute call goes to the CUDA library; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _capi
+from ._capi import (LPM_KERNEL_BIOT_SAVART_SPHERE, LPM_KERNEL_POISSON_3D, LPM_MESH_CUBED_SPHERE,
+                    LPM_MESH_ICOS_TRI, LPM_PREC_F32, LPM_PREC_F64, KernelDesc, LpmError, check, lib, ptr)
+
+__all__ = [
+    "Context", "SphereMesh", "build_mesh", "mesh_counts", "biot_savart_kernel", "poisson_kernel", "LpmError",
+    "LPM_MESH_ICOS_TRI", "LPM_MESH_CUBED_SPHERE", "LPM_PREC_F64", "LPM_PREC_F32",
+]
+
+MESH_KINDS = {"icos": LPM_MESH_ICOS_TRI, "cube": LPM_MESH_CUBED_SPHERE}
+
+
+def biot_savart_kernel(radius: float = 1.0, delta: float = 0.0) -> KernelDesc:
+    """BiotSavartSphere(delta, sphRadius) (src/LpmVectorKernel.h:19-39)."""
+    return KernelDesc(LPM_KERNEL_BIOT_SAVART_SPHERE, 0, float(radius), float(delta))
+
+
+def poisson_kernel() -> KernelDesc:
+    """1/(4 pi |x - y|), zero at x == y."""
+    return KernelDesc(LPM_KERNEL_POISSON_3D, 0, 1.0, 0.0)
+
+
+@dataclass
+class SphereMesh:
+    """Arrays of a refined sphere mesh in the reference's index order."""
+    kind: str
+    level: int
+    vert_xyz: np.ndarray      # (n_verts, 3)
+    face_xyz: np.ndarray      # (n_faces, 3) centroids
+    face_area: np.ndarray     # (n_faces,) zero for divided faces
+    face_divided: np.ndarray  # (n_faces,) uint8
+
+    @property
+    def leaf(self) -> np.ndarray:
+        return self.face_divided == 0
+
+    @property
+    def n_verts(self) -> int:
+        return self.vert_xyz.shape[0]
+
+    @property
+    def n_faces(self) -> int:
+        return self.face_xyz.shape[0]
+
+
+def mesh_counts(kind: str, level: int) -> tuple[int, int, int]:
+    nv, nf, nl = C.c_int64(), C.c_int64(), C.c_int64()
+    check(lib().lpm_mesh_counts(MESH_KINDS[kind], level, C.byref(nv), C.byref(nf), C.byref(nl)), "lpm_mesh_counts")
+    return nv.value, nf.value, nl.value
+
+
+def build_mesh(kind: str, level: int, radius: float = 1.0) -> SphereMesh:
+    """PolyMesh2d(seed, level) (src/LpmPolyMesh2d.cpp:20-93), generated by the library's host code."""
+    nv, nf, _ = mesh_counts(kind, level)
+    v = np.empty((nv, 3)); f = np.empty((nf, 3)); a = np.empty(nf); d = np.empty(nf, dtype=np.uint8)
+    check(lib().lpm_mesh_build(MESH_KINDS[kind], level, radius, ptr(v), ptr(f), ptr(a), ptr(d)), "lpm_mesh_build")
+    return SphereMesh(kind, level, v, f, a, d)
+
+
+class Context:
+    """One device + stream + scratch buffers (lpm_ctx)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().lpm_ctx_create(device, C.byref(h)), "lpm_ctx_create")
+        self.h = h
+        self.device = device
+
+    def close(self) -> None:
+        if self.h:
+            lib().lpm_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        check(lib().lpm_ctx_set_stream(self.h, stream_handle), "lpm_ctx_set_stream")
+
+    def synchronize(self) -> None:
+        check(lib().lpm_ctx_synchronize(self.h), "lpm_ctx_synchronize")
+
+    @property
+    def launch_count(self) -> int:
+        return lib().lpm_ctx_launch_count(self.h)
+
+    # ---- direct sums
+    def direct_sum_dev(self, kernel: KernelDesc, precision: int, src, tgt, out) -> None:
+        """Device tensors: src (n_src,4) f64, tgt (n_tgt,4) f64, out ({3|1}, n_tgt) f64."""
+        check(lib().lpm_direct_sum_dev(self.h, C.byref(kernel), precision, ptr(src), src.shape[0], ptr(tgt),
+                                       tgt.shape[0], ptr(out)), "lpm_direct_sum_dev")
+
+    def direct_sum_mesh(self, kernel: KernelDesc, precision: int, mesh: SphereMesh, face_src: np.ndarray,
+                        vert_range=None, face_range=None, vert_out=None, face_out=None):
+        """DirectSum::meshSolve on host arrays; returns (vert_out (3,nv), face_out (3,nf))."""
+        nv, nf = mesh.n_verts, mesh.n_faces
+        vb, ve = vert_range if vert_range is not None else (0, nv - 1)
+        fb, fe = face_range if face_range is not None else (0, nf - 1)
+        vx, vy, vz = (np.ascontiguousarray(mesh.vert_xyz[:, c]) for c in range(3))
+        fx, fy, fz = (np.ascontiguousarray(mesh.face_xyz[:, c]) for c in range(3))
+        vo = np.zeros((3, nv)) if vert_out is None else vert_out
+        fo = np.zeros((3, nf)) if face_out is None else face_out
+        src = np.ascontiguousarray(face_src, dtype=np.float64)
+        check(lib().lpm_direct_sum_mesh(self.h, C.byref(kernel), precision, nv, ptr(vx), ptr(vy), ptr(vz), nf,
+                                        ptr(fx), ptr(fy), ptr(fz), ptr(mesh.face_area), ptr(mesh.face_divided),
+                                        ptr(src), vb, ve, fb, fe, ptr(vo[0]), ptr(vo[1]), ptr(vo[2]),
+                                        ptr(fo[0]), ptr(fo[1]), ptr(fo[2])), "lpm_direct_sum_mesh")
+        return vo, fo
+
+    def direct_sum_meshfree(self, kernel: KernelDesc, precision: int, xyz: np.ndarray, src: np.ndarray,
+                            weights: np.ndarray | None = None, rng=None, out=None) -> np.ndarray:
+        n = xyz.shape[0]
+        b, e = rng if rng is not None else (0, n - 1)
+        x, y, z = (np.ascontiguousarray(xyz[:, c]) for c in range(3))
+        o = np.zeros(n) if out is None else out
+        s = np.ascontiguousarray(src, dtype=np.float64)
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        check(lib().lpm_direct_sum_meshfree(self.h, C.byref(kernel), precision, n, ptr(x), ptr(y), ptr(z), ptr(s),
+                                            ptr(w), b, e, ptr(o)), "lpm_direct_sum_meshfree")
+        return o

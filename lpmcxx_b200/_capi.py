@@ -1,0 +1,93 @@
+"""ctypes binding of the C ABI declared in include/lpm_b200.h.
+
+The library is loaded from the package directory (built in-tree by lpmcxx_b200/build.py).  A
+missing library is an error: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "liblpm_b200.so"
+
+LPM_OK = 0
+LPM_ERR_ARG = 1
+LPM_ERR_KERNEL = 2
+LPM_ERR_OOM = 3
+LPM_ERR_CUDA = 4
+LPM_ERR_TIMEOUT = 5
+LPM_ERR_CAPACITY = 6
+LPM_ERR_INTERNAL = 7
+LPM_ERR_NO_DEVICE = 8
+
+LPM_MESH_ICOS_TRI = 1
+LPM_MESH_CUBED_SPHERE = 2
+LPM_KERNEL_BIOT_SAVART_SPHERE = 1
+LPM_KERNEL_POISSON_3D = 2
+LPM_PREC_F64 = 0
+LPM_PREC_F32 = 1
+
+
+class KernelDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("radius", C.c_double), ("delta", C.c_double)]
+
+
+class LpmError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where} failed with status {code}: {msg}")
+        self.code = code
+
+
+P = C.c_void_p
+I64 = C.c_int64
+D = C.c_double
+PD = C.POINTER(C.c_double)
+
+# (name, restype, argtypes): every entry point declared in include/lpm_b200.h
+SIGNATURES = {
+    "lpm_ctx_create": (C.c_int, [C.c_int, C.POINTER(P)]),
+    "lpm_ctx_destroy": (C.c_int, [P]),
+    "lpm_ctx_set_stream": (C.c_int, [P, P]),
+    "lpm_ctx_synchronize": (C.c_int, [P]),
+    "lpm_last_error": (C.c_char_p, []),
+    "lpm_ctx_launch_count": (C.c_int64, [P]),
+    "lpm_mesh_counts": (C.c_int, [C.c_int, C.c_int, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
+    "lpm_mesh_build": (C.c_int, [C.c_int, C.c_int, D, P, P, P, P]),
+    "lpm_direct_sum_dev": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, P, I64, P, I64, P]),
+    "lpm_direct_sum_mesh": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, I64, P, P, P, I64, P, P, P, P, P, P,
+                                      I64, I64, I64, I64, P, P, P, P, P, P]),
+    "lpm_direct_sum_meshfree": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, I64, P, P, P, P, P, I64, I64, P]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load liblpm_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m lpmcxx_b200.build`")
+        h = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | os.RTLD_LOCAL)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(h, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = h
+    return _lib
+
+
+def check(code: int, where: str) -> None:
+    if code != LPM_OK:
+        msg = lib().lpm_last_error()
+        raise LpmError(code, where, msg.decode() if msg else "")
+
+
+def ptr(a) -> int | None:
+    """Address of a numpy array or torch tensor (None for None)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data

@@ -1,0 +1,547 @@
+// Direct (all-pairs) sums: the pair loops of DirectSum::meshSolve (src/LpmDirectSum.cpp:94-167)
+// and DirectSum::meshfreeSolve (src/LpmDirectSum.cpp:175-254) as shared-memory-tiled sm_100a
+// kernels.
+//
+// Layout: sources are packed n x 4 (x, y, z, w) with w = strength (vorticity * area, or charge);
+// a block stages SRC_TILE sources in shared memory and every thread sweeps them against its
+// TPT register-resident targets, so each source is read once per block from HBM/L2 and once
+// per thread from shared memory as a broadcast 128-bit load.
+//
+// FP64 kernels follow the reference formula term by term: den = (R^2 - x.y) + delta^2, the term
+// is dropped when |den| <= 1e-13 (src/LpmVectorKernel.h:24-28).  The sum is reorganised as
+// u = mult * (x cross sum_j (w_j/den_j) y_j), since x cross (.) is linear, which saves the
+// per-pair cross product.
+//
+// FP32 kernels use 1 - x.y = |x - y|^2 / 2 for points on the sphere (no cancellation for close
+// pairs), accumulate sum_j (2 w_j / (r_j^2 + 2 delta^2)) (x - y_j) in FP32 over one shared-memory
+// tile and add each tile's partial into FP64 accumulators (a compensated two-level sum); the
+// final u = -mult * (x cross D) uses the FP64 target position.
+#include "lpm_internal.h"
+
+#include <cmath>
+
+namespace lpm {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double kZeroTol = 1.0e-13;  // ZERO_TOL (src/LpmTypeDefs.h:33-34)
+
+// Reciprocal: hardware approximation refined by two Newton-Raphson steps r <- r + r(1 - d r)
+// (quadratic convergence from ~2^-22 gives full double precision, within one ulp).
+__device__ __forceinline__ double rcp64(double d) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    return fma(r, e, r);
+}
+
+// Reciprocal square root: hardware approximation refined by two Newton-Raphson steps
+// y <- y + (y/2)(1 - a y^2).
+__device__ __forceinline__ double rsqrt64(double a) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+    double t = a * y;
+    double e = fma(-t, y, 1.0);
+    y = fma(0.5 * y, e, y);
+    t = a * y;
+    e = fma(-t, y, 1.0);
+    return fma(0.5 * y, e, y);
+}
+
+__device__ __forceinline__ float rcp32(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rsqrt32(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+constexpr int kThreads = 256;
+constexpr int kTile = 256;
+constexpr int kTpt64 = 2;
+constexpr int kTpt32 = 4;
+
+// ------------------------------------------------------------------ FP64 Biot-Savart
+template <bool kDelta>
+__global__ void __launch_bounds__(kThreads) bs_f64_kernel(const double4* __restrict__ src, int64_t n_src,
+                                                          const double4* __restrict__ tgt, int64_t n_tgt, double r2,
+                                                          double d2, double mult, double* __restrict__ out,
+                                                          int64_t stride) {
+    __shared__ double4 tile[kTile];
+    const int64_t base = (int64_t)blockIdx.x * (kThreads * kTpt64) + threadIdx.x;
+    double tx[kTpt64], ty[kTpt64], tz[kTpt64], sx[kTpt64], sy[kTpt64], sz[kTpt64];
+#pragma unroll
+    for (int t = 0; t < kTpt64; ++t) {
+        const int64_t i = base + t * kThreads;
+        const double4 p = i < n_tgt ? tgt[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+        tx[t] = p.x; ty[t] = p.y; tz[t] = p.z;
+        sx[t] = 0.0; sy[t] = 0.0; sz[t] = 0.0;
+    }
+    for (int64_t j0 = 0; j0 < n_src; j0 += kTile) {
+        __syncthreads();
+        const int64_t j = j0 + threadIdx.x;
+        tile[threadIdx.x] = j < n_src ? src[j] : make_double4(0.0, 0.0, 0.0, 0.0);
+        __syncthreads();
+        const int m = (int)min((int64_t)kTile, n_src - j0);
+#pragma unroll 4
+        for (int k = 0; k < m; ++k) {
+            const double4 s = tile[k];
+#pragma unroll
+            for (int t = 0; t < kTpt64; ++t) {
+                const double dot = tx[t] * s.x + ty[t] * s.y + tz[t] * s.z;
+                double den = r2 - dot;
+                if (kDelta) den += d2;
+                double f = s.w * rcp64(den);
+                f = fabs(den) > kZeroTol ? f : 0.0;
+                sx[t] = fma(f, s.x, sx[t]);
+                sy[t] = fma(f, s.y, sy[t]);
+                sz[t] = fma(f, s.z, sz[t]);
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < kTpt64; ++t) {
+        const int64_t i = base + t * kThreads;
+        if (i < n_tgt) {
+            out[i] = mult * (ty[t] * sz[t] - tz[t] * sy[t]);
+            out[stride + i] = mult * (tz[t] * sx[t] - tx[t] * sz[t]);
+            out[2 * stride + i] = mult * (tx[t] * sy[t] - ty[t] * sx[t]);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ FP64 Poisson 1/(4 pi r)
+__global__ void __launch_bounds__(kThreads) poisson_f64_kernel(const double4* __restrict__ src, int64_t n_src,
+                                                               const double4* __restrict__ tgt, int64_t n_tgt,
+                                                               double mult, double* __restrict__ out) {
+    __shared__ double4 tile[kTile];
+    const int64_t base = (int64_t)blockIdx.x * (kThreads * kTpt64) + threadIdx.x;
+    double tx[kTpt64], ty[kTpt64], tz[kTpt64], phi[kTpt64];
+#pragma unroll
+    for (int t = 0; t < kTpt64; ++t) {
+        const int64_t i = base + t * kThreads;
+        const double4 p = i < n_tgt ? tgt[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+        tx[t] = p.x; ty[t] = p.y; tz[t] = p.z;
+        phi[t] = 0.0;
+    }
+    for (int64_t j0 = 0; j0 < n_src; j0 += kTile) {
+        __syncthreads();
+        const int64_t j = j0 + threadIdx.x;
+        tile[threadIdx.x] = j < n_src ? src[j] : make_double4(0.0, 0.0, 0.0, 0.0);
+        __syncthreads();
+        const int m = (int)min((int64_t)kTile, n_src - j0);
+#pragma unroll 4
+        for (int k = 0; k < m; ++k) {
+            const double4 s = tile[k];
+#pragma unroll
+            for (int t = 0; t < kTpt64; ++t) {
+                const double dx = tx[t] - s.x, dy = ty[t] - s.y, dz = tz[t] - s.z;
+                const double rr = dx * dx + dy * dy + dz * dz;
+                const double inv = rr > 0.0 ? rsqrt64(rr) : 0.0;
+                phi[t] = fma(s.w, inv, phi[t]);
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < kTpt64; ++t) {
+        const int64_t i = base + t * kThreads;
+        if (i < n_tgt) out[i] = mult * phi[t];
+    }
+}
+
+// ------------------------------------------------------------------ FP32 Biot-Savart
+// src.w holds 2*strength.  Coincident (target, source) pairs -- a face-centroid target and its
+// own source -- can only sit at equal indices (see coinc_* arguments); tiles that may contain one
+// run the guarded loop, all others the unguarded one.
+template <bool kGuard, bool kDelta>
+__device__ __forceinline__ void bs_f32_tile(const float4* tile, int m, const float* tx, const float* ty,
+                                            const float* tz, float* ax, float* ay, float* az, float d2x2) {
+#pragma unroll 4
+    for (int k = 0; k < m; ++k) {
+        const float4 s = tile[k];
+#pragma unroll
+        for (int t = 0; t < kTpt32; ++t) {
+            const float dx = tx[t] - s.x, dy = ty[t] - s.y, dz = tz[t] - s.z;
+            float rr = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            if (kDelta) rr += d2x2;
+            float inv = rcp32(rr);
+            if (kGuard) inv = rr > 2.0e-13f ? inv : 0.0f;
+            const float f = s.w * inv;
+            ax[t] = fmaf(f, dx, ax[t]);
+            ay[t] = fmaf(f, dy, ay[t]);
+            az[t] = fmaf(f, dz, az[t]);
+        }
+    }
+}
+
+template <bool kDelta>
+__global__ void __launch_bounds__(kThreads) bs_f32_kernel(const float4* __restrict__ src, int64_t n_src,
+                                                          const float4* __restrict__ tgt,
+                                                          const double4* __restrict__ tgt64, int64_t n_tgt,
+                                                          float d2x2, double mult, double* __restrict__ out,
+                                                          int64_t stride, int64_t coinc_n, int64_t coinc_off) {
+    __shared__ float4 tile[kTile];
+    const int64_t blk0 = (int64_t)blockIdx.x * (kThreads * kTpt32);
+    const int64_t base = blk0 + threadIdx.x;
+    float tx[kTpt32], ty[kTpt32], tz[kTpt32], ax[kTpt32], ay[kTpt32], az[kTpt32];
+    double Dx[kTpt32], Dy[kTpt32], Dz[kTpt32];
+#pragma unroll
+    for (int t = 0; t < kTpt32; ++t) {
+        const int64_t i = base + t * kThreads;
+        const float4 p = i < n_tgt ? tgt[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        tx[t] = p.x; ty[t] = p.y; tz[t] = p.z;
+        Dx[t] = 0.0; Dy[t] = 0.0; Dz[t] = 0.0;
+    }
+    // source indices that may coincide with this block's targets
+    const int64_t c_lo = blk0 < coinc_n ? blk0 + coinc_off : INT64_MAX;
+    const int64_t c_hi = blk0 < coinc_n ? min(blk0 + kThreads * kTpt32, coinc_n) + coinc_off : INT64_MIN;
+    for (int64_t j0 = 0; j0 < n_src; j0 += kTile) {
+        __syncthreads();
+        const int64_t j = j0 + threadIdx.x;
+        tile[threadIdx.x] = j < n_src ? src[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        const int m = (int)min((int64_t)kTile, n_src - j0);
+#pragma unroll
+        for (int t = 0; t < kTpt32; ++t) { ax[t] = 0.f; ay[t] = 0.f; az[t] = 0.f; }
+        if (j0 < c_hi && j0 + m > c_lo)
+            bs_f32_tile<true, kDelta>(tile, m, tx, ty, tz, ax, ay, az, d2x2);
+        else
+            bs_f32_tile<false, kDelta>(tile, m, tx, ty, tz, ax, ay, az, d2x2);
+#pragma unroll
+        for (int t = 0; t < kTpt32; ++t) { Dx[t] += ax[t]; Dy[t] += ay[t]; Dz[t] += az[t]; }
+    }
+#pragma unroll
+    for (int t = 0; t < kTpt32; ++t) {
+        const int64_t i = base + t * kThreads;
+        if (i < n_tgt) {
+            const double4 p = tgt64[i];
+            const double nm = -mult;
+            out[i] = nm * (p.y * Dz[t] - p.z * Dy[t]);
+            out[stride + i] = nm * (p.z * Dx[t] - p.x * Dz[t]);
+            out[2 * stride + i] = nm * (p.x * Dy[t] - p.y * Dx[t]);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ FP32 Poisson
+template <bool kGuard>
+__device__ __forceinline__ void poisson_f32_tile(const float4* tile, int m, const float* tx, const float* ty,
+                                                 const float* tz, float* acc) {
+#pragma unroll 4
+    for (int k = 0; k < m; ++k) {
+        const float4 s = tile[k];
+#pragma unroll
+        for (int t = 0; t < kTpt32; ++t) {
+            const float dx = tx[t] - s.x, dy = ty[t] - s.y, dz = tz[t] - s.z;
+            const float rr = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            float inv = rsqrt32(rr);
+            if (kGuard) inv = rr > 0.0f ? inv : 0.0f;
+            acc[t] = fmaf(s.w, inv, acc[t]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) poisson_f32_kernel(const float4* __restrict__ src, int64_t n_src,
+                                                               const float4* __restrict__ tgt, int64_t n_tgt,
+                                                               double mult, double* __restrict__ out, int64_t coinc_n,
+                                                               int64_t coinc_off) {
+    __shared__ float4 tile[kTile];
+    const int64_t blk0 = (int64_t)blockIdx.x * (kThreads * kTpt32);
+    const int64_t base = blk0 + threadIdx.x;
+    float tx[kTpt32], ty[kTpt32], tz[kTpt32], acc[kTpt32];
+    double phi[kTpt32];
+#pragma unroll
+    for (int t = 0; t < kTpt32; ++t) {
+        const int64_t i = base + t * kThreads;
+        const float4 p = i < n_tgt ? tgt[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        tx[t] = p.x; ty[t] = p.y; tz[t] = p.z;
+        phi[t] = 0.0;
+    }
+    const int64_t c_lo = blk0 < coinc_n ? blk0 + coinc_off : INT64_MAX;
+    const int64_t c_hi = blk0 < coinc_n ? min(blk0 + kThreads * kTpt32, coinc_n) + coinc_off : INT64_MIN;
+    for (int64_t j0 = 0; j0 < n_src; j0 += kTile) {
+        __syncthreads();
+        const int64_t j = j0 + threadIdx.x;
+        tile[threadIdx.x] = j < n_src ? src[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        const int m = (int)min((int64_t)kTile, n_src - j0);
+#pragma unroll
+        for (int t = 0; t < kTpt32; ++t) acc[t] = 0.f;
+        if (j0 < c_hi && j0 + m > c_lo)
+            poisson_f32_tile<true>(tile, m, tx, ty, tz, acc);
+        else
+            poisson_f32_tile<false>(tile, m, tx, ty, tz, acc);
+#pragma unroll
+        for (int t = 0; t < kTpt32; ++t) phi[t] += acc[t];
+    }
+#pragma unroll
+    for (int t = 0; t < kTpt32; ++t) {
+        const int64_t i = base + t * kThreads;
+        if (i < n_tgt) out[i] = mult * phi[t];
+    }
+}
+
+__global__ void pack_f32_kernel(const double4* __restrict__ in, int64_t n, float4* __restrict__ out, float wscale) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const double4 p = in[i];
+        out[i] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)(p.w * wscale));
+    }
+}
+
+}  // namespace
+
+int pack_f32(lpm_ctx* ctx, const double4* in, int64_t n, float4* out, bool scale_w2) {
+    if (n <= 0) return LPM_OK;
+    pack_f32_kernel<<<grid_for(n, 256), 256, 0, ctx->stream>>>(in, n, out, scale_w2 ? 2.0f : 1.0f);
+    LPM_LAUNCH_CHECK(ctx);
+    return LPM_OK;
+}
+
+int direct_sum_f64(lpm_ctx* ctx, const lpm_kernel_desc& k, const double4* src, int64_t n_src, const double4* tgt,
+                   int64_t n_tgt, double* out, int64_t out_stride) {
+    if (n_tgt <= 0) return LPM_OK;
+    const unsigned grid = grid_for(n_tgt, kThreads * kTpt64);
+    if (k.kind == LPM_KERNEL_BIOT_SAVART_SPHERE) {
+        const double mult = -1.0 / (4.0 * kPi * k.radius);
+        const double r2 = k.radius * k.radius, d2 = k.delta * k.delta;
+        if (k.delta != 0.0)
+            bs_f64_kernel<true><<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, n_tgt, r2, d2, mult, out,
+                                                                    out_stride);
+        else
+            bs_f64_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, n_tgt, r2, d2, mult, out,
+                                                                     out_stride);
+    } else if (k.kind == LPM_KERNEL_POISSON_3D) {
+        poisson_f64_kernel<<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, n_tgt, 1.0 / (4.0 * kPi), out);
+    } else {
+        set_error("invalid kernel");
+        return LPM_ERR_KERNEL;
+    }
+    LPM_LAUNCH_CHECK(ctx);
+    return LPM_OK;
+}
+
+// FP32 sums take FP32 copies of sources (w pre-scaled by 2 for Biot-Savart) and targets, plus the
+// FP64 targets for the Biot-Savart epilogue.  Targets 0..coinc_n-1 may coincide with sources
+// coinc_off..coinc_off+coinc_n-1 (face-centroid targets and their own sources).
+int direct_sum_f32_impl(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* src, int64_t n_src, const float4* tgt,
+                        const double4* tgt64, int64_t n_tgt, double* out, int64_t out_stride, int64_t coinc_n,
+                        int64_t coinc_off) {
+    if (n_tgt <= 0) return LPM_OK;
+    const unsigned grid = grid_for(n_tgt, kThreads * kTpt32);
+    if (k.kind == LPM_KERNEL_BIOT_SAVART_SPHERE) {
+        const double mult = -1.0 / (4.0 * kPi * k.radius);
+        if (k.delta != 0.0)
+            bs_f32_kernel<true><<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, tgt64, n_tgt,
+                                                                    (float)(2.0 * k.delta * k.delta), mult, out,
+                                                                    out_stride, coinc_n, coinc_off);
+        else
+            bs_f32_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, tgt64, n_tgt, 0.0f, mult, out,
+                                                                     out_stride, coinc_n, coinc_off);
+    } else if (k.kind == LPM_KERNEL_POISSON_3D) {
+        poisson_f32_kernel<<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, n_tgt, 1.0 / (4.0 * kPi), out,
+                                                               coinc_n, coinc_off);
+    } else {
+        set_error("invalid kernel");
+        return LPM_ERR_KERNEL;
+    }
+    LPM_LAUNCH_CHECK(ctx);
+    return LPM_OK;
+}
+
+static int check_kernel(const lpm_kernel_desc* k) {
+    if (!k) {
+        set_error("null kernel descriptor");
+        return LPM_ERR_ARG;
+    }
+    if (k->kind != LPM_KERNEL_BIOT_SAVART_SPHERE && k->kind != LPM_KERNEL_POISSON_3D) {
+        set_error("invalid kernel");
+        return LPM_ERR_KERNEL;
+    }
+    if (k->kind == LPM_KERNEL_BIOT_SAVART_SPHERE && !(k->radius > 0.0)) {
+        set_error("Biot-Savart kernel needs radius > 0");
+        return LPM_ERR_ARG;
+    }
+    return LPM_OK;
+}
+
+// Device entry shared by the C ABI: FP64 or FP32 (FP32 copies go to scratch slots).
+int direct_sum_any(lpm_ctx* ctx, const lpm_kernel_desc& k, int precision, const double4* src, int64_t n_src,
+                   const double4* tgt, int64_t n_tgt, double* out, int64_t coinc_n, int64_t coinc_off) {
+    if (precision == LPM_PREC_F64) return direct_sum_f64(ctx, k, src, n_src, tgt, n_tgt, out, n_tgt);
+    if (precision != LPM_PREC_F32) {
+        set_error("unknown precision %d", precision);
+        return LPM_ERR_ARG;
+    }
+    float4* s32 = (float4*)scratch(ctx, kSlotSrc32, sizeof(float4) * (size_t)std::max<int64_t>(n_src, 1));
+    float4* t32 = (float4*)scratch(ctx, kSlotTgt32, sizeof(float4) * (size_t)std::max<int64_t>(n_tgt, 1));
+    if (!s32 || !t32) return LPM_ERR_OOM;
+    int rc = pack_f32(ctx, src, n_src, s32, k.kind == LPM_KERNEL_BIOT_SAVART_SPHERE);
+    if (rc) return rc;
+    rc = pack_f32(ctx, tgt, n_tgt, t32, false);
+    if (rc) return rc;
+    return direct_sum_f32_impl(ctx, k, s32, n_src, t32, tgt, n_tgt, out, n_tgt, coinc_n, coinc_off);
+}
+
+}  // namespace lpm
+
+using namespace lpm;
+
+extern "C" int lpm_direct_sum_dev(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precision, const double* src,
+                                  int64_t n_src, const double* tgt, int64_t n_tgt, double* out) {
+    if (!ctx) {
+        set_error("null context");
+        return LPM_ERR_ARG;
+    }
+    int rc = check_kernel(kernel);
+    if (rc) return rc;
+    if (n_src < 0 || n_tgt < 0 || (n_src > 0 && !src) || (n_tgt > 0 && (!tgt || !out))) {
+        set_error("lpm_direct_sum_dev: bad sizes or null pointers");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(ctx->device));
+    // targets that alias the source array coincide with them index by index
+    int64_t coinc_n = 0;
+    if ((const double*)tgt == src) coinc_n = std::min(n_src, n_tgt);
+    return direct_sum_any(ctx, *kernel, precision, (const double4*)src, n_src, (const double4*)tgt, n_tgt, out,
+                          coinc_n, 0);
+}
+
+extern "C" int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precision, int64_t n_verts,
+                                   const double* vx, const double* vy, const double* vz, int64_t n_faces,
+                                   const double* fx, const double* fy, const double* fz, const double* face_area,
+                                   const uint8_t* face_divided, const double* face_src, int64_t vert_begin,
+                                   int64_t vert_end, int64_t face_begin, int64_t face_end, double* vert_out0,
+                                   double* vert_out1, double* vert_out2, double* face_out0, double* face_out1,
+                                   double* face_out2) {
+    if (!ctx) {
+        set_error("null context");
+        return LPM_ERR_ARG;
+    }
+    int rc = check_kernel(kernel);
+    if (rc) return rc;
+    if (kernel->kind != LPM_KERNEL_BIOT_SAVART_SPHERE) {
+        set_error("invalid kernel: lpm_direct_sum_mesh takes a vector kernel");
+        return LPM_ERR_KERNEL;
+    }
+    if (n_verts < 0 || n_faces < 0 || (n_verts > 0 && (!vx || !vy || !vz)) ||
+        (n_faces > 0 && (!fx || !fy || !fz || !face_area || !face_divided || !face_src))) {
+        set_error("lpm_direct_sum_mesh: null input arrays");
+        return LPM_ERR_ARG;
+    }
+    // empty ranges (end < begin) are allowed, as for a rank with no items
+    const bool do_v = vert_end >= vert_begin, do_f = face_end >= face_begin;
+    if ((do_v && (vert_begin < 0 || vert_end >= n_verts || !vert_out0 || !vert_out1 || !vert_out2)) ||
+        (do_f && (face_begin < 0 || face_end >= n_faces || !face_out0 || !face_out1 || !face_out2))) {
+        set_error("lpm_direct_sum_mesh: target range out of bounds or null outputs");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(ctx->device));
+    // sources: undivided faces in index order; face targets: undivided faces in [face_begin, face_end]
+    int64_t n_src = 0, src_before_fb = 0, n_ft = 0;
+    for (int64_t i = 0; i < n_faces; ++i) {
+        if (!face_divided[i]) {
+            if (i < face_begin) ++src_before_fb;
+            if (do_f && i >= face_begin && i <= face_end) ++n_ft;
+            ++n_src;
+        }
+    }
+    const int64_t n_vt = do_v ? vert_end - vert_begin + 1 : 0;
+    const int64_t n_tgt = n_ft + n_vt;
+    const size_t in_bytes = sizeof(double4) * (size_t)(n_src + n_tgt);
+    const size_t out_bytes = sizeof(double) * 3 * (size_t)n_tgt;
+    double* host = (double*)pinned(ctx, in_bytes + out_bytes);
+    if (!host) return LPM_ERR_OOM;
+    double4* hsrc = (double4*)host;
+    double4* htgt = hsrc + n_src;
+    double* hout = (double*)(htgt + n_tgt);
+    int64_t s = 0, t = 0;
+    for (int64_t i = 0; i < n_faces; ++i) {
+        if (face_divided[i]) continue;
+        hsrc[s++] = make_double4(fx[i], fy[i], fz[i], face_src[i] * face_area[i]);
+        if (do_f && i >= face_begin && i <= face_end) htgt[t++] = make_double4(fx[i], fy[i], fz[i], 0.0);
+    }
+    for (int64_t i = 0; i < n_vt; ++i) {
+        const int64_t v = vert_begin + i;
+        htgt[t++] = make_double4(vx[v], vy[v], vz[v], 0.0);
+    }
+    double4* dsrc = (double4*)scratch(ctx, kSlotSrcPack, sizeof(double4) * (size_t)std::max<int64_t>(n_src, 1));
+    double4* dtgt = (double4*)scratch(ctx, kSlotTgtPack, sizeof(double4) * (size_t)std::max<int64_t>(n_tgt, 1));
+    double* dout = (double*)scratch(ctx, kSlotOut, std::max<size_t>(out_bytes, 8));
+    if (!dsrc || !dtgt || !dout) return LPM_ERR_OOM;
+    if (n_tgt > 0) {
+        if (n_src > 0)
+            LPM_CUDA_TRY(cudaMemcpyAsync(dsrc, hsrc, sizeof(double4) * (size_t)n_src, cudaMemcpyHostToDevice,
+                                         ctx->stream));
+        LPM_CUDA_TRY(cudaMemcpyAsync(dtgt, htgt, sizeof(double4) * (size_t)n_tgt, cudaMemcpyHostToDevice, ctx->stream));
+        rc = direct_sum_any(ctx, *kernel, precision, dsrc, n_src, dtgt, n_tgt, dout, n_ft, src_before_fb);
+        if (rc) return rc;
+        LPM_CUDA_TRY(cudaMemcpyAsync(hout, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    }
+    t = 0;
+    for (int64_t i = face_begin; do_f && i <= face_end; ++i) {
+        if (face_divided[i]) continue;
+        face_out0[i] = hout[t];
+        face_out1[i] = hout[n_tgt + t];
+        face_out2[i] = hout[2 * n_tgt + t];
+        ++t;
+    }
+    for (int64_t i = 0; i < n_vt; ++i, ++t) {
+        vert_out0[vert_begin + i] = hout[t];
+        vert_out1[vert_begin + i] = hout[n_tgt + t];
+        vert_out2[vert_begin + i] = hout[2 * n_tgt + t];
+    }
+    return LPM_OK;
+}
+
+extern "C" int lpm_direct_sum_meshfree(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precision, int64_t n,
+                                       const double* x, const double* y, const double* z, const double* src,
+                                       const double* weights, int64_t begin, int64_t end, double* out) {
+    if (!ctx) {
+        set_error("null context");
+        return LPM_ERR_ARG;
+    }
+    int rc = check_kernel(kernel);
+    if (rc) return rc;
+    if (kernel->kind != LPM_KERNEL_POISSON_3D) {
+        set_error("invalid kernel: lpm_direct_sum_meshfree takes a scalar kernel");
+        return LPM_ERR_KERNEL;
+    }
+    if (n < 0 || (n > 0 && (!x || !y || !z || !src))) {
+        set_error("lpm_direct_sum_meshfree: null input arrays");
+        return LPM_ERR_ARG;
+    }
+    const bool any = end >= begin;
+    if (any && (begin < 0 || end >= n || !out)) {
+        set_error("lpm_direct_sum_meshfree: target range out of bounds");
+        return LPM_ERR_ARG;
+    }
+    if (!any || n == 0) return LPM_OK;
+    LPM_CUDA_TRY(cudaSetDevice(ctx->device));
+    const int64_t n_tgt = end - begin + 1;
+    const size_t in_bytes = sizeof(double4) * (size_t)n;
+    const size_t out_bytes = sizeof(double) * (size_t)n_tgt;
+    double* host = (double*)pinned(ctx, in_bytes + out_bytes);
+    if (!host) return LPM_ERR_OOM;
+    double4* hsrc = (double4*)host;
+    double* hout = (double*)(hsrc + n);
+    for (int64_t i = 0; i < n; ++i)
+        hsrc[i] = make_double4(x[i], y[i], z[i], weights ? src[i] * weights[i] : src[i]);
+    double4* dsrc = (double4*)scratch(ctx, kSlotSrcPack, in_bytes);
+    double* dout = (double*)scratch(ctx, kSlotOut, out_bytes);
+    if (!dsrc || !dout) return LPM_ERR_OOM;
+    LPM_CUDA_TRY(cudaMemcpyAsync(dsrc, hsrc, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    rc = direct_sum_any(ctx, *kernel, precision, dsrc, n, dsrc + begin, n_tgt, dout, n_tgt, begin);
+    if (rc) return rc;
+    LPM_CUDA_TRY(cudaMemcpyAsync(hout, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int64_t i = 0; i < n_tgt; ++i) out[begin + i] = hout[i];
+    return LPM_OK;
+}

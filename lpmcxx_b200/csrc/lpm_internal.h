@@ -1,0 +1,110 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include "../../include/lpm_b200.h"
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#endif
+
+namespace lpm {
+
+// Thread-local last-error message behind lpm_last_error().
+void set_error(const char* fmt, ...);
+
+}  // namespace lpm
+
+#ifdef __CUDACC__
+
+// A growable device buffer owned by a context.  Buffers only grow; they are freed with the
+// context.  Growth happens outside any stream capture (the RK4 graph is captured after warm-up).
+struct LpmBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct lpm_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int64_t launches = 0;
+    // scratch slots, indexed by the enum below
+    LpmBuffer buf[32];
+    // pinned host staging (host-facing entry points)
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+};
+
+namespace lpm {
+
+enum ScratchSlot {
+    kSlotSrcPack = 0,   // packed sources (double4)
+    kSlotTgtPack,       // packed targets (double4)
+    kSlotOut,           // outputs (component-major)
+    kSlotSrc32,         // FP32 source copies
+    kSlotTgt32,         // FP32 target copies
+    kSlotMisc0,
+    kSlotMisc1,
+    kSlotMisc2,
+    kSlotMisc3,
+    kSlotTree0,
+    kSlotTree1,
+    kSlotTree2,
+    kSlotTree3,
+    kSlotTree4,
+    kSlotTree5,
+    kSlotTree6,
+    kSlotTree7,
+    kSlotTree8,
+    kSlotTree9,
+    kSlotTree10,
+    kSlotTree11,
+    kSlotTree12,
+    kSlotTree13,
+    kSlotTree14,
+    kSlotRk0,
+    kSlotRk1,
+    kSlotRk2,
+    kSlotRk3,
+    kSlotRk4,
+    kSlotRk5,
+    kSlotCount
+};
+
+// Ensure ctx scratch slot `slot` holds at least `bytes`; returns nullptr (and sets the error)
+// on allocation failure.
+void* scratch(lpm_ctx* ctx, int slot, size_t bytes);
+void* pinned(lpm_ctx* ctx, size_t bytes);
+
+int cuda_status(cudaError_t e, const char* what);
+
+#define LPM_CUDA_TRY(call)                                              \
+    do {                                                                \
+        cudaError_t e_ = (call);                                        \
+        if (e_ != cudaSuccess) return ::lpm::cuda_status(e_, #call);    \
+    } while (0)
+
+#define LPM_LAUNCH_CHECK(ctx)                                           \
+    do {                                                                \
+        (ctx)->launches += 1;                                           \
+        cudaError_t e_ = cudaGetLastError();                            \
+        if (e_ != cudaSuccess) return ::lpm::cuda_status(e_, "kernel launch"); \
+    } while (0)
+
+inline unsigned grid_for(int64_t n, int per_block) { return (unsigned)((n + per_block - 1) / per_block); }
+
+// direct sums (direct_sum.cu)
+int direct_sum_f64(lpm_ctx* ctx, const lpm_kernel_desc& k, const double4* src, int64_t n_src, const double4* tgt,
+                   int64_t n_tgt, double* out, int64_t out_stride);
+int direct_sum_f32(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* src, int64_t n_src, const float4* tgt,
+                   int64_t n_tgt, double* out, int64_t out_stride, bool maybe_coincident);
+int pack_f32(lpm_ctx* ctx, const double4* in, int64_t n, float4* out, bool scale_w2);
+
+}  // namespace lpm
+
+#endif  // __CUDACC__

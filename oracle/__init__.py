@@ -1,0 +1,84 @@
+"""FP64 CPU oracle for the DirectSum / TreeSum hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this package.  It is
+the checker the CUDA library is compared against, never part of the product path.
+
+* liboracle.so: the repo's own C restatement (lpm_oracle.c), pinned against the reference;
+* _ref/ref_harness: the unmodified reference built from its sources (Makefile target `ref`),
+  present only where the reference tree was available at build time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF_HARNESS = HERE / "_ref" / "ref_harness"
+
+_lib = None
+
+
+def build(ref: bool = False) -> None:
+    """Compile liboracle.so (and, with ref=True, the reference harness under _ref/)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        h = C.CDLL(str(LIB))
+        P, I, D = C.c_void_p, C.c_int64, C.c_double
+        h.oracle_bs_direct.argtypes = [P, I, P, I, D, D, P]
+        h.oracle_poisson_direct.argtypes = [P, I, P, I, P]
+        _lib = h
+    return _lib
+
+
+def _c(a, dtype=np.float64):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def pack4(xyz: np.ndarray, w: np.ndarray | None = None) -> np.ndarray:
+    out = np.zeros((xyz.shape[0], 4))
+    out[:, :3] = xyz
+    if w is not None:
+        out[:, 3] = w
+    return out
+
+
+def bs_direct(src4: np.ndarray, tgt4: np.ndarray, radius: float = 1.0, delta: float = 0.0) -> np.ndarray:
+    """Biot-Savart direct sum (reference formula per pair); returns (3, n_tgt)."""
+    src4, tgt4 = _c(src4), _c(tgt4)
+    out = np.zeros((3, tgt4.shape[0]))
+    lib().oracle_bs_direct(src4.ctypes.data, src4.shape[0], tgt4.ctypes.data, tgt4.shape[0], radius, delta,
+                           out.ctypes.data)
+    return out
+
+
+def poisson_direct(src4: np.ndarray, tgt4: np.ndarray) -> np.ndarray:
+    src4, tgt4 = _c(src4), _c(tgt4)
+    out = np.zeros(tgt4.shape[0])
+    lib().oracle_poisson_direct(src4.ctypes.data, src4.shape[0], tgt4.ctypes.data, tgt4.shape[0], out.ctypes.data)
+    return out
+
+
+def run_ref_harness(*args: str, env: dict | None = None) -> str:
+    """Run the compiled reference harness (raises FileNotFoundError when it was not built)."""
+    if not REF_HARNESS.exists():
+        raise FileNotFoundError(str(REF_HARNESS))
+    e = dict(os.environ)
+    e.setdefault("LPM_MESH_SEED_DIR", str(HERE / "_ref" / "meshSeeds"))
+    if env:
+        e.update(env)
+    p = subprocess.run([str(REF_HARNESS), *map(str, args)], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                       env=e, check=True)
+    return p.stdout

@@ -1,0 +1,130 @@
+/*
+ * lpm_oracle.c -- FP64 CPU restatement of lpmCxx's DirectSum / TreeSum hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see lpm_oracle.h): the checker, never the product.  Parity is pinned
+ * against the reference itself: tests/test_oracle.py compares these functions with outputs of the
+ * reference compiled from its sources (tests/golden/, made by tests/golden/make_golden.py).
+ */
+#include "lpm_oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+/* ---- minimal thread pool: split [0, n) into contiguous chunks over ORACLE_THREADS threads
+ * (default: all online cores).  Results do not depend on the thread count: every index is
+ * computed by exactly one thread with the same sequential inner loop. */
+typedef void (*range_fn)(void* arg, int64_t i0, int64_t i1);
+typedef struct {
+    range_fn fn;
+    void* arg;
+    int64_t i0, i1;
+} range_job;
+static void* range_thread(void* p) {
+    range_job* j = (range_job*)p;
+    j->fn(j->arg, j->i0, j->i1);
+    return NULL;
+}
+int oracle_threads(void) {
+    const char* s = getenv("ORACLE_THREADS");
+    int n = s ? atoi(s) : (int)sysconf(_SC_NPROCESSORS_ONLN);
+    return n < 1 ? 1 : (n > 256 ? 256 : n);
+}
+static void parallel_range(int64_t n, range_fn fn, void* arg) {
+    int nt = oracle_threads();
+    if (n < 256 || nt == 1) {
+        fn(arg, 0, n);
+        return;
+    }
+    if (nt > n) nt = (int)n;
+    pthread_t th[256];
+    range_job jobs[256];
+    const int64_t chunk = (n + nt - 1) / nt;
+    int started = 0;
+    for (int t = 0; t < nt; ++t) {
+        jobs[t].fn = fn; jobs[t].arg = arg;
+        jobs[t].i0 = t * chunk;
+        jobs[t].i1 = (t + 1) * chunk < n ? (t + 1) * chunk : n;
+        if (jobs[t].i0 >= jobs[t].i1) break;
+        if (pthread_create(&th[t], NULL, range_thread, &jobs[t]) != 0) {
+            range_thread(&jobs[t]);
+            th[t] = 0;
+        }
+        started = t + 1;
+    }
+    for (int t = 0; t < started; ++t)
+        if (th[t]) pthread_join(th[t], NULL);
+}
+
+static const double kPi = 3.1415926535897932384626433832795027975; /* src/LpmTypeDefs.h:18 */
+static const double kZeroTol = 1.0e-13;                              /* src/LpmTypeDefs.h:33 */
+
+/* BiotSavartSphere::evaluate (src/LpmVectorKernel.h:24-28) accumulated as in the vector branch of
+ * DirectSum::meshSolve (src/LpmDirectSum.cpp:104-118): k = (t x s) / den, k *= strength, sum += k,
+ * then sum *= -1/(4 pi R). */
+typedef struct {
+    const double *src, *tgt;
+    int64_t n_src, n_tgt;
+    double radius, delta;
+    double* out;
+} direct_args;
+
+static void bs_direct_range(void* p, int64_t i0, int64_t i1) {
+    const direct_args* a = (const direct_args*)p;
+    const double* src = a->src;
+    const double* tgt = a->tgt;
+    const int64_t n_src = a->n_src, n_tgt = a->n_tgt;
+    const double radius = a->radius, delta = a->delta;
+    double* out = a->out;
+    const double mult = -1.0 / (4.0 * kPi * radius);
+    for (int64_t i = i0; i < i1; ++i) {
+        const double tx = tgt[4 * i], ty = tgt[4 * i + 1], tz = tgt[4 * i + 2];
+        double ux = 0.0, uy = 0.0, uz = 0.0;
+        for (int64_t j = 0; j < n_src; ++j) {
+            const double sx = src[4 * j], sy = src[4 * j + 1], sz = src[4 * j + 2], w = src[4 * j + 3];
+            double cx = ty * sz - tz * sy, cy = tz * sx - tx * sz, cz = tx * sy - ty * sx;
+            const double den = radius * radius - (tx * sx + ty * sy + tz * sz) + delta * delta;
+            if (fabs(den) > kZeroTol) {
+                const double inv = 1.0 / den;
+                cx *= inv; cy *= inv; cz *= inv;
+            } else {
+                cx = 0.0; cy = 0.0; cz = 0.0;
+            }
+            ux += cx * w; uy += cy * w; uz += cz * w;
+        }
+        out[i] = ux * mult;
+        out[n_tgt + i] = uy * mult;
+        out[2 * n_tgt + i] = uz * mult;
+    }
+}
+
+void oracle_bs_direct(const double* src, int64_t n_src, const double* tgt, int64_t n_tgt, double radius,
+                      double delta, double* out) {
+    direct_args a = {src, tgt, n_src, n_tgt, radius, delta, out};
+    parallel_range(n_tgt, bs_direct_range, &a);
+}
+
+static void poisson_direct_range(void* p, int64_t i0, int64_t i1) {
+    const direct_args* a = (const direct_args*)p;
+    const double* src = a->src;
+    const double* tgt = a->tgt;
+    const int64_t n_src = a->n_src;
+    double* out = a->out;
+    for (int64_t i = i0; i < i1; ++i) {
+        const double tx = tgt[4 * i], ty = tgt[4 * i + 1], tz = tgt[4 * i + 2];
+        double phi = 0.0;
+        for (int64_t j = 0; j < n_src; ++j) {
+            const double dx = tx - src[4 * j], dy = ty - src[4 * j + 1], dz = tz - src[4 * j + 2];
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            phi += (r > 0.0 ? 1.0 / (4.0 * kPi * r) : 0.0) * src[4 * j + 3];
+        }
+        out[i] = phi;
+    }
+}
+
+void oracle_poisson_direct(const double* src, int64_t n_src, const double* tgt, int64_t n_tgt, double* out) {
+    direct_args a = {src, tgt, n_src, n_tgt, 0.0, 0.0, out};
+    parallel_range(n_tgt, poisson_direct_range, &a);
+}

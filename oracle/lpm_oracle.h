@@ -1,0 +1,26 @@
+/*
+ * lpm_oracle.h -- FP64 CPU restatement of lpmCxx's DirectSum / TreeSum hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker the CUDA library is compared against.  Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it; the product never does.
+ * Each function cites the reference code it restates.  The restatement itself is pinned against
+ * the reference compiled from its own sources (oracle/_ref/ref_harness) through the golden
+ * fixtures in tests/golden/.
+ */
+#ifndef LPM_ORACLE_H
+#define LPM_ORACLE_H
+#include <stdint.h>
+
+/* Biot-Savart direct sum, reference formula per pair (src/LpmVectorKernel.h:24-28,
+ * src/LpmDirectSum.cpp:104-166): out[c*n_tgt+i] = -1/(4 pi R) sum_j w_j (t_i x s_j)/(R^2 - t.s + d^2),
+ * terms with |den| <= 1e-13 dropped.  src: n_src x 4 (x,y,z,w); tgt: n_tgt x 4. */
+void oracle_bs_direct(const double* src, int64_t n_src, const double* tgt, int64_t n_tgt, double radius,
+                      double delta, double* out);
+
+/* 1/(4 pi |x-y|) direct sum, zero at x == y (DirectSum::meshfreeSolve, src/LpmDirectSum.cpp:240-252). */
+void oracle_poisson_direct(const double* src, int64_t n_src, const double* tgt, int64_t n_tgt, double* out);
+
+/* Number of host threads the oracle uses (ORACLE_THREADS, default: all online cores). */
+int oracle_threads(void);
+
+#endif

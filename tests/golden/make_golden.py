@@ -1,0 +1,70 @@
+"""Regenerate the golden fixtures in this directory from the UNMODIFIED lpmCxx reference.
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+The reference is compiled from its own sources by oracle/Makefile (target `ref`) against the
+single-rank MPI stub in oracle/mpi_stub/; oracle/ref_harness.cpp drives its public API and dumps
+.npy files, which this script packs into small .npz fixtures.  The fixtures are committed; the
+reference tree itself is not needed to run the tests.
+
+Fixtures
+  mesh_{icos,cube}3.npz      PolyMesh2d(seed, 3): vertices, centroids, areas, divided mask
+  direct_icos4_rh.npz        DirectSum::meshSolve, BiotSavartSphere(), icos level 4, RH m=4 wave
+  direct_cube3_gauss_d05.npz DirectSum::meshSolve, BiotSavartSphere(0.05) (non-singular branch),
+                             cube level 3, Gaussian vortex
+  direct_icos3_rh_r2.npz     MPIReplicatedData rank 1 of 3: only that rank's target slice is written
+  poisson_2000.npz           DirectSum::meshfreeSolve with a 1/(4 pi r) ScalarKernel, 2000 points
+"""
+from __future__ import annotations
+
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+
+import oracle  # noqa: E402
+
+
+def harness(*args, env=None) -> Path:
+    out = Path(tempfile.mkdtemp(prefix="lpm_golden_"))
+    oracle.run_ref_harness(*args, out, env=env)
+    return out
+
+
+def load(d: Path, *names) -> dict:
+    return {n: np.load(d / f"{n}.npy") for n in names}
+
+
+def main() -> None:
+    for kind in ("icos", "cube"):
+        d = harness("mesh", kind, 3)
+        np.savez_compressed(HERE / f"mesh_{kind}3.npz",
+                            **load(d, "vert_xyz", "face_xyz", "face_area", "face_divided"))
+
+    d = harness("direct", "icos", 4, "rh", 0.0)
+    np.savez_compressed(HERE / "direct_icos4_rh.npz", **load(d, "face_zeta", "vert_vel", "face_vel"),
+                        face_xyz_sum=np.load(d / "face_xyz.npy").sum(axis=0))
+
+    d = harness("direct", "cube", 3, "gauss", 0.05)
+    np.savez_compressed(HERE / "direct_cube3_gauss_d05.npz", **load(d, "face_zeta", "vert_vel", "face_vel"))
+
+    d = harness("direct", "icos", 3, "rh", 0.0, env={"LPM_STUB_RANK": "1", "LPM_STUB_SIZE": "3"})
+    np.savez_compressed(HERE / "direct_icos3_rh_r2.npz", face_zeta=np.load(d / "face_zeta_r1.npy"),
+                        vert_vel=np.load(d / "vert_vel_r1.npy"), face_vel=np.load(d / "face_vel_r1.npy"),
+                        slice=np.load(d / "slice_r1.npy"))
+
+    d = harness("poisson", 2000, "0x2B")
+    np.savez_compressed(HERE / "poisson_2000.npz", **load(d, "xyz", "charge", "potential"))
+
+    for f in sorted(HERE.glob("*.npz")):
+        print(f.name, f.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,159 @@
+"""Direct sums on the GPU (through the C ABI) against the reference's outputs and the FP64 oracle.
+
+Tolerances: the FP64 path must match the reference DirectSum to 1e-12 relative (L-infinity over
+all components, relative to the largest component); the FP32 path (FP32 pair arithmetic, FP64
+accumulation of per-tile partials) must stay within F32_TOL relative L2 of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+import lpmcxx_b200 as L
+import oracle
+from conftest import golden, rel_l2, rel_linf
+
+pytestmark = pytest.mark.gpu
+
+F64_TOL = 1e-12
+F32_TOL = 5e-6
+BS = L.biot_savart_kernel()
+
+
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
+def on_torch_stream(ctx):
+    torch = torch_cuda()
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    return torch
+
+
+def test_f64_mesh_matches_reference(ctx):
+    g = golden("direct_icos4_rh.npz")
+    m = L.build_mesh("icos", 4)
+    vo, fo = ctx.direct_sum_mesh(BS, L.LPM_PREC_F64, m, g["face_zeta"])
+    leaf = m.leaf
+    got = np.concatenate([fo.T[leaf], vo.T])
+    ref = np.concatenate([g["face_vel"][leaf], g["vert_vel"]])
+    assert rel_linf(got, ref) < F64_TOL
+    assert np.all(fo[:, ~leaf] == 0.0)  # divided faces untouched
+
+
+def test_f64_nonsingular_delta(ctx):
+    g = golden("direct_cube3_gauss_d05.npz")
+    m = L.build_mesh("cube", 3)
+    vo, fo = ctx.direct_sum_mesh(L.biot_savart_kernel(1.0, 0.05), L.LPM_PREC_F64, m, g["face_zeta"])
+    leaf = m.leaf
+    assert rel_linf(np.concatenate([fo.T[leaf], vo.T]), np.concatenate([g["face_vel"][leaf], g["vert_vel"]])) < F64_TOL
+
+
+def test_f64_rank_slice_like_mpi_replicated_data(ctx):
+    # MPIReplicatedData(n, rank=1, size=3) slice: only those targets are written
+    g = golden("direct_icos3_rh_r2.npz")
+    vb, ve, fb, fe = (int(x) for x in g["slice"])
+    m = L.build_mesh("icos", 3)
+    vo = np.full((3, m.n_verts), 7.0)
+    fo = np.full((3, m.n_faces), 7.0)
+    ctx.direct_sum_mesh(BS, L.LPM_PREC_F64, m, g["face_zeta"], (vb, ve), (fb, fe), vo, fo)
+    assert rel_linf(vo.T[vb:ve + 1], g["vert_vel"][vb:ve + 1]) < F64_TOL
+    fsl = np.zeros(m.n_faces, bool)
+    fsl[fb:fe + 1] = True
+    written = fsl & m.leaf
+    assert rel_linf(fo.T[written], g["face_vel"][written]) < F64_TOL
+    assert np.all(vo[:, :vb] == 7.0) and np.all(vo[:, ve + 1:] == 7.0)
+    assert np.all(fo[:, ~written] == 7.0)
+
+
+def test_f32_mesh_vs_oracle(ctx):
+    g = golden("direct_icos4_rh.npz")
+    m = L.build_mesh("icos", 4)
+    vo, fo = ctx.direct_sum_mesh(BS, L.LPM_PREC_F32, m, g["face_zeta"])
+    leaf = m.leaf
+    got = np.concatenate([fo.T[leaf], vo.T])
+    ref = np.concatenate([g["face_vel"][leaf], g["vert_vel"]])
+    err = rel_l2(got, ref)
+    print("FP32 rel L2 vs reference, icos L4:", err)
+    assert err < F32_TOL
+
+
+def random_sphere(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n, 3))
+    return x / np.linalg.norm(x, axis=1, keepdims=True)
+
+
+@pytest.mark.parametrize("n_src,n_tgt", [(1, 1), (255, 257), (257, 1023), (1000, 1), (4099, 2050)])
+def test_dev_api_ragged_sizes(ctx, n_src, n_tgt):
+    torch = on_torch_stream(ctx)
+    rng = np.random.default_rng(n_src * 7 + n_tgt)
+    src = oracle.pack4(random_sphere(n_src, 1 + n_src), rng.uniform(-1, 1, n_src) / max(n_src, 1))
+    tgt = oracle.pack4(random_sphere(n_tgt, 2 + n_tgt))
+    ref = oracle.bs_direct(src, tgt)
+    ds = torch.tensor(src, device="cuda")
+    dt = torch.tensor(tgt, device="cuda")
+    for prec, tol in ((L.LPM_PREC_F64, F64_TOL), (L.LPM_PREC_F32, F32_TOL)):
+        out = torch.full((3, n_tgt), float("nan"), dtype=torch.float64, device="cuda")
+        ctx.direct_sum_dev(BS, prec, ds, dt, out)
+        got = out.cpu().numpy()
+        assert np.isfinite(got).all()
+        assert rel_l2(got, ref) < tol, (prec, rel_l2(got, ref))
+
+
+def test_dev_api_targets_alias_sources(ctx):
+    # targets == sources (face-centroid targets): the self pair contributes nothing in both precisions
+    torch = on_torch_stream(ctx)
+    n = 3000
+    rng = np.random.default_rng(5)
+    pts = oracle.pack4(random_sphere(n, 9), rng.uniform(-1, 1, n) / n)
+    ref = oracle.bs_direct(pts, pts)
+    d = torch.tensor(pts, device="cuda")
+    for prec, tol in ((L.LPM_PREC_F64, F64_TOL), (L.LPM_PREC_F32, F32_TOL)):
+        out = torch.empty((3, n), dtype=torch.float64, device="cuda")
+        ctx.direct_sum_dev(BS, prec, d, d, out)
+        assert rel_l2(out.cpu().numpy(), ref) < tol
+
+
+def test_empty_inputs(ctx):
+    torch = on_torch_stream(ctx)
+    tgt = torch.tensor(oracle.pack4(random_sphere(10, 3)), device="cuda")
+    src = torch.empty((0, 4), dtype=torch.float64, device="cuda")
+    out = torch.full((3, 10), 5.0, dtype=torch.float64, device="cuda")
+    for prec in (L.LPM_PREC_F64, L.LPM_PREC_F32):
+        ctx.direct_sum_dev(BS, prec, src, tgt, out)
+        assert torch.all(out == 0)
+    ctx.direct_sum_dev(BS, L.LPM_PREC_F64, tgt, src, torch.empty((3, 0), dtype=torch.float64, device="cuda"))
+
+
+def test_poisson_meshfree_vs_reference(ctx):
+    g = golden("poisson_2000.npz")
+    k = L.poisson_kernel()
+    phi = ctx.direct_sum_meshfree(k, L.LPM_PREC_F64, g["xyz"], g["charge"])
+    assert rel_linf(phi, g["potential"]) < F64_TOL
+    phi32 = ctx.direct_sum_meshfree(k, L.LPM_PREC_F32, g["xyz"], g["charge"])
+    assert rel_l2(phi32, g["potential"]) < F32_TOL
+    # a target slice with weights (meshfree srcWeightName branch)
+    w = np.linspace(0.5, 1.5, 2000)
+    part = ctx.direct_sum_meshfree(k, L.LPM_PREC_F64, g["xyz"], g["charge"], w, (100, 899))
+    ref = oracle.poisson_direct(oracle.pack4(g["xyz"], g["charge"] * w), oracle.pack4(g["xyz"][100:900]))
+    assert rel_linf(part[100:900], ref) < F64_TOL
+    assert np.all(part[:100] == 0) and np.all(part[900:] == 0)
+
+
+def test_invalid_kernel_and_ranges(ctx):
+    m = L.build_mesh("icos", 1)
+    zeta = np.ones(m.n_faces)
+    bad = L.KernelDesc(99, 0, 1.0, 0.0)
+    with pytest.raises(L.LpmError) as e:
+        ctx.direct_sum_mesh(bad, L.LPM_PREC_F64, m, zeta)
+    assert e.value.code == L._capi.LPM_ERR_KERNEL
+    with pytest.raises(L.LpmError) as e:
+        ctx.direct_sum_mesh(L.poisson_kernel(), L.LPM_PREC_F64, m, zeta)
+    assert e.value.code == L._capi.LPM_ERR_KERNEL
+    with pytest.raises(L.LpmError) as e:
+        ctx.direct_sum_mesh(BS, L.LPM_PREC_F64, m, zeta, vert_range=(0, m.n_verts))
+    assert e.value.code == L._capi.LPM_ERR_ARG
+    with pytest.raises(L.LpmError) as e:
+        ctx.direct_sum_mesh(BS, 7, m, zeta)
+    assert e.value.code == L._capi.LPM_ERR_ARG

@@ -1,0 +1,50 @@
+"""The FP64 oracle against the reference's own outputs (golden fixtures made by the unmodified
+reference, tests/golden/make_golden.py).  CPU only."""
+import numpy as np
+
+import lpmcxx_b200 as L
+import oracle
+from conftest import golden, rel_l2
+
+
+def mesh_inputs(kind, level, zeta):
+    m = L.build_mesh(kind, level)
+    leaf = m.leaf
+    src = oracle.pack4(m.face_xyz[leaf], zeta[leaf] * m.face_area[leaf])
+    return m, leaf, src
+
+
+def test_direct_icos4_bit_exact():
+    g = golden("direct_icos4_rh.npz")
+    m, leaf, src = mesh_inputs("icos", 4, g["face_zeta"])
+    assert np.array_equal(m.face_xyz.sum(axis=0), g["face_xyz_sum"])
+    tgt = np.concatenate([oracle.pack4(m.face_xyz[leaf]), oracle.pack4(m.vert_xyz)])
+    u = oracle.bs_direct(src, tgt)
+    ref = np.concatenate([g["face_vel"][leaf], g["vert_vel"]]).T
+    # same operations in the same order as src/LpmDirectSum.cpp:104-146
+    assert np.array_equal(u, ref)
+
+
+def test_direct_nonsingular_delta():
+    g = golden("direct_cube3_gauss_d05.npz")
+    m, leaf, src = mesh_inputs("cube", 3, g["face_zeta"])
+    tgt = np.concatenate([oracle.pack4(m.face_xyz[leaf]), oracle.pack4(m.vert_xyz)])
+    u = oracle.bs_direct(src, tgt, delta=0.05)
+    ref = np.concatenate([g["face_vel"][leaf], g["vert_vel"]]).T
+    assert rel_l2(u, ref) < 1e-14
+
+
+def test_poisson_meshfree():
+    g = golden("poisson_2000.npz")
+    src = oracle.pack4(g["xyz"], g["charge"])
+    phi = oracle.poisson_direct(src, src)
+    assert rel_l2(phi, g["potential"]) < 1e-14
+
+
+def test_oracle_thread_count_independent(monkeypatch):
+    g = golden("poisson_2000.npz")
+    src = oracle.pack4(g["xyz"], g["charge"])
+    a = oracle.poisson_direct(src, src)
+    monkeypatch.setenv("ORACLE_THREADS", "1")
+    b = oracle.poisson_direct(src, src)
+    assert np.array_equal(a, b)
