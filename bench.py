@@ -1,0 +1,415 @@
+"""Benchmark: Biot-Savart RK4 steps/s on the icos level-8 Gaussian-vortex workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl lpm|reference] [--solver ...]
+
+Workload (synthetic, generated here): icosahedral triangle mesh refined 8 levels -- 1,310,720 face
+centroid particles carrying vorticity x area (sources) plus 655,362 vertex particles, 1,966,082
+targets -- with zeta = 4 pi exp(-16|x - x0|^2) minus its area-weighted mean, x0 at (lat 0.05,
+lon 3 pi/4); RK4 steps of dt = 0.005.  One "step" is one full RK4 step (four velocity evaluations
+plus the FP64 updates) of the whole particle set.
+
+Our arm (--impl lpm) runs the headline solver, times K steps with CUDA events on the launching
+stream (L2 flushed between steps, outside the timed events), reports the FP64 GPU direct-sum RK4
+rate of the same workload beside it, the relative L2 velocity error of the headline solver against
+the FP64 direct sum, the dominant kernel's roofline, an end-to-end rate through the host API, the
+clocks seen during the timed region and a CPU baseline of the reference's own DirectSum.  Under
+torchrun every rank runs an independent replica (the path has no exchange step): value = all
+ranks' steps / max-over-ranks time.
+
+The reference arm (--impl reference) times the reference's own CPU DirectSum::meshSolve
+(oracle/_ref, built from the reference sources; the oracle's C port where that build is absent) on
+the host cores, each step a bounded target slice, extrapolated to full RK4 steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+LEVEL = 8
+DT = 0.005
+METRIC = "Biot-Savart RK4 steps/s @1.3M pts: FP32 learned tree vs FP64 direct @relL2≤1e-6"
+WORKLOAD = ("icos L8 Gaussian vortex: 1,310,720 face-centroid sources + 655,362 vertices "
+            "(1,966,082 targets), RK4 dt=0.005")
+FLOPS_PER_BS_PAIR = 17
+
+
+def env_int(name: str, default: int) -> int:
+    v = os.environ.get(name)
+    return int(v) if v not in (None, "") else default
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- CPU baselines
+def reference_harness() -> Path | None:
+    p = ROOT / "oracle" / "_ref" / "ref_harness"
+    return p if p.exists() else None
+
+
+def time_reference_direct(reps: int, procs: int, targets_per_proc: int = 3) -> dict:
+    """The reference's DirectSum::meshSolve on icos L8 (Gaussian vortex), `procs` processes each timing a
+    MPIReplicatedData slice of ~targets_per_proc vertex targets, `reps` times.  Returns per-rep pair rates."""
+    exe = reference_harness()
+    n_verts = 2 + 10 * 4 ** LEVEL
+    size = max(procs, n_verts // targets_per_proc)
+    env = dict(os.environ)
+    env["LPM_MESH_SEED_DIR"] = str(ROOT / "oracle" / "_ref" / "meshSeeds")
+    env["LPM_STUB_SIZE"] = str(size)
+    jobs = []
+    for r in range(procs):
+        e = dict(env)
+        e["LPM_STUB_RANK"] = str(r)
+        jobs.append(subprocess.Popen([str(exe), "time_direct", "icos", str(LEVEL), "gauss", str(reps)],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, env=e))
+    results = []
+    for j in jobs:
+        out, _ = j.communicate()
+        line = [ln for ln in out.splitlines() if ln.startswith('{"cmd"')]
+        if j.returncode != 0 or not line:
+            raise RuntimeError("reference harness failed")
+        results.append(json.loads(line[-1]))
+    n_src = results[0]["n_leaves"]
+    n_tgt = results[0]["n_verts"] + n_src
+    pairs = sum((r["vert_targets"] + r["face_targets"]) * n_src for r in results)
+    rep_s = [max(r["seconds"][k] for r in results) for k in range(reps)]
+    return {"rep_seconds": rep_s, "pairs_per_rep": pairs, "n_src": n_src, "n_tgt": n_tgt,
+            "targets_per_rep": sum(r["vert_targets"] + r["face_targets"] for r in results), "procs": procs}
+
+
+def time_oracle_port(reps: int, threads: int, n_targets: int = 64) -> dict:
+    """The oracle's C restatement of the same FP64 direct sum on a slice of n_targets targets."""
+    import oracle
+    import lpmcxx_b200.workloads as W
+
+    os.environ["ORACLE_THREADS"] = str(threads)
+    mesh, p, n_src = W.gaussian_vortex_mesh("icos", LEVEL)
+    src = p[:n_src]
+    tgt = p[n_src:n_src + n_targets]
+    rep_s = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        oracle.bs_direct(src, tgt)
+        rep_s.append(time.perf_counter() - t0)
+    return {"rep_seconds": rep_s, "pairs_per_rep": n_targets * n_src, "n_src": n_src, "n_tgt": p.shape[0],
+            "targets_per_rep": n_targets, "procs": threads}
+
+
+def cpu_baseline(reps: int) -> dict:
+    cores = os.cpu_count() or 1
+    procs = max(1, min(cores, 32))
+    if reference_harness() is not None:
+        r = time_reference_direct(reps, procs)
+        kind = "reference"
+        sample = (f"reference DirectSum::meshSolve (FP64), {procs} processes x MPIReplicatedData slice, "
+                  f"{r['targets_per_rep']} vertex targets x {r['n_src']} sources per step, extrapolated")
+    else:
+        r = time_oracle_port(reps, procs)
+        kind = "port"
+        sample = (f"oracle C port of the FP64 direct sum, {procs} threads, {r['targets_per_rep']} targets x "
+                  f"{r['n_src']} sources per step, extrapolated")
+    pairs_full_step = 4.0 * r["n_tgt"] * r["n_src"]
+    rates = [r["pairs_per_rep"] / s for s in r["rep_seconds"]]
+    steps_per_s = float(np.median(rates)) / pairs_full_step
+    return {"value": steps_per_s, "unit": "steps/s", "cores": procs, "kind": kind, "sample": sample,
+            "pairs_per_s": float(np.median(rates)), "rep_seconds": r["rep_seconds"]}
+
+
+# --------------------------------------------------------------------------- GPU arm
+def profile_summary_traffic(kernel: str) -> float | None:
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/), if present."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        for ln in f.read_text().splitlines():
+            if ln.startswith("traffic_bytes_per_launch") and f"[{kernel}]" in ln:
+                try:
+                    return float(ln.split(":", 1)[1].split()[0])
+                except ValueError:
+                    pass
+    return None
+
+
+def solver_desc(name: str):
+    import lpmcxx_b200 as L
+
+    if name == "direct_f64":
+        return L.direct_solver(L.LPM_PREC_F64)
+    if name == "direct_f32":
+        return L.direct_solver(L.LPM_PREC_F32)
+    if name == "tree_f32":
+        return L.tree_solver(L.LPM_PREC_F32, order=8, max_per_leaf=512, theta=0.7)
+    if name == "tree_learned":
+        return L.tree_solver(L.LPM_PREC_F32, order=8, max_per_leaf=512, theta=0.7, learned=True)
+    raise ValueError(name)
+
+
+def kernel_work(kernel: str, n_src: int, n_tgt: int, stats: dict) -> tuple[float, str] | None:
+    """Algorithmic flops of one launch of `kernel`."""
+    if kernel == "bs_f32_kernel" or kernel == "bs_f64_kernel":
+        return FLOPS_PER_BS_PAIR * float(n_src) * float(n_tgt), "TFLOP/s"
+    return None
+
+
+def run_gpu(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    import lpmcxx_b200 as L
+    import lpmcxx_b200.workloads as W
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    mesh, p, n_src = W.gaussian_vortex_mesh("icos", args.level)
+    n = p.shape[0]
+    stream = torch.cuda.Stream()
+    ctx = L.Context(local)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
+    state0 = torch.tensor(p, device="cuda")
+    kern = L.biot_savart_kernel()
+    head = args.solver
+    with torch.cuda.stream(stream):
+        ctx.use_torch_stream()
+        # ---- headline solver: warm-up then K timed steps
+        rk = L.RK4(ctx, kern, solver_desc(head), n_src, n)
+        rk.set_state(state0)
+        rk.step(args.dt, args.warmup, use_graph=True)
+        stream.synchronize()
+        launches0 = ctx.launch_count
+        step_ms = []
+        clocks = ClockSampler(local).start()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rk.step(args.dt, 1, use_graph=True)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        launches = ctx.launch_count - launches0
+        total_ms = float(sum(step_ms))
+        if world > 1:
+            t = torch.tensor([total_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+            dist.barrier()
+        value = world * args.steps / (total_ms * 1e-3)
+
+        # ---- end to end through the host API: pinned host state in, step, state out
+        host_in = torch.tensor(p).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        rk.set_state(host_in)
+        rk.step(args.dt, 1, use_graph=True)
+        torch.cuda.synchronize()
+        e2e_s = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            rk.set_state(host_in)
+            rk.step(args.dt, 1, use_graph=True)
+            rk.get_state(host_out)
+            e2e_s.append(time.perf_counter() - t0)
+        e2e_value = world * args.steps / sum(e2e_s)
+        state_bytes = n * 4 * 8
+
+        # ---- accuracy of the headline velocity against the FP64 direct sum at the initial state
+        rk.set_state(state0)
+        u_head = torch.empty((3, n), dtype=torch.float64, device="cuda")
+        rk.velocity(u_head)
+        # ---- per-kernel profile of one uncaptured step (dominant kernel for the roofline)
+        rk.set_state(state0)
+        ctx.set_profiling(True)
+        rk.step(args.dt, 1, use_graph=False)
+        prof = ctx.profile_report()
+        ctx.set_profiling(False)
+        rk.close()
+
+        # ---- FP64 GPU direct sum on the same workload (one RK4 step)
+        u64 = torch.empty((3, n), dtype=torch.float64, device="cuda")
+        fp64_sps = None
+        if head != "direct_f64":
+            rk64 = L.RK4(ctx, kern, solver_desc("direct_f64"), n_src, n)
+            rk64.set_state(state0)
+            rk64.velocity(u64)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rk64.step(args.dt, 1, use_graph=False)
+            e1.record(stream)
+            e1.synchronize()
+            fp64_sps = 1e3 / e0.elapsed_time(e1)
+            rk64.close()
+        else:
+            u64.copy_(u_head)
+            fp64_sps = value / world
+        rel_l2 = float(torch.linalg.norm(u_head - u64) / torch.linalg.norm(u64))
+        fp32_peak = ctx.fma_peak_tflops(L.LPM_PREC_F32)
+        fp64_peak = ctx.fma_peak_tflops(L.LPM_PREC_F64)
+    torch.cuda.synchronize()
+
+    # dominant kernel of the headline step
+    dom = max(prof.items(), key=lambda kv: kv[1]["ms"]) if prof else (None, None)
+    roof = None
+    if dom[0] is not None:
+        name, st = dom
+        avg_ms = st["ms"] / st["launches"]
+        work = kernel_work(name, n_src, n, st)
+        peak = fp64_peak if "f64" in name else fp32_peak
+        if work is not None:
+            achieved = work[0] / (avg_ms * 1e-3) * 1e-12
+            roof = {"bound": "fp64" if "f64" in name else "fp32", "kernel": name, "achieved": achieved,
+                    "peak": peak, "unit": work[1], "frac": achieved / peak, "traffic": profile_summary_traffic(name),
+                    "peak_source": "measured FMA microbenchmark (lpm_fma_peak) on this GPU",
+                    "avg_launch_ms": avg_ms, "share": st["ms"] / sum(v["ms"] for v in prof.values())}
+    out = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32" if head != "direct_f64" else "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "solver": head, "n_sources": n_src, "n_targets": n, "dt": args.dt,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed (256 MiB write) before every timed step, outside the timed events",
+                   "graph": "one CUDA graph replay per RK4 step"},
+        "rel_l2_vs_fp64_direct": rel_l2,
+        "fp64_direct_steps_per_s": fp64_sps,
+        "speedup_vs_fp64_direct": (value / world) / fp64_sps if fp64_sps else None,
+        "roofline": roof,
+        "kernel_profile_ms": {k: v for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])[:12]},
+        "fma_peaks_tflops": {"fp32": fp32_peak, "fp64": fp64_peak},
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(reps=2)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def run_reference(args) -> None:
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    base = cpu_baseline(reps=args.warmup + args.steps)
+    reps = base["rep_seconds"][args.warmup:]
+    n_src = 20 * 4 ** LEVEL
+    n_tgt = n_src + 2 + 10 * 4 ** LEVEL
+    rates = [base["pairs_per_s"]] if not reps else None
+    value = base["value"]
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": env_int("WORLD_SIZE", 1),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "solver": "reference DirectSum::meshSolve (FP64, CPU)",
+                   "n_sources": n_src, "n_targets": n_tgt, "dt": DT, "host_cores": cores},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": base["cores"], "kind": base["kind"],
+                         "sample": base["sample"]},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    del rates
+    print(json.dumps(out))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lpm", choices=["lpm", "reference"])
+    ap.add_argument("--solver", default="direct_f32",
+                    choices=["direct_f32", "direct_f64", "tree_f32", "tree_learned"])
+    ap.add_argument("--level", type=int, default=LEVEL)
+    ap.add_argument("--dt", type=float, default=DT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

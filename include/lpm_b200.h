@@ -68,12 +68,23 @@ typedef struct lpm_ctx lpm_ctx;
 /* ---- context (replaces the per-rank MPI state; one context per device) */
 int lpm_ctx_create(int device, lpm_ctx** out);
 int lpm_ctx_destroy(lpm_ctx* ctx);
-/* Use an existing cudaStream_t (passed as void*) for all later work; NULL = the context's own stream. */
+/* Enqueue all later work on an existing cudaStream_t (passed as void*, used as-is; NULL is the
+ * legacy default stream).  A new context starts on its own non-blocking stream; lpm_ctx_own_stream
+ * returns that stream and lpm_ctx_set_stream(ctx, lpm_ctx_own_stream(ctx)) switches back to it. */
 int lpm_ctx_set_stream(lpm_ctx* ctx, void* cuda_stream);
+void* lpm_ctx_own_stream(const lpm_ctx* ctx);
 int lpm_ctx_synchronize(lpm_ctx* ctx);
 const char* lpm_last_error(void);
 /* Number of kernel launches this library has made on ctx so far (for launch accounting). */
 int64_t lpm_ctx_launch_count(const lpm_ctx* ctx);
+/* Per-kernel CUDA-event timing of uncaptured launches (on = 1).  lpm_ctx_profile_report synchronises,
+ * writes {"kernel": {"ms": total, "launches": n}, ...} as JSON into buf and clears the records. */
+int lpm_ctx_set_profiling(lpm_ctx* ctx, int on);
+int lpm_ctx_profile_report(lpm_ctx* ctx, char* buf, size_t len);
+
+/* Measured FMA-pipe peak (TFLOP/s, FMA = 2 flops) of this device for LPM_PREC_F32 or LPM_PREC_F64: the
+ * roofline denominator of the pairwise and far-field kernels.  Synchronous; takes ~100 ms. */
+int lpm_fma_peak(lpm_ctx* ctx, int precision, double* tflops);
 
 /* ---- mesh generation (host).  The reference's PolyMesh2d(seed, level) constructor
  * (src/LpmPolyMesh2d.cpp:20-93) in the same vertex / face index order.  Arrays are caller-owned:
@@ -87,10 +98,13 @@ int lpm_mesh_build(int kind, int level, double radius, double* vert_xyz, double*
 
 /* Device-resident direct sum: out[c*n_tgt + i] = mult * sum_j K(tgt_i, src_j) w_j.
  * src: n_src x 4 (x,y,z,w); tgt: n_tgt x 4 (x,y,z,-); out: {3|1} x n_tgt.
+ * n_coincident: targets 0..n_coincident-1 sit exactly on sources 0..n_coincident-1 (face-centroid
+ * targets listed first); their self pairs contribute zero, as in the reference.  Any other exactly
+ * coincident (target, source) pair is handled by the FP64 path only.
  * Replaces the pair loops of DirectSum::meshSolve (src/LpmDirectSum.cpp:104-166, vector kernel)
  * and DirectSum::meshfreeSolve (src/LpmDirectSum.cpp:240-252, scalar kernel). */
 int lpm_direct_sum_dev(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precision, const double* src, int64_t n_src,
-                       const double* tgt, int64_t n_tgt, double* out);
+                       const double* tgt, int64_t n_tgt, int64_t n_coincident, double* out);
 
 /* Host-facing mesh direct sum with the reference's data: DirectSum::meshSolve
  * (src/LpmDirectSum.cpp:25-167).  Vertex coordinates vx/vy/vz (n_verts), face centroids fx/fy/fz,
@@ -112,6 +126,45 @@ int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precisi
 int lpm_direct_sum_meshfree(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precision, int64_t n, const double* x,
                             const double* y, const double* z, const double* src, const double* weights, int64_t begin,
                             int64_t end, double* out);
+
+/* ---- velocity solver selection (DirectSum or TreeSum, and the arithmetic they use) */
+#define LPM_METHOD_DIRECT 0 /* all pairs (DirectSum) */
+#define LPM_METHOD_TREE 1   /* octree treecode (TreeSum) */
+
+#define LPM_ORDER_FIXED 0   /* every accepted (target leaf, cluster) pair uses `order` */
+#define LPM_ORDER_LEARNED 1 /* an MLP picks the order (or direct) per pair; `order` is the fallback */
+
+typedef struct lpm_solver_desc {
+    int32_t method;       /* LPM_METHOD_* */
+    int32_t precision;    /* LPM_PREC_* for the pairwise (near-field) arithmetic */
+    int32_t order;        /* Taylor order p: multi-indices |k| < p, as SumNode (src/LpmTreeSum.cpp:9-18) */
+    int32_t max_per_leaf; /* octree leaf capacity (maxParticlesPerBox) */
+    double theta;         /* multipole acceptance parameter */
+    int32_t order_policy; /* LPM_ORDER_* */
+    int32_t reserved;
+} lpm_solver_desc;
+
+/* ---- RK4 integration of the particles (vertices and face-centroid particles as independent
+ * Lagrangian particles carrying constant strengths).  The reference's C++ tree has no time
+ * integrator; this is the classical four-stage Runge-Kutta step, every stage position and the final
+ * position re-projected onto the sphere x <- R x/|x|, stage velocities from a full evaluation of the
+ * chosen solver at the stage positions.  FP64 state and update. */
+typedef struct lpm_rk4 lpm_rk4;
+
+/* n_pts particles, the first n_src of which are sources (w != 0); the rest are targets only. */
+int lpm_rk4_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver, int64_t n_src,
+                   int64_t n_pts, lpm_rk4** out);
+int lpm_rk4_destroy(lpm_rk4* rk);
+/* State as n_pts x 4 (x, y, z, w) doubles: _dev = device pointer (enqueued), host otherwise. */
+int lpm_rk4_set_state_dev(lpm_rk4* rk, const double* xyzw);
+int lpm_rk4_get_state_dev(lpm_rk4* rk, double* xyzw);
+int lpm_rk4_set_state(lpm_rk4* rk, const double* xyzw);
+int lpm_rk4_get_state(lpm_rk4* rk, double* xyzw);
+/* Advance nsteps steps of size dt.  use_graph != 0 replays one captured CUDA graph per step (the graph is
+ * captured on the first call, after one uncaptured warm-up step allocates all scratch). */
+int lpm_rk4_step(lpm_rk4* rk, double dt, int nsteps, int use_graph);
+/* Velocity (3 x n_pts, component-major, device) at the current state; for diagnostics and tests. */
+int lpm_rk4_velocity_dev(lpm_rk4* rk, double* out);
 
 #ifdef __cplusplus
 }

@@ -97,7 +97,18 @@ class Context:
             pass
 
     def set_stream(self, stream_handle: int | None) -> None:
-        check(lib().lpm_ctx_set_stream(self.h, stream_handle), "lpm_ctx_set_stream")
+        """Run on this cudaStream_t handle (0/None = the legacy default stream, as torch's default)."""
+        check(lib().lpm_ctx_set_stream(self.h, stream_handle or None), "lpm_ctx_set_stream")
+
+    def use_torch_stream(self):
+        """Run on torch's current stream; returns the torch module."""
+        import torch
+
+        self.set_stream(torch.cuda.current_stream().cuda_stream)
+        return torch
+
+    def use_own_stream(self) -> None:
+        check(lib().lpm_ctx_set_stream(self.h, lib().lpm_ctx_own_stream(self.h)), "lpm_ctx_set_stream")
 
     def synchronize(self) -> None:
         check(lib().lpm_ctx_synchronize(self.h), "lpm_ctx_synchronize")
@@ -106,11 +117,28 @@ class Context:
     def launch_count(self) -> int:
         return lib().lpm_ctx_launch_count(self.h)
 
+    def set_profiling(self, on: bool) -> None:
+        check(lib().lpm_ctx_set_profiling(self.h, 1 if on else 0), "lpm_ctx_set_profiling")
+
+    def profile_report(self) -> dict:
+        """Per-kernel {name: {"ms": total, "launches": n}} since profiling was switched on (then cleared)."""
+        import json
+
+        buf = C.create_string_buffer(1 << 16)
+        check(lib().lpm_ctx_profile_report(self.h, buf, len(buf)), "lpm_ctx_profile_report")
+        return json.loads(buf.value.decode())
+
+    def fma_peak_tflops(self, precision: int) -> float:
+        t = C.c_double()
+        check(lib().lpm_fma_peak(self.h, precision, C.byref(t)), "lpm_fma_peak")
+        return t.value
+
     # ---- direct sums
-    def direct_sum_dev(self, kernel: KernelDesc, precision: int, src, tgt, out) -> None:
-        """Device tensors: src (n_src,4) f64, tgt (n_tgt,4) f64, out ({3|1}, n_tgt) f64."""
+    def direct_sum_dev(self, kernel: KernelDesc, precision: int, src, tgt, out, n_coincident: int = 0) -> None:
+        """Device tensors: src (n_src,4) f64, tgt (n_tgt,4) f64, out ({3|1}, n_tgt) f64.  Targets
+        0..n_coincident-1 sit on sources 0..n_coincident-1."""
         check(lib().lpm_direct_sum_dev(self.h, C.byref(kernel), precision, ptr(src), src.shape[0], ptr(tgt),
-                                       tgt.shape[0], ptr(out)), "lpm_direct_sum_dev")
+                                       tgt.shape[0], n_coincident, ptr(out)), "lpm_direct_sum_dev")
 
     def direct_sum_mesh(self, kernel: KernelDesc, precision: int, mesh: SphereMesh, face_src: np.ndarray,
                         vert_range=None, face_range=None, vert_out=None, face_out=None):
@@ -140,3 +168,59 @@ class Context:
         check(lib().lpm_direct_sum_meshfree(self.h, C.byref(kernel), precision, n, ptr(x), ptr(y), ptr(z), ptr(s),
                                             ptr(w), b, e, ptr(o)), "lpm_direct_sum_meshfree")
         return o
+
+
+def direct_solver(precision: int = LPM_PREC_F64) -> _capi.SolverDesc:
+    return _capi.SolverDesc(_capi.LPM_METHOD_DIRECT, precision, 0, 0, 0.0, 0, 0)
+
+
+def tree_solver(precision: int = LPM_PREC_F32, order: int = 8, max_per_leaf: int = 512, theta: float = 0.7,
+                learned: bool = False) -> _capi.SolverDesc:
+    return _capi.SolverDesc(_capi.LPM_METHOD_TREE, precision, order, max_per_leaf, theta,
+                            _capi.LPM_ORDER_LEARNED if learned else _capi.LPM_ORDER_FIXED, 0)
+
+
+class RK4:
+    """Device-resident RK4 integrator of sphere particles (lpm_rk4).  The first n_src particles carry
+    strengths (sources); state is (n, 4) float64 (x, y, z, w)."""
+
+    def __init__(self, ctx: Context, kernel: KernelDesc, solver: _capi.SolverDesc, n_src: int, n_pts: int):
+        h = C.c_void_p()
+        check(lib().lpm_rk4_create(ctx.h, C.byref(kernel), C.byref(solver), n_src, n_pts, C.byref(h)),
+              "lpm_rk4_create")
+        self.h, self.ctx, self.n_src, self.n = h, ctx, n_src, n_pts
+
+    def close(self) -> None:
+        if self.h:
+            lib().lpm_rk4_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, state) -> None:
+        """From a CUDA tensor (device copy, enqueued) or a host array / CPU tensor (synchronous)."""
+        if getattr(state, "is_cuda", False):
+            check(lib().lpm_rk4_set_state_dev(self.h, ptr(state)), "lpm_rk4_set_state_dev")
+        else:
+            s = state if hasattr(state, "data_ptr") else np.ascontiguousarray(state, dtype=np.float64)
+            check(lib().lpm_rk4_set_state(self.h, ptr(s)), "lpm_rk4_set_state")
+
+    def get_state(self, out=None):
+        """Into a CUDA tensor (enqueued), a CPU tensor / host array (synchronous), or a new array."""
+        if out is not None and getattr(out, "is_cuda", False):
+            check(lib().lpm_rk4_get_state_dev(self.h, ptr(out)), "lpm_rk4_get_state_dev")
+            return out
+        o = np.empty((self.n, 4)) if out is None else out
+        check(lib().lpm_rk4_get_state(self.h, ptr(o)), "lpm_rk4_get_state")
+        return o
+
+    def step(self, dt: float, nsteps: int = 1, use_graph: bool = False) -> None:
+        check(lib().lpm_rk4_step(self.h, dt, nsteps, 1 if use_graph else 0), "lpm_rk4_step")
+
+    def velocity(self, out) -> None:
+        """Velocity (3, n) at the current state into a device tensor."""
+        check(lib().lpm_rk4_velocity_dev(self.h, ptr(out)), "lpm_rk4_velocity_dev")

@@ -33,6 +33,17 @@ class KernelDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("radius", C.c_double), ("delta", C.c_double)]
 
 
+LPM_METHOD_DIRECT = 0
+LPM_METHOD_TREE = 1
+LPM_ORDER_FIXED = 0
+LPM_ORDER_LEARNED = 1
+
+
+class SolverDesc(C.Structure):
+    _fields_ = [("method", C.c_int32), ("precision", C.c_int32), ("order", C.c_int32), ("max_per_leaf", C.c_int32),
+                ("theta", C.c_double), ("order_policy", C.c_int32), ("reserved", C.c_int32)]
+
+
 class LpmError(RuntimeError):
     def __init__(self, code: int, where: str, msg: str):
         super().__init__(f"{where} failed with status {code}: {msg}")
@@ -49,15 +60,27 @@ SIGNATURES = {
     "lpm_ctx_create": (C.c_int, [C.c_int, C.POINTER(P)]),
     "lpm_ctx_destroy": (C.c_int, [P]),
     "lpm_ctx_set_stream": (C.c_int, [P, P]),
+    "lpm_ctx_own_stream": (P, [P]),
     "lpm_ctx_synchronize": (C.c_int, [P]),
     "lpm_last_error": (C.c_char_p, []),
     "lpm_ctx_launch_count": (C.c_int64, [P]),
+    "lpm_fma_peak": (C.c_int, [P, C.c_int, C.POINTER(D)]),
+    "lpm_ctx_set_profiling": (C.c_int, [P, C.c_int]),
+    "lpm_ctx_profile_report": (C.c_int, [P, C.c_char_p, C.c_size_t]),
     "lpm_mesh_counts": (C.c_int, [C.c_int, C.c_int, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
     "lpm_mesh_build": (C.c_int, [C.c_int, C.c_int, D, P, P, P, P]),
-    "lpm_direct_sum_dev": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, P, I64, P, I64, P]),
+    "lpm_direct_sum_dev": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, P, I64, P, I64, I64, P]),
     "lpm_direct_sum_mesh": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, I64, P, P, P, I64, P, P, P, P, P, P,
                                       I64, I64, I64, I64, P, P, P, P, P, P]),
     "lpm_direct_sum_meshfree": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, I64, P, P, P, P, P, I64, I64, P]),
+    "lpm_rk4_create": (C.c_int, [P, C.POINTER(KernelDesc), C.POINTER(SolverDesc), I64, I64, C.POINTER(P)]),
+    "lpm_rk4_destroy": (C.c_int, [P]),
+    "lpm_rk4_set_state_dev": (C.c_int, [P, P]),
+    "lpm_rk4_get_state_dev": (C.c_int, [P, P]),
+    "lpm_rk4_set_state": (C.c_int, [P, P]),
+    "lpm_rk4_get_state": (C.c_int, [P, P]),
+    "lpm_rk4_step": (C.c_int, [P, D, C.c_int, C.c_int]),
+    "lpm_rk4_velocity_dev": (C.c_int, [P, P]),
 }
 
 _lib = None

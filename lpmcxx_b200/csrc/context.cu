@@ -72,9 +72,82 @@ void* pinned(lpm_ctx* ctx, size_t bytes) {
     return ctx->pinned;
 }
 
+void prof_begin(lpm_ctx* ctx, LpmProfRecord& r) {
+    if (cudaEventCreate(&r.start) != cudaSuccess || cudaEventCreate(&r.stop) != cudaSuccess) {
+        cudaGetLastError();
+        r.start = r.stop = nullptr;
+        return;
+    }
+    cudaEventRecord(r.start, ctx->stream);
+}
+
+void prof_end(lpm_ctx* ctx, LpmProfRecord& r) {
+    if (!r.start) return;
+    cudaEventRecord(r.stop, ctx->stream);
+    if (!ctx->prof) ctx->prof = new std::vector<LpmProfRecord>();
+    ctx->prof->push_back(r);
+}
+
+static void prof_clear(lpm_ctx* ctx) {
+    if (!ctx->prof) return;
+    for (auto& r : *ctx->prof) {
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    ctx->prof->clear();
+}
+
 }  // namespace lpm
 
 extern "C" {
+
+int lpm_ctx_set_profiling(lpm_ctx* ctx, int on) {
+    if (!ctx) {
+        lpm::set_error("null context");
+        return LPM_ERR_ARG;
+    }
+    cudaStreamSynchronize(ctx->stream);
+    lpm::prof_clear(ctx);
+    ctx->profiling = on != 0;
+    return LPM_OK;
+}
+
+int lpm_ctx_profile_report(lpm_ctx* ctx, char* buf, size_t len) {
+    if (!ctx || !buf || len == 0) {
+        lpm::set_error("lpm_ctx_profile_report: bad argument");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    // aggregate by kernel name, in first-seen order
+    std::vector<const char*> names;
+    std::vector<double> ms;
+    std::vector<int64_t> count;
+    if (ctx->prof) {
+        for (auto& r : *ctx->prof) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, r.start, r.stop) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            size_t k = 0;
+            while (k < names.size() && std::strcmp(names[k], r.name) != 0) ++k;
+            if (k == names.size()) {
+                names.push_back(r.name);
+                ms.push_back(0.0);
+                count.push_back(0);
+            }
+            ms[k] += t;
+            count[k] += 1;
+        }
+    }
+    size_t off = (size_t)snprintf(buf, len, "{");
+    for (size_t k = 0; k < names.size() && off < len; ++k)
+        off += (size_t)snprintf(buf + off, len - off, "%s\"%s\": {\"ms\": %.6f, \"launches\": %lld}", k ? ", " : "",
+                                names[k], ms[k], (long long)count[k]);
+    if (off < len) snprintf(buf + off, len - off, "}");
+    lpm::prof_clear(ctx);
+    return LPM_OK;
+}
 
 const char* lpm_last_error(void) { return lpm::g_err; }
 
@@ -122,6 +195,8 @@ int lpm_ctx_destroy(lpm_ctx* ctx) {
     if (!ctx) return LPM_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    lpm::prof_clear(ctx);
+    delete ctx->prof;
     for (auto& b : ctx->buf)
         if (b.ptr) cudaFree(b.ptr);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -135,9 +210,11 @@ int lpm_ctx_set_stream(lpm_ctx* ctx, void* cuda_stream) {
         lpm::set_error("null context");
         return LPM_ERR_ARG;
     }
-    ctx->stream = cuda_stream ? (cudaStream_t)cuda_stream : ctx->own_stream;
+    ctx->stream = (cudaStream_t)cuda_stream;
     return LPM_OK;
 }
+
+void* lpm_ctx_own_stream(const lpm_ctx* ctx) { return ctx ? (void*)ctx->own_stream : nullptr; }
 
 int lpm_ctx_synchronize(lpm_ctx* ctx) {
     if (!ctx) {

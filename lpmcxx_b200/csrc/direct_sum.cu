@@ -299,8 +299,8 @@ __global__ void pack_f32_kernel(const double4* __restrict__ in, int64_t n, float
 
 int pack_f32(lpm_ctx* ctx, const double4* in, int64_t n, float4* out, bool scale_w2) {
     if (n <= 0) return LPM_OK;
-    pack_f32_kernel<<<grid_for(n, 256), 256, 0, ctx->stream>>>(in, n, out, scale_w2 ? 2.0f : 1.0f);
-    LPM_LAUNCH_CHECK(ctx);
+    LPM_LAUNCH(ctx, "pack_f32_kernel", pack_f32_kernel, grid_for(n, 256), 256, 0, in, n, out,
+               scale_w2 ? 2.0f : 1.0f);
     return LPM_OK;
 }
 
@@ -312,18 +312,17 @@ int direct_sum_f64(lpm_ctx* ctx, const lpm_kernel_desc& k, const double4* src, i
         const double mult = -1.0 / (4.0 * kPi * k.radius);
         const double r2 = k.radius * k.radius, d2 = k.delta * k.delta;
         if (k.delta != 0.0)
-            bs_f64_kernel<true><<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, n_tgt, r2, d2, mult, out,
+            LPM_LAUNCH(ctx, "bs_f64_kernel", bs_f64_kernel<true>, grid, kThreads, 0, src, n_src, tgt, n_tgt, r2, d2, mult, out,
                                                                     out_stride);
         else
-            bs_f64_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, n_tgt, r2, d2, mult, out,
+            LPM_LAUNCH(ctx, "bs_f64_kernel", bs_f64_kernel<false>, grid, kThreads, 0, src, n_src, tgt, n_tgt, r2, d2, mult, out,
                                                                      out_stride);
     } else if (k.kind == LPM_KERNEL_POISSON_3D) {
-        poisson_f64_kernel<<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, n_tgt, 1.0 / (4.0 * kPi), out);
+        LPM_LAUNCH(ctx, "poisson_f64_kernel", poisson_f64_kernel, grid, kThreads, 0, src, n_src, tgt, n_tgt, 1.0 / (4.0 * kPi), out);
     } else {
         set_error("invalid kernel");
         return LPM_ERR_KERNEL;
     }
-    LPM_LAUNCH_CHECK(ctx);
     return LPM_OK;
 }
 
@@ -338,24 +337,23 @@ int direct_sum_f32_impl(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* sr
     if (k.kind == LPM_KERNEL_BIOT_SAVART_SPHERE) {
         const double mult = -1.0 / (4.0 * kPi * k.radius);
         if (k.delta != 0.0)
-            bs_f32_kernel<true><<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, tgt64, n_tgt,
+            LPM_LAUNCH(ctx, "bs_f32_kernel", bs_f32_kernel<true>, grid, kThreads, 0, src, n_src, tgt, tgt64, n_tgt,
                                                                     (float)(2.0 * k.delta * k.delta), mult, out,
                                                                     out_stride, coinc_n, coinc_off);
         else
-            bs_f32_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, tgt64, n_tgt, 0.0f, mult, out,
+            LPM_LAUNCH(ctx, "bs_f32_kernel", bs_f32_kernel<false>, grid, kThreads, 0, src, n_src, tgt, tgt64, n_tgt, 0.0f, mult, out,
                                                                      out_stride, coinc_n, coinc_off);
     } else if (k.kind == LPM_KERNEL_POISSON_3D) {
-        poisson_f32_kernel<<<grid, kThreads, 0, ctx->stream>>>(src, n_src, tgt, n_tgt, 1.0 / (4.0 * kPi), out,
+        LPM_LAUNCH(ctx, "poisson_f32_kernel", poisson_f32_kernel, grid, kThreads, 0, src, n_src, tgt, n_tgt, 1.0 / (4.0 * kPi), out,
                                                                coinc_n, coinc_off);
     } else {
         set_error("invalid kernel");
         return LPM_ERR_KERNEL;
     }
-    LPM_LAUNCH_CHECK(ctx);
     return LPM_OK;
 }
 
-static int check_kernel(const lpm_kernel_desc* k) {
+int check_kernel_desc(const lpm_kernel_desc* k) {
     if (!k) {
         set_error("null kernel descriptor");
         return LPM_ERR_ARG;
@@ -394,23 +392,22 @@ int direct_sum_any(lpm_ctx* ctx, const lpm_kernel_desc& k, int precision, const 
 using namespace lpm;
 
 extern "C" int lpm_direct_sum_dev(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precision, const double* src,
-                                  int64_t n_src, const double* tgt, int64_t n_tgt, double* out) {
+                                  int64_t n_src, const double* tgt, int64_t n_tgt, int64_t n_coincident,
+                                  double* out) {
     if (!ctx) {
         set_error("null context");
         return LPM_ERR_ARG;
     }
-    int rc = check_kernel(kernel);
+    int rc = check_kernel_desc(kernel);
     if (rc) return rc;
-    if (n_src < 0 || n_tgt < 0 || (n_src > 0 && !src) || (n_tgt > 0 && (!tgt || !out))) {
+    if (n_src < 0 || n_tgt < 0 || (n_src > 0 && !src) || (n_tgt > 0 && (!tgt || !out)) || n_coincident < 0 ||
+        n_coincident > std::min(n_src, n_tgt)) {
         set_error("lpm_direct_sum_dev: bad sizes or null pointers");
         return LPM_ERR_ARG;
     }
     LPM_CUDA_TRY(cudaSetDevice(ctx->device));
-    // targets that alias the source array coincide with them index by index
-    int64_t coinc_n = 0;
-    if ((const double*)tgt == src) coinc_n = std::min(n_src, n_tgt);
     return direct_sum_any(ctx, *kernel, precision, (const double4*)src, n_src, (const double4*)tgt, n_tgt, out,
-                          coinc_n, 0);
+                          n_coincident, 0);
 }
 
 extern "C" int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precision, int64_t n_verts,
@@ -424,7 +421,7 @@ extern "C" int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, 
         set_error("null context");
         return LPM_ERR_ARG;
     }
-    int rc = check_kernel(kernel);
+    int rc = check_kernel_desc(kernel);
     if (rc) return rc;
     if (kernel->kind != LPM_KERNEL_BIOT_SAVART_SPHERE) {
         set_error("invalid kernel: lpm_direct_sum_mesh takes a vector kernel");
@@ -508,7 +505,7 @@ extern "C" int lpm_direct_sum_meshfree(lpm_ctx* ctx, const lpm_kernel_desc* kern
         set_error("null context");
         return LPM_ERR_ARG;
     }
-    int rc = check_kernel(kernel);
+    int rc = check_kernel_desc(kernel);
     if (rc) return rc;
     if (kernel->kind != LPM_KERNEL_POISSON_3D) {
         set_error("invalid kernel: lpm_direct_sum_meshfree takes a scalar kernel");

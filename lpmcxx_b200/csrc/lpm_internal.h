@@ -9,6 +9,7 @@
 
 #ifdef __CUDACC__
 #include <cuda_runtime.h>
+#include <vector>
 #endif
 
 namespace lpm {
@@ -27,12 +28,21 @@ struct LpmBuffer {
     size_t bytes = 0;
 };
 
+// One profiled launch: events recorded around it on the launching stream.
+struct LpmProfRecord {
+    const char* name;
+    cudaEvent_t start, stop;
+};
+
 struct lpm_ctx {
     int device = 0;
     int num_sms = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     int64_t launches = 0;
+    // per-kernel CUDA-event timing (lpm_ctx_set_profiling); off by default and never on during capture
+    bool profiling = false;
+    std::vector<LpmProfRecord>* prof = nullptr;
     // scratch slots, indexed by the enum below
     LpmBuffer buf[32];
     // pinned host staging (host-facing entry points)
@@ -96,14 +106,33 @@ int cuda_status(cudaError_t e, const char* what);
         if (e_ != cudaSuccess) return ::lpm::cuda_status(e_, "kernel launch"); \
     } while (0)
 
+// Launch `kernel<<<grid, block, smem, ctx->stream>>>(args...)`, count it, and when profiling is on
+// bracket it with CUDA events on the same stream under `name`.
+#define LPM_LAUNCH(ctx, name, kernel, grid, block, smem, ...)                                 \
+    do {                                                                                      \
+        ::LpmProfRecord rec_{name, nullptr, nullptr};                                    \
+        if ((ctx)->profiling) ::lpm::prof_begin(ctx, rec_);                                   \
+        kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);                      \
+        if ((ctx)->profiling) ::lpm::prof_end(ctx, rec_);                                     \
+        LPM_LAUNCH_CHECK(ctx);                                                                \
+    } while (0)
+
+void prof_begin(lpm_ctx* ctx, LpmProfRecord& r);
+void prof_end(lpm_ctx* ctx, LpmProfRecord& r);
+
 inline unsigned grid_for(int64_t n, int per_block) { return (unsigned)((n + per_block - 1) / per_block); }
 
 // direct sums (direct_sum.cu)
 int direct_sum_f64(lpm_ctx* ctx, const lpm_kernel_desc& k, const double4* src, int64_t n_src, const double4* tgt,
                    int64_t n_tgt, double* out, int64_t out_stride);
-int direct_sum_f32(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* src, int64_t n_src, const float4* tgt,
-                   int64_t n_tgt, double* out, int64_t out_stride, bool maybe_coincident);
+// FP32 sums: src.w = 2*strength for Biot-Savart; targets 0..coinc_n-1 sit on sources coinc_off.. .
+int direct_sum_f32_impl(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* src, int64_t n_src, const float4* tgt,
+                        const double4* tgt64, int64_t n_tgt, double* out, int64_t out_stride, int64_t coinc_n,
+                        int64_t coinc_off);
+int direct_sum_any(lpm_ctx* ctx, const lpm_kernel_desc& k, int precision, const double4* src, int64_t n_src,
+                   const double4* tgt, int64_t n_tgt, double* out, int64_t coinc_n, int64_t coinc_off);
 int pack_f32(lpm_ctx* ctx, const double4* in, int64_t n, float4* out, bool scale_w2);
+int check_kernel_desc(const lpm_kernel_desc* k);
 
 }  // namespace lpm
 

@@ -1,0 +1,60 @@
+// FMA-pipe microbenchmark: the FP32 / FP64 non-tensor peak the pairwise kernels are measured
+// against (the measured-peaks file carries only HBM and tensor-core figures).  Every thread runs
+// 8 independent FMA chains; the result is written so the chains cannot be removed.
+#include "lpm_internal.h"
+
+namespace lpm {
+namespace {
+
+template <typename T>
+__global__ void __launch_bounds__(256) fma_chain_kernel(T* out, int iters, T a, T b) {
+    T x0 = (T)threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+        }
+    }
+    const T s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+    if (s == (T)-1.2345) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace
+}  // namespace lpm
+
+using namespace lpm;
+
+extern "C" int lpm_fma_peak(lpm_ctx* ctx, int precision, double* tflops) {
+    if (!ctx || !tflops || (precision != LPM_PREC_F32 && precision != LPM_PREC_F64)) {
+        set_error("lpm_fma_peak: bad argument");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(ctx->device));
+    const int blocks = ctx->num_sms * 8, threads = 256;
+    const int iters = precision == LPM_PREC_F32 ? 4096 : 1024;
+    void* out = scratch(ctx, kSlotMisc3, (size_t)blocks * threads * sizeof(double));
+    if (!out) return LPM_ERR_OOM;
+    cudaEvent_t e0, e1;
+    LPM_CUDA_TRY(cudaEventCreate(&e0));
+    LPM_CUDA_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(e0, ctx->stream);
+        if (precision == LPM_PREC_F32)
+            fma_chain_kernel<float><<<blocks, threads, 0, ctx->stream>>>((float*)out, iters, 0.999999f, 1e-7f);
+        else
+            fma_chain_kernel<double><<<blocks, threads, 0, ctx->stream>>>((double*)out, iters, 0.999999, 1e-7);
+        cudaEventRecord(e1, ctx->stream);
+        LPM_LAUNCH_CHECK(ctx);
+        LPM_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && ms < best) best = ms;  // first repetition is warm-up
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double flops = 2.0 * 8.0 * 16.0 * (double)iters * blocks * threads;
+    *tflops = flops / (best * 1e-3) * 1e-12;
+    return LPM_OK;
+}

@@ -39,6 +39,7 @@ def lib() -> C.CDLL:
         P, I, D = C.c_void_p, C.c_int64, C.c_double
         h.oracle_bs_direct.argtypes = [P, I, P, I, D, D, P]
         h.oracle_poisson_direct.argtypes = [P, I, P, I, P]
+        h.oracle_rk4_direct.argtypes = [P, I, I, D, D, D, C.c_int]
         _lib = h
     return _lib
 
@@ -69,6 +70,14 @@ def poisson_direct(src4: np.ndarray, tgt4: np.ndarray) -> np.ndarray:
     out = np.zeros(tgt4.shape[0])
     lib().oracle_poisson_direct(src4.ctypes.data, src4.shape[0], tgt4.ctypes.data, tgt4.shape[0], out.ctypes.data)
     return out
+
+
+def rk4_direct(state: np.ndarray, n_src: int, dt: float, nsteps: int, radius: float = 1.0,
+               delta: float = 0.0) -> np.ndarray:
+    """nsteps RK4 steps (direct-sum velocity, re-projection); returns the new (n, 4) state."""
+    s = _c(state).copy()
+    lib().oracle_rk4_direct(s.ctypes.data, n_src, s.shape[0], radius, delta, dt, nsteps)
+    return s
 
 
 def run_ref_harness(*args: str, env: dict | None = None) -> str:

@@ -128,3 +128,44 @@ void oracle_poisson_direct(const double* src, int64_t n_src, const double* tgt, 
     direct_args a = {src, tgt, n_src, n_tgt, 0.0, 0.0, out};
     parallel_range(n_tgt, poisson_direct_range, &a);
 }
+
+/* RK4 of Lagrangian particles on the sphere with the FP64 direct-sum velocity.  The reference's C++
+ * tree has no integrator (README.md:75 describes the Fortran one); these are the library's stated
+ * semantics: classical RK4, stage positions and the new position re-projected x <- R x/|x|,
+ * stage velocities from a full Biot-Savart direct sum with sources = the first n_src particles. */
+static void project(double* p, double radius) {
+    const double s = radius / sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    p[0] *= s; p[1] *= s; p[2] *= s;
+}
+
+void oracle_rk4_direct(double* state, int64_t n_src, int64_t n, double radius, double delta, double dt,
+                       int nsteps) {
+    double* xs = (double*)malloc(sizeof(double) * 4 * n);
+    double* u = (double*)malloc(sizeof(double) * 3 * n);
+    double* k = (double*)malloc(sizeof(double) * 3 * n);
+    const double a[4] = {0.5 * dt, 0.5 * dt, dt, dt / 6.0};
+    for (int s = 0; s < nsteps; ++s) {
+        memcpy(xs, state, sizeof(double) * 4 * n);
+        for (int stage = 1; stage <= 4; ++stage) {
+            oracle_bs_direct(xs, n_src, xs, n, radius, delta, u);
+            for (int64_t i = 0; i < n; ++i) {
+                double v[3];
+                for (int c = 0; c < 3; ++c) {
+                    const double uc = u[c * n + i];
+                    if (stage == 1) k[c * n + i] = uc;
+                    else if (stage < 4) k[c * n + i] += 2.0 * uc;
+                    v[c] = stage < 4 ? uc : k[c * n + i] + uc;
+                }
+                double p[3];
+                for (int c = 0; c < 3; ++c) p[c] = state[4 * i + c] + a[stage - 1] * v[c];
+                project(p, radius);
+                for (int c = 0; c < 3; ++c) xs[4 * i + c] = p[c];
+            }
+        }
+        for (int64_t i = 0; i < n; ++i)
+            for (int c = 0; c < 3; ++c) state[4 * i + c] = xs[4 * i + c];
+    }
+    free(xs);
+    free(u);
+    free(k);
+}

@@ -20,6 +20,10 @@ void oracle_bs_direct(const double* src, int64_t n_src, const double* tgt, int64
 /* 1/(4 pi |x-y|) direct sum, zero at x == y (DirectSum::meshfreeSolve, src/LpmDirectSum.cpp:240-252). */
 void oracle_poisson_direct(const double* src, int64_t n_src, const double* tgt, int64_t n_tgt, double* out);
 
+/* nsteps classical RK4 steps of the particles state (n x 4: x,y,z,w; the first n_src are sources) with
+ * the Biot-Savart direct-sum velocity, stage and final positions re-projected onto the sphere. */
+void oracle_rk4_direct(double* state, int64_t n_src, int64_t n, double radius, double delta, double dt, int nsteps);
+
 /* Number of host threads the oracle uses (ORACLE_THREADS, default: all online cores). */
 int oracle_threads(void);
 

@@ -285,6 +285,32 @@ int main(int argc, char** argv) {
             npy_f64(out, "face_vel" + tag, field3(pm->getFaceFieldPtr("velocity"), pm->nFaces()), 3);
             npy_i64(out, "slice" + tag, {mv.startIndex(rank), mv.endIndex(rank), mf.startIndex(rank), mf.endIndex(rank)});
             printf("{\"cmd\": \"direct\", \"rank\": %d, \"size\": %d, \"seconds\": %.6f}\n", rank, size, secs);
+        } else if (cmd == "time_direct" && (argc == 5 || argc == 6)) {
+            // times DirectSum::meshSolve on this rank's slice only (no output files), REPS times: the
+            // CPU baseline.  Prints one JSON line with the per-repetition seconds.
+            auto seed = make_seed(argv[2]);
+            auto pm = std::make_shared<MeshedParticles>(*seed, atoi(argv[3]), false, 1.0, rank);
+            init_vorticity(*pm, argv[4]);
+            const int reps = argc == 6 ? atoi(argv[5]) : 1;
+            pm->createVertexField("velocity", "length/time", 3);
+            pm->createFaceField("velocity", "length/time", 3);
+            std::shared_ptr<VectorKernel> kernel(new BiotSavartSphere());
+            MPIReplicatedData mv(pm->nVertices(), rank, size), mf(pm->nFaces(), rank, size);
+            DirectSum solver(pm, kernel, "velocity", "vorticity");
+            std::string secs = "[";
+            for (int r = 0; r < reps; ++r) {
+                const auto t0 = std::chrono::steady_clock::now();
+                solver.meshSolve(mv, mf);
+                const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                secs += (r ? ", " : "") + std::to_string(s);
+            }
+            secs += "]";
+            long nft = 0;
+            for (index_type i = mf.startIndex(rank); i <= mf.endIndex(rank); ++i) nft += pm->faceIsDivided(i) ? 0 : 1;
+            printf("{\"cmd\": \"time_direct\", \"rank\": %d, \"size\": %d, \"seconds\": %s, \"vert_targets\": %ld, "
+                   "\"face_targets\": %ld, \"sources\": %ld, \"n_verts\": %ld, \"n_leaves\": %ld}\n",
+                   rank, size, secs.c_str(), (long)mv.msgSize(rank), nft, (long)pm->nLeafFaces(),
+                   (long)pm->nVertices(), (long)pm->nLeafFaces());
         } else if (cmd == "tree" && argc == 6) {
             auto seed = make_seed(argv[2]);
             auto pm = std::make_shared<MeshedParticles>(*seed, atoi(argv[3]), false, 1.0, rank);

@@ -46,4 +46,4 @@ def test_no_device_is_a_status_not_a_crash():
 
 def test_null_context_rejected():
     k = _capi.KernelDesc(_capi.LPM_KERNEL_BIOT_SAVART_SPHERE, 0, 1.0, 0.0)
-    assert _capi.lib().lpm_direct_sum_dev(None, C.byref(k), 0, None, 0, None, 0, None) == _capi.LPM_ERR_ARG
+    assert _capi.lib().lpm_direct_sum_dev(None, C.byref(k), 0, None, 0, None, 0, 0, None) == _capi.LPM_ERR_ARG

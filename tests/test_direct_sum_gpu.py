@@ -25,9 +25,8 @@ def torch_cuda():
 
 
 def on_torch_stream(ctx):
-    torch = torch_cuda()
-    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
-    return torch
+    torch_cuda()
+    return ctx.use_torch_stream()
 
 
 def test_f64_mesh_matches_reference(ctx):
@@ -111,7 +110,7 @@ def test_dev_api_targets_alias_sources(ctx):
     d = torch.tensor(pts, device="cuda")
     for prec, tol in ((L.LPM_PREC_F64, F64_TOL), (L.LPM_PREC_F32, F32_TOL)):
         out = torch.empty((3, n), dtype=torch.float64, device="cuda")
-        ctx.direct_sum_dev(BS, prec, d, d, out)
+        ctx.direct_sum_dev(BS, prec, d, d, out, n_coincident=n)
         assert rel_l2(out.cpu().numpy(), ref) < tol
 
 
