@@ -127,6 +127,28 @@ int lpm_direct_sum_meshfree(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int pre
                             const double* y, const double* z, const double* src, const double* weights, int64_t begin,
                             int64_t end, double* out);
 
+/* ---- octree (the tree of TreeSum / Tree) */
+typedef struct lpm_tree lpm_tree;
+
+/* Build an octree over device points pts (n x 4; x,y,z used) inside the root box
+ * box = {xmin, xmax, ymin, ymax, zmin, zmax} (host): nodes holding more than max_per_leaf points are
+ * bisected at their FP64 midpoints, points go to the child whose half-open box holds them, empty
+ * children are dropped (TreeSum::generateTreeFromMesh, src/LpmTreeSum.cpp:266-290;
+ * Tree::generateTreeMaxNodes, src/LpmOctree.cpp:84-143, without box shrinking).  Points outside the root
+ * box belong to no leaf.  max_depth <= 0 means the deepest supported level (21).  Returns
+ * LPM_ERR_CAPACITY (tree still created) if a leaf at max_depth holds more than max_per_leaf points. */
+int lpm_tree_build(lpm_ctx* ctx, const double* pts, int64_t n, const double* box, int max_per_leaf, int max_depth,
+                   lpm_tree** out);
+int lpm_tree_destroy(lpm_tree* tree);
+int lpm_tree_counts(const lpm_tree* tree, int64_t* n_in_tree, int64_t* n_nodes, int64_t* n_leaves, int* depth);
+/* Leaf membership as the reference holds it: members (host, n_in_tree) lists the point indices of every
+ * leaf, leaves in depth-first order, each in increasing index order; leaf k is
+ * members[leaf_offsets[k] .. leaf_offsets[k+1]) (host, n_leaves + 1). */
+int lpm_tree_leaf_membership(lpm_tree* tree, int64_t* members, int64_t* leaf_offsets);
+/* All nodes in depth-first pre-order (host arrays, n_nodes each; box n_nodes x 6):
+ * level, parent position (-1 for the root), point count, box bounds. */
+int lpm_tree_nodes(lpm_tree* tree, int64_t* level, int64_t* parent, int64_t* count, double* box);
+
 /* ---- velocity solver selection (DirectSum or TreeSum, and the arithmetic they use) */
 #define LPM_METHOD_DIRECT 0 /* all pairs (DirectSum) */
 #define LPM_METHOD_TREE 1   /* octree treecode (TreeSum) */

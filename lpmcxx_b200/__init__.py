@@ -224,3 +224,49 @@ class RK4:
     def velocity(self, out) -> None:
         """Velocity (3, n) at the current state into a device tensor."""
         check(lib().lpm_rk4_velocity_dev(self.h, ptr(out)), "lpm_rk4_velocity_dev")
+
+
+class Tree:
+    """Device octree (lpm_tree) over a (n, 4) float64 CUDA tensor of points."""
+
+    def __init__(self, ctx: Context, pts, box, max_per_leaf: int, max_depth: int = 0, allow_overflow: bool = False):
+        h = C.c_void_p()
+        b = np.ascontiguousarray(box, dtype=np.float64)
+        rc = lib().lpm_tree_build(ctx.h, ptr(pts), pts.shape[0], ptr(b), max_per_leaf, max_depth, C.byref(h))
+        self.h = h
+        if rc != _capi.LPM_OK and not (allow_overflow and rc == _capi.LPM_ERR_CAPACITY and h):
+            if h:
+                lib().lpm_tree_destroy(h)
+                self.h = None
+            check(rc, "lpm_tree_build")
+        self.overflow = rc == _capi.LPM_ERR_CAPACITY
+
+    def close(self):
+        if self.h:
+            lib().lpm_tree_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def counts(self) -> dict:
+        a, b, c, d = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int()
+        check(lib().lpm_tree_counts(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)), "lpm_tree_counts")
+        return {"n_in_tree": a.value, "n_nodes": b.value, "n_leaves": c.value, "depth": d.value}
+
+    def leaf_membership(self):
+        c = self.counts()
+        members = np.zeros(max(c["n_in_tree"], 1), np.int64)
+        offs = np.zeros(c["n_leaves"] + 1, np.int64)
+        check(lib().lpm_tree_leaf_membership(self.h, ptr(members), ptr(offs)), "lpm_tree_leaf_membership")
+        return members[:c["n_in_tree"]], offs
+
+    def nodes(self) -> dict:
+        m = self.counts()["n_nodes"]
+        lv, par, cnt = (np.zeros(m, np.int64) for _ in range(3))
+        box = np.zeros((m, 6))
+        check(lib().lpm_tree_nodes(self.h, ptr(lv), ptr(par), ptr(cnt), ptr(box)), "lpm_tree_nodes")
+        return {"node_level": lv, "node_parent": par, "node_count": cnt, "node_box": box}

@@ -1,0 +1,487 @@
+// Device octree with the reference's leaf membership.
+//
+// The reference builds its tree recursively (src/LpmTreeSum.cpp:266-290, src/LpmOctree.cpp:84-143):
+// a node whose point count exceeds the leaf capacity is bisected at 0.5*(min+max) along all three
+// axes in FP64 (src/LpmBox3d.cpp:140-151), points go to the child whose half-open box contains them
+// (src/LpmBox3d.h:37-39), children are ordered ix + 2 iy + 4 iz and empty children are dropped.
+//
+// Here every point gets a 63-bit key that replays exactly those FP64 midpoint comparisons for 21
+// levels (bit 63 set = outside the root box), the (key, index) pairs are radix sorted, and nodes are
+// key ranges split level by level on the GPU: a node at level l with more than max_per_leaf points
+// splits into the non-empty ranges of its points' level-(l+1) digits.  Sorted order is the
+// reference's depth-first order, so leaves sorted by range start are its leaves in DFS order.
+#include "octree.h"
+
+#include <algorithm>
+
+namespace lpm {
+
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 items per block
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int32_t warp_incl_scan(int32_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Exclusive scan of one value per thread over a block of up to 1024 threads; returns the block total.
+__device__ int32_t block_excl_scan(int32_t v, int32_t* total) {
+    __shared__ int32_t warp_sums[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    const int32_t incl = warp_incl_scan(v);
+    if (lane == 31) warp_sums[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int32_t s = lane < nw ? warp_sums[lane] : 0;
+        s = warp_incl_scan(s);
+        if (lane < nw) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    const int32_t base = w ? warp_sums[w - 1] : 0;
+    const int32_t tot = warp_sums[nw - 1];
+    __syncthreads();
+    if (total) *total = tot;
+    return base + incl - v;
+}
+
+// ---------------------------------------------------------------------------------- scan
+__global__ void scan_block_sums_kernel(const int32_t* __restrict__ in, int64_t n, int32_t* __restrict__ sums) {
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    int32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t i = base + k * kScanThreads + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    int32_t tot;
+    block_excl_scan(s, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+// In-place exclusive scan of m values by one block; writes the total to *total if given.
+__global__ void scan_single_block_kernel(int32_t* __restrict__ data, int64_t m, int32_t* __restrict__ total) {
+    const int64_t per = (m + blockDim.x - 1) / blockDim.x;
+    const int64_t b = threadIdx.x * per, e = min(b + per, m);
+    int32_t s = 0;
+    for (int64_t i = b; i < e; ++i) s += data[i];
+    int32_t tot;
+    int32_t run = block_excl_scan(s, &tot);
+    for (int64_t i = b; i < e; ++i) {
+        const int32_t v = data[i];
+        data[i] = run;
+        run += v;
+    }
+    if (threadIdx.x == 0 && total) *total = tot;
+}
+
+__global__ void scan_apply_kernel(const int32_t* __restrict__ in, int32_t* __restrict__ out, int64_t n,
+                                  const int32_t* __restrict__ sums) {
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int32_t v[kScanItems];
+    int32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        s += v[k];
+    }
+    int32_t run = block_excl_scan(s, nullptr) + sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+}
+
+// ---------------------------------------------------------------------------------- radix sort
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const K* __restrict__ keys, int64_t n, int shift,
+                                                                  int32_t* __restrict__ counts, int nblocks) {
+    __shared__ int32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+    for (int k = 0; k < kSortItems; ++k) {
+        const int64_t i = base + k * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(int)((keys[i] >> shift) & 255)], 1);
+    }
+    __syncthreads();
+    counts[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Stable scatter: warp w of a block owns items [w*512, (w+1)*512) of the block's tile and walks them
+// in chunks of 32; __match_any_sync groups equal digits inside a chunk.
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const K* __restrict__ kin,
+                                                                     const int32_t* __restrict__ vin,
+                                                                     K* __restrict__ kout, int32_t* __restrict__ vout,
+                                                                     int64_t n, int shift,
+                                                                     const int32_t* __restrict__ offsets,
+                                                                     int nblocks) {
+    constexpr int kWarps = kSortThreads / 32;
+    constexpr int kPerWarp = kSortTile / kWarps;
+    __shared__ int32_t wh[kWarps][256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < kWarps * 256; d += kSortThreads) (&wh[0][0])[d] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)w * kPerWarp;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int c = 0; c < kPerWarp / 32; ++c) {
+        const int64_t i = base + c * 32 + lane;
+        const bool valid = i < n;
+        const int d = valid ? (int)((kin[i] >> shift) & 255) : 256;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (valid && lane == __ffs(peers) - 1) wh[w][d] += __popc(peers);
+    }
+    __syncthreads();
+    {
+        const int d = threadIdx.x;  // 256 threads, one per digit
+        int32_t run = offsets[(int64_t)d * nblocks + blockIdx.x];
+#pragma unroll
+        for (int q = 0; q < kWarps; ++q) {
+            const int32_t t = wh[q][d];
+            wh[q][d] = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+    for (int c = 0; c < kPerWarp / 32; ++c) {
+        const int64_t i = base + c * 32 + lane;
+        const bool valid = i < n;
+        K key = 0;
+        int d = 256;
+        if (valid) {
+            key = kin[i];
+            d = (int)((key >> shift) & 255);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int32_t pos = valid ? wh[w][d] + __popc(peers & lt) : 0;
+        __syncwarp();
+        if (valid) {
+            kout[pos] = key;
+            vout[pos] = vin[i];
+            if (lane == __ffs(peers) - 1) wh[w][d] += __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+template <typename K>
+int radix_sort_impl(lpm_ctx* ctx, K* keys, int32_t* vals, K* tk, int32_t* tv, int64_t n, int bit_lo, int bit_hi) {
+    if (n <= 1) return LPM_OK;
+    const int nblocks = (int)((n + kSortTile - 1) / kSortTile);
+    int32_t* counts = (int32_t*)scratch(ctx, kSlotMisc1, sizeof(int32_t) * 256 * (size_t)nblocks);
+    if (!counts) return LPM_ERR_OOM;
+    K* src_k = keys;
+    int32_t* src_v = vals;
+    K* dst_k = tk;
+    int32_t* dst_v = tv;
+    for (int shift = bit_lo; shift < bit_hi; shift += 8) {
+        LPM_LAUNCH(ctx, "radix_hist_kernel", radix_hist_kernel<K>, nblocks, kSortThreads, 0, src_k, n, shift, counts,
+                   nblocks);
+        LPM_LAUNCH(ctx, "scan_single_block_kernel", scan_single_block_kernel, 1, 1024, 0, counts,
+                   (int64_t)256 * nblocks, (int32_t*)nullptr);
+        LPM_LAUNCH(ctx, "radix_scatter_kernel", radix_scatter_kernel<K>, nblocks, kSortThreads, 0, src_k, src_v, dst_k,
+                   dst_v, n, shift, counts, nblocks);
+        std::swap(src_k, dst_k);
+        std::swap(src_v, dst_v);
+    }
+    if (src_k != keys) {
+        LPM_CUDA_TRY(cudaMemcpyAsync(keys, src_k, sizeof(K) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
+        LPM_CUDA_TRY(cudaMemcpyAsync(vals, src_v, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return LPM_OK;
+}
+
+// ---------------------------------------------------------------------------------- keys
+__global__ void morton_keys_kernel(const double4* __restrict__ pts, int64_t n, RootBox root,
+                                   uint64_t* __restrict__ keys, int32_t* __restrict__ vals,
+                                   int32_t* __restrict__ counters) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool in = false;
+    if (i < n) {
+        const double4 p = pts[i];
+        const double c[3] = {p.x, p.y, p.z};
+        in = root.lo[0] <= c[0] && c[0] < root.hi[0] && root.lo[1] <= c[1] && c[1] < root.hi[1] &&
+             root.lo[2] <= c[2] && c[2] < root.hi[2];
+        uint64_t key = kKeyOutside;
+        if (in) {
+            double lo[3] = {root.lo[0], root.lo[1], root.lo[2]};
+            double hi[3] = {root.hi[0], root.hi[1], root.hi[2]};
+            key = 0;
+            for (int l = 1; l <= kKeyLevels; ++l) {
+                uint64_t digit = 0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const double mid = 0.5 * (lo[a] + hi[a]);  // Box3d::bisectAll midpoint
+                    if (c[a] < mid) {
+                        hi[a] = mid;
+                    } else {
+                        lo[a] = mid;
+                        digit |= 1ull << a;
+                    }
+                }
+                key |= digit << (3 * (kKeyLevels - l));
+            }
+        }
+        keys[i] = key;
+        vals[i] = (int32_t)i;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, in);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(&counters[0], __popc(b));
+}
+
+__device__ __forceinline__ int level_digit(uint64_t key, int level) {
+    return (int)((key >> (3 * (kKeyLevels - level))) & 7ull);
+}
+
+__global__ void tree_init_kernel(Octree t) {
+    t.node_start[0] = 0;
+    t.node_end[0] = t.counters[0];
+    t.node_parent[0] = -1;
+    t.node_first_child[0] = -1;
+    t.node_nchild[0] = 0;
+    t.node_level[0] = 0;
+    for (int a = 0; a < 3; ++a) {
+        t.node_box[2 * a] = t.root.lo[a];
+        t.node_box[2 * a + 1] = t.root.hi[a];
+    }
+    t.level_range[0] = 0;
+    t.level_range[1] = 1;
+    for (int l = 1; l < kKeyLevels + 2; ++l) {
+        t.level_range[2 * l] = 1;
+        t.level_range[2 * l + 1] = 1;
+    }
+    t.counters[1] = 1;
+    t.counters[2] = 0;
+    t.counters[4] = 0;
+}
+
+// For each node of level l holding more than max_per_leaf points: the 9 boundaries of its
+// level-(l+1) digit ranges, and the number of non-empty children.
+__global__ void split_level_kernel(Octree t, int l) {
+    const int lb = t.level_range[2 * l], le = t.level_range[2 * l + 1];
+    for (int i = lb + blockIdx.x * blockDim.x + threadIdx.x; i < le; i += gridDim.x * blockDim.x) {
+        const int s = t.node_start[i], e = t.node_end[i];
+        int32_t* cs = t.child_start + (int64_t)(i - lb) * 9;
+        int nchild = 0;
+        if (e - s > t.max_per_leaf) {
+            cs[0] = s;
+            cs[8] = e;
+            for (int d = 1; d < 8; ++d) {  // first position whose digit >= d
+                int lo = s, hi = e;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (level_digit(t.keys[mid], l + 1) < d) lo = mid + 1;
+                    else hi = mid;
+                }
+                cs[d] = lo;
+            }
+            for (int d = 0; d < 8; ++d) nchild += cs[d + 1] > cs[d];
+        }
+        t.node_split[i - lb] = nchild;
+    }
+}
+
+// One block: scan the level's child counts and append the children as level l+1.
+__global__ void emit_level_kernel(Octree t, int l) {
+    __shared__ int32_t s_total;
+    const int lb = t.level_range[2 * l], le = t.level_range[2 * l + 1];
+    const int m = le - lb;
+    const int per = (m + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per, e = min(b + per, m);
+    int32_t s = 0;
+    for (int i = b; i < e; ++i) s += t.node_split[i];
+    int32_t tot;
+    int32_t run = block_excl_scan(s, &tot) + le;
+    if (threadIdx.x == 0) s_total = tot;
+    for (int i = b; i < e; ++i) {
+        const int node = lb + i;
+        const int nc = t.node_split[i];
+        if (nc == 0 || run + nc > t.node_cap) {
+            if (nc > 0) atomicOr(&t.counters[2], 2);  // node capacity exhausted
+            t.node_first_child[node] = -1;
+            t.node_nchild[node] = 0;
+            continue;
+        }
+        t.node_first_child[node] = run;
+        t.node_nchild[node] = (int8_t)nc;
+        const int32_t* cs = t.child_start + (int64_t)i * 9;
+        const double* pb = t.node_box + 6 * (int64_t)node;
+        double mid[3];
+        for (int a = 0; a < 3; ++a) mid[a] = 0.5 * (pb[2 * a] + pb[2 * a + 1]);
+        int k = run;
+        for (int d = 0; d < 8; ++d) {
+            if (cs[d + 1] <= cs[d]) continue;
+            t.node_start[k] = cs[d];
+            t.node_end[k] = cs[d + 1];
+            t.node_parent[k] = node;
+            t.node_first_child[k] = -1;
+            t.node_nchild[k] = 0;
+            t.node_level[k] = (int8_t)(l + 1);
+            double* cb = t.node_box + 6 * (int64_t)k;
+            for (int a = 0; a < 3; ++a) {
+                const bool upper = (d >> a) & 1;
+                cb[2 * a] = upper ? mid[a] : pb[2 * a];
+                cb[2 * a + 1] = upper ? pb[2 * a + 1] : mid[a];
+            }
+            ++k;
+        }
+        run += nc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int tot2 = (int)min((int64_t)s_total, t.node_cap - (int64_t)le);
+        t.level_range[2 * (l + 1)] = le;
+        t.level_range[2 * (l + 1) + 1] = le + max(tot2, 0);
+        t.counters[1] = le + max(tot2, 0);
+        if (tot2 > 0) t.counters[4] = l + 1;
+    }
+}
+
+__global__ void leaf_flags_kernel(Octree t, int64_t n) {
+    const int nn = t.counters[1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+        if (t.node_nchild[i] == 0) {
+            t.leaf_flag[t.node_start[i]] = 1;
+            if (t.node_end[i] - t.node_start[i] > t.max_per_leaf) atomicOr(&t.counters[2], 1);  // depth limit
+        }
+    }
+    (void)n;
+}
+
+__global__ void leaf_ids_kernel(Octree t, int64_t n) {
+    const int nn = t.counters[1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+        if (t.node_nchild[i] == 0) {
+            const int leaf = t.leaf_flag[t.node_start[i]];
+            t.node_leaf[i] = leaf;
+            t.leaf_node[leaf] = i;
+        } else {
+            t.node_leaf[i] = -1;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) t.counters[3] = t.leaf_flag[n];
+}
+
+__global__ void fill_i32_kernel(int32_t* p, int64_t n, int32_t v) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+}  // namespace
+
+int scan_exclusive_i32(lpm_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, int32_t* total_dev) {
+    if (n <= 0) return LPM_OK;
+    const int nblocks = (int)((n + kScanTile - 1) / kScanTile);
+    int32_t* sums = (int32_t*)scratch(ctx, kSlotMisc2, sizeof(int32_t) * (size_t)(nblocks + 1));
+    if (!sums) return LPM_ERR_OOM;
+    LPM_LAUNCH(ctx, "scan_block_sums_kernel", scan_block_sums_kernel, nblocks, kScanThreads, 0, in, n, sums);
+    LPM_LAUNCH(ctx, "scan_single_block_kernel", scan_single_block_kernel, 1, 1024, 0, sums, (int64_t)nblocks,
+               total_dev);
+    LPM_LAUNCH(ctx, "scan_apply_kernel", scan_apply_kernel, nblocks, kScanThreads, 0, in, out, n, sums);
+    return LPM_OK;
+}
+
+int radix_sort_u64(lpm_ctx* ctx, uint64_t* keys, int32_t* vals, uint64_t* tk, int32_t* tv, int64_t n, int bit_lo) {
+    return radix_sort_impl<uint64_t>(ctx, keys, vals, tk, tv, n, bit_lo, 64);
+}
+
+int radix_sort_u32(lpm_ctx* ctx, uint32_t* keys, int32_t* vals, uint32_t* tk, int32_t* tv, int64_t n, int bits) {
+    return radix_sort_impl<uint32_t>(ctx, keys, vals, tk, tv, n, 0, bits);
+}
+
+int octree_alloc(Octree& t, int64_t n, int max_per_leaf, int max_depth) {
+    octree_free(t);
+    t.n = n;
+    t.max_per_leaf = max_per_leaf;
+    t.max_depth = std::min(std::max(max_depth, 1), kKeyLevels);
+    // every internal node has >= 2 points in distinct children or splits a range of > max points:
+    // n_nodes <= 8 * (internal nodes) + 1 and internal nodes <= depth * n / (max_per_leaf + 1) + 1
+    const int64_t internal = (int64_t)t.max_depth * (n / (max_per_leaf + 1) + 1) + 1;
+    t.node_cap = std::min<int64_t>(8 * internal + 1, std::max<int64_t>(2 * n + 16, 64));
+    const size_t nn = (size_t)std::max<int64_t>(n, 1), nc = (size_t)t.node_cap;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void** p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    };
+    A((void**)&t.keys, nn * 8);
+    A((void**)&t.perm, nn * 4);
+    A((void**)&t.tmp_keys, nn * 8);
+    A((void**)&t.tmp_vals, nn * 4);
+    A((void**)&t.leaf_flag, (nn + 1) * 4);
+    A((void**)&t.node_start, nc * 4);
+    A((void**)&t.node_end, nc * 4);
+    A((void**)&t.node_parent, nc * 4);
+    A((void**)&t.node_first_child, nc * 4);
+    A((void**)&t.node_nchild, nc);
+    A((void**)&t.node_level, nc);
+    A((void**)&t.node_box, nc * 6 * 8);
+    A((void**)&t.node_split, nc * 4);
+    A((void**)&t.child_start, nc * 9 * 4);
+    A((void**)&t.level_range, 2 * (kKeyLevels + 2) * 4);
+    A((void**)&t.counters, 16 * 4);
+    A((void**)&t.leaf_node, nc * 4);
+    A((void**)&t.node_leaf, nc * 4);
+    if (e != cudaSuccess) {
+        octree_free(t);
+        return cuda_status(e, "cudaMalloc (octree)");
+    }
+    return LPM_OK;
+}
+
+void octree_free(Octree& t) {
+    void* ps[] = {t.keys, t.perm, t.tmp_keys, t.tmp_vals, t.leaf_flag, t.node_start, t.node_end, t.node_parent,
+                  t.node_first_child, t.node_nchild, t.node_level, t.node_box, t.node_split, t.child_start,
+                  t.level_range, t.counters, t.leaf_node, t.node_leaf};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    const int64_t n = t.n;
+    const int mpl = t.max_per_leaf, md = t.max_depth;
+    t = Octree();
+    t.n = n;
+    t.max_per_leaf = mpl;
+    t.max_depth = md;
+}
+
+int octree_build(lpm_ctx* ctx, Octree& t, const double4* pts, int64_t n, const RootBox& root) {
+    if (n > t.n || n >= INT32_MAX) {
+        set_error("octree_build: %lld points exceed the tree's capacity", (long long)n);
+        return LPM_ERR_CAPACITY;
+    }
+    t.root = root;
+    LPM_CUDA_TRY(cudaMemsetAsync(t.counters, 0, 16 * 4, ctx->stream));
+    if (n > 0)
+        LPM_LAUNCH(ctx, "morton_keys_kernel", morton_keys_kernel, grid_for(n, 256), 256, 0, pts, n, root, t.keys,
+                   t.perm, t.counters);
+    // the key bits that decide levels 1..max_depth (and the outside flag in bit 63)
+    const int bit_lo = std::max(0, 3 * (kKeyLevels - t.max_depth)) & ~7;
+    int rc = radix_sort_u64(ctx, t.keys, t.perm, t.tmp_keys, t.tmp_vals, n, bit_lo);
+    if (rc) return rc;
+    LPM_LAUNCH(ctx, "tree_init_kernel", tree_init_kernel, 1, 1, 0, t);
+    const unsigned sgrid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(t.node_cap, 256),
+                                                                             4 * ctx->num_sms));
+    for (int l = 0; l < t.max_depth; ++l) {
+        LPM_LAUNCH(ctx, "split_level_kernel", split_level_kernel, sgrid, 256, 0, t, l);
+        LPM_LAUNCH(ctx, "emit_level_kernel", emit_level_kernel, 1, 1024, 0, t, l);
+    }
+    LPM_LAUNCH(ctx, "fill_i32_kernel", fill_i32_kernel, grid_for(n + 1, 256), 256, 0, t.leaf_flag, n + 1, 0);
+    LPM_LAUNCH(ctx, "leaf_flags_kernel", leaf_flags_kernel, sgrid, 256, 0, t, n);
+    rc = scan_exclusive_i32(ctx, t.leaf_flag, t.leaf_flag, n + 1, nullptr);
+    if (rc) return rc;
+    LPM_LAUNCH(ctx, "leaf_ids_kernel", leaf_ids_kernel, sgrid, 256, 0, t, n);
+    return LPM_OK;
+}
+
+}  // namespace lpm

@@ -1,0 +1,61 @@
+// Device octree: Morton keys that replay the reference's FP64 midpoint bisection, an LSD radix
+// sort, and a level-synchronous split of key ranges into nodes.
+#pragma once
+
+#include "lpm_internal.h"
+
+namespace lpm {
+
+constexpr int kKeyLevels = 21;        // 3 bits per level in a 63-bit key; bit 63 marks "outside the root box"
+constexpr uint64_t kKeyOutside = ~0ull;
+
+// Exclusive prefix sum of n int32 values (in may equal out).  Uses ctx scratch slot kSlotMisc2.
+int scan_exclusive_i32(lpm_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, int32_t* total_dev);
+
+// Stable LSD radix sort of (key, value) pairs over key bits [bit_lo, 64), 8 bits per pass.
+// keys/vals are sorted in place (ping-pong through tmp_keys/tmp_vals, which must hold n items).
+int radix_sort_u64(lpm_ctx* ctx, uint64_t* keys, int32_t* vals, uint64_t* tmp_keys, int32_t* tmp_vals, int64_t n,
+                   int bit_lo);
+int radix_sort_u32(lpm_ctx* ctx, uint32_t* keys, int32_t* vals, uint32_t* tmp_keys, int32_t* tmp_vals, int64_t n,
+                   int bits);
+
+struct RootBox {
+    double lo[3], hi[3];
+};
+
+// Octree over points (double4, xyz used).  All arrays device-resident; sizes are capacities.
+struct Octree {
+    int64_t n = 0;          // points given
+    int max_per_leaf = 0;
+    int max_depth = 0;      // levels the keys are split to (<= kKeyLevels)
+    int64_t node_cap = 0;
+    RootBox root{};
+    // per point (sorted order)
+    uint64_t* keys = nullptr;      // sorted keys
+    int32_t* perm = nullptr;       // sorted position -> original index
+    uint64_t* tmp_keys = nullptr;
+    int32_t* tmp_vals = nullptr;
+    // per node (level order)
+    int32_t* node_start = nullptr;
+    int32_t* node_end = nullptr;
+    int32_t* node_parent = nullptr;
+    int32_t* node_first_child = nullptr;  // -1 for a leaf
+    int8_t* node_nchild = nullptr;
+    int8_t* node_level = nullptr;
+    double* node_box = nullptr;           // 6 per node: xlo, xhi, ylo, yhi, zlo, zhi
+    int32_t* node_split = nullptr;        // scratch: child counts of a level
+    int32_t* child_start = nullptr;       // scratch: 9 boundaries per node of a level
+    int32_t* level_range = nullptr;       // [2 * (kKeyLevels + 2)]: begin/end of each level's nodes
+    int32_t* counters = nullptr;          // [0] n_valid, [1] n_nodes, [2] overflow flag, [3] n_leaves, [4] depth
+    // leaves in depth-first order
+    int32_t* leaf_node = nullptr;         // leaf index -> node id
+    int32_t* node_leaf = nullptr;         // node id -> leaf index (or -1)
+    int32_t* leaf_flag = nullptr;         // scratch over points
+};
+
+int octree_alloc(Octree& t, int64_t n, int max_per_leaf, int max_depth);
+void octree_free(Octree& t);
+// Build over pts[0:n] with the given root box.  Fully asynchronous (capturable): no host reads.
+int octree_build(lpm_ctx* ctx, Octree& t, const double4* pts, int64_t n, const RootBox& root);
+
+}  // namespace lpm

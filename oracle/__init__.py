@@ -40,6 +40,7 @@ def lib() -> C.CDLL:
         h.oracle_bs_direct.argtypes = [P, I, P, I, D, D, P]
         h.oracle_poisson_direct.argtypes = [P, I, P, I, P]
         h.oracle_rk4_direct.argtypes = [P, I, I, D, D, D, C.c_int]
+        h.oracle_tree_build.argtypes = [P, I, P, C.c_int, C.c_int, P, P, P, P, P, P, P, P, I, P]
         _lib = h
     return _lib
 
@@ -78,6 +79,43 @@ def rk4_direct(state: np.ndarray, n_src: int, dt: float, nsteps: int, radius: fl
     s = _c(state).copy()
     lib().oracle_rk4_direct(s.ctypes.data, n_src, s.shape[0], radius, delta, dt, nsteps)
     return s
+
+
+def tree_build(pts4: np.ndarray, box, max_per_leaf: int, max_depth: int = 21) -> dict:
+    """Recursive octree with the reference's semantics; returns members / leaf_offsets / node arrays
+    (nodes in depth-first pre-order) and the overflow mask."""
+    pts4 = _c(pts4)
+    n = pts4.shape[0]
+    cap = max(64, 4 * n + 16)
+    box = _c(box)
+    members = np.zeros(max(n, 1), np.int64)
+    offs = np.zeros(n + 2, np.int64)
+    lv, par, cnt = (np.zeros(cap, np.int64) for _ in range(3))
+    nbox = np.zeros((cap, 6))
+    nl, nm, nn = C.c_int64(), C.c_int64(), C.c_int64()
+    flags = lib().oracle_tree_build(pts4.ctypes.data, n, box.ctypes.data, max_per_leaf, max_depth,
+                                    members.ctypes.data, offs.ctypes.data, C.byref(nl), C.byref(nm), lv.ctypes.data,
+                                    par.ctypes.data, cnt.ctypes.data, nbox.ctypes.data, cap, C.byref(nn))
+    k = nn.value
+    return {"members": members[:nm.value], "leaf_offsets": offs[:nl.value + 1], "node_level": lv[:k],
+            "node_parent": par[:k], "node_count": cnt[:k], "node_box": nbox[:k], "flags": flags}
+
+
+def mesh_root_box(vert_xyz: np.ndarray) -> np.ndarray:
+    """Box3d(maxR) with its 1e-5 padding (src/LpmBox3d.h:21-33), maxR over the vertices
+    (Coords::maxR, src/LpmCoords.cpp:136-143) -- the root of TreeSum's mesh constructor."""
+    r2 = (vert_xyz[:, 0] * vert_xyz[:, 0] + vert_xyz[:, 1] * vert_xyz[:, 1]) + vert_xyz[:, 2] * vert_xyz[:, 2]
+    maxr = float(np.sqrt(r2.max()))
+    lo, hi = -maxr - 1e-5, maxr + 1e-5
+    return np.array([lo, hi, lo, hi, lo, hi])
+
+
+def coords_root_box(xyz: np.ndarray) -> np.ndarray:
+    """Tree(coords) root box min - 1e-5*min, max + 1e-5*max per axis (src/LpmOctree.cpp:20-25)."""
+    mn, mx = xyz.min(axis=0), xyz.max(axis=0)
+    lo = mn - 1e-5 * mn
+    hi = mx + 1e-5 * mx
+    return np.array([lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]])
 
 
 def run_ref_harness(*args: str, env: dict | None = None) -> str:

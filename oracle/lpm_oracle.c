@@ -169,3 +169,75 @@ void oracle_rk4_direct(double* state, int64_t n_src, int64_t n, double radius, d
     free(u);
     free(k);
 }
+
+/* ---- octree: the reference's recursive build (TreeSum::generateTreeFromMesh,
+ * src/LpmTreeSum.cpp:266-290; Tree::generateTreeMaxNodes, src/LpmOctree.cpp:84-143): a node holding more
+ * than max_per_leaf indices is bisected at 0.5*(min+max) on all axes (src/LpmBox3d.cpp:140-151), each
+ * child keeps, in the parent's order, the indices its half-open box contains (src/LpmBox3d.h:37-39),
+ * children are visited in order ix + 2 iy + 4 iz and empty children are dropped.  Nodes are recorded in
+ * depth-first pre-order; leaves append their indices to `members`. */
+typedef struct {
+    const double* pts;
+    int max_per_leaf, max_depth;
+    int64_t* members;
+    int64_t n_members;
+    int64_t* leaf_offsets;
+    int64_t n_leaves;
+    int64_t *level, *parent, *count;
+    double* box;
+    int64_t n_nodes, node_cap;
+    int overflow;
+} tree_state;
+
+static void tree_node(tree_state* s, const double* b, const int64_t* idx, int64_t cnt, int level, int64_t parent) {
+    const int64_t me = s->n_nodes;
+    if (me >= s->node_cap) {
+        s->overflow |= 2;
+        return;
+    }
+    s->n_nodes++;
+    s->level[me] = level;
+    s->parent[me] = parent;
+    s->count[me] = cnt;
+    memcpy(s->box + 6 * me, b, 6 * sizeof(double));
+    if (cnt <= s->max_per_leaf || level >= s->max_depth) {
+        if (cnt > s->max_per_leaf) s->overflow |= 1;
+        s->leaf_offsets[s->n_leaves++] = s->n_members;
+        memcpy(s->members + s->n_members, idx, (size_t)cnt * sizeof(int64_t));
+        s->n_members += cnt;
+        return;
+    }
+    const double mx = 0.5 * (b[0] + b[1]), my = 0.5 * (b[2] + b[3]), mz = 0.5 * (b[4] + b[5]);
+    int64_t* kid = (int64_t*)malloc((size_t)cnt * sizeof(int64_t));
+    for (int d = 0; d < 8; ++d) {
+        double cb[6];
+        cb[0] = (d & 1) ? mx : b[0]; cb[1] = (d & 1) ? b[1] : mx;
+        cb[2] = (d & 2) ? my : b[2]; cb[3] = (d & 2) ? b[3] : my;
+        cb[4] = (d & 4) ? mz : b[4]; cb[5] = (d & 4) ? b[5] : mz;
+        int64_t k = 0;
+        for (int64_t j = 0; j < cnt; ++j) {
+            const double* p = s->pts + 4 * idx[j];
+            if (cb[0] <= p[0] && p[0] < cb[1] && cb[2] <= p[1] && p[1] < cb[3] && cb[4] <= p[2] && p[2] < cb[5])
+                kid[k++] = idx[j];
+        }
+        if (k > 0) tree_node(s, cb, kid, k, level + 1, me);
+    }
+    free(kid);
+}
+
+int oracle_tree_build(const double* pts, int64_t n, const double* box, int max_per_leaf, int max_depth,
+                      int64_t* members, int64_t* leaf_offsets, int64_t* n_leaves, int64_t* n_members,
+                      int64_t* node_level, int64_t* node_parent, int64_t* node_count, double* node_box,
+                      int64_t node_cap, int64_t* n_nodes) {
+    tree_state s = {pts, max_per_leaf, max_depth, members, 0, leaf_offsets, 0, node_level, node_parent, node_count,
+                    node_box, 0, node_cap, 0};
+    int64_t* all = (int64_t*)malloc((size_t)(n > 0 ? n : 1) * sizeof(int64_t));
+    for (int64_t i = 0; i < n; ++i) all[i] = i;
+    tree_node(&s, box, all, n, 0, -1);
+    free(all);
+    s.leaf_offsets[s.n_leaves] = s.n_members;
+    *n_leaves = s.n_leaves;
+    *n_members = s.n_members;
+    *n_nodes = s.n_nodes;
+    return s.overflow;
+}

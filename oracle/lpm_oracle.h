@@ -24,6 +24,14 @@ void oracle_poisson_direct(const double* src, int64_t n_src, const double* tgt, 
  * the Biot-Savart direct-sum velocity, stage and final positions re-projected onto the sphere. */
 void oracle_rk4_direct(double* state, int64_t n_src, int64_t n, double radius, double delta, double dt, int nsteps);
 
+/* Recursive octree build with the reference's semantics (see lpm_oracle.c).  pts n x 4; box =
+ * {xmin,xmax,ymin,ymax,zmin,zmax}.  Outputs: members (n), leaf_offsets (n+1), node arrays (node_cap).
+ * Returns a bit mask: 1 = a leaf at max_depth exceeds max_per_leaf, 2 = node_cap exhausted. */
+int oracle_tree_build(const double* pts, int64_t n, const double* box, int max_per_leaf, int max_depth,
+                      int64_t* members, int64_t* leaf_offsets, int64_t* n_leaves, int64_t* n_members,
+                      int64_t* node_level, int64_t* node_parent, int64_t* node_count, double* node_box,
+                      int64_t node_cap, int64_t* n_nodes);
+
 /* Number of host threads the oracle uses (ORACLE_THREADS, default: all online cores). */
 int oracle_threads(void);
 

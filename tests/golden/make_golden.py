@@ -62,6 +62,19 @@ def main() -> None:
     d = harness("poisson", 2000, "0x2B")
     np.savez_compressed(HERE / "poisson_2000.npz", **load(d, "xyz", "charge", "potential"))
 
+    # octrees: TreeSum's mesh constructor (leaf-face centroids, Box3d(maxR) root) and its meshfree
+    # constructor (Tree(coords) root with relative padding)
+    for kind, level, max_leaf in (("icos", 4, 64), ("icos", 5, 100), ("cube", 4, 32)):
+        d = harness("tree", kind, level, max_leaf)
+        z = load(d, "node_level", "node_parent", "node_nkids", "node_ncoords", "node_box", "leaf_offsets",
+                 "leaf_members", "maxr")
+        z["leaf_members"] = z["leaf_members"].astype(np.int32)
+        np.savez_compressed(HERE / f"tree_{kind}{level}_m{max_leaf}.npz", **z)
+    d = harness("pointtree", 8000, "0x5EED", 10)
+    z = load(d, "node_level", "node_parent", "node_nkids", "node_ncoords", "node_box", "leaf_offsets",
+             "leaf_members", "xyz")
+    np.savez_compressed(HERE / "pointtree_8000_m10.npz", **z)
+
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
