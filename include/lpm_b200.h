@@ -166,6 +166,30 @@ typedef struct lpm_solver_desc {
     int32_t reserved;
 } lpm_solver_desc;
 
+/* ---- treecode (TreeSum).  Biot-Savart on the unit sphere (radius 1, delta 0).  The far field expands
+ * 1/|x-y|^2 (equal to 1/(2(1 - x.y)) on the sphere) about each cluster's centre to Taylor order p
+ * (|k| < p) and accepts (target batch, cluster) pairs with rho < theta (|x_batch - c| - r_batch); see
+ * treecode.cu.  A reusable solver object for fixed sizes: */
+typedef struct lpm_treesum lpm_treesum;
+int lpm_treesum_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver, int64_t n_src,
+                       int64_t n_tgt, lpm_treesum** out);
+int lpm_treesum_destroy(lpm_treesum* ts);
+/* Device arrays: src n_src x 4 (x,y,z,w), tgt n_tgt x 4, out 3 x n_tgt (component-major).  Replaces
+ * TreeSum::computeMeshMoments + meshSolve (src/LpmTreeSum.cpp:55-86,182-197) for device-resident data. */
+int lpm_treesum_eval_dev(lpm_treesum* ts, const double* src, const double* tgt, double* out);
+/* Statistics of the last evaluation: nodes, leaves, depth, far (batch, cluster) pairs, near leaf runs,
+ * target batches, overflow flags, 0.  Synchronises. */
+int lpm_treesum_stats(lpm_treesum* ts, int64_t* out8);
+/* Host-facing TreeSum::meshSolve (src/LpmTreeSum.cpp:55-86) with the same data as lpm_direct_sum_mesh;
+ * mac_count (may be NULL) receives the number of accepted far-field (batch, cluster) pairs, the
+ * counterpart of the reference's macCounter. */
+int lpm_tree_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver, int64_t n_verts,
+                      const double* vx, const double* vy, const double* vz, int64_t n_faces, const double* fx,
+                      const double* fy, const double* fz, const double* face_area, const uint8_t* face_divided,
+                      const double* face_src, int64_t vert_begin, int64_t vert_end, int64_t face_begin,
+                      int64_t face_end, double* vert_out0, double* vert_out1, double* vert_out2, double* face_out0,
+                      double* face_out1, double* face_out2, int64_t* mac_count);
+
 /* ---- RK4 integration of the particles (vertices and face-centroid particles as independent
  * Lagrangian particles carrying constant strengths).  The reference's C++ tree has no time
  * integrator; this is the classical four-stage Runge-Kutta step, every stage position and the final

@@ -270,3 +270,54 @@ class Tree:
         box = np.zeros((m, 6))
         check(lib().lpm_tree_nodes(self.h, ptr(lv), ptr(par), ptr(cnt), ptr(box)), "lpm_tree_nodes")
         return {"node_level": lv, "node_parent": par, "node_count": cnt, "node_box": box}
+
+
+class TreeSum:
+    """Device-resident treecode solver (lpm_treesum) for fixed source / target counts."""
+
+    STAT_KEYS = ("nodes", "leaves", "depth", "far_pairs", "near_runs", "batches", "overflow", "reserved")
+
+    def __init__(self, ctx: Context, kernel: KernelDesc, solver: _capi.SolverDesc, n_src: int, n_tgt: int):
+        h = C.c_void_p()
+        check(lib().lpm_treesum_create(ctx.h, C.byref(kernel), C.byref(solver), n_src, n_tgt, C.byref(h)),
+              "lpm_treesum_create")
+        self.h, self.ctx, self.n_src, self.n_tgt = h, ctx, n_src, n_tgt
+
+    def close(self):
+        if self.h:
+            lib().lpm_treesum_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def eval(self, src, tgt, out) -> None:
+        """src (n_src,4), tgt (n_tgt,4), out (3,n_tgt): float64 CUDA tensors."""
+        check(lib().lpm_treesum_eval_dev(self.h, ptr(src), ptr(tgt), ptr(out)), "lpm_treesum_eval_dev")
+
+    def stats(self) -> dict:
+        o = np.zeros(8, np.int64)
+        check(lib().lpm_treesum_stats(self.h, ptr(o)), "lpm_treesum_stats")
+        return dict(zip(self.STAT_KEYS, (int(v) for v in o)))
+
+
+def tree_sum_mesh(ctx: Context, kernel: KernelDesc, solver: _capi.SolverDesc, mesh: SphereMesh, face_src,
+                  vert_range=None, face_range=None, vert_out=None, face_out=None):
+    """TreeSum::meshSolve on host arrays; returns (vert_out (3,nv), face_out (3,nf), mac_count)."""
+    nv, nf = mesh.n_verts, mesh.n_faces
+    vb, ve = vert_range if vert_range is not None else (0, nv - 1)
+    fb, fe = face_range if face_range is not None else (0, nf - 1)
+    vx, vy, vz = (np.ascontiguousarray(mesh.vert_xyz[:, c]) for c in range(3))
+    fx, fy, fz = (np.ascontiguousarray(mesh.face_xyz[:, c]) for c in range(3))
+    vo = np.zeros((3, nv)) if vert_out is None else vert_out
+    fo = np.zeros((3, nf)) if face_out is None else face_out
+    src = np.ascontiguousarray(face_src, dtype=np.float64)
+    mac = C.c_int64()
+    check(lib().lpm_tree_sum_mesh(ctx.h, C.byref(kernel), C.byref(solver), nv, ptr(vx), ptr(vy), ptr(vz), nf,
+                                  ptr(fx), ptr(fy), ptr(fz), ptr(mesh.face_area), ptr(mesh.face_divided), ptr(src),
+                                  vb, ve, fb, fe, ptr(vo[0]), ptr(vo[1]), ptr(vo[2]), ptr(fo[0]), ptr(fo[1]),
+                                  ptr(fo[2]), C.byref(mac)), "lpm_tree_sum_mesh")
+    return vo, fo, mac.value

@@ -78,6 +78,12 @@ SIGNATURES = {
     "lpm_tree_counts": (C.c_int, [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(C.c_int)]),
     "lpm_tree_leaf_membership": (C.c_int, [P, P, P]),
     "lpm_tree_nodes": (C.c_int, [P, P, P, P, P]),
+    "lpm_treesum_create": (C.c_int, [P, C.POINTER(KernelDesc), C.POINTER(SolverDesc), I64, I64, C.POINTER(P)]),
+    "lpm_treesum_destroy": (C.c_int, [P]),
+    "lpm_treesum_eval_dev": (C.c_int, [P, P, P, P]),
+    "lpm_treesum_stats": (C.c_int, [P, P]),
+    "lpm_tree_sum_mesh": (C.c_int, [P, C.POINTER(KernelDesc), C.POINTER(SolverDesc), I64, P, P, P, I64, P, P, P, P, P,
+                                    P, I64, I64, I64, I64, P, P, P, P, P, P, C.POINTER(I64)]),
     "lpm_rk4_create": (C.c_int, [P, C.POINTER(KernelDesc), C.POINTER(SolverDesc), I64, I64, C.POINTER(P)]),
     "lpm_rk4_destroy": (C.c_int, [P]),
     "lpm_rk4_set_state_dev": (C.c_int, [P, P]),

@@ -394,6 +394,14 @@ int scan_exclusive_i32(lpm_ctx* ctx, const int32_t* in, int32_t* out, int64_t n,
     return LPM_OK;
 }
 
+int morton_keys(lpm_ctx* ctx, const double4* pts, int64_t n, const RootBox& root, uint64_t* keys, int32_t* vals,
+                int32_t* counter) {
+    if (n <= 0) return LPM_OK;
+    LPM_LAUNCH(ctx, "morton_keys_kernel", morton_keys_kernel, grid_for(n, 256), 256, 0, pts, n, root, keys, vals,
+               counter);
+    return LPM_OK;
+}
+
 int radix_sort_u64(lpm_ctx* ctx, uint64_t* keys, int32_t* vals, uint64_t* tk, int32_t* tv, int64_t n, int bit_lo) {
     return radix_sort_impl<uint64_t>(ctx, keys, vals, tk, tv, n, bit_lo, 64);
 }

@@ -53,6 +53,10 @@ struct Octree {
     int32_t* leaf_flag = nullptr;         // scratch over points
 };
 
+// keys[i], vals[i] = i for pts[0:n]; counter[0] += number of points inside the root box.
+int morton_keys(lpm_ctx* ctx, const double4* pts, int64_t n, const RootBox& root, uint64_t* keys, int32_t* vals,
+                int32_t* counter);
+
 int octree_alloc(Octree& t, int64_t n, int max_per_leaf, int max_depth);
 void octree_free(Octree& t);
 // Build over pts[0:n] with the given root box.  Fully asynchronous (capturable): no host reads.

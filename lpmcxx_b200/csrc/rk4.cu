@@ -91,7 +91,7 @@ int rk4_velocity(lpm_rk4* rk, double* U) {
         return direct_sum_f32_impl(ctx, rk->kernel, rk->Xs32, rk->n_src, rk->Xs32, rk->Xs, rk->n, U, rk->n, rk->n_src,
                                    0);
     }
-    return tree_velocity(rk->tree, rk->Xs, rk->Xs32, rk->n_src, rk->n, U);
+    return tree_velocity(rk->tree, rk->Xs, rk->n_src, rk->Xs, rk->n, U);
 }
 
 static int rk4_one_step(lpm_rk4* rk, double dt) {

@@ -1,26 +1,923 @@
-// Treecode (TreeSum) evaluation.
+// Treecode (TreeSum) for the spherical Biot-Savart kernel on the GPU.
+//
+// The reference's TreeSum (src/LpmTreeSum.cpp:55-197) is a per-target recursion over a source octree
+// with Taylor moments and far-field coefficients of 1/(1 - x.y) about each box centre.  For points on
+// the unit sphere 1 - x.y = |x - y|^2 / 2, so the kernel is
+//     K(x, y) = (x cross y)/(1 - x.y) = 2 (x cross y) g(y),   g(y) = 1/|x - y|^2,
+// and this file expands g instead: its Taylor series about a centre c converges for |y - c| < |x - c|
+// (a Euclidean acceptance criterion, like the reference's box.maxRadius/|c - x| < theta at
+// src/LpmTreeSum.cpp:22-24), whereas the series of 1/(1 - x.y) about a point off the sphere converges
+// only inside the tangent-plane distance and its Cartesian terms cancel catastrophically for nearby
+// clusters.
+//
+// Far field.  With d = c - x, h = y - c, e = d/|d|^2 and s = |e|^2, the generating function of the
+// Chebyshev polynomials of the second kind, 1/(1 - 2tu + t^2) = sum_n U_n(u) t^n, gives
+//     g(c + h) = (1/|d|^2) sum_{q,m} (-1)^m C(q+m, m) (-2)^q (e.h)^q (s |h|^2)^m,
+// truncated at total degree q + 2m < P (Taylor order P, multi-indices |k| < P as SumNode's
+// (src/LpmTreeSum.cpp:9-18)).  Expanding (e.h)^q = sum_{|k|=q} (q!/k!) e^k h^k turns a cluster's
+// contribution into four polynomials in (e, s) whose coefficients depend on the cluster only:
+//     B^0_{m,k} = (-1)^m C(|k|+m, m) (-2)^{|k|} (|k|!/k!) N_{k,m},     N_{k,m} = sum_j w_j h_j^k |h_j|^{2m},
+//     B^i_{m,k} = same prefactor * N_{k+e_i,m}                          (the h_i part of y = c + h),
+// evaluated per target by nested Horner schemes (4 FMAs per coefficient, a few registers live):
+//     G0 = sum_j w_j g(y_j),  G_i = sum_j w_j h_ij g(y_j),
+//     sum_j w_j (x cross y_j) 2 g(y_j) = 2 [ (x cross d) G0 + x cross G ].
+// Moments are FP64: ordinary moments sum_j w_j h^k of every leaf from its particles, shifted to parents
+// (M2M) level by level, then converted to the B coefficients.  Orders >= 8 evaluate in FP64, lower
+// orders in FP32, always accumulated in FP64.
+//
+// Near field.  Targets are sorted by Morton key into batches of kBatch; a batch and a source node
+// interact in the far field when rho_node < theta (|x_batch - c| - r_batch), otherwise leaves interact
+// directly: FP32 pair arithmetic on coordinates relative to the leaf centre (so |x - y|^2 keeps its
+// relative accuracy for close pairs), FP64 accumulation per leaf.
 #include "treecode.h"
+
+#include "octree.h"
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <vector>
 
 namespace lpm {
 
-struct TreeSolver {
-    lpm_ctx* ctx;
+namespace {
+
+constexpr int kPMax = 12;        // highest supported Taylor order
+constexpr int kBatch = 128;      // targets per batch (threads per far/near block)
+constexpr int kTreeDepth = 10;   // key levels sorted for the treecode's source tree
+constexpr int kStack = 96;
+constexpr int kNearTile = 256;
+constexpr double kPi = 3.14159265358979323846264338327950288;
+
+__host__ __device__ constexpr int tet(int q) { return q * (q + 1) * (q + 2) / 6; }  // #{k : |k| < q}
+__host__ __device__ constexpr int entries_for(int P) {                             // #{(m,k): |k| + 2m < P}
+    int e = 0;
+    for (int m = 0; 2 * m < P; ++m) e += tet(P - 2 * m);
+    return e;
+}
+__host__ __device__ constexpr int cube_dim(int pm) { return pm + 1; }
+
+struct CutoffTable {
+    int32_t direct_below[kPMax + 1];  // a cluster with fewer sources than this is summed directly
+    int32_t table_off[kPMax + 2];     // offsets of each order's gather table
 };
+
+__constant__ double c_binom[kPMax + 2][kPMax + 2];
+__constant__ double c_fact[2 * kPMax + 2];
+
+// ---------------------------------------------------------------------------------- block helpers
+template <typename T>
+__device__ T block_sum(T v, T* sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    T r = 0;
+    for (int i = 0; i < nw; ++i) r += sh[i];
+    return r;
+}
+__device__ double block_max(double v, double* sh) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0;
+    for (int i = 0; i < nw; ++i) r = fmax(r, sh[i]);
+    return r;
+}
+
+__device__ __forceinline__ float rcp32(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// ---------------------------------------------------------------------------------- per-evaluation kernels
+__global__ void gather_sources_kernel(const double4* __restrict__ X, const int32_t* __restrict__ perm,
+                                      const int32_t* __restrict__ counters, double4* __restrict__ out) {
+    const int n = counters[0];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) out[q] = X[perm[q]];
+}
+
+// Leaves: centre (mean position), radius, relative FP32 source copies and ordinary moments
+// mom[a][b][c] = sum_j w_j h^(a,b,c) for a+b+c <= pm.
+__global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* __restrict__ src, int pm,
+                                                       const int4* __restrict__ mono, int n_mono,
+                                                       double4* __restrict__ node_ctr, double* __restrict__ node_wabs,
+                                                       double* __restrict__ node_mom, float4* __restrict__ src_rel) {
+    __shared__ double sh[32];
+    __shared__ double pw[32][3][kPMax + 1];
+    __shared__ double ww[32];
+    const int nleaves = t.counters[3];
+    const int cd = cube_dim(pm);
+    for (int leaf = blockIdx.x; leaf < nleaves; leaf += gridDim.x) {
+        const int node = t.leaf_node[leaf];
+        const int s = t.node_start[node], e = t.node_end[node];
+        double sx = 0, sy = 0, sz = 0, sw = 0;
+        for (int q = s + threadIdx.x; q < e; q += blockDim.x) {
+            const double4 p = src[q];
+            sx += p.x; sy += p.y; sz += p.z; sw += fabs(p.w);
+        }
+        const double inv = 1.0 / (double)max(e - s, 1);
+        const double cx = block_sum(sx, sh) * inv, cy = block_sum(sy, sh) * inv, cz = block_sum(sz, sh) * inv;
+        const double wabs = block_sum(sw, sh);
+        double r = 0;
+        for (int q = s + threadIdx.x; q < e; q += blockDim.x) {
+            const double4 p = src[q];
+            const double hx = p.x - cx, hy = p.y - cy, hz = p.z - cz;
+            r = fmax(r, sqrt(hx * hx + hy * hy + hz * hz));
+            src_rel[q] = make_float4((float)hx, (float)hy, (float)hz, (float)(2.0 * p.w));
+        }
+        r = block_max(r, sh);
+        if (threadIdx.x == 0) {
+            node_ctr[node] = make_double4(cx, cy, cz, r);
+            node_wabs[node] = wabs;
+        }
+        // moments, 32 particles at a time with their power tables in shared memory
+        double acc[4] = {0, 0, 0, 0};
+        for (int q0 = s; q0 < e; q0 += 32) {
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                const int q = q0 + threadIdx.x;
+                double h[3] = {0, 0, 0}, w = 0;
+                if (q < e) {
+                    const double4 p = src[q];
+                    h[0] = p.x - cx; h[1] = p.y - cy; h[2] = p.z - cz; w = p.w;
+                }
+                ww[threadIdx.x] = w;
+                for (int a = 0; a < 3; ++a) {
+                    double v = 1.0;
+                    for (int k = 0; k <= pm; ++k) {
+                        pw[threadIdx.x][a][k] = v;
+                        v *= h[a];
+                    }
+                }
+            }
+            __syncthreads();
+            const int np = min(32, e - q0);
+#pragma unroll
+            for (int r4 = 0; r4 < 4; ++r4) {
+                const int term = threadIdx.x + r4 * blockDim.x;
+                if (term < n_mono) {
+                    const int4 k = mono[term];
+                    double a2 = acc[r4];
+                    for (int j = 0; j < np; ++j) a2 = fma(ww[j] * pw[j][0][k.x], pw[j][1][k.y] * pw[j][2][k.z], a2);
+                    acc[r4] = a2;
+                }
+            }
+        }
+        double* mout = node_mom + (size_t)node * cd * cd * cd;
+#pragma unroll
+        for (int r4 = 0; r4 < 4; ++r4) {
+            const int term = threadIdx.x + r4 * blockDim.x;
+            if (term < n_mono) {
+                const int4 k = mono[term];
+                mout[(k.x * cd + k.y) * cd + k.z] = acc[r4];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Internal nodes of level l: centre = count-weighted mean of the children's centres, radius bound
+// max(|c_child - c| + r_child), moments shifted from the children:
+// m_k(c) = sum_child sum_{j <= k} C(k, j) (c_child - c)^(k-j) m_j(c_child).
+__global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm, const int4* __restrict__ mono,
+                                                        int n_mono, double4* __restrict__ node_ctr,
+                                                        double* __restrict__ node_wabs,
+                                                        double* __restrict__ node_mom) {
+    __shared__ double dp[8][3][kPMax + 1];
+    const int lb = t.level_range[2 * l], le = t.level_range[2 * l + 1];
+    const int cd = cube_dim(pm);
+    for (int node = lb + blockIdx.x; node < le; node += gridDim.x) {
+        const int nc = t.node_nchild[node];
+        if (nc == 0) continue;  // a leaf: done by leaf_p2m_kernel
+        const int fc = t.node_first_child[node];
+        double cx = 0, cy = 0, cz = 0, cnt = 0, wabs = 0;
+        for (int k = 0; k < nc; ++k) {
+            const double4 cc = node_ctr[fc + k];
+            const double m = (double)(t.node_end[fc + k] - t.node_start[fc + k]);
+            cx += m * cc.x; cy += m * cc.y; cz += m * cc.z; cnt += m;
+            wabs += node_wabs[fc + k];
+        }
+        cx /= cnt; cy /= cnt; cz /= cnt;
+        double r = 0;
+        for (int k = 0; k < nc; ++k) {
+            const double4 cc = node_ctr[fc + k];
+            const double dx = cc.x - cx, dy = cc.y - cy, dz = cc.z - cz;
+            r = fmax(r, sqrt(dx * dx + dy * dy + dz * dz) + cc.w);
+        }
+        __syncthreads();
+        if (threadIdx.x < nc * 3) {
+            const int k = threadIdx.x / 3, a = threadIdx.x % 3;
+            const double4 cc = node_ctr[fc + k];
+            const double d = a == 0 ? cc.x - cx : (a == 1 ? cc.y - cy : cc.z - cz);
+            double v = 1.0;
+            for (int q = 0; q <= pm; ++q) {
+                dp[k][a][q] = v;
+                v *= d;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            node_ctr[node] = make_double4(cx, cy, cz, r);
+            node_wabs[node] = wabs;
+        }
+        double* mout = node_mom + (size_t)node * cd * cd * cd;
+        for (int term = threadIdx.x; term < n_mono; term += blockDim.x) {
+            const int4 kk = mono[term];
+            double acc = 0;
+            for (int k = 0; k < nc; ++k) {
+                const double* mc = node_mom + (size_t)(fc + k) * cd * cd * cd;
+                for (int j0 = 0; j0 <= kk.x; ++j0) {
+                    const double f0 = c_binom[kk.x][j0] * dp[k][0][kk.x - j0];
+                    for (int j1 = 0; j1 <= kk.y; ++j1) {
+                        const double f1 = f0 * c_binom[kk.y][j1] * dp[k][1][kk.y - j1];
+                        const double* row = mc + (j0 * cd + j1) * cd;
+                        for (int j2 = 0; j2 <= kk.z; ++j2)
+                            acc = fma(f1 * c_binom[kk.z][j2] * dp[k][2][kk.z - j2], row[j2], acc);
+                    }
+                }
+            }
+            mout[(kk.x * cd + kk.y) * cd + kk.z] = acc;
+        }
+    }
+}
+
+// Far-field coefficients B^{0..3}_{m,k} of every node in canonical (order-pm Horner) layout.
+__global__ void coeff_kernel(Octree t, int pm, const int4* __restrict__ ent, int n_ent,
+                             const double* __restrict__ node_mom, double4* __restrict__ B64,
+                             float4* __restrict__ B32) {
+    const int nn = t.counters[1];
+    const int cd = cube_dim(pm);
+    for (int node = blockIdx.x; node < nn; node += gridDim.x) {
+        const double* mom = node_mom + (size_t)node * cd * cd * cd;
+        for (int i = threadIdx.x; i < n_ent; i += blockDim.x) {
+            const int4 mk = ent[i];  // (m, a, b, c)
+            const int m = mk.x, a = mk.y, b = mk.z, c = mk.w, q = a + b + c;
+            double n0 = 0, n1 = 0, n2 = 0, n3 = 0;
+            for (int j0 = 0; j0 <= m; ++j0) {
+                for (int j1 = 0; j1 <= m - j0; ++j1) {
+                    const int j2 = m - j0 - j1;
+                    const double mult = c_fact[m] / (c_fact[j0] * c_fact[j1] * c_fact[j2]);
+                    const int A = a + 2 * j0, Bb = b + 2 * j1, Cc = c + 2 * j2;
+                    n0 += mult * mom[(A * cd + Bb) * cd + Cc];
+                    n1 += mult * mom[((A + 1) * cd + Bb) * cd + Cc];
+                    n2 += mult * mom[(A * cd + Bb + 1) * cd + Cc];
+                    n3 += mult * mom[(A * cd + Bb) * cd + Cc + 1];
+                }
+            }
+            const double pre = ((m & 1) ? -1.0 : 1.0) * c_binom[q + m][m] * ((q & 1) ? -1.0 : 1.0) *
+                               (double)(1ull << q) * c_fact[q] / (c_fact[a] * c_fact[b] * c_fact[c]);
+            const double4 v = make_double4(pre * n0, pre * n1, pre * n2, pre * n3);
+            B64[(size_t)node * n_ent + i] = v;
+            B32[(size_t)node * n_ent + i] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
+        }
+    }
+}
+
+// Target batches: gather targets in Morton order, batch centre and radius.
+__global__ void __launch_bounds__(kBatch) batch_kernel(const double4* __restrict__ X, const int32_t* __restrict__ tperm,
+                                                       int64_t n_tgt, double4* __restrict__ tgt_sorted,
+                                                       double4* __restrict__ batch_ctr) {
+    __shared__ double sh[32];
+    const int64_t q = (int64_t)blockIdx.x * kBatch + threadIdx.x;
+    double4 p = make_double4(0, 0, 0, 0);
+    const bool ok = q < n_tgt;
+    if (ok) {
+        p = X[tperm[q]];
+        tgt_sorted[q] = p;
+    }
+    const int cnt = (int)min((int64_t)kBatch, n_tgt - (int64_t)blockIdx.x * kBatch);
+    const double cx = block_sum(ok ? p.x : 0.0, sh) / cnt, cy = block_sum(ok ? p.y : 0.0, sh) / cnt,
+                 cz = block_sum(ok ? p.z : 0.0, sh) / cnt;
+    double r = 0;
+    if (ok) r = sqrt((p.x - cx) * (p.x - cx) + (p.y - cy) * (p.y - cy) + (p.z - cz) * (p.z - cz));
+    r = block_max(r, sh);
+    if (threadIdx.x == 0) batch_ctr[blockIdx.x] = make_double4(cx, cy, cz, r);
+}
+
+struct TraverseArgs {
+    Octree t;
+    const double4* node_ctr;
+    const double4* batch_ctr;
+    int64_t n_batches;
+    double theta;
+    int order;
+    int direct_below;
+    int fill;  // 0 = count, 1 = fill
+    int32_t* far_cnt;
+    int32_t* near_cnt;
+    const int32_t* far_off;
+    const int32_t* near_off;
+    int2* far_list;
+    int2* near_list;
+    int64_t far_cap, near_cap;
+    int32_t* flags;
+};
+
+// One thread per batch walks the source tree: (batch, node) pairs that pass the acceptance test go to
+// the far list with the order to use; leaves that fail it (and clusters too small to be worth an
+// expansion) go to the near list as runs of consecutive leaves.
+__global__ void traverse_kernel(TraverseArgs A) {
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= A.n_batches) return;
+    const Octree& t = A.t;
+    if (t.counters[1] == 0 || t.counters[0] == 0) {
+        if (!A.fill) { A.far_cnt[b] = 0; A.near_cnt[b] = 0; }
+        return;
+    }
+    const double4 bc = A.batch_ctr[b];
+    int stack[kStack];
+    int top = 0;
+    stack[top++] = 0;
+    int nfar = 0, nnear = 0;
+    int run_lo = -2, run_hi = -2;
+    const int64_t foff = A.fill ? A.far_off[b] : 0, noff = A.fill ? A.near_off[b] : 0;
+    auto flush_run = [&]() {
+        if (run_lo >= 0) {
+            if (A.fill) {
+                const int64_t at = noff + nnear;
+                if (at < A.near_cap) A.near_list[at] = make_int2(run_lo, run_hi);
+                else atomicOr(&A.flags[0], 2);
+            }
+            ++nnear;
+        }
+    };
+    auto add_leaves = [&](int lo, int hi) {
+        if (lo == run_hi + 1) {
+            run_hi = hi;
+        } else {
+            flush_run();
+            run_lo = lo;
+            run_hi = hi;
+        }
+    };
+    while (top > 0) {
+        const int node = stack[--top];
+        const double4 c = A.node_ctr[node];
+        const int s = t.node_start[node], e = t.node_end[node];
+        const double dx = bc.x - c.x, dy = bc.y - c.y, dz = bc.z - c.z;
+        const double R = sqrt(dx * dx + dy * dy + dz * dz);
+        const bool far_ok = R > bc.w && c.w < A.theta * (R - bc.w);
+        const int nch = t.node_nchild[node];
+        if (far_ok && e - s >= A.direct_below) {
+            if (A.fill) {
+                const int64_t at = foff + nfar;
+                if (at < A.far_cap) A.far_list[at] = make_int2(node, A.order);
+                else atomicOr(&A.flags[0], 1);
+            }
+            ++nfar;
+        } else if (far_ok || nch == 0) {
+            add_leaves(t.leaf_flag[s], t.leaf_flag[e] - 1);
+        } else {
+            const int fc = t.node_first_child[node];
+            if (top + nch > kStack) {
+                atomicOr(&A.flags[0], 4);
+                continue;
+            }
+            for (int k = nch - 1; k >= 0; --k) stack[top++] = fc + k;
+        }
+    }
+    flush_run();
+    if (!A.fill) {
+        A.far_cnt[b] = nfar;
+        A.near_cnt[b] = nnear;
+    }
+}
+
+// ---------------------------------------------------------------------------------- far field
+template <int P, typename T, typename T4>
+__device__ __forceinline__ void horner(const T4* __restrict__ Bc, T e0, T e1, T e2, T s, T& g0, T& g1, T& g2,
+                                       T& g3) {
+    int q = 0;
+    T G0 = 0, G1 = 0, G2 = 0, G3 = 0;
+#pragma unroll
+    for (int m = (P - 1) / 2; m >= 0; --m) {
+        const int Q = P - 2 * m;
+        T P0 = 0, P1 = 0, P2 = 0, P3 = 0;
+#pragma unroll
+        for (int a = Q - 1; a >= 0; --a) {
+            T Q0 = 0, Q1 = 0, Q2 = 0, Q3 = 0;
+#pragma unroll
+            for (int b = Q - 1 - a; b >= 0; --b) {
+                T R0 = 0, R1 = 0, R2 = 0, R3 = 0;
+#pragma unroll
+                for (int c = Q - 1 - a - b; c >= 0; --c) {
+                    const T4 v = Bc[q++];
+                    R0 = fma(R0, e2, v.x); R1 = fma(R1, e2, v.y); R2 = fma(R2, e2, v.z); R3 = fma(R3, e2, v.w);
+                }
+                Q0 = fma(Q0, e1, R0); Q1 = fma(Q1, e1, R1); Q2 = fma(Q2, e1, R2); Q3 = fma(Q3, e1, R3);
+            }
+            P0 = fma(P0, e0, Q0); P1 = fma(P1, e0, Q1); P2 = fma(P2, e0, Q2); P3 = fma(P3, e0, Q3);
+        }
+        G0 = fma(G0, s, P0); G1 = fma(G1, s, P1); G2 = fma(G2, s, P2); G3 = fma(G3, s, P3);
+    }
+    g0 = G0; g1 = G1; g2 = G2; g3 = G3;
+}
+
+// Adds 2 [(x cross d) G0 + x cross G] of one cluster to V, d = c - x.
+template <int P, typename T, typename T4>
+__device__ __forceinline__ void far_one(const T4* Bc, const double4& x, const double4& c, double* V) {
+    const double dx = c.x - x.x, dy = c.y - x.y, dz = c.z - x.z;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const double inv = 1.0 / r2;
+    T g0, g1, g2, g3;
+    horner<P, T, T4>(Bc, (T)(dx * inv), (T)(dy * inv), (T)(dz * inv), (T)inv, g0, g1, g2, g3);
+    const double G0 = 2.0 * inv * (double)g0, Gx = 2.0 * inv * (double)g1, Gy = 2.0 * inv * (double)g2,
+                 Gz = 2.0 * inv * (double)g3;
+    V[0] += (x.y * dz - x.z * dy) * G0 + (x.y * Gz - x.z * Gy);
+    V[1] += (x.z * dx - x.x * dz) * G0 + (x.z * Gx - x.x * Gz);
+    V[2] += (x.x * dy - x.y * dx) * G0 + (x.x * Gy - x.y * Gx);
+}
+
+template <typename T, typename T4>
+__device__ void far_dispatch(int P, const T4* Bc, const double4& x, const double4& c, double* V) {
+    switch (P) {
+        case 1: far_one<1, T, T4>(Bc, x, c, V); break;
+        case 2: far_one<2, T, T4>(Bc, x, c, V); break;
+        case 3: far_one<3, T, T4>(Bc, x, c, V); break;
+        case 4: far_one<4, T, T4>(Bc, x, c, V); break;
+        case 5: far_one<5, T, T4>(Bc, x, c, V); break;
+        case 6: far_one<6, T, T4>(Bc, x, c, V); break;
+        case 7: far_one<7, T, T4>(Bc, x, c, V); break;
+        case 8: far_one<8, T, T4>(Bc, x, c, V); break;
+        case 9: far_one<9, T, T4>(Bc, x, c, V); break;
+        case 10: far_one<10, T, T4>(Bc, x, c, V); break;
+        case 11: far_one<11, T, T4>(Bc, x, c, V); break;
+        case 12: far_one<12, T, T4>(Bc, x, c, V); break;
+        default: break;
+    }
+}
+
+constexpr int kF64From = 8;  // orders >= this evaluate in FP64
+
+__global__ void __launch_bounds__(kBatch) far_kernel(const double4* __restrict__ tgt_sorted, int64_t n_tgt,
+                                                     const int32_t* __restrict__ far_off,
+                                                     const int32_t* __restrict__ far_cnt,
+                                                     const int2* __restrict__ far_list, int64_t far_cap,
+                                                     const double4* __restrict__ node_ctr,
+                                                     const double4* __restrict__ B64, const float4* __restrict__ B32,
+                                                     int n_ent, const int32_t* __restrict__ gtab, CutoffTable ct,
+                                                     double* __restrict__ V) {
+    extern __shared__ double4 sbuf[];
+    const int64_t b = blockIdx.x;
+    const int64_t q = b * kBatch + threadIdx.x;
+    const bool ok = q < n_tgt;
+    const double4 x = ok ? tgt_sorted[q] : make_double4(0, 0, 0, 0);
+    double acc[3] = {0, 0, 0};
+    const int64_t f0 = far_off[b];
+    const int64_t f1 = min(f0 + (int64_t)far_cnt[b], far_cap);
+    for (int64_t f = f0; f < f1; ++f) {
+        const int2 ent = far_list[f];
+        const int P = ent.y;
+        if (P <= 0) continue;  // summed directly by the near kernel
+        const int nterm = ct.table_off[P + 1] - ct.table_off[P];
+        const int32_t* tab = gtab + ct.table_off[P];
+        __syncthreads();
+        if (P >= kF64From) {
+            const double4* src = B64 + (size_t)ent.x * n_ent;
+            for (int i = threadIdx.x; i < nterm; i += kBatch) sbuf[i] = src[tab[i]];
+        } else {
+            float4* s32 = (float4*)sbuf;
+            const float4* src = B32 + (size_t)ent.x * n_ent;
+            for (int i = threadIdx.x; i < nterm; i += kBatch) s32[i] = src[tab[i]];
+        }
+        __syncthreads();
+        const double4 c = node_ctr[ent.x];
+        if (P >= kF64From)
+            far_dispatch<double, double4>(P, sbuf, x, c, acc);
+        else
+            far_dispatch<float, float4>(P, (const float4*)sbuf, x, c, acc);
+    }
+    if (ok) {
+        V[q] = acc[0];
+        V[n_tgt + q] = acc[1];
+        V[2 * n_tgt + q] = acc[2];
+    }
+}
+
+// ---------------------------------------------------------------------------------- near field
+__device__ __forceinline__ void near_leaf(const Octree& t, int leaf, const double4& x,
+                                          const double4* __restrict__ node_ctr, const float4* __restrict__ src_rel,
+                                          float4* tile, double* D) {
+    const int node = t.leaf_node[leaf];
+    const int s = t.node_start[node], e = t.node_end[node];
+    const double4 c = node_ctr[node];
+    const float rx = (float)(x.x - c.x), ry = (float)(x.y - c.y), rz = (float)(x.z - c.z);
+    for (int j0 = s; j0 < e; j0 += kNearTile) {
+        const int m = min(kNearTile, e - j0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < m; j += kBatch) tile[j] = src_rel[j0 + j];
+        __syncthreads();
+        float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll 8
+        for (int j = 0; j < m; ++j) {
+            const float4 y = tile[j];
+            const float dx = rx - y.x, dy = ry - y.y, dz = rz - y.z;
+            const float rr = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1e-30f);  // self pair: d = 0
+            const float f = y.w * rcp32(rr);
+            ax = fmaf(f, dx, ax);
+            ay = fmaf(f, dy, ay);
+            az = fmaf(f, dz, az);
+        }
+        D[0] += ax;
+        D[1] += ay;
+        D[2] += az;
+    }
+}
+
+__global__ void __launch_bounds__(kBatch) near_kernel(Octree t, const double4* __restrict__ tgt_sorted, int64_t n_tgt,
+                                                      const int32_t* __restrict__ tperm,
+                                                      const int32_t* __restrict__ near_off,
+                                                      const int32_t* __restrict__ near_cnt,
+                                                      const int2* __restrict__ near_list, int64_t near_cap,
+                                                      const int32_t* __restrict__ far_off,
+                                                      const int32_t* __restrict__ far_cnt,
+                                                      const int2* __restrict__ far_list, int64_t far_cap,
+                                                      const double4* __restrict__ node_ctr,
+                                                      const float4* __restrict__ src_rel, const double* __restrict__ V,
+                                                      double mult, double* __restrict__ U) {
+    __shared__ float4 tile[kNearTile];
+    const int64_t b = blockIdx.x;
+    const int64_t q = b * kBatch + threadIdx.x;
+    const bool ok = q < n_tgt;
+    const double4 x = ok ? tgt_sorted[q] : make_double4(2, 2, 2, 0);
+    double D[3] = {0, 0, 0};
+    const int64_t n0 = near_off[b], n1 = min(n0 + (int64_t)near_cnt[b], near_cap);
+    for (int64_t k = n0; k < n1; ++k) {
+        const int2 r = near_list[k];
+        for (int leaf = r.x; leaf <= r.y; ++leaf) near_leaf(t, leaf, x, node_ctr, src_rel, tile, D);
+    }
+    // clusters whose order was set to "direct"
+    const int64_t f0 = far_off[b], f1 = min(f0 + (int64_t)far_cnt[b], far_cap);
+    for (int64_t k = f0; k < f1; ++k) {
+        const int2 ent = far_list[k];
+        if (ent.y > 0) continue;
+        const int node = ent.x;
+        const int lo = t.leaf_flag[t.node_start[node]], hi = t.leaf_flag[t.node_end[node]] - 1;
+        for (int leaf = lo; leaf <= hi; ++leaf) near_leaf(t, leaf, x, node_ctr, src_rel, tile, D);
+    }
+    if (ok) {
+        const double v0 = V[q], v1 = V[n_tgt + q], v2 = V[2 * n_tgt + q];
+        // u = mult (V - x cross D)
+        const int64_t o = tperm[q];
+        U[o] = mult * (v0 - (x.y * D[2] - x.z * D[1]));
+        U[n_tgt + o] = mult * (v1 - (x.z * D[0] - x.x * D[2]));
+        U[2 * n_tgt + o] = mult * (v2 - (x.x * D[1] - x.y * D[0]));
+    }
+}
+
+__global__ void zero_f64_kernel(double* p, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = 0.0;
+}
+
+// host-side tables --------------------------------------------------------------------------------
+void canonical_entries(int pm, std::vector<int4>& ent) {
+    ent.clear();
+    for (int m = (pm - 1) / 2; m >= 0; --m) {
+        const int Q = pm - 2 * m;
+        for (int a = Q - 1; a >= 0; --a)
+            for (int b = Q - 1 - a; b >= 0; --b)
+                for (int c = Q - 1 - a - b; c >= 0; --c) ent.push_back(make_int4(m, a, b, c));
+    }
+}
+
+}  // namespace
+
+struct TreeSolver {
+    lpm_ctx* ctx = nullptr;
+    lpm_kernel_desc kernel{};
+    lpm_solver_desc solver{};
+    int64_t n_src = 0, n_tgt = 0, n_batches = 0;
+    int pm = 8;
+    Octree st;
+    // target ordering
+    uint64_t* tkeys = nullptr;
+    int32_t* tperm = nullptr;
+    uint64_t* ttmpk = nullptr;
+    int32_t* ttmpv = nullptr;
+    int32_t* tcount = nullptr;
+    double4* tgt_sorted = nullptr;
+    double4* batch_ctr = nullptr;
+    // sources and nodes
+    double4* src_sorted = nullptr;
+    float4* src_rel = nullptr;
+    double4* node_ctr = nullptr;
+    double* node_wabs = nullptr;
+    double* node_mom = nullptr;
+    double4* B64 = nullptr;
+    float4* B32 = nullptr;
+    int n_ent = 0;
+    int4* ent = nullptr;
+    int4* mono = nullptr;
+    int n_mono = 0;
+    int32_t* gtab = nullptr;
+    CutoffTable ct{};
+    // interaction lists
+    int32_t *far_cnt = nullptr, *near_cnt = nullptr, *far_off = nullptr, *near_off = nullptr, *flags = nullptr;
+    int2 *far_list = nullptr, *near_list = nullptr;
+    int64_t far_cap = 0, near_cap = 0;
+    double* V = nullptr;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+template <typename Tp>
+cudaError_t talloc(TreeSolver* t, Tp** p, size_t count) {
+    cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(Tp));
+    if (e == cudaSuccess) t->allocs.push_back(*p);
+    return e;
+}
+
+int alloc_lists(TreeSolver* t, int64_t far_cap, int64_t near_cap) {
+    for (void** p : {(void**)&t->far_list, (void**)&t->near_list}) {
+        if (*p) {
+            cudaFree(*p);
+            t->allocs.erase(std::find(t->allocs.begin(), t->allocs.end(), *p));
+            *p = nullptr;
+        }
+    }
+    cudaError_t e = talloc(t, &t->far_list, (size_t)far_cap);
+    if (e == cudaSuccess) e = talloc(t, &t->near_list, (size_t)near_cap);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc (interaction lists)");
+    t->far_cap = far_cap;
+    t->near_cap = near_cap;
+    return LPM_OK;
+}
+
+bool constants_ready = false;
+
+int upload_constants() {
+    if (constants_ready) return LPM_OK;
+    double binom[kPMax + 2][kPMax + 2] = {};
+    for (int n = 0; n < kPMax + 2; ++n) {
+        binom[n][0] = 1.0;
+        for (int k = 1; k <= n; ++k) binom[n][k] = binom[n - 1][k - 1] + (k <= n - 1 ? binom[n - 1][k] : 0.0);
+    }
+    double fact[2 * kPMax + 2];
+    fact[0] = 1.0;
+    for (int i = 1; i < 2 * kPMax + 2; ++i) fact[i] = fact[i - 1] * i;
+    LPM_CUDA_TRY(cudaMemcpyToSymbol(c_binom, binom, sizeof(binom)));
+    LPM_CUDA_TRY(cudaMemcpyToSymbol(c_fact, fact, sizeof(fact)));
+    constants_ready = true;
+    return LPM_OK;
+}
+
+}  // namespace
 
 int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_solver_desc& solver, int64_t n_src,
                        int64_t n_tgt, TreeSolver** out) {
-    (void)ctx; (void)kernel; (void)solver; (void)n_src; (void)n_tgt;
     *out = nullptr;
-    set_error("tree solver not available");
-    return LPM_ERR_ARG;
+    if (kernel.kind != LPM_KERNEL_BIOT_SAVART_SPHERE || kernel.radius != 1.0 || kernel.delta != 0.0) {
+        set_error("tree solver: only the singular Biot-Savart kernel on the unit sphere is supported");
+        return LPM_ERR_KERNEL;
+    }
+    if (solver.order < 1 || solver.order > kPMax || solver.max_per_leaf < 1 || !(solver.theta > 0.0) ||
+        solver.theta >= 1.0 || n_src >= INT32_MAX || n_tgt >= INT32_MAX) {
+        set_error("tree solver: need 1 <= order <= %d, max_per_leaf >= 1, 0 < theta < 1", kPMax);
+        return LPM_ERR_ARG;
+    }
+    int rc = upload_constants();
+    if (rc) return rc;
+    TreeSolver* t = new (std::nothrow) TreeSolver();
+    if (!t) return LPM_ERR_OOM;
+    t->ctx = ctx;
+    t->kernel = kernel;
+    t->solver = solver;
+    t->n_src = n_src;
+    t->n_tgt = n_tgt;
+    t->pm = solver.order_policy == LPM_ORDER_LEARNED ? kPMax : solver.order;
+    t->n_batches = (n_tgt + kBatch - 1) / kBatch;
+    rc = octree_alloc(t->st, std::max<int64_t>(n_src, 1), solver.max_per_leaf, kTreeDepth);
+    if (rc) {
+        delete t;
+        return rc;
+    }
+    const size_t nn = (size_t)t->st.node_cap;
+    const int cd = cube_dim(t->pm);
+    std::vector<int4> ent, mono;
+    canonical_entries(t->pm, ent);
+    for (int a = 0; a <= t->pm; ++a)
+        for (int b = 0; a + b <= t->pm; ++b)
+            for (int c = 0; a + b + c <= t->pm; ++c) mono.push_back(make_int4(a, b, c, 0));
+    t->n_ent = (int)ent.size();
+    t->n_mono = (int)mono.size();
+    // gather tables: for order P, the canonical index of each entry of the order-P Horner sequence
+    std::vector<int32_t> gtab;
+    for (int P = 1; P <= kPMax; ++P) {
+        t->ct.table_off[P] = (int32_t)gtab.size();
+        if (P > t->pm) continue;
+        std::vector<int4> eP;
+        canonical_entries(P, eP);
+        for (const int4& e : eP) {
+            int idx = -1;
+            for (int i = 0; i < (int)ent.size(); ++i)
+                if (ent[i].x == e.x && ent[i].y == e.y && ent[i].z == e.z && ent[i].w == e.w) {
+                    idx = i;
+                    break;
+                }
+            gtab.push_back(idx);
+        }
+    }
+    t->ct.table_off[kPMax + 1] = (int32_t)gtab.size();
+    // a cluster is cheaper to sum directly when its far-field work per target (4 FMAs per coefficient,
+    // FP64 counted double) exceeds ~11 FP32 operations per direct pair
+    for (int P = 0; P <= kPMax; ++P)
+        t->ct.direct_below[P] = (int32_t)((P >= kF64From ? 8.0 : 4.0) * entries_for(P) / 11.0);
+    cudaError_t e = cudaSuccess;
+    auto A = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+    };
+    const size_t ns = (size_t)std::max<int64_t>(n_src, 1), ntg = (size_t)std::max<int64_t>(n_tgt, 1);
+    A(talloc(t, &t->tkeys, ntg));
+    A(talloc(t, &t->tperm, ntg));
+    A(talloc(t, &t->ttmpk, ntg));
+    A(talloc(t, &t->ttmpv, ntg));
+    A(talloc(t, &t->tcount, 4));
+    A(talloc(t, &t->tgt_sorted, ntg));
+    A(talloc(t, &t->batch_ctr, (size_t)t->n_batches));
+    A(talloc(t, &t->src_sorted, ns));
+    A(talloc(t, &t->src_rel, ns));
+    A(talloc(t, &t->node_ctr, nn));
+    A(talloc(t, &t->node_wabs, nn));
+    A(talloc(t, &t->node_mom, nn * cd * cd * cd));
+    A(talloc(t, &t->B64, nn * t->n_ent));
+    A(talloc(t, &t->B32, nn * t->n_ent));
+    A(talloc(t, &t->ent, ent.size()));
+    A(talloc(t, &t->mono, mono.size()));
+    A(talloc(t, &t->gtab, gtab.size()));
+    A(talloc(t, &t->far_cnt, (size_t)t->n_batches + 1));
+    A(talloc(t, &t->near_cnt, (size_t)t->n_batches + 1));
+    A(talloc(t, &t->far_off, (size_t)t->n_batches + 1));
+    A(talloc(t, &t->near_off, (size_t)t->n_batches + 1));
+    A(talloc(t, &t->flags, 8));
+    A(talloc(t, &t->V, 3 * ntg));
+    if (e == cudaSuccess) e = cudaMemcpy(t->ent, ent.data(), ent.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(t->mono, mono.data(), mono.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !gtab.empty())
+        e = cudaMemcpy(t->gtab, gtab.data(), gtab.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(t->node_mom, 0, nn * cd * cd * cd * sizeof(double));
+    if (e != cudaSuccess) {
+        tree_solver_destroy(t);
+        return cuda_status(e, "tree solver allocation");
+    }
+    rc = alloc_lists(t, std::max<int64_t>(t->n_batches * 256, 1024), std::max<int64_t>(t->n_batches * 64, 1024));
+    if (rc) {
+        tree_solver_destroy(t);
+        return rc;
+    }
+    *out = t;
+    return LPM_OK;
 }
 
-void tree_solver_destroy(TreeSolver* t) { delete t; }
+void tree_solver_destroy(TreeSolver* t) {
+    if (!t) return;
+    octree_free(t->st);
+    for (void* p : t->allocs) cudaFree(p);
+    delete t;
+}
 
-int tree_velocity(TreeSolver* t, const double4* X, const float4* X32, int64_t n_src, int64_t n_tgt, double* U) {
-    (void)t; (void)X; (void)X32; (void)n_src; (void)n_tgt; (void)U;
-    set_error("tree solver not available");
-    return LPM_ERR_ARG;
+static int build_lists(TreeSolver* t, bool can_sync) {
+    lpm_ctx* ctx = t->ctx;
+    TraverseArgs A{};
+    A.t = t->st;
+    A.node_ctr = t->node_ctr;
+    A.batch_ctr = t->batch_ctr;
+    A.n_batches = t->n_batches;
+    A.theta = t->solver.theta;
+    A.order = t->solver.order;
+    A.direct_below = t->ct.direct_below[t->solver.order];
+    A.far_cnt = t->far_cnt;
+    A.near_cnt = t->near_cnt;
+    A.far_off = t->far_off;
+    A.near_off = t->near_off;
+    A.flags = t->flags;
+    A.fill = 0;
+    const unsigned g = grid_for(t->n_batches, 128);
+    LPM_LAUNCH(ctx, "traverse_kernel", traverse_kernel, g, 128, 0, A);
+    int rc = scan_exclusive_i32(ctx, t->far_cnt, t->far_off, t->n_batches + 1, t->flags + 2);
+    if (rc) return rc;
+    rc = scan_exclusive_i32(ctx, t->near_cnt, t->near_off, t->n_batches + 1, t->flags + 3);
+    if (rc) return rc;
+    if (can_sync) {
+        int32_t tot[2];
+        LPM_CUDA_TRY(cudaMemcpyAsync(tot, t->flags + 2, sizeof(tot), cudaMemcpyDeviceToHost, ctx->stream));
+        LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (tot[0] > t->far_cap || tot[1] > t->near_cap) {
+            rc = alloc_lists(t, std::max<int64_t>(t->far_cap, (int64_t)(tot[0] * 1.5) + 1024),
+                             std::max<int64_t>(t->near_cap, (int64_t)(tot[1] * 1.5) + 1024));
+            if (rc) return rc;
+        }
+    }
+    A.fill = 1;
+    A.far_list = t->far_list;
+    A.near_list = t->near_list;
+    A.far_cap = t->far_cap;
+    A.near_cap = t->near_cap;
+    LPM_LAUNCH(ctx, "traverse_kernel", traverse_kernel, g, 128, 0, A);
+    return LPM_OK;
+}
+
+int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double4* X, int64_t n_tgt, double* U) {
+    lpm_ctx* ctx = t->ctx;
+    if (n_src != t->n_src || n_tgt != t->n_tgt) {
+        set_error("tree_velocity: sizes differ from the solver's");
+        return LPM_ERR_ARG;
+    }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    LPM_CUDA_TRY(cudaStreamIsCapturing(ctx->stream, &cap));
+    const bool can_sync = cap == cudaStreamCaptureStatusNone;
+    if (n_tgt == 0) return LPM_OK;
+    if (n_src == 0) {
+        LPM_CUDA_TRY(cudaMemsetAsync(U, 0, 3 * (size_t)n_tgt * sizeof(double), ctx->stream));
+        return LPM_OK;
+    }
+    LPM_CUDA_TRY(cudaMemsetAsync(t->flags, 0, 8 * sizeof(int32_t), ctx->stream));
+    // unit-sphere particles: a fixed root box |x| <= 1 (+1e-12), padded like Box3d(maxR)
+    const double maxr = 1.0 + 1e-12;
+    RootBox rb;
+    for (int a = 0; a < 3; ++a) {
+        rb.lo[a] = -maxr - 1e-5;
+        rb.hi[a] = maxr + 1e-5;
+    }
+    int rc = octree_build(ctx, t->st, src, n_src, rb);
+    if (rc) return rc;
+    const unsigned gs = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(n_src, 256), 8 * ctx->num_sms));
+    LPM_LAUNCH(ctx, "gather_sources_kernel", gather_sources_kernel, gs, 256, 0, src, t->st.perm, t->st.counters,
+               t->src_sorted);
+    const unsigned gl = (unsigned)std::max<int64_t>(1, std::min<int64_t>(t->st.node_cap, 16 * ctx->num_sms));
+    LPM_LAUNCH(ctx, "leaf_p2m_kernel", leaf_p2m_kernel, gl, 128, 0, t->st, t->src_sorted, t->pm, t->mono, t->n_mono,
+               t->node_ctr, t->node_wabs, t->node_mom, t->src_rel);
+    for (int l = kTreeDepth - 1; l >= 0; --l)
+        LPM_LAUNCH(ctx, "m2m_level_kernel", m2m_level_kernel, gl, 128, 0, t->st, l, t->pm, t->mono, t->n_mono,
+                   t->node_ctr, t->node_wabs, t->node_mom);
+    LPM_LAUNCH(ctx, "coeff_kernel", coeff_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->node_mom, t->B64,
+               t->B32);
+    // targets in Morton order, batches of kBatch
+    LPM_CUDA_TRY(cudaMemsetAsync(t->tcount, 0, 4 * sizeof(int32_t), ctx->stream));
+    rc = morton_keys(ctx, X, n_tgt, rb, t->tkeys, t->tperm, t->tcount);
+    if (rc) return rc;
+    rc = radix_sort_u64(ctx, t->tkeys, t->tperm, t->ttmpk, t->ttmpv, n_tgt, 32);
+    if (rc) return rc;
+    LPM_LAUNCH(ctx, "batch_kernel", batch_kernel, (unsigned)t->n_batches, kBatch, 0, X, t->tperm, n_tgt,
+               t->tgt_sorted, t->batch_ctr);
+    rc = build_lists(t, can_sync);
+    if (rc) return rc;
+    const size_t smem = (size_t)entries_for(t->pm) * sizeof(double4);
+    if (smem > 48 * 1024) LPM_CUDA_TRY(cudaFuncSetAttribute(far_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                            (int)smem));
+    LPM_LAUNCH(ctx, "far_kernel", far_kernel, (unsigned)t->n_batches, kBatch, smem, t->tgt_sorted, n_tgt, t->far_off,
+               t->far_cnt, t->far_list, t->far_cap, t->node_ctr, t->B64, t->B32, t->n_ent, t->gtab, t->ct, t->V);
+    const double mult = -1.0 / (4.0 * kPi * t->kernel.radius);
+    LPM_LAUNCH(ctx, "near_kernel", near_kernel, (unsigned)t->n_batches, kBatch, 0, t->st, t->tgt_sorted, n_tgt,
+               t->tperm, t->near_off, t->near_cnt, t->near_list, t->near_cap, t->far_off, t->far_cnt, t->far_list,
+               t->far_cap, t->node_ctr, t->src_rel, t->V, mult, U);
+    if (can_sync) return tree_check(t);
+    return LPM_OK;
+}
+
+int tree_check(TreeSolver* t) {
+    int32_t f[8], c[8];
+    lpm_ctx* ctx = t->ctx;
+    LPM_CUDA_TRY(cudaMemcpyAsync(f, t->flags, sizeof(f), cudaMemcpyDeviceToHost, ctx->stream));
+    LPM_CUDA_TRY(cudaMemcpyAsync(c, t->st.counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+    LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (f[0]) {
+        set_error("tree solver: interaction list capacity exceeded (flags %d)", f[0]);
+        return LPM_ERR_CAPACITY;
+    }
+    if (c[2] & 2) {
+        set_error("tree solver: octree node capacity exhausted");
+        return LPM_ERR_CAPACITY;
+    }
+    if (c[0] != t->n_src) {
+        set_error("tree solver: %d of %lld sources lie outside the unit-sphere root box", (int)(t->n_src - c[0]),
+                  (long long)t->n_src);
+        return LPM_ERR_ARG;
+    }
+    return LPM_OK;
+}
+
+int tree_stats(TreeSolver* t, int64_t* out8) {
+    int32_t f[8], c[8];
+    lpm_ctx* ctx = t->ctx;
+    LPM_CUDA_TRY(cudaMemcpyAsync(f, t->flags, sizeof(f), cudaMemcpyDeviceToHost, ctx->stream));
+    LPM_CUDA_TRY(cudaMemcpyAsync(c, t->st.counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+    LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    out8[0] = c[1];   // nodes
+    out8[1] = c[3];   // leaves
+    out8[2] = c[4];   // depth
+    out8[3] = f[2];   // far (batch, cluster) pairs
+    out8[4] = f[3];   // near runs
+    out8[5] = t->n_batches;
+    out8[6] = f[0];
+    out8[7] = 0;
+    return LPM_OK;
 }
 
 }  // namespace lpm

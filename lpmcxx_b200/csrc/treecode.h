@@ -10,7 +10,12 @@ struct TreeSolver;
 int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_solver_desc& solver, int64_t n_src,
                        int64_t n_tgt, TreeSolver** out);
 void tree_solver_destroy(TreeSolver* t);
-// Velocity (3 x n_tgt) of targets X[0:n_tgt] from sources X[0:n_src] (X32: FP32 copy, w pre-scaled).
-int tree_velocity(TreeSolver* t, const double4* X, const float4* X32, int64_t n_src, int64_t n_tgt, double* U);
+// Velocity (3 x n_tgt, component-major) at targets tgt[0:n_tgt] from sources src[0:n_src] (x, y, z, w).
+// Targets may coincide with sources (their self pair contributes nothing).
+int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double4* tgt, int64_t n_tgt, double* U);
+// Synchronises and reports capacity overflows of the last evaluation (LPM_ERR_CAPACITY).
+int tree_check(TreeSolver* t);
+// nodes, leaves, depth, far pairs, near runs, batches, overflow flags, 0 (synchronises)
+int tree_stats(TreeSolver* t, int64_t* out8);
 
 }  // namespace lpm

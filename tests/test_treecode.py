@@ -1,0 +1,86 @@
+"""Treecode (TreeSum) accuracy against the FP64 direct sum, and the far-field series it uses."""
+import numpy as np
+import pytest
+
+import lpmcxx_b200 as L
+import lpmcxx_b200.workloads as W
+import oracle
+from oracle.treecode import direct_velocity_sum, far_velocity_sum
+from conftest import rel_l2
+
+
+def sph(v):
+    return v / np.linalg.norm(v, axis=-1, keepdims=True)
+
+
+def test_far_series_converges_geometrically():
+    # the expansion of 1/|x-y|^2 about a cluster centre: error shrinks with the order for rho/R < 1
+    rng = np.random.default_rng(0)
+    a = sph(np.array([1.0, 0.2, 0.1]))
+    y = sph(a + 0.05 * rng.normal(size=(300, 3)))
+    w = rng.uniform(0.5, 1.0, 300)
+    c = y.mean(0)
+    x = sph(a + np.array([0.0, 0.6, 0.0]))
+    exact = direct_velocity_sum(x, y, w)
+    errs = [np.linalg.norm(far_velocity_sum(x, y, w, c, p) - exact) / np.linalg.norm(exact) for p in (3, 7, 11, 13)]
+    assert errs[0] > errs[1] > errs[2] > errs[3]
+    assert errs[3] < 1e-7
+
+
+def gpu_tree_vs_direct(ctx, kind, level, order, theta, max_leaf, prec=L.LPM_PREC_F32):
+    torch = ctx.use_torch_stream()
+    mesh, p, n_src = W.gaussian_vortex_mesh(kind, level)
+    ref = oracle.bs_direct(p[:n_src], p)
+    d = torch.tensor(p, device="cuda")
+    ts = L.TreeSum(ctx, L.biot_savart_kernel(), L.tree_solver(prec, order, max_leaf, theta), n_src, p.shape[0])
+    out = torch.empty((3, p.shape[0]), dtype=torch.float64, device="cuda")
+    ts.eval(d[:n_src], d, out)
+    st = ts.stats()
+    ts.close()
+    return rel_l2(out.cpu().numpy(), ref), st
+
+
+@pytest.mark.gpu
+def test_tree_all_near_field_equals_fp32_direct(ctx):
+    # theta -> 0: nothing is accepted, every pair is summed directly in FP32
+    err, st = gpu_tree_vs_direct(ctx, "icos", 4, 4, 1e-6, 64)
+    assert st["far_pairs"] == 0
+    assert err < 2e-7
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order,theta,tol", [(4, 0.5, 2e-3), (8, 0.5, 1e-4), (12, 0.3, 1e-8)])
+def test_tree_accuracy_vs_fp64_direct(ctx, order, theta, tol):
+    err, st = gpu_tree_vs_direct(ctx, "icos", 6, order, theta, 128)
+    print(order, theta, err, st)
+    assert st["far_pairs"] > 0
+    assert err < tol
+
+
+@pytest.mark.gpu
+def test_tree_error_decreases_with_order(ctx):
+    errs = [gpu_tree_vs_direct(ctx, "cube", 5, p, 0.6, 64)[0] for p in (2, 4, 6, 8, 10)]
+    print(errs)
+    assert all(errs[i + 1] < errs[i] for i in range(len(errs) - 1))
+
+
+@pytest.mark.gpu
+def test_tree_sum_mesh_host_api(ctx):
+    g = np.load("tests/golden/direct_icos4_rh.npz")
+    mesh = L.build_mesh("icos", 4)
+    vo, fo, mac = L.tree_sum_mesh(ctx, L.biot_savart_kernel(), L.tree_solver(L.LPM_PREC_F32, 10, 64, 0.4), mesh,
+                                  g["face_zeta"])
+    leaf = mesh.leaf
+    got = np.concatenate([fo.T[leaf], vo.T])
+    ref = np.concatenate([g["face_vel"][leaf], g["vert_vel"]])
+    assert mac > 0
+    assert rel_l2(got, ref) < 1e-6
+    assert np.all(fo[:, ~leaf] == 0)
+
+
+@pytest.mark.gpu
+def test_tree_rejects_unsupported_kernels(ctx):
+    with pytest.raises(L.LpmError):
+        L.TreeSum(ctx, L.biot_savart_kernel(1.0, 0.1), L.tree_solver(), 10, 10)
+    with pytest.raises(L.LpmError):
+        L.TreeSum(ctx, L.biot_savart_kernel(), L.tree_solver(order=13), 10, 10)
