@@ -9,8 +9,8 @@
 //
 // FP64 kernels follow the reference formula term by term: den = (R^2 - x.y) + delta^2, the term
 // is dropped when |den| <= 1e-13 (src/LpmVectorKernel.h:24-28).  The sum is reorganised as
-// u = mult * (x cross sum_j (w_j/den_j) y_j), since x cross (.) is linear, which saves the
-// per-pair cross product.
+// u = mult * (x cross sum_j (w_j/den_j) (y_j - x)), since x cross (.) is linear and x cross x = 0,
+// which saves the per-pair cross product.
 //
 // FP32 kernels use 1 - x.y = |x - y|^2 / 2 for points on the sphere (no cancellation for close
 // pairs), accumulate sum_j (2 w_j / (r_j^2 + 2 delta^2)) (x - y_j) in FP32 over one shared-memory
@@ -99,9 +99,11 @@ __global__ void __launch_bounds__(kThreads) bs_f64_kernel(const double4* __restr
                 if (kDelta) den += d2;
                 double f = s.w * rcp64(den);
                 f = fabs(den) > kZeroTol ? f : 0.0;
-                sx[t] = fma(f, s.x, sx[t]);
-                sy[t] = fma(f, s.y, sy[t]);
-                sz[t] = fma(f, s.z, sz[t]);
+                // x cross y = x cross (y - x): accumulating (y - x) keeps the terms at the size of
+                // their cross products, so the final x cross S loses no digits to cancellation
+                sx[t] = fma(f, s.x - tx[t], sx[t]);
+                sy[t] = fma(f, s.y - ty[t], sy[t]);
+                sz[t] = fma(f, s.z - tz[t], sz[t]);
             }
         }
     }

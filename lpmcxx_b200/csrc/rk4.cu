@@ -311,6 +311,8 @@ extern "C" int lpm_rk4_step(lpm_rk4* rk, double dt, int nsteps, int use_graph) {
         LPM_CUDA_TRY(cudaGraphLaunch(rk->graph_exec, ctx->stream));
         ctx->launches += rk->graph_nodes;
     }
+    // replays cannot grow the treecode's buffers: report an overflow instead of returning wrong data
+    if (rk->tree) return tree_check(rk->tree);
     return LPM_OK;
 }
 
