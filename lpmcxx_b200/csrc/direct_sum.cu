@@ -94,7 +94,10 @@ __global__ void __launch_bounds__(kThreads) bs_f64_kernel(const double4* __restr
             const double4 s = tile[k];
 #pragma unroll
             for (int t = 0; t < kTpt64; ++t) {
-                const double dot = tx[t] * s.x + ty[t] * s.y + tz[t] * s.z;
+                // (x*x' + y*y') + z*z' rounded exactly like XyzVector::dotProduct in the reference (no
+                // fused multiply-add), so den carries the same rounding error for close pairs
+                const double dot = __dadd_rn(__dadd_rn(__dmul_rn(tx[t], s.x), __dmul_rn(ty[t], s.y)),
+                                             __dmul_rn(tz[t], s.z));
                 double den = r2 - dot;
                 if (kDelta) den += d2;
                 double f = s.w * rcp64(den);

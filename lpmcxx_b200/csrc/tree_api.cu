@@ -75,6 +75,12 @@ extern "C" int lpm_tree_build(lpm_ctx* ctx, const double* pts, int64_t n, const 
     tr->flags = c[2];
     tr->n_leaves = c[3];
     tr->depth = c[4];
+    // the reference's root holds every index it is given; only splitting filters by containment, so an
+    // unsplit root keeps points that lie outside its box
+    if (tr->n_nodes == 1) {
+        tr->n_valid = n;
+        tr->n_leaves = n > 0 ? 1 : tr->n_leaves;
+    }
     *out = tr;
     if (tr->flags) {
         set_error("lpm_tree_build: %s", (tr->flags & 2) ? "node capacity exhausted"
@@ -116,6 +122,12 @@ extern "C" int lpm_tree_leaf_membership(lpm_tree* tr, int64_t* members, int64_t*
     LPM_CUDA_TRY(cudaSetDevice(ctx->device));
     if (n == 0) {
         leaf_offsets[0] = 0;
+        return LPM_OK;
+    }
+    if (tr->n_nodes == 1) {  // unsplit root: every given index, in order
+        for (int64_t i = 0; i < n; ++i) members[i] = i;
+        leaf_offsets[0] = 0;
+        leaf_offsets[1] = n;
         return LPM_OK;
     }
     uint32_t* key = (uint32_t*)scratch(ctx, kSlotTree0, sizeof(uint32_t) * (size_t)n);
@@ -169,7 +181,7 @@ extern "C" int lpm_tree_nodes(lpm_tree* tr, int64_t* level, int64_t* parent, int
         const int64_t i = order[k];
         level[k] = lv[i];
         parent[k] = p[i] < 0 ? -1 : rank[p[i]];
-        count[k] = e[i] - s[i];
+        count[k] = p[i] < 0 ? tr->n : e[i] - s[i];  // the root holds every given index
         for (int a = 0; a < 6; ++a) box[6 * k + a] = b[6 * i + a];
     }
     return LPM_OK;

@@ -762,6 +762,9 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     if (e == cudaSuccess && !gtab.empty())
         e = cudaMemcpy(t->gtab, gtab.data(), gtab.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(t->node_mom, 0, nn * cd * cd * cd * sizeof(double));
+    // the count arrays carry one extra zero entry so that their exclusive scans also yield the totals
+    if (e == cudaSuccess) e = cudaMemset(t->far_cnt, 0, ((size_t)t->n_batches + 1) * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(t->near_cnt, 0, ((size_t)t->n_batches + 1) * sizeof(int32_t));
     if (e != cudaSuccess) {
         tree_solver_destroy(t);
         return cuda_status(e, "tree solver allocation");
