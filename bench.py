@@ -194,6 +194,12 @@ def profile_summary_traffic(kernel: str) -> float | None:
     return None
 
 
+# (order, theta, max_per_leaf) of the fixed-order treecodes: "tree_f32" is the fastest fixed setting
+# measured to reach relative L2 <= 1e-6 against the FP64 direct sum on this workload; "tree_cfg2a" is
+# the p=8, theta=0.7, 512-per-leaf configuration (whose error is ~1e-4).
+TREE_SETTINGS = {"tree_f32": (10, 0.5, 256), "tree_cfg2a": (8, 0.7, 512), "tree_learned": (8, 0.7, 512)}
+
+
 def solver_desc(name: str):
     import lpmcxx_b200 as L
 
@@ -201,17 +207,27 @@ def solver_desc(name: str):
         return L.direct_solver(L.LPM_PREC_F64)
     if name == "direct_f32":
         return L.direct_solver(L.LPM_PREC_F32)
-    if name == "tree_f32":
-        return L.tree_solver(L.LPM_PREC_F32, order=8, max_per_leaf=512, theta=0.7)
-    if name == "tree_learned":
-        return L.tree_solver(L.LPM_PREC_F32, order=8, max_per_leaf=512, theta=0.7, learned=True)
+    if name in TREE_SETTINGS:
+        p, theta, leaf = TREE_SETTINGS[name]
+        return L.tree_solver(L.LPM_PREC_F32, order=p, max_per_leaf=leaf, theta=theta,
+                             learned=name == "tree_learned")
     raise ValueError(name)
 
 
-def kernel_work(kernel: str, n_src: int, n_tgt: int, stats: dict) -> tuple[float, str] | None:
-    """Algorithmic flops of one launch of `kernel`."""
-    if kernel == "bs_f32_kernel" or kernel == "bs_f64_kernel":
+def far_entries(p: int) -> int:
+    """Coefficients of the order-p far-field expansion (multi-indices k, m with |k| + 2m < p)."""
+    return sum((q * (q + 1) * (q + 2)) // 6 for q in range(p, 0, -2))
+
+
+def kernel_work(kernel: str, n_src: int, n_tgt: int, stats: dict | None, order: int) -> tuple[float, str] | None:
+    """Algorithmic flops of one launch of `kernel` (see the work conventions in DESIGN.md)."""
+    if kernel in ("bs_f32_kernel", "bs_f64_kernel"):
         return FLOPS_PER_BS_PAIR * float(n_src) * float(n_tgt), "TFLOP/s"
+    if kernel == "near_kernel" and stats:
+        return FLOPS_PER_BS_PAIR * float(stats["near_pairs"]), "TFLOP/s"
+    if kernel == "far_kernel" and stats:
+        # 4 coefficient FMAs (8 flops) per expansion coefficient + ~40 flops of setup per evaluation
+        return (8.0 * far_entries(order) + 40.0) * float(stats["far_evals"]), "TFLOP/s"
     return None
 
 
@@ -289,15 +305,14 @@ def run_gpu(args) -> None:
         state_bytes = n * 4 * 8
 
         # ---- accuracy of the headline velocity against the FP64 direct sum at the initial state
+        # (one uncaptured evaluation, with per-kernel CUDA-event timing for the roofline)
         rk.set_state(state0)
         u_head = torch.empty((3, n), dtype=torch.float64, device="cuda")
-        rk.velocity(u_head)
-        # ---- per-kernel profile of one uncaptured step (dominant kernel for the roofline)
-        rk.set_state(state0)
         ctx.set_profiling(True)
-        rk.step(args.dt, 1, use_graph=False)
+        rk.velocity(u_head)
         prof = ctx.profile_report()
         ctx.set_profiling(False)
+        tstats = rk.tree_stats() if head.startswith("tree") else None
         rk.close()
 
         # ---- FP64 GPU direct sum on the same workload (one RK4 step)
@@ -330,11 +345,13 @@ def run_gpu(args) -> None:
     if dom[0] is not None:
         name, st = dom
         avg_ms = st["ms"] / st["launches"]
-        work = kernel_work(name, n_src, n, st)
-        peak = fp64_peak if "f64" in name else fp32_peak
+        order = TREE_SETTINGS.get(head, (0,))[0]
+        work = kernel_work(name, n_src, n, tstats, order)
+        fp64_bound = "f64" in name or (name == "far_kernel" and order >= 8)
+        peak = fp64_peak if fp64_bound else fp32_peak
         if work is not None:
             achieved = work[0] / (avg_ms * 1e-3) * 1e-12
-            roof = {"bound": "fp64" if "f64" in name else "fp32", "kernel": name, "achieved": achieved,
+            roof = {"bound": "fp64" if fp64_bound else "fp32", "kernel": name, "achieved": achieved,
                     "peak": peak, "unit": work[1], "frac": achieved / peak, "traffic": profile_summary_traffic(name),
                     "peak_source": "measured FMA microbenchmark (lpm_fma_peak) on this GPU",
                     "avg_launch_ms": avg_ms, "share": st["ms"] / sum(v["ms"] for v in prof.values())}
@@ -351,6 +368,7 @@ def run_gpu(args) -> None:
         "speedup_vs_fp64_direct": (value / world) / fp64_sps if fp64_sps else None,
         "roofline": roof,
         "kernel_profile_ms": {k: v for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])[:12]},
+        "tree_stats": tstats,
         "fma_peaks_tflops": {"fp32": fp32_peak, "fp64": fp64_peak},
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes},
@@ -397,8 +415,8 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lpm", choices=["lpm", "reference"])
-    ap.add_argument("--solver", default="direct_f32",
-                    choices=["direct_f32", "direct_f64", "tree_f32", "tree_learned"])
+    ap.add_argument("--solver", default="tree_f32",
+                    choices=["direct_f32", "direct_f64", "tree_f32", "tree_cfg2a", "tree_learned"])
     ap.add_argument("--level", type=int, default=LEVEL)
     ap.add_argument("--dt", type=float, default=DT)
     ap.add_argument("--no-cpu-baseline", action="store_true")

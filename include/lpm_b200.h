@@ -177,9 +177,10 @@ int lpm_treesum_destroy(lpm_treesum* ts);
 /* Device arrays: src n_src x 4 (x,y,z,w), tgt n_tgt x 4, out 3 x n_tgt (component-major).  Replaces
  * TreeSum::computeMeshMoments + meshSolve (src/LpmTreeSum.cpp:55-86,182-197) for device-resident data. */
 int lpm_treesum_eval_dev(lpm_treesum* ts, const double* src, const double* tgt, double* out);
-/* Statistics of the last evaluation: nodes, leaves, depth, far (batch, cluster) pairs, near leaf runs,
- * target batches, overflow flags, 0.  Synchronises. */
-int lpm_treesum_stats(lpm_treesum* ts, int64_t* out8);
+/* Statistics of the last evaluation, 10 values: nodes, leaves, depth, far (batch, cluster) pairs, near
+ * leaf ranges, target batches, overflow flags, far-field (target, cluster) evaluations, near-field
+ * (target, source) pairs, 0.  Synchronises. */
+int lpm_treesum_stats(lpm_treesum* ts, int64_t* out10);
 /* Host-facing TreeSum::meshSolve (src/LpmTreeSum.cpp:55-86) with the same data as lpm_direct_sum_mesh;
  * mac_count (may be NULL) receives the number of accepted far-field (batch, cluster) pairs, the
  * counterpart of the reference's macCounter. */
@@ -211,6 +212,8 @@ int lpm_rk4_get_state(lpm_rk4* rk, double* xyzw);
 int lpm_rk4_step(lpm_rk4* rk, double dt, int nsteps, int use_graph);
 /* Velocity (3 x n_pts, component-major, device) at the current state; for diagnostics and tests. */
 int lpm_rk4_velocity_dev(lpm_rk4* rk, double* out);
+/* Treecode statistics of the last velocity evaluation (the 10 values of lpm_treesum_stats). */
+int lpm_rk4_tree_stats(lpm_rk4* rk, int64_t* out10);
 
 #ifdef __cplusplus
 }

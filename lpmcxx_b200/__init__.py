@@ -225,6 +225,11 @@ class RK4:
         """Velocity (3, n) at the current state into a device tensor."""
         check(lib().lpm_rk4_velocity_dev(self.h, ptr(out)), "lpm_rk4_velocity_dev")
 
+    def tree_stats(self) -> dict:
+        o = np.zeros(10, np.int64)
+        check(lib().lpm_rk4_tree_stats(self.h, ptr(o)), "lpm_rk4_tree_stats")
+        return dict(zip(TreeSum.STAT_KEYS, (int(v) for v in o)))
+
 
 class Tree:
     """Device octree (lpm_tree) over a (n, 4) float64 CUDA tensor of points."""
@@ -275,7 +280,8 @@ class Tree:
 class TreeSum:
     """Device-resident treecode solver (lpm_treesum) for fixed source / target counts."""
 
-    STAT_KEYS = ("nodes", "leaves", "depth", "far_pairs", "near_runs", "batches", "overflow", "reserved")
+    STAT_KEYS = ("nodes", "leaves", "depth", "far_pairs", "near_runs", "batches", "overflow", "far_evals",
+                 "near_pairs", "reserved")
 
     def __init__(self, ctx: Context, kernel: KernelDesc, solver: _capi.SolverDesc, n_src: int, n_tgt: int):
         h = C.c_void_p()
@@ -299,7 +305,7 @@ class TreeSum:
         check(lib().lpm_treesum_eval_dev(self.h, ptr(src), ptr(tgt), ptr(out)), "lpm_treesum_eval_dev")
 
     def stats(self) -> dict:
-        o = np.zeros(8, np.int64)
+        o = np.zeros(10, np.int64)
         check(lib().lpm_treesum_stats(self.h, ptr(o)), "lpm_treesum_stats")
         return dict(zip(self.STAT_KEYS, (int(v) for v in o)))
 

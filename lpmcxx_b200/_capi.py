@@ -92,6 +92,7 @@ SIGNATURES = {
     "lpm_rk4_get_state": (C.c_int, [P, P]),
     "lpm_rk4_step": (C.c_int, [P, D, C.c_int, C.c_int]),
     "lpm_rk4_velocity_dev": (C.c_int, [P, P]),
+    "lpm_rk4_tree_stats": (C.c_int, [P, P]),
 }
 
 _lib = None

@@ -316,6 +316,19 @@ extern "C" int lpm_rk4_step(lpm_rk4* rk, double dt, int nsteps, int use_graph) {
     return LPM_OK;
 }
 
+extern "C" int lpm_rk4_tree_stats(lpm_rk4* rk, int64_t* out10) {
+    if (!rk || !out10) {
+        set_error("lpm_rk4_tree_stats: null argument");
+        return LPM_ERR_ARG;
+    }
+    if (!rk->tree) {
+        set_error("lpm_rk4_tree_stats: the integrator does not use the treecode");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(rk->ctx->device));
+    return tree_stats(rk->tree, out10);
+}
+
 extern "C" int lpm_rk4_velocity_dev(lpm_rk4* rk, double* out) {
     if (!rk || !out) {
         set_error("lpm_rk4_velocity_dev: null argument");

@@ -303,7 +303,7 @@ struct TraverseArgs {
     Octree t;
     const double4* node_ctr;
     const double4* batch_ctr;
-    int64_t n_batches;
+    int64_t n_batches, n_tgt;
     double theta;
     int order;
     int direct_below;
@@ -316,75 +316,103 @@ struct TraverseArgs {
     int2* near_list;
     int64_t far_cap, near_cap;
     int32_t* flags;
+    unsigned long long* pair_counts;  // [0] target-cluster far evaluations, [1] target-source near pairs
 };
 
-// One thread per batch walks the source tree: (batch, node) pairs that pass the acceptance test go to
-// the far list with the order to use; leaves that fail it (and clusters too small to be worth an
-// expansion) go to the near list as runs of consecutive leaves.
-__global__ void traverse_kernel(TraverseArgs A) {
-    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= A.n_batches) return;
+constexpr int kWarpStack = 1024;
+
+// One warp per target batch walks the source tree breadth-first, up to 32 nodes per step: (batch, node)
+// pairs that pass the acceptance test go to the far list with the order to use; leaves that fail it,
+// and accepted clusters too small to be worth an expansion, go to the near list as leaf-id ranges.
+// Entries are appended in lane order, so the lists are deterministic.
+__global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
+    __shared__ int sstack[4][kWarpStack];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t b = (int64_t)blockIdx.x * 4 + w;
+    if (b >= A.n_batches) return;  // uniform per warp
     const Octree& t = A.t;
+    const unsigned full = 0xffffffffu, lt = (1u << lane) - 1u;
+    int* st = sstack[w];
     if (t.counters[1] == 0 || t.counters[0] == 0) {
-        if (!A.fill) { A.far_cnt[b] = 0; A.near_cnt[b] = 0; }
+        if (!A.fill && lane == 0) {
+            A.far_cnt[b] = 0;
+            A.near_cnt[b] = 0;
+        }
         return;
     }
     const double4 bc = A.batch_ctr[b];
-    int stack[kStack];
-    int top = 0;
-    stack[top++] = 0;
+    const unsigned long long nb = (unsigned long long)min((int64_t)kBatch, A.n_tgt - b * kBatch);
+    int size = 1;
+    if (lane == 0) st[0] = 0;
+    __syncwarp();
     int nfar = 0, nnear = 0;
-    int run_lo = -2, run_hi = -2;
+    unsigned long long far_pairs = 0, near_pairs = 0;
     const int64_t foff = A.fill ? A.far_off[b] : 0, noff = A.fill ? A.near_off[b] : 0;
-    auto flush_run = [&]() {
-        if (run_lo >= 0) {
-            if (A.fill) {
-                const int64_t at = noff + nnear;
-                if (at < A.near_cap) A.near_list[at] = make_int2(run_lo, run_hi);
-                else atomicOr(&A.flags[0], 2);
+    while (size > 0) {
+        const int m = min(32, size);
+        const int node = lane < m ? st[size - 1 - lane] : -1;
+        __syncwarp();
+        size -= m;
+        int kind = 0, nch = 0, lo = 0, hi = 0, cnt = 0, fc = 0;
+        if (node >= 0) {
+            const double4 c = A.node_ctr[node];
+            const int s = t.node_start[node], e = t.node_end[node];
+            const double dx = bc.x - c.x, dy = bc.y - c.y, dz = bc.z - c.z;
+            const double R = sqrt(dx * dx + dy * dy + dz * dz);
+            const bool far_ok = R > bc.w && c.w < A.theta * (R - bc.w);
+            const int nc = t.node_nchild[node];
+            if (far_ok && e - s >= A.direct_below) {
+                kind = 1;
+            } else if (far_ok || nc == 0) {
+                kind = 2;
+                lo = t.leaf_flag[s];
+                hi = t.leaf_flag[e] - 1;
+                cnt = e - s;
+            } else {
+                kind = 3;
+                nch = nc;
+                fc = t.node_first_child[node];
             }
-            ++nnear;
         }
-    };
-    auto add_leaves = [&](int lo, int hi) {
-        if (lo == run_hi + 1) {
-            run_hi = hi;
-        } else {
-            flush_run();
-            run_lo = lo;
-            run_hi = hi;
+        const unsigned fm = __ballot_sync(full, kind == 1);
+        if (kind == 1 && A.fill) {
+            const int64_t at = foff + nfar + __popc(fm & lt);
+            if (at < A.far_cap) A.far_list[at] = make_int2(node, A.order);
+            else atomicOr(&A.flags[0], 1);
         }
-    };
-    while (top > 0) {
-        const int node = stack[--top];
-        const double4 c = A.node_ctr[node];
-        const int s = t.node_start[node], e = t.node_end[node];
-        const double dx = bc.x - c.x, dy = bc.y - c.y, dz = bc.z - c.z;
-        const double R = sqrt(dx * dx + dy * dy + dz * dz);
-        const bool far_ok = R > bc.w && c.w < A.theta * (R - bc.w);
-        const int nch = t.node_nchild[node];
-        if (far_ok && e - s >= A.direct_below) {
-            if (A.fill) {
-                const int64_t at = foff + nfar;
-                if (at < A.far_cap) A.far_list[at] = make_int2(node, A.order);
-                else atomicOr(&A.flags[0], 1);
-            }
-            ++nfar;
-        } else if (far_ok || nch == 0) {
-            add_leaves(t.leaf_flag[s], t.leaf_flag[e] - 1);
-        } else {
-            const int fc = t.node_first_child[node];
-            if (top + nch > kStack) {
-                atomicOr(&A.flags[0], 4);
-                continue;
-            }
-            for (int k = nch - 1; k >= 0; --k) stack[top++] = fc + k;
+        nfar += __popc(fm);
+        far_pairs += (unsigned long long)__popc(fm) * nb;
+        const unsigned nm = __ballot_sync(full, kind == 2);
+        if (kind == 2 && A.fill) {
+            const int64_t at = noff + nnear + __popc(nm & lt);
+            if (at < A.near_cap) A.near_list[at] = make_int2(lo, hi);
+            else atomicOr(&A.flags[0], 2);
         }
+        nnear += __popc(nm);
+        unsigned long long np = (unsigned long long)cnt * nb;
+        for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(full, np, o);
+        near_pairs += np;
+        // push the children of split nodes
+        int incl = nch;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(full, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(full, incl, 31);
+        if (size + total > kWarpStack) {
+            if (lane == 0) atomicOr(&A.flags[0], 4);
+        } else if (kind == 3) {
+            const int base = size + incl - nch;
+            for (int k = 0; k < nch; ++k) st[base + k] = fc + nch - 1 - k;
+        }
+        __syncwarp();
+        if (size + total <= kWarpStack) size += total;
     }
-    flush_run();
-    if (!A.fill) {
+    if (!A.fill && lane == 0) {
         A.far_cnt[b] = nfar;
         A.near_cnt[b] = nnear;
+        atomicAdd(&A.pair_counts[0], far_pairs);
+        atomicAdd(&A.pair_counts[1], near_pairs);
     }
 }
 
@@ -619,6 +647,7 @@ struct TreeSolver {
     CutoffTable ct{};
     // interaction lists
     int32_t *far_cnt = nullptr, *near_cnt = nullptr, *far_off = nullptr, *near_off = nullptr, *flags = nullptr;
+    unsigned long long* pair_counts = nullptr;
     int2 *far_list = nullptr, *near_list = nullptr;
     int64_t far_cap = 0, near_cap = 0;
     double* V = nullptr;
@@ -756,6 +785,7 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->far_off, (size_t)t->n_batches + 1));
     A(talloc(t, &t->near_off, (size_t)t->n_batches + 1));
     A(talloc(t, &t->flags, 8));
+    A(talloc(t, &t->pair_counts, 2));
     A(talloc(t, &t->V, 3 * ntg));
     if (e == cudaSuccess) e = cudaMemcpy(t->ent, ent.data(), ent.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(t->mono, mono.data(), mono.size() * sizeof(int4), cudaMemcpyHostToDevice);
@@ -792,6 +822,7 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     A.node_ctr = t->node_ctr;
     A.batch_ctr = t->batch_ctr;
     A.n_batches = t->n_batches;
+    A.n_tgt = t->n_tgt;
     A.theta = t->solver.theta;
     A.order = t->solver.order;
     A.direct_below = t->ct.direct_below[t->solver.order];
@@ -800,8 +831,10 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     A.far_off = t->far_off;
     A.near_off = t->near_off;
     A.flags = t->flags;
+    A.pair_counts = t->pair_counts;
     A.fill = 0;
-    const unsigned g = grid_for(t->n_batches, 128);
+    LPM_CUDA_TRY(cudaMemsetAsync(t->pair_counts, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    const unsigned g = grid_for(t->n_batches, 4);
     LPM_LAUNCH(ctx, "traverse_kernel", traverse_kernel, g, 128, 0, A);
     int rc = scan_exclusive_i32(ctx, t->far_cnt, t->far_off, t->n_batches + 1, t->flags + 2);
     if (rc) return rc;
@@ -908,7 +941,9 @@ int tree_check(TreeSolver* t) {
 
 int tree_stats(TreeSolver* t, int64_t* out8) {
     int32_t f[8], c[8];
+    unsigned long long pc[2];
     lpm_ctx* ctx = t->ctx;
+    LPM_CUDA_TRY(cudaMemcpyAsync(pc, t->pair_counts, sizeof(pc), cudaMemcpyDeviceToHost, ctx->stream));
     LPM_CUDA_TRY(cudaMemcpyAsync(f, t->flags, sizeof(f), cudaMemcpyDeviceToHost, ctx->stream));
     LPM_CUDA_TRY(cudaMemcpyAsync(c, t->st.counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
     LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -919,7 +954,9 @@ int tree_stats(TreeSolver* t, int64_t* out8) {
     out8[4] = f[3];   // near runs
     out8[5] = t->n_batches;
     out8[6] = f[0];
-    out8[7] = 0;
+    out8[7] = (int64_t)pc[0];  // far-field target-cluster evaluations
+    out8[8] = (int64_t)pc[1];  // near-field target-source pairs
+    out8[9] = 0;
     return LPM_OK;
 }
 

@@ -15,7 +15,8 @@ void tree_solver_destroy(TreeSolver* t);
 int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double4* tgt, int64_t n_tgt, double* U);
 // Synchronises and reports capacity overflows of the last evaluation (LPM_ERR_CAPACITY).
 int tree_check(TreeSolver* t);
-// nodes, leaves, depth, far pairs, near runs, batches, overflow flags, 0 (synchronises)
-int tree_stats(TreeSolver* t, int64_t* out8);
+// nodes, leaves, depth, far (batch, cluster) pairs, near runs, batches, overflow flags,
+// far target-cluster evaluations, near target-source pairs, 0 (10 values; synchronises)
+int tree_stats(TreeSolver* t, int64_t* out10);
 
 }  // namespace lpm

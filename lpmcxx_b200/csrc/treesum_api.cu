@@ -135,7 +135,7 @@ extern "C" int lpm_tree_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, co
         e = cudaMemcpyAsync(dtgt, htgt, sizeof(double4) * (size_t)n_tgt, cudaMemcpyHostToDevice, ctx->stream);
     if (e != cudaSuccess) rc = cuda_status(e, "copy inputs");
     if (!rc && n_tgt > 0) rc = tree_velocity(ts, dsrc, n_src, dtgt, n_tgt, dout);
-    int64_t st[8] = {0};
+    int64_t st[10] = {0};
     if (!rc && n_tgt > 0 && n_src > 0) rc = tree_stats(ts, st);
     if (!rc && n_tgt > 0) {
         e = cudaMemcpyAsync(hout, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream);

@@ -94,15 +94,18 @@ def random_sphere(n, seed):
 @pytest.mark.parametrize("n_src,n_tgt", [(1, 1), (255, 257), (257, 1023), (1000, 1), (4099, 2050)])
 def test_dev_api_ragged_sizes(ctx, n_src, n_tgt):
     torch = on_torch_stream(ctx)
+    # sources and targets are prefixes of one quasi-uniform point set (like face sources and
+    # face-centroid targets): coincident at equal indices, well separated otherwise
     rng = np.random.default_rng(n_src * 7 + n_tgt)
-    src = oracle.pack4(random_sphere(n_src, 1 + n_src), rng.uniform(-1, 1, n_src) / max(n_src, 1))
-    tgt = oracle.pack4(random_sphere(n_tgt, 2 + n_tgt))
+    pts = random_sphere(max(n_src, n_tgt), 1 + n_src)
+    src = oracle.pack4(pts[:n_src], rng.uniform(-1, 1, n_src) / max(n_src, 1))
+    tgt = oracle.pack4(pts[:n_tgt])
     ref = oracle.bs_direct(src, tgt)
     ds = torch.tensor(src, device="cuda")
     dt = torch.tensor(tgt, device="cuda")
     for prec, tol in ((L.LPM_PREC_F64, F64_TOL), (L.LPM_PREC_F32, F32_TOL)):
         out = torch.full((3, n_tgt), float("nan"), dtype=torch.float64, device="cuda")
-        ctx.direct_sum_dev(BS, prec, ds, dt, out)
+        ctx.direct_sum_dev(BS, prec, ds, dt, out, n_coincident=min(n_src, n_tgt))
         got = out.cpu().numpy()
         assert np.isfinite(got).all()
         assert rel_l2(got, ref) < tol, (prec, rel_l2(got, ref))
