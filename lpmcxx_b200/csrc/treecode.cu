@@ -27,8 +27,8 @@
 //
 // Near field.  Targets are sorted by Morton key into batches of kBatch; a batch and a source node
 // interact in the far field when rho_node < theta (|x_batch - c| - r_batch), otherwise leaves interact
-// directly: FP32 pair arithmetic on coordinates relative to the leaf centre (so |x - y|^2 keeps its
-// relative accuracy for close pairs), FP64 accumulation per leaf.
+// directly: runs of consecutive leaves are contiguous ranges of tree-ordered sources, summed with FP32
+// pair arithmetic (|x - y|^2 form, as the FP32 direct sum) and FP64 accumulation across tiles.
 #include "treecode.h"
 
 #include "octree.h"
@@ -45,7 +45,6 @@ namespace {
 constexpr int kPMax = 12;        // highest supported Taylor order
 constexpr int kBatch = 128;      // targets per batch (threads per far/near block)
 constexpr int kTreeDepth = 10;   // key levels sorted for the treecode's source tree
-constexpr int kStack = 96;
 constexpr int kNearTile = 256;
 constexpr double kPi = 3.14159265358979323846264338327950288;
 
@@ -101,12 +100,12 @@ __global__ void gather_sources_kernel(const double4* __restrict__ X, const int32
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) out[q] = X[perm[q]];
 }
 
-// Leaves: centre (mean position), radius, relative FP32 source copies and ordinary moments
+// Leaves: centre (mean position), radius, FP32 source copies (w pre-scaled by 2) and ordinary moments
 // mom[a][b][c] = sum_j w_j h^(a,b,c) for a+b+c <= pm.
 __global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* __restrict__ src, int pm,
                                                        const int4* __restrict__ mono, int n_mono,
                                                        double4* __restrict__ node_ctr, double* __restrict__ node_wabs,
-                                                       double* __restrict__ node_mom, float4* __restrict__ src_rel) {
+                                                       double* __restrict__ node_mom, float4* __restrict__ src32) {
     __shared__ double sh[32];
     __shared__ double pw[32][3][kPMax + 1];
     __shared__ double ww[32];
@@ -128,7 +127,7 @@ __global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* 
             const double4 p = src[q];
             const double hx = p.x - cx, hy = p.y - cy, hz = p.z - cz;
             r = fmax(r, sqrt(hx * hx + hy * hy + hz * hz));
-            src_rel[q] = make_float4((float)hx, (float)hy, (float)hz, (float)(2.0 * p.w));
+            src32[q] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)(2.0 * p.w));
         }
         r = block_max(r, sh);
         if (threadIdx.x == 0) {
@@ -528,79 +527,87 @@ __global__ void __launch_bounds__(kBatch) far_kernel(const double4* __restrict__
 }
 
 // ---------------------------------------------------------------------------------- near field
-__device__ __forceinline__ void near_leaf(const Octree& t, int leaf, const double4& x,
-                                          const double4* __restrict__ node_ctr, const float4* __restrict__ src_rel,
-                                          float4* tile, double* D) {
-    const int node = t.leaf_node[leaf];
-    const int s = t.node_start[node], e = t.node_end[node];
-    const double4 c = node_ctr[node];
-    const float rx = (float)(x.x - c.x), ry = (float)(x.y - c.y), rz = (float)(x.z - c.z);
+constexpr int kNearThreads = 64;  // 2 targets per thread, kBatch targets per block
+
+// Sum over a contiguous range of tree-ordered sources (FP32 absolute coordinates, w pre-scaled by 2),
+// staged through shared memory: D += sum_j (2 w_j / |x - y_j|^2) (x - y_j), FP32 within a tile, FP64
+// across tiles.  A target's own source (d = 0) contributes 0 through the clamped denominator.
+__device__ __forceinline__ void near_range(int s, int e, const float4* __restrict__ src32, float4* tile, float tx0,
+                                           float ty0, float tz0, float tx1, float ty1, float tz1, double* D0,
+                                           double* D1) {
     for (int j0 = s; j0 < e; j0 += kNearTile) {
         const int m = min(kNearTile, e - j0);
         __syncthreads();
-        for (int j = threadIdx.x; j < m; j += kBatch) tile[j] = src_rel[j0 + j];
+        for (int j = threadIdx.x; j < m; j += kNearThreads) tile[j] = src32[j0 + j];
         __syncthreads();
-        float ax = 0.f, ay = 0.f, az = 0.f;
-#pragma unroll 8
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
+#pragma unroll 4
         for (int j = 0; j < m; ++j) {
             const float4 y = tile[j];
-            const float dx = rx - y.x, dy = ry - y.y, dz = rz - y.z;
-            const float rr = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1e-30f);  // self pair: d = 0
+            const float dx = tx0 - y.x, dy = ty0 - y.y, dz = tz0 - y.z;
+            const float rr = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1e-30f);
             const float f = y.w * rcp32(rr);
-            ax = fmaf(f, dx, ax);
-            ay = fmaf(f, dy, ay);
-            az = fmaf(f, dz, az);
+            a0 = fmaf(f, dx, a0);
+            a1 = fmaf(f, dy, a1);
+            a2 = fmaf(f, dz, a2);
+            const float ex = tx1 - y.x, ey = ty1 - y.y, ez = tz1 - y.z;
+            const float ss = fmaxf(fmaf(ez, ez, fmaf(ey, ey, ex * ex)), 1e-30f);
+            const float g = y.w * rcp32(ss);
+            b0 = fmaf(g, ex, b0);
+            b1 = fmaf(g, ey, b1);
+            b2 = fmaf(g, ez, b2);
         }
-        D[0] += ax;
-        D[1] += ay;
-        D[2] += az;
+        D0[0] += a0; D0[1] += a1; D0[2] += a2;
+        D1[0] += b0; D1[1] += b1; D1[2] += b2;
     }
 }
 
-__global__ void __launch_bounds__(kBatch) near_kernel(Octree t, const double4* __restrict__ tgt_sorted, int64_t n_tgt,
-                                                      const int32_t* __restrict__ tperm,
-                                                      const int32_t* __restrict__ near_off,
-                                                      const int32_t* __restrict__ near_cnt,
-                                                      const int2* __restrict__ near_list, int64_t near_cap,
-                                                      const int32_t* __restrict__ far_off,
-                                                      const int32_t* __restrict__ far_cnt,
-                                                      const int2* __restrict__ far_list, int64_t far_cap,
-                                                      const double4* __restrict__ node_ctr,
-                                                      const float4* __restrict__ src_rel, const double* __restrict__ V,
-                                                      double mult, double* __restrict__ U) {
+__device__ __forceinline__ void finish_target(int64_t q, int64_t n_tgt, const double4& x, const double* D,
+                                              const int32_t* __restrict__ tperm, const double* __restrict__ V,
+                                              double mult, double* __restrict__ U) {
+    if (q >= n_tgt) return;
+    const double v0 = V[q], v1 = V[n_tgt + q], v2 = V[2 * n_tgt + q];
+    const int64_t o = tperm[q];  // u = mult (V - x cross D)
+    U[o] = mult * (v0 - (x.y * D[2] - x.z * D[1]));
+    U[n_tgt + o] = mult * (v1 - (x.z * D[0] - x.x * D[2]));
+    U[2 * n_tgt + o] = mult * (v2 - (x.x * D[1] - x.y * D[0]));
+}
+
+__global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const double4* __restrict__ tgt_sorted,
+                                                            int64_t n_tgt, const int32_t* __restrict__ tperm,
+                                                            const int32_t* __restrict__ near_off,
+                                                            const int32_t* __restrict__ near_cnt,
+                                                            const int2* __restrict__ near_list, int64_t near_cap,
+                                                            const int32_t* __restrict__ far_off,
+                                                            const int32_t* __restrict__ far_cnt,
+                                                            const int2* __restrict__ far_list, int64_t far_cap,
+                                                            const float4* __restrict__ src32,
+                                                            const double* __restrict__ V, double mult,
+                                                            double* __restrict__ U) {
     __shared__ float4 tile[kNearTile];
     const int64_t b = blockIdx.x;
-    const int64_t q = b * kBatch + threadIdx.x;
-    const bool ok = q < n_tgt;
-    const double4 x = ok ? tgt_sorted[q] : make_double4(2, 2, 2, 0);
-    double D[3] = {0, 0, 0};
+    const int64_t q0 = b * kBatch + threadIdx.x, q1 = q0 + kNearThreads;
+    const double4 x0 = q0 < n_tgt ? tgt_sorted[q0] : make_double4(2, 2, 2, 0);
+    const double4 x1 = q1 < n_tgt ? tgt_sorted[q1] : make_double4(2, 2, 2, 0);
+    const float tx0 = (float)x0.x, ty0 = (float)x0.y, tz0 = (float)x0.z;
+    const float tx1 = (float)x1.x, ty1 = (float)x1.y, tz1 = (float)x1.z;
+    double D0[3] = {0, 0, 0}, D1[3] = {0, 0, 0};
+    // near entries are ranges of consecutive leaves: contiguous tree-ordered source ranges
     const int64_t n0 = near_off[b], n1 = min(n0 + (int64_t)near_cnt[b], near_cap);
     for (int64_t k = n0; k < n1; ++k) {
         const int2 r = near_list[k];
-        for (int leaf = r.x; leaf <= r.y; ++leaf) near_leaf(t, leaf, x, node_ctr, src_rel, tile, D);
+        const int s = t.node_start[t.leaf_node[r.x]], e = t.node_end[t.leaf_node[r.y]];
+        near_range(s, e, src32, tile, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
     }
     // clusters whose order was set to "direct"
     const int64_t f0 = far_off[b], f1 = min(f0 + (int64_t)far_cnt[b], far_cap);
     for (int64_t k = f0; k < f1; ++k) {
         const int2 ent = far_list[k];
         if (ent.y > 0) continue;
-        const int node = ent.x;
-        const int lo = t.leaf_flag[t.node_start[node]], hi = t.leaf_flag[t.node_end[node]] - 1;
-        for (int leaf = lo; leaf <= hi; ++leaf) near_leaf(t, leaf, x, node_ctr, src_rel, tile, D);
+        near_range(t.node_start[ent.x], t.node_end[ent.x], src32, tile, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
     }
-    if (ok) {
-        const double v0 = V[q], v1 = V[n_tgt + q], v2 = V[2 * n_tgt + q];
-        // u = mult (V - x cross D)
-        const int64_t o = tperm[q];
-        U[o] = mult * (v0 - (x.y * D[2] - x.z * D[1]));
-        U[n_tgt + o] = mult * (v1 - (x.z * D[0] - x.x * D[2]));
-        U[2 * n_tgt + o] = mult * (v2 - (x.x * D[1] - x.y * D[0]));
-    }
-}
-
-__global__ void zero_f64_kernel(double* p, int64_t n) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = 0.0;
+    finish_target(q0, n_tgt, x0, D0, tperm, V, mult, U);
+    finish_target(q1, n_tgt, x1, D1, tperm, V, mult, U);
 }
 
 // host-side tables --------------------------------------------------------------------------------
@@ -633,7 +640,7 @@ struct TreeSolver {
     double4* batch_ctr = nullptr;
     // sources and nodes
     double4* src_sorted = nullptr;
-    float4* src_rel = nullptr;
+    float4* src32 = nullptr;
     double4* node_ctr = nullptr;
     double* node_wabs = nullptr;
     double* node_mom = nullptr;
@@ -754,10 +761,10 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
         }
     }
     t->ct.table_off[kPMax + 1] = (int32_t)gtab.size();
-    // a cluster is cheaper to sum directly when its far-field work per target (4 FMAs per coefficient,
-    // FP64 counted double) exceeds ~11 FP32 operations per direct pair
+    // a cluster is cheaper to sum directly when its far-field work per target (8 flops per coefficient
+    // plus ~40 of setup, at FP64 or FP32 rate) exceeds ~17 flops per direct pair at the FP32 rate
     for (int P = 0; P <= kPMax; ++P)
-        t->ct.direct_below[P] = (int32_t)((P >= kF64From ? 8.0 : 4.0) * entries_for(P) / 11.0);
+        t->ct.direct_below[P] = (int32_t)((P >= kF64From ? 2.0 : 1.0) * (8.0 * entries_for(P) + 40.0) / 17.0);
     cudaError_t e = cudaSuccess;
     auto A = [&](cudaError_t r) {
         if (e == cudaSuccess) e = r;
@@ -771,7 +778,7 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->tgt_sorted, ntg));
     A(talloc(t, &t->batch_ctr, (size_t)t->n_batches));
     A(talloc(t, &t->src_sorted, ns));
-    A(talloc(t, &t->src_rel, ns));
+    A(talloc(t, &t->src32, ns));
     A(talloc(t, &t->node_ctr, nn));
     A(talloc(t, &t->node_wabs, nn));
     A(talloc(t, &t->node_mom, nn * cd * cd * cd));
@@ -888,7 +895,7 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
                t->src_sorted);
     const unsigned gl = (unsigned)std::max<int64_t>(1, std::min<int64_t>(t->st.node_cap, 16 * ctx->num_sms));
     LPM_LAUNCH(ctx, "leaf_p2m_kernel", leaf_p2m_kernel, gl, 128, 0, t->st, t->src_sorted, t->pm, t->mono, t->n_mono,
-               t->node_ctr, t->node_wabs, t->node_mom, t->src_rel);
+               t->node_ctr, t->node_wabs, t->node_mom, t->src32);
     for (int l = kTreeDepth - 1; l >= 0; --l)
         LPM_LAUNCH(ctx, "m2m_level_kernel", m2m_level_kernel, gl, 128, 0, t->st, l, t->pm, t->mono, t->n_mono,
                    t->node_ctr, t->node_wabs, t->node_mom);
@@ -910,9 +917,9 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     LPM_LAUNCH(ctx, "far_kernel", far_kernel, (unsigned)t->n_batches, kBatch, smem, t->tgt_sorted, n_tgt, t->far_off,
                t->far_cnt, t->far_list, t->far_cap, t->node_ctr, t->B64, t->B32, t->n_ent, t->gtab, t->ct, t->V);
     const double mult = -1.0 / (4.0 * kPi * t->kernel.radius);
-    LPM_LAUNCH(ctx, "near_kernel", near_kernel, (unsigned)t->n_batches, kBatch, 0, t->st, t->tgt_sorted, n_tgt,
+    LPM_LAUNCH(ctx, "near_kernel", near_kernel, (unsigned)t->n_batches, kNearThreads, 0, t->st, t->tgt_sorted, n_tgt,
                t->tperm, t->near_off, t->near_cnt, t->near_list, t->near_cap, t->far_off, t->far_cnt, t->far_list,
-               t->far_cap, t->node_ctr, t->src_rel, t->V, mult, U);
+               t->far_cap, t->src32, t->V, mult, U);
     if (can_sync) return tree_check(t);
     return LPM_OK;
 }
