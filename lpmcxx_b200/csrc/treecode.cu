@@ -45,7 +45,6 @@ namespace {
 constexpr int kPMax = 12;        // highest supported Taylor order
 constexpr int kBatch = 128;      // targets per batch (threads per far/near block)
 constexpr int kTreeDepth = 10;   // key levels sorted for the treecode's source tree
-constexpr int kNearTile = 256;
 constexpr double kPi = 3.14159265358979323846264338327950288;
 
 __host__ __device__ constexpr int tet(int q) { return q * (q + 1) * (q + 2) / 6; }  // #{k : |k| < q}
@@ -529,37 +528,33 @@ __global__ void __launch_bounds__(kBatch) far_kernel(const double4* __restrict__
 // ---------------------------------------------------------------------------------- near field
 constexpr int kNearThreads = 64;  // 2 targets per thread, kBatch targets per block
 
-// Sum over a contiguous range of tree-ordered sources (FP32 absolute coordinates, w pre-scaled by 2),
-// staged through shared memory: D += sum_j (2 w_j / |x - y_j|^2) (x - y_j), FP32 within a tile, FP64
-// across tiles.  A target's own source (d = 0) contributes 0 through the clamped denominator.
-__device__ __forceinline__ void near_range(int s, int e, const float4* __restrict__ src32, float4* tile, float tx0,
-                                           float ty0, float tz0, float tx1, float ty1, float tz1, double* D0,
-                                           double* D1) {
-    for (int j0 = s; j0 < e; j0 += kNearTile) {
-        const int m = min(kNearTile, e - j0);
-        __syncthreads();
-        for (int j = threadIdx.x; j < m; j += kNearThreads) tile[j] = src32[j0 + j];
-        __syncthreads();
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
+constexpr int kNearStreamTile = 512;  // sources staged per tile
+constexpr int kNearRuns = 128;        // source ranges resolved per chunk
+
+// One tile of the stream: m tree-ordered sources (FP32 absolute coordinates, w pre-scaled by 2)
+// against the thread's two targets: D += sum_j (2 w_j / |x - y_j|^2) (x - y_j), FP32 within the tile,
+// FP64 across tiles.  A target's own source (d = 0) contributes 0 through the clamped denominator.
+__device__ __forceinline__ void near_tile(const float4* tile, int m, float tx0, float ty0, float tz0, float tx1,
+                                          float ty1, float tz1, double* D0, double* D1) {
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
 #pragma unroll 4
-        for (int j = 0; j < m; ++j) {
-            const float4 y = tile[j];
-            const float dx = tx0 - y.x, dy = ty0 - y.y, dz = tz0 - y.z;
-            const float rr = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1e-30f);
-            const float f = y.w * rcp32(rr);
-            a0 = fmaf(f, dx, a0);
-            a1 = fmaf(f, dy, a1);
-            a2 = fmaf(f, dz, a2);
-            const float ex = tx1 - y.x, ey = ty1 - y.y, ez = tz1 - y.z;
-            const float ss = fmaxf(fmaf(ez, ez, fmaf(ey, ey, ex * ex)), 1e-30f);
-            const float g = y.w * rcp32(ss);
-            b0 = fmaf(g, ex, b0);
-            b1 = fmaf(g, ey, b1);
-            b2 = fmaf(g, ez, b2);
-        }
-        D0[0] += a0; D0[1] += a1; D0[2] += a2;
-        D1[0] += b0; D1[1] += b1; D1[2] += b2;
+    for (int j = 0; j < m; ++j) {
+        const float4 y = tile[j];
+        const float dx = tx0 - y.x, dy = ty0 - y.y, dz = tz0 - y.z;
+        const float rr = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1e-30f);
+        const float f = y.w * rcp32(rr);
+        a0 = fmaf(f, dx, a0);
+        a1 = fmaf(f, dy, a1);
+        a2 = fmaf(f, dz, a2);
+        const float ex = tx1 - y.x, ey = ty1 - y.y, ez = tz1 - y.z;
+        const float ss = fmaxf(fmaf(ez, ez, fmaf(ey, ey, ex * ex)), 1e-30f);
+        const float g = y.w * rcp32(ss);
+        b0 = fmaf(g, ex, b0);
+        b1 = fmaf(g, ey, b1);
+        b2 = fmaf(g, ez, b2);
     }
+    D0[0] += a0; D0[1] += a1; D0[2] += a2;
+    D1[0] += b0; D1[1] += b1; D1[2] += b2;
 }
 
 __device__ __forceinline__ void finish_target(int64_t q, int64_t n_tgt, const double4& x, const double* D,
@@ -573,6 +568,9 @@ __device__ __forceinline__ void finish_target(int64_t q, int64_t n_tgt, const do
     U[2 * n_tgt + o] = mult * (v2 - (x.x * D[1] - x.y * D[0]));
 }
 
+// A batch's near work is the concatenation of its source ranges (runs of consecutive leaves, then
+// clusters whose order was set to "direct"); it is streamed through shared memory in tiles of
+// kNearStreamTile sources regardless of how short the individual ranges are.
 __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const double4* __restrict__ tgt_sorted,
                                                             int64_t n_tgt, const int32_t* __restrict__ tperm,
                                                             const int32_t* __restrict__ near_off,
@@ -584,7 +582,8 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
                                                             const float4* __restrict__ src32,
                                                             const double* __restrict__ V, double mult,
                                                             double* __restrict__ U) {
-    __shared__ float4 tile[kNearTile];
+    __shared__ float4 tile[kNearStreamTile];
+    __shared__ int r_start[kNearRuns], r_pre[kNearRuns + 1];
     const int64_t b = blockIdx.x;
     const int64_t q0 = b * kBatch + threadIdx.x, q1 = q0 + kNearThreads;
     const double4 x0 = q0 < n_tgt ? tgt_sorted[q0] : make_double4(2, 2, 2, 0);
@@ -592,19 +591,67 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
     const float tx0 = (float)x0.x, ty0 = (float)x0.y, tz0 = (float)x0.z;
     const float tx1 = (float)x1.x, ty1 = (float)x1.y, tz1 = (float)x1.z;
     double D0[3] = {0, 0, 0}, D1[3] = {0, 0, 0};
-    // near entries are ranges of consecutive leaves: contiguous tree-ordered source ranges
     const int64_t n0 = near_off[b], n1 = min(n0 + (int64_t)near_cnt[b], near_cap);
-    for (int64_t k = n0; k < n1; ++k) {
-        const int2 r = near_list[k];
-        const int s = t.node_start[t.leaf_node[r.x]], e = t.node_end[t.leaf_node[r.y]];
-        near_range(s, e, src32, tile, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
-    }
-    // clusters whose order was set to "direct"
     const int64_t f0 = far_off[b], f1 = min(f0 + (int64_t)far_cnt[b], far_cap);
-    for (int64_t k = f0; k < f1; ++k) {
-        const int2 ent = far_list[k];
-        if (ent.y > 0) continue;
-        near_range(t.node_start[ent.x], t.node_end[ent.x], src32, tile, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
+    const int64_t n_near = n1 - n0, n_all = n_near + (f1 - f0);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t c0 = 0; c0 < n_all; c0 += kNearRuns) {
+        // resolve up to kNearRuns entries into source ranges and their prefix offsets
+        int len[2], st[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t k = c0 + threadIdx.x * 2 + h;
+            len[h] = 0;
+            st[h] = 0;
+            if (k < n_all) {
+                if (k < n_near) {
+                    const int2 r = near_list[n0 + k];
+                    st[h] = t.node_start[t.leaf_node[r.x]];
+                    len[h] = t.node_end[t.leaf_node[r.y]] - st[h];
+                } else {
+                    const int2 ent = far_list[f0 + (k - n_near)];
+                    if (ent.y <= 0) {
+                        st[h] = t.node_start[ent.x];
+                        len[h] = t.node_end[ent.x] - st[h];
+                    }
+                }
+            }
+        }
+        // exclusive scan of the 2 x 64 lengths (two warps)
+        int v = len[0] + len[1];
+        int incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        __syncthreads();  // previous chunk's readers of r_pre / r_start / tile are done
+        __shared__ int warp_tot[2];
+        if (lane == 31) warp_tot[w] = incl;
+        __syncthreads();
+        const int base = (w ? warp_tot[0] : 0) + incl - v;
+        r_pre[threadIdx.x * 2] = base;
+        r_pre[threadIdx.x * 2 + 1] = base + len[0];
+        r_start[threadIdx.x * 2] = st[0];
+        r_start[threadIdx.x * 2 + 1] = st[1];
+        const int total = warp_tot[0] + warp_tot[1];
+        if (threadIdx.x == 0) r_pre[kNearRuns] = total;
+        __syncthreads();
+        for (int p0 = 0; p0 < total; p0 += kNearStreamTile) {
+            const int m = min(kNearStreamTile, total - p0);
+            if (p0 > 0) __syncthreads();
+            for (int j = threadIdx.x; j < m; j += kNearThreads) {
+                const int p = p0 + j;
+                int lo = 0, hi = kNearRuns;  // last run r with r_pre[r] <= p
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (r_pre[mid] <= p) lo = mid;
+                    else hi = mid;
+                }
+                tile[j] = src32[r_start[lo] + (p - r_pre[lo])];
+            }
+            __syncthreads();
+            near_tile(tile, m, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
+        }
     }
     finish_target(q0, n_tgt, x0, D0, tperm, V, mult, U);
     finish_target(q1, n_tgt, x1, D1, tperm, V, mult, U);
