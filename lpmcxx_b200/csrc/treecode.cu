@@ -276,19 +276,46 @@ __global__ void coeff_kernel(Octree t, int pm, const int4* __restrict__ ent, int
     }
 }
 
-// Target batches: gather targets in Morton order, batch centre and radius.
+// Target batches.  Targets sorted by Morton key are cut into batches of at most kBatch consecutive
+// targets that also share one octree cell of level `level` (cells of edge 2/2^level): consecutive
+// Morton positions can be far apart across a cell boundary, and a batch's radius decides how many
+// clusters it can accept.  bflag[q] = 1 where a batch starts; one thread per cell walks its cell.
+__global__ void batch_flags_kernel(const uint64_t* __restrict__ keys, int64_t n, int shift, int32_t* __restrict__ bflag) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t cell = keys[q] >> shift;
+        if (q > 0 && (keys[q - 1] >> shift) == cell) continue;
+        for (int64_t j = q; j < n && (j == q || (keys[j] >> shift) == cell); ++j) bflag[j] = ((j - q) % kBatch) == 0;
+    }
+}
+
+// batch_first[b] = first sorted target of batch b (b < n_batches), batch_first[n_batches] = n; the number
+// of batches goes to *nbat.  bscan is the exclusive scan of bflag over n + 1 entries.
+__global__ void batch_first_kernel(const int32_t* __restrict__ bscan, int64_t n, int32_t* __restrict__ batch_first,
+                                   int32_t* __restrict__ nbat, int64_t cap) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q <= n; q += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t b = bscan[q];
+        const bool start = q == n || bscan[q + 1] != b;
+        if (start && b <= cap) batch_first[b] = (int32_t)q;
+        if (q == n) *nbat = b;
+    }
+}
+
+// Per batch: gather its targets into tgt_sorted, centre (mean) and radius.
 __global__ void __launch_bounds__(kBatch) batch_kernel(const double4* __restrict__ X, const int32_t* __restrict__ tperm,
-                                                       int64_t n_tgt, double4* __restrict__ tgt_sorted,
+                                                       const int32_t* __restrict__ batch_first,
+                                                       const int32_t* __restrict__ nbat, double4* __restrict__ tgt_sorted,
                                                        double4* __restrict__ batch_ctr) {
     __shared__ double sh[32];
-    const int64_t q = (int64_t)blockIdx.x * kBatch + threadIdx.x;
+    if ((int)blockIdx.x >= *nbat) return;  // uniform per block
+    const int64_t q0 = batch_first[blockIdx.x], q1 = batch_first[blockIdx.x + 1];
+    const int64_t q = q0 + threadIdx.x;
     double4 p = make_double4(0, 0, 0, 0);
-    const bool ok = q < n_tgt;
+    const bool ok = q < q1;
     if (ok) {
         p = X[tperm[q]];
         tgt_sorted[q] = p;
     }
-    const int cnt = (int)min((int64_t)kBatch, n_tgt - (int64_t)blockIdx.x * kBatch);
+    const int cnt = (int)(q1 - q0);
     const double cx = block_sum(ok ? p.x : 0.0, sh) / cnt, cy = block_sum(ok ? p.y : 0.0, sh) / cnt,
                  cz = block_sum(ok ? p.z : 0.0, sh) / cnt;
     double r = 0;
@@ -301,7 +328,9 @@ struct TraverseArgs {
     Octree t;
     const double4* node_ctr;
     const double4* batch_ctr;
-    int64_t n_batches, n_tgt;
+    const int32_t* batch_first;
+    const int32_t* nbat;
+    int64_t n_batches;  // capacity (launch size); *nbat batches exist
     double theta;
     int order;
     int direct_below;
@@ -331,7 +360,7 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
     const Octree& t = A.t;
     const unsigned full = 0xffffffffu, lt = (1u << lane) - 1u;
     int* st = sstack[w];
-    if (t.counters[1] == 0 || t.counters[0] == 0) {
+    if (t.counters[1] == 0 || t.counters[0] == 0 || b >= *A.nbat) {
         if (!A.fill && lane == 0) {
             A.far_cnt[b] = 0;
             A.near_cnt[b] = 0;
@@ -339,7 +368,7 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
         return;
     }
     const double4 bc = A.batch_ctr[b];
-    const unsigned long long nb = (unsigned long long)min((int64_t)kBatch, A.n_tgt - b * kBatch);
+    const unsigned long long nb = (unsigned long long)(A.batch_first[b + 1] - A.batch_first[b]);
     int size = 1;
     if (lane == 0) st[0] = 0;
     __syncwarp();
@@ -480,43 +509,72 @@ __device__ void far_dispatch(int P, const T4* Bc, const double4& x, const double
 
 constexpr int kF64From = 8;  // orders >= this evaluate in FP64
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit_wait() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Issue the asynchronous gather of one far entry's coefficients (order-P Horner sequence) into buf.
+__device__ __forceinline__ void far_gather(int2 ent, const double4* __restrict__ B64, const float4* __restrict__ B32,
+                                           int n_ent, const int32_t* __restrict__ gtab, const CutoffTable& ct,
+                                           double4* buf) {
+    const int P = ent.y;
+    if (P <= 0) return;
+    const int nterm = ct.table_off[P + 1] - ct.table_off[P];
+    const int32_t* tab = gtab + ct.table_off[P];
+    if (P >= kF64From) {
+        const double4* src = B64 + (size_t)ent.x * n_ent;
+        for (int i = threadIdx.x; i < 2 * nterm; i += kBatch) {
+            const double4* g = src + tab[i >> 1];
+            cp_async16((char*)(buf + (i >> 1)) + 16 * (i & 1), (const char*)g + 16 * (i & 1));
+        }
+    } else {
+        float4* s32 = (float4*)buf;
+        const float4* src = B32 + (size_t)ent.x * n_ent;
+        for (int i = threadIdx.x; i < nterm; i += kBatch) cp_async16(s32 + i, src + tab[i]);
+    }
+}
+
+// One block per target batch; each thread owns one target and sweeps the batch's far list.  The next
+// entry's coefficients are gathered into the other half of a double buffer (cp.async) while the
+// current one is evaluated.
 __global__ void __launch_bounds__(kBatch) far_kernel(const double4* __restrict__ tgt_sorted, int64_t n_tgt,
+                                                     const int32_t* __restrict__ batch_first,
+                                                     const int32_t* __restrict__ nbat,
                                                      const int32_t* __restrict__ far_off,
                                                      const int32_t* __restrict__ far_cnt,
                                                      const int2* __restrict__ far_list, int64_t far_cap,
                                                      const double4* __restrict__ node_ctr,
                                                      const double4* __restrict__ B64, const float4* __restrict__ B32,
                                                      int n_ent, const int32_t* __restrict__ gtab, CutoffTable ct,
-                                                     double* __restrict__ V) {
+                                                     int buf_terms, double* __restrict__ V) {
     extern __shared__ double4 sbuf[];
     const int64_t b = blockIdx.x;
-    const int64_t q = b * kBatch + threadIdx.x;
-    const bool ok = q < n_tgt;
+    if (b >= *nbat) return;  // uniform per block
+    const int64_t q = batch_first[b] + threadIdx.x;
+    const bool ok = q < batch_first[b + 1];
     const double4 x = ok ? tgt_sorted[q] : make_double4(0, 0, 0, 0);
     double acc[3] = {0, 0, 0};
     const int64_t f0 = far_off[b];
     const int64_t f1 = min(f0 + (int64_t)far_cnt[b], far_cap);
+    if (f0 < f1) far_gather(far_list[f0], B64, B32, n_ent, gtab, ct, sbuf);
     for (int64_t f = f0; f < f1; ++f) {
+        cp_async_commit_wait();
+        __syncthreads();  // entry f is in buffer (f - f0) & 1; the other buffer is free
         const int2 ent = far_list[f];
+        if (f + 1 < f1)
+            far_gather(far_list[f + 1], B64, B32, n_ent, gtab, ct, sbuf + (size_t)((f + 1 - f0) & 1) * buf_terms);
         const int P = ent.y;
         if (P <= 0) continue;  // summed directly by the near kernel
-        const int nterm = ct.table_off[P + 1] - ct.table_off[P];
-        const int32_t* tab = gtab + ct.table_off[P];
-        __syncthreads();
-        if (P >= kF64From) {
-            const double4* src = B64 + (size_t)ent.x * n_ent;
-            for (int i = threadIdx.x; i < nterm; i += kBatch) sbuf[i] = src[tab[i]];
-        } else {
-            float4* s32 = (float4*)sbuf;
-            const float4* src = B32 + (size_t)ent.x * n_ent;
-            for (int i = threadIdx.x; i < nterm; i += kBatch) s32[i] = src[tab[i]];
-        }
-        __syncthreads();
+        const double4* cur = sbuf + (size_t)((f - f0) & 1) * buf_terms;
         const double4 c = node_ctr[ent.x];
         if (P >= kF64From)
-            far_dispatch<double, double4>(P, sbuf, x, c, acc);
+            far_dispatch<double, double4>(P, cur, x, c, acc);
         else
-            far_dispatch<float, float4>(P, (const float4*)sbuf, x, c, acc);
+            far_dispatch<float, float4>(P, (const float4*)cur, x, c, acc);
     }
     if (ok) {
         V[q] = acc[0];
@@ -557,10 +615,10 @@ __device__ __forceinline__ void near_tile(const float4* tile, int m, float tx0, 
     D1[0] += b0; D1[1] += b1; D1[2] += b2;
 }
 
-__device__ __forceinline__ void finish_target(int64_t q, int64_t n_tgt, const double4& x, const double* D,
-                                              const int32_t* __restrict__ tperm, const double* __restrict__ V,
-                                              double mult, double* __restrict__ U) {
-    if (q >= n_tgt) return;
+__device__ __forceinline__ void finish_target(int64_t q, int64_t qe, int64_t n_tgt, const double4& x,
+                                              const double* D, const int32_t* __restrict__ tperm,
+                                              const double* __restrict__ V, double mult, double* __restrict__ U) {
+    if (q >= qe) return;
     const double v0 = V[q], v1 = V[n_tgt + q], v2 = V[2 * n_tgt + q];
     const int64_t o = tperm[q];  // u = mult (V - x cross D)
     U[o] = mult * (v0 - (x.y * D[2] - x.z * D[1]));
@@ -573,6 +631,8 @@ __device__ __forceinline__ void finish_target(int64_t q, int64_t n_tgt, const do
 // kNearStreamTile sources regardless of how short the individual ranges are.
 __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const double4* __restrict__ tgt_sorted,
                                                             int64_t n_tgt, const int32_t* __restrict__ tperm,
+                                                            const int32_t* __restrict__ batch_first,
+                                                            const int32_t* __restrict__ nbat,
                                                             const int32_t* __restrict__ near_off,
                                                             const int32_t* __restrict__ near_cnt,
                                                             const int2* __restrict__ near_list, int64_t near_cap,
@@ -585,9 +645,11 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
     __shared__ float4 tile[kNearStreamTile];
     __shared__ int r_start[kNearRuns], r_pre[kNearRuns + 1];
     const int64_t b = blockIdx.x;
-    const int64_t q0 = b * kBatch + threadIdx.x, q1 = q0 + kNearThreads;
-    const double4 x0 = q0 < n_tgt ? tgt_sorted[q0] : make_double4(2, 2, 2, 0);
-    const double4 x1 = q1 < n_tgt ? tgt_sorted[q1] : make_double4(2, 2, 2, 0);
+    if (b >= *nbat) return;  // uniform per block
+    const int64_t qe = batch_first[b + 1];
+    const int64_t q0 = batch_first[b] + threadIdx.x, q1 = q0 + kNearThreads;
+    const double4 x0 = q0 < qe ? tgt_sorted[q0] : make_double4(2, 2, 2, 0);
+    const double4 x1 = q1 < qe ? tgt_sorted[q1] : make_double4(2, 2, 2, 0);
     const float tx0 = (float)x0.x, ty0 = (float)x0.y, tz0 = (float)x0.z;
     const float tx1 = (float)x1.x, ty1 = (float)x1.y, tz1 = (float)x1.z;
     double D0[3] = {0, 0, 0}, D1[3] = {0, 0, 0};
@@ -653,8 +715,8 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
             near_tile(tile, m, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
         }
     }
-    finish_target(q0, n_tgt, x0, D0, tperm, V, mult, U);
-    finish_target(q1, n_tgt, x1, D1, tperm, V, mult, U);
+    finish_target(q0, qe, n_tgt, x0, D0, tperm, V, mult, U);
+    finish_target(q1, qe, n_tgt, x1, D1, tperm, V, mult, U);
 }
 
 // host-side tables --------------------------------------------------------------------------------
@@ -674,7 +736,11 @@ struct TreeSolver {
     lpm_ctx* ctx = nullptr;
     lpm_kernel_desc kernel{};
     lpm_solver_desc solver{};
-    int64_t n_src = 0, n_tgt = 0, n_batches = 0;
+    int64_t n_src = 0, n_tgt = 0;
+    int64_t n_batches = 0;  // capacity: launch size of the per-batch kernels
+    int batch_level = 1;    // octree level whose cells batches may not straddle
+    int32_t* bflag = nullptr;
+    int32_t* batch_first = nullptr;
     int pm = 8;
     Octree st;
     // target ordering
@@ -775,7 +841,14 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     t->n_src = n_src;
     t->n_tgt = n_tgt;
     t->pm = solver.order_policy == LPM_ORDER_LEARNED ? kPMax : solver.order;
-    t->n_batches = (n_tgt + kBatch - 1) / kBatch;
+    // about 4.7 * 4^L cells of level L meet the unit sphere: pick L so a cell holds ~kBatch targets
+    {
+        int L = 1;
+        while (L < kTreeDepth && 4.7 * std::pow(4.0, L + 1) * kBatch <= 1.5 * (double)n_tgt) ++L;
+        t->batch_level = L;
+        const int64_t cells = std::min<int64_t>(std::max<int64_t>(n_tgt, 1), (int64_t)(8.0 * std::pow(4.0, L)) + 64);
+        t->n_batches = (n_tgt + kBatch - 1) / kBatch + cells;
+    }
     rc = octree_alloc(t->st, std::max<int64_t>(n_src, 1), solver.max_per_leaf, kTreeDepth);
     if (rc) {
         delete t;
@@ -824,6 +897,8 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->tcount, 4));
     A(talloc(t, &t->tgt_sorted, ntg));
     A(talloc(t, &t->batch_ctr, (size_t)t->n_batches));
+    A(talloc(t, &t->bflag, ntg + 1));
+    A(talloc(t, &t->batch_first, (size_t)t->n_batches + 1));
     A(talloc(t, &t->src_sorted, ns));
     A(talloc(t, &t->src32, ns));
     A(talloc(t, &t->node_ctr, nn));
@@ -853,6 +928,16 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
         tree_solver_destroy(t);
         return cuda_status(e, "tree solver allocation");
     }
+    {
+        const size_t smem = 2 * (size_t)entries_for(t->pm) * sizeof(double4);
+        if (smem > 48 * 1024) {
+            cudaError_t ea = cudaFuncSetAttribute(far_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (ea != cudaSuccess) {
+                tree_solver_destroy(t);
+                return cuda_status(ea, "cudaFuncSetAttribute (far_kernel)");
+            }
+        }
+    }
     rc = alloc_lists(t, std::max<int64_t>(t->n_batches * 256, 1024), std::max<int64_t>(t->n_batches * 64, 1024));
     if (rc) {
         tree_solver_destroy(t);
@@ -875,8 +960,9 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     A.t = t->st;
     A.node_ctr = t->node_ctr;
     A.batch_ctr = t->batch_ctr;
+    A.batch_first = t->batch_first;
+    A.nbat = t->tcount + 1;
     A.n_batches = t->n_batches;
-    A.n_tgt = t->n_tgt;
     A.theta = t->solver.theta;
     A.order = t->solver.order;
     A.direct_below = t->ct.direct_below[t->solver.order];
@@ -948,37 +1034,50 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
                    t->node_ctr, t->node_wabs, t->node_mom);
     LPM_LAUNCH(ctx, "coeff_kernel", coeff_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->node_mom, t->B64,
                t->B32);
-    // targets in Morton order, batches of kBatch
+    // targets in Morton order, cut into compact batches of at most kBatch
     LPM_CUDA_TRY(cudaMemsetAsync(t->tcount, 0, 4 * sizeof(int32_t), ctx->stream));
     rc = morton_keys(ctx, X, n_tgt, rb, t->tkeys, t->tperm, t->tcount);
     if (rc) return rc;
     rc = radix_sort_u64(ctx, t->tkeys, t->tperm, t->ttmpk, t->ttmpv, n_tgt, 32);
     if (rc) return rc;
-    LPM_LAUNCH(ctx, "batch_kernel", batch_kernel, (unsigned)t->n_batches, kBatch, 0, X, t->tperm, n_tgt,
-               t->tgt_sorted, t->batch_ctr);
+    const unsigned gt = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(n_tgt + 1, 256), 8 * ctx->num_sms));
+    LPM_CUDA_TRY(cudaMemsetAsync(t->bflag + n_tgt, 0, sizeof(int32_t), ctx->stream));
+    LPM_LAUNCH(ctx, "batch_flags_kernel", batch_flags_kernel, gt, 256, 0, t->tkeys, n_tgt,
+               3 * (kKeyLevels - t->batch_level), t->bflag);
+    rc = scan_exclusive_i32(ctx, t->bflag, t->bflag, n_tgt + 1, nullptr);
+    if (rc) return rc;
+    LPM_LAUNCH(ctx, "batch_first_kernel", batch_first_kernel, gt, 256, 0, t->bflag, n_tgt, t->batch_first,
+               t->tcount + 1, t->n_batches);
+    LPM_LAUNCH(ctx, "batch_kernel", batch_kernel, (unsigned)t->n_batches, kBatch, 0, X, t->tperm, t->batch_first,
+               t->tcount + 1, t->tgt_sorted, t->batch_ctr);
     rc = build_lists(t, can_sync);
     if (rc) return rc;
-    const size_t smem = (size_t)entries_for(t->pm) * sizeof(double4);
-    if (smem > 48 * 1024) LPM_CUDA_TRY(cudaFuncSetAttribute(far_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                            (int)smem));
-    LPM_LAUNCH(ctx, "far_kernel", far_kernel, (unsigned)t->n_batches, kBatch, smem, t->tgt_sorted, n_tgt, t->far_off,
-               t->far_cnt, t->far_list, t->far_cap, t->node_ctr, t->B64, t->B32, t->n_ent, t->gtab, t->ct, t->V);
+    const int buf_terms = entries_for(t->pm);
+    const size_t smem = 2 * (size_t)buf_terms * sizeof(double4);  // attribute raised at creation
+    LPM_LAUNCH(ctx, "far_kernel", far_kernel, (unsigned)t->n_batches, kBatch, smem, t->tgt_sorted, n_tgt,
+               t->batch_first, t->tcount + 1, t->far_off, t->far_cnt, t->far_list, t->far_cap, t->node_ctr, t->B64,
+               t->B32, t->n_ent, t->gtab, t->ct, buf_terms, t->V);
     const double mult = -1.0 / (4.0 * kPi * t->kernel.radius);
     LPM_LAUNCH(ctx, "near_kernel", near_kernel, (unsigned)t->n_batches, kNearThreads, 0, t->st, t->tgt_sorted, n_tgt,
-               t->tperm, t->near_off, t->near_cnt, t->near_list, t->near_cap, t->far_off, t->far_cnt, t->far_list,
-               t->far_cap, t->src32, t->V, mult, U);
+               t->tperm, t->batch_first, t->tcount + 1, t->near_off, t->near_cnt, t->near_list, t->near_cap,
+               t->far_off, t->far_cnt, t->far_list, t->far_cap, t->src32, t->V, mult, U);
     if (can_sync) return tree_check(t);
     return LPM_OK;
 }
 
 int tree_check(TreeSolver* t) {
-    int32_t f[8], c[8];
+    int32_t f[8], c[8], tc[4];
     lpm_ctx* ctx = t->ctx;
     LPM_CUDA_TRY(cudaMemcpyAsync(f, t->flags, sizeof(f), cudaMemcpyDeviceToHost, ctx->stream));
     LPM_CUDA_TRY(cudaMemcpyAsync(c, t->st.counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+    LPM_CUDA_TRY(cudaMemcpyAsync(tc, t->tcount, sizeof(tc), cudaMemcpyDeviceToHost, ctx->stream));
     LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (f[0]) {
         set_error("tree solver: interaction list capacity exceeded (flags %d)", f[0]);
+        return LPM_ERR_CAPACITY;
+    }
+    if (tc[1] > t->n_batches) {
+        set_error("tree solver: %d target batches exceed the capacity of %lld", tc[1], (long long)t->n_batches);
         return LPM_ERR_CAPACITY;
     }
     if (c[2] & 2) {
@@ -1006,7 +1105,9 @@ int tree_stats(TreeSolver* t, int64_t* out8) {
     out8[2] = c[4];   // depth
     out8[3] = f[2];   // far (batch, cluster) pairs
     out8[4] = f[3];   // near runs
-    out8[5] = t->n_batches;
+    int32_t tc[4];
+    LPM_CUDA_TRY(cudaMemcpy(tc, t->tcount, sizeof(tc), cudaMemcpyDeviceToHost));
+    out8[5] = tc[1];  // target batches
     out8[6] = f[0];
     out8[7] = (int64_t)pc[0];  // far-field target-cluster evaluations
     out8[8] = (int64_t)pc[1];  // near-field target-source pairs
