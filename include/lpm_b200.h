@@ -106,6 +106,19 @@ int lpm_mesh_build(int kind, int level, double radius, double* vert_xyz, double*
 int lpm_direct_sum_dev(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precision, const double* src, int64_t n_src,
                        const double* tgt, int64_t n_tgt, int64_t n_coincident, double* out);
 
+/* Allocation-free variant of lpm_direct_sum_dev at LPM_PREC_F32 (no counterpart in the reference, which
+ * has no GPU path).  For callers that cannot allocate device memory while they run: code inside a CUDA
+ * graph being captured, hosts that reserve the whole device for their own pool, real-time loops that may
+ * not block in the allocator.  Arguments as lpm_direct_sum_dev, device pointers, enqueued on cuda_stream
+ * (NULL = legacy default stream) of the current device; no context.  The FP32 copies live in one
+ * file-scope device array of 524,288 points (8 MiB, held by every GPU that loads the library): n_src +
+ * n_tgt above that returns LPM_ERR_CAPACITY.  Calls never call cudaMalloc / cudaFree.  The first call on a
+ * device looks the array up once (cudaGetSymbolAddress) and should therefore come before any stream
+ * capture.  All calls on a device share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+int lpm_direct_sum_f32_noalloc(const lpm_kernel_desc* kernel, const double* src, int64_t n_src, const double* tgt,
+                               int64_t n_tgt, int64_t n_coincident, double* out, void* cuda_stream);
+
 /* Host-facing mesh direct sum with the reference's data: DirectSum::meshSolve
  * (src/LpmDirectSum.cpp:25-167).  Vertex coordinates vx/vy/vz (n_verts), face centroids fx/fy/fz,
  * face areas, divided-face mask and the face source field (n_faces) are host arrays.  Targets are

@@ -70,6 +70,7 @@ SIGNATURES = {
     "lpm_mesh_counts": (C.c_int, [C.c_int, C.c_int, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
     "lpm_mesh_build": (C.c_int, [C.c_int, C.c_int, D, P, P, P, P]),
     "lpm_direct_sum_dev": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, P, I64, P, I64, I64, P]),
+    "lpm_direct_sum_f32_noalloc": (C.c_int, [C.POINTER(KernelDesc), P, I64, P, I64, I64, P, P]),
     "lpm_direct_sum_mesh": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, I64, P, P, P, I64, P, P, P, P, P, P,
                                       I64, I64, I64, I64, P, P, P, P, P, P]),
     "lpm_direct_sum_meshfree": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, I64, P, P, P, P, P, I64, I64, P]),
