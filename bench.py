@@ -41,6 +41,11 @@ DT = 0.005
 METRIC = "Biot-Savart RK4 steps/s @1.3M pts: FP32 learned tree vs FP64 direct @relL2≤1e-6"
 WORKLOAD = ("icos L8 Gaussian vortex: 1,310,720 face-centroid sources + 655,362 vertices "
             "(1,966,082 targets), RK4 dt=0.005")
+
+
+def workload_name(level: int, n_src: int, n_tgt: int, dt: float) -> str:
+    return (f"icos L{level} Gaussian vortex: {n_src:,} face-centroid sources + {n_tgt - n_src:,} vertices "
+            f"({n_tgt:,} targets), RK4 dt={dt:g}")
 FLOPS_PER_BS_PAIR = 17
 
 
@@ -359,7 +364,8 @@ def run_gpu(args) -> None:
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32" if head != "direct_f64" else "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "solver": head, "n_sources": n_src, "n_targets": n, "dt": args.dt,
+        "config": {"workload": workload_name(args.level, n_src, n, args.dt), "solver": head, "n_sources": n_src,
+                   "n_targets": n, "dt": args.dt,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "flushed (256 MiB write) before every timed step, outside the timed events",
                    "graph": "one CUDA graph replay per RK4 step"},
