@@ -194,6 +194,12 @@ int lpm_treesum_eval_dev(lpm_treesum* ts, const double* src, const double* tgt, 
  * leaf ranges, target batches, overflow flags, far-field (target, cluster) evaluations, near-field
  * (target, source) pairs, 0.  Synchronises. */
 int lpm_treesum_stats(lpm_treesum* ts, int64_t* out10);
+/* Run-time parameters of a tree solver (no reference counterpart: the reference fixes them at
+ * construction).  "theta": acceptance criterion, 0 < theta < 1; "f64_from": far expansions of this
+ * order and above evaluate in FP64 (1..13; default 13 = all FP32 for LPM_PREC_F32 solvers, 1 for
+ * LPM_PREC_F64); "batch_level": octree level whose cells a target batch may not straddle (1 .. the
+ * level chosen at creation; coarser levels give fuller batches).  Takes effect at the next evaluation. */
+int lpm_treesum_set_param(lpm_treesum* ts, const char* name, double value);
 /* Host-facing TreeSum::meshSolve (src/LpmTreeSum.cpp:55-86) with the same data as lpm_direct_sum_mesh;
  * mac_count (may be NULL) receives the number of accepted far-field (batch, cluster) pairs, the
  * counterpart of the reference's macCounter. */
@@ -227,6 +233,8 @@ int lpm_rk4_step(lpm_rk4* rk, double dt, int nsteps, int use_graph);
 int lpm_rk4_velocity_dev(lpm_rk4* rk, double* out);
 /* Treecode statistics of the last velocity evaluation (the 10 values of lpm_treesum_stats). */
 int lpm_rk4_tree_stats(lpm_rk4* rk, int64_t* out10);
+/* lpm_treesum_set_param for the integrator's treecode; drops a captured step graph (synchronises). */
+int lpm_rk4_set_param(lpm_rk4* rk, const char* name, double value);
 
 #ifdef __cplusplus
 }

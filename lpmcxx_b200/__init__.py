@@ -230,6 +230,9 @@ class RK4:
         check(lib().lpm_rk4_tree_stats(self.h, ptr(o)), "lpm_rk4_tree_stats")
         return dict(zip(TreeSum.STAT_KEYS, (int(v) for v in o)))
 
+    def set_param(self, name: str, value: float) -> None:
+        check(lib().lpm_rk4_set_param(self.h, name.encode(), float(value)), "lpm_rk4_set_param")
+
 
 class Tree:
     """Device octree (lpm_tree) over a (n, 4) float64 CUDA tensor of points."""
@@ -308,6 +311,10 @@ class TreeSum:
         o = np.zeros(10, np.int64)
         check(lib().lpm_treesum_stats(self.h, ptr(o)), "lpm_treesum_stats")
         return dict(zip(self.STAT_KEYS, (int(v) for v in o)))
+
+    def set_param(self, name: str, value: float) -> None:
+        """Run-time parameter (lpm_treesum_set_param): "theta" or "f64_from"."""
+        check(lib().lpm_treesum_set_param(self.h, name.encode(), float(value)), "lpm_treesum_set_param")
 
 
 def tree_sum_mesh(ctx: Context, kernel: KernelDesc, solver: _capi.SolverDesc, mesh: SphereMesh, face_src,

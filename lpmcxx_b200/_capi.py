@@ -83,6 +83,7 @@ SIGNATURES = {
     "lpm_treesum_destroy": (C.c_int, [P]),
     "lpm_treesum_eval_dev": (C.c_int, [P, P, P, P]),
     "lpm_treesum_stats": (C.c_int, [P, P]),
+    "lpm_treesum_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
     "lpm_tree_sum_mesh": (C.c_int, [P, C.POINTER(KernelDesc), C.POINTER(SolverDesc), I64, P, P, P, I64, P, P, P, P, P,
                                     P, I64, I64, I64, I64, P, P, P, P, P, P, C.POINTER(I64)]),
     "lpm_rk4_create": (C.c_int, [P, C.POINTER(KernelDesc), C.POINTER(SolverDesc), I64, I64, C.POINTER(P)]),
@@ -94,6 +95,7 @@ SIGNATURES = {
     "lpm_rk4_step": (C.c_int, [P, D, C.c_int, C.c_int]),
     "lpm_rk4_velocity_dev": (C.c_int, [P, P]),
     "lpm_rk4_tree_stats": (C.c_int, [P, P]),
+    "lpm_rk4_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
 }
 
 _lib = None

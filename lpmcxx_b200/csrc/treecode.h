@@ -18,5 +18,9 @@ int tree_check(TreeSolver* t);
 // nodes, leaves, depth, far (batch, cluster) pairs, near runs, batches, overflow flags,
 // far target-cluster evaluations, near target-source pairs, 0 (10 values; synchronises)
 int tree_stats(TreeSolver* t, int64_t* out10);
+// Run-time parameters: "theta" (0 < theta < 1, acceptance criterion), "f64_from" (1..kPMax+1: far
+// expansions of this order and above evaluate in FP64), "batch_level" (octree level whose cells target
+// batches may not straddle; 1 .. the level chosen at creation).
+int tree_set_param(TreeSolver* t, const char* name, double value);
 
 }  // namespace lpm

@@ -68,6 +68,14 @@ extern "C" int lpm_treesum_stats(lpm_treesum* ts, int64_t* out8) {
     return tree_stats(ts->solver, out8);
 }
 
+extern "C" int lpm_treesum_set_param(lpm_treesum* ts, const char* name, double value) {
+    if (!ts) {
+        set_error("lpm_treesum_set_param: null solver");
+        return LPM_ERR_ARG;
+    }
+    return tree_set_param(ts->solver, name, value);
+}
+
 extern "C" int lpm_tree_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver,
                                  int64_t n_verts, const double* vx, const double* vy, const double* vz, int64_t n_faces,
                                  const double* fx, const double* fy, const double* fz, const double* face_area,
