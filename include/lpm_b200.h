@@ -171,12 +171,14 @@ int lpm_tree_nodes(lpm_tree* tree, int64_t* level, int64_t* parent, int64_t* cou
 
 typedef struct lpm_solver_desc {
     int32_t method;       /* LPM_METHOD_* */
-    int32_t precision;    /* LPM_PREC_* for the pairwise (near-field) arithmetic */
+    int32_t precision;    /* LPM_PREC_*: direct sums' pairwise arithmetic; treecode: LPM_PREC_F64 evaluates
+                             the far expansions in FP64 (the near field is FP32 with FP64 sums either way) */
     int32_t order;        /* Taylor order p: multi-indices |k| < p, as SumNode (src/LpmTreeSum.cpp:9-18) */
     int32_t max_per_leaf; /* octree leaf capacity (maxParticlesPerBox) */
     double theta;         /* multipole acceptance parameter */
     int32_t order_policy; /* LPM_ORDER_* */
     int32_t reserved;
+    double tolerance;     /* LPM_ORDER_LEARNED: per-pair error budget relative to |mult| * sum|w| (0 = 2e-8) */
 } lpm_solver_desc;
 
 /* ---- treecode (TreeSum).  Biot-Savart on the unit sphere (radius 1, delta 0).  The far field expands
@@ -192,7 +194,8 @@ int lpm_treesum_destroy(lpm_treesum* ts);
 int lpm_treesum_eval_dev(lpm_treesum* ts, const double* src, const double* tgt, double* out);
 /* Statistics of the last evaluation, 10 values: nodes, leaves, depth, far (batch, cluster) pairs, near
  * leaf ranges, target batches, overflow flags, far-field (target, cluster) evaluations, near-field
- * (target, source) pairs, 0.  Synchronises. */
+ * (target, source) pairs, far-field coefficient evaluations (the sum over far evaluations of the order's
+ * coefficient count: 8 flops each).  Synchronises. */
 int lpm_treesum_stats(lpm_treesum* ts, int64_t* out10);
 /* Run-time parameters of a tree solver (no reference counterpart: the reference fixes them at
  * construction).  "theta": acceptance criterion, 0 < theta < 1; "f64_from": far expansions of this
@@ -200,6 +203,34 @@ int lpm_treesum_stats(lpm_treesum* ts, int64_t* out10);
  * LPM_PREC_F64); "batch_level": octree level whose cells a target batch may not straddle (1 .. the
  * level chosen at creation; coarser levels give fuller batches).  Takes effect at the next evaluation. */
 int lpm_treesum_set_param(lpm_treesum* ts, const char* name, double value);
+
+/* ---- learned Taylor-order selection (no reference counterpart: the reference's TreeSum uses one
+ * fixed order).  An MLP (8 -> 64 -> 64 -> 12, GELU) maps the features of an accepted (target batch,
+ * cluster) pair to the smallest order 1..11 whose error stays within tolerance * |mult| * sum|w|, or to
+ * "none": the cluster is then opened (or, for a leaf or a small cluster, summed directly).  Parameters are
+ * LPM_MLP_PARAMS floats: W1[64][8] b1[64] W2[64][64] b2[64] W3[12][64] b3[12] mean[8] inv_std[8]. */
+#define LPM_MLP_PARAMS 5532
+#define LPM_MLP_TRAINABLE 5516
+/* Load the selector (host array, copied and converted to BF16) into a LPM_ORDER_LEARNED solver, or pass
+ * NULL to fall back to the fixed order. */
+int lpm_treesum_set_mlp(lpm_treesum* ts, const float* params);
+/* Training data from one evaluation of device-resident src / tgt: every stride-th accepted pair (stride
+ * <= 0: max_pairs pairs spread evenly over all accepted pairs; at most max_pairs) with its 8 features
+ * (feats, max_pairs x 8), label (0..10 = order 1..11, 11 = none within budget) and, if errs is not NULL,
+ * the error of every order 1..11 relative to the budget (max_pairs x 11), all judged against the FP64 direct
+ * sum of the pair.  Host outputs; *n_out = pairs written.  Synchronous. */
+int lpm_treesum_sample_labels(lpm_treesum* ts, const double* src, const double* tgt, int64_t stride,
+                              int64_t max_pairs, float* feats, int32_t* labels, float* errs, int64_t* n_out);
+/* Train the selector on the GPU (softmax cross-entropy, Adam, mini-batches of `minibatch`, samples shuffled
+ * per epoch with `seed`; deterministic).  params: in/out, LPM_MLP_PARAMS floats (the last 16, the feature
+ * standardisation, are kept); loss_out: epochs floats (mean loss per epoch) or NULL.  Synchronous. */
+int lpm_mlp_train(lpm_ctx* ctx, const float* feats, const int32_t* labels, int64_t n, int epochs, int minibatch,
+                  float lr, uint64_t seed, float* params, float* loss_out);
+/* Mean cross-entropy loss and its gradient (LPM_MLP_TRAINABLE floats) over n <= 2^20 samples (FP32). */
+int lpm_mlp_grad(lpm_ctx* ctx, const float* params, const float* feats, const int32_t* labels, int64_t n,
+                 float* grad, float* loss);
+/* Classes of n feature vectors with the BF16 inference path the treecode uses. */
+int lpm_mlp_predict(lpm_ctx* ctx, const float* params, const float* feats, int64_t n, int32_t* classes);
 /* Host-facing TreeSum::meshSolve (src/LpmTreeSum.cpp:55-86) with the same data as lpm_direct_sum_mesh;
  * mac_count (may be NULL) receives the number of accepted far-field (batch, cluster) pairs, the
  * counterpart of the reference's macCounter. */
@@ -235,6 +266,8 @@ int lpm_rk4_velocity_dev(lpm_rk4* rk, double* out);
 int lpm_rk4_tree_stats(lpm_rk4* rk, int64_t* out10);
 /* lpm_treesum_set_param for the integrator's treecode; drops a captured step graph (synchronises). */
 int lpm_rk4_set_param(lpm_rk4* rk, const char* name, double value);
+/* lpm_treesum_set_mlp for the integrator's treecode; drops a captured step graph (synchronises). */
+int lpm_rk4_set_mlp(lpm_rk4* rk, const float* params);
 
 #ifdef __cplusplus
 }

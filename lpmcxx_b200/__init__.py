@@ -171,13 +171,13 @@ class Context:
 
 
 def direct_solver(precision: int = LPM_PREC_F64) -> _capi.SolverDesc:
-    return _capi.SolverDesc(_capi.LPM_METHOD_DIRECT, precision, 0, 0, 0.0, 0, 0)
+    return _capi.SolverDesc(_capi.LPM_METHOD_DIRECT, precision, 0, 0, 0.0, 0, 0, 0.0)
 
 
 def tree_solver(precision: int = LPM_PREC_F32, order: int = 8, max_per_leaf: int = 512, theta: float = 0.7,
-                learned: bool = False) -> _capi.SolverDesc:
+                learned: bool = False, tolerance: float = 0.0) -> _capi.SolverDesc:
     return _capi.SolverDesc(_capi.LPM_METHOD_TREE, precision, order, max_per_leaf, theta,
-                            _capi.LPM_ORDER_LEARNED if learned else _capi.LPM_ORDER_FIXED, 0)
+                            _capi.LPM_ORDER_LEARNED if learned else _capi.LPM_ORDER_FIXED, 0, tolerance)
 
 
 class RK4:
@@ -233,6 +233,10 @@ class RK4:
     def set_param(self, name: str, value: float) -> None:
         check(lib().lpm_rk4_set_param(self.h, name.encode(), float(value)), "lpm_rk4_set_param")
 
+    def set_mlp(self, params) -> None:
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        check(lib().lpm_rk4_set_mlp(self.h, ptr(p)), "lpm_rk4_set_mlp")
+
 
 class Tree:
     """Device octree (lpm_tree) over a (n, 4) float64 CUDA tensor of points."""
@@ -284,7 +288,7 @@ class TreeSum:
     """Device-resident treecode solver (lpm_treesum) for fixed source / target counts."""
 
     STAT_KEYS = ("nodes", "leaves", "depth", "far_pairs", "near_runs", "batches", "overflow", "far_evals",
-                 "near_pairs", "reserved")
+                 "near_pairs", "far_terms")
 
     def __init__(self, ctx: Context, kernel: KernelDesc, solver: _capi.SolverDesc, n_src: int, n_tgt: int):
         h = C.c_void_p()
@@ -313,8 +317,25 @@ class TreeSum:
         return dict(zip(self.STAT_KEYS, (int(v) for v in o)))
 
     def set_param(self, name: str, value: float) -> None:
-        """Run-time parameter (lpm_treesum_set_param): "theta" or "f64_from"."""
+        """Run-time parameter (lpm_treesum_set_param): "theta", "f64_from", "eps" or "batch_level"."""
         check(lib().lpm_treesum_set_param(self.h, name.encode(), float(value)), "lpm_treesum_set_param")
+
+    def set_mlp(self, params) -> None:
+        """Load the order selector (MLP_PARAMS floats), or None for the fixed-order fallback."""
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        check(lib().lpm_treesum_set_mlp(self.h, ptr(p)), "lpm_treesum_set_mlp")
+
+    def sample_labels(self, src, tgt, stride: int, max_pairs: int, with_errors: bool = False):
+        """(features (n, 8), labels (n,), errors (n, 11) or None) of accepted pairs of one evaluation:
+        every stride-th, or (stride <= 0) max_pairs spread over all of them."""
+        f = np.zeros((max_pairs, 8), np.float32)
+        lab = np.zeros(max_pairs, np.int32)
+        err = np.zeros((max_pairs, 11), np.float32) if with_errors else None
+        n = C.c_int64()
+        check(lib().lpm_treesum_sample_labels(self.h, ptr(src), ptr(tgt), stride, max_pairs, ptr(f), ptr(lab),
+                                              ptr(err), C.byref(n)), "lpm_treesum_sample_labels")
+        k = n.value
+        return f[:k], lab[:k], (err[:k] if err is not None else None)
 
 
 def tree_sum_mesh(ctx: Context, kernel: KernelDesc, solver: _capi.SolverDesc, mesh: SphereMesh, face_src,
@@ -334,3 +355,56 @@ def tree_sum_mesh(ctx: Context, kernel: KernelDesc, solver: _capi.SolverDesc, me
                                   vb, ve, fb, fe, ptr(vo[0]), ptr(vo[1]), ptr(vo[2]), ptr(fo[0]), ptr(fo[1]),
                                   ptr(fo[2]), C.byref(mac)), "lpm_tree_sum_mesh")
     return vo, fo, mac.value
+
+
+# ---- order-selection MLP (training and inference run in the library's CUDA kernels)
+MLP_PARAMS = _capi.LPM_MLP_PARAMS
+MLP_TRAINABLE = _capi.LPM_MLP_TRAINABLE
+
+
+def mlp_init(feats: np.ndarray, seed: int = 0) -> np.ndarray:
+    """Initial parameters: scaled Gaussian weights, zero biases, standardisation from `feats`."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(MLP_PARAMS, np.float32)
+    o = 0
+    for fan_out, fan_in in ((64, 8), (64, 64), (12, 64)):
+        p[o:o + fan_out * fan_in] = rng.normal(0.0, 1.0 / np.sqrt(fan_in), fan_out * fan_in)
+        o += fan_out * fan_in + fan_out
+    mean = feats.mean(axis=0)
+    std = feats.std(axis=0)
+    p[o:o + 8] = mean
+    p[o + 8:o + 16] = 1.0 / np.where(std > 1e-6, std, 1.0)
+    return p
+
+
+def mlp_train(ctx: Context, feats, labels, params, epochs: int = 20, minibatch: int = 512, lr: float = 2e-3,
+              seed: int = 0):
+    """Train `params` in place on the GPU; returns the per-epoch mean loss."""
+    f = np.ascontiguousarray(feats, dtype=np.float32)
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    if params.dtype != np.float32 or not params.flags.c_contiguous:
+        raise TypeError("params must be a contiguous float32 array")
+    loss = np.zeros(max(epochs, 1), np.float32)
+    check(lib().lpm_mlp_train(ctx.h, ptr(f), ptr(lab), f.shape[0], epochs, minibatch, lr, seed, ptr(params),
+                              ptr(loss)), "lpm_mlp_train")
+    return loss[:epochs]
+
+
+def mlp_grad(ctx: Context, params, feats, labels):
+    """(gradient of the mean loss (MLP_TRAINABLE,), mean loss) computed by the training kernels."""
+    f = np.ascontiguousarray(feats, dtype=np.float32)
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    g = np.zeros(MLP_TRAINABLE, np.float32)
+    loss = C.c_float()
+    check(lib().lpm_mlp_grad(ctx.h, ptr(np.ascontiguousarray(params, np.float32)), ptr(f), ptr(lab), f.shape[0],
+                             ptr(g), C.byref(loss)), "lpm_mlp_grad")
+    return g, loss.value
+
+
+def mlp_predict(ctx: Context, params, feats) -> np.ndarray:
+    """Classes from the BF16 inference path the treecode uses."""
+    f = np.ascontiguousarray(feats, dtype=np.float32)
+    cls = np.zeros(f.shape[0], np.int32)
+    check(lib().lpm_mlp_predict(ctx.h, ptr(np.ascontiguousarray(params, np.float32)), ptr(f), f.shape[0], ptr(cls)),
+          "lpm_mlp_predict")
+    return cls

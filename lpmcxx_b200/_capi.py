@@ -37,11 +37,14 @@ LPM_METHOD_DIRECT = 0
 LPM_METHOD_TREE = 1
 LPM_ORDER_FIXED = 0
 LPM_ORDER_LEARNED = 1
+LPM_MLP_PARAMS = 5532
+LPM_MLP_TRAINABLE = 5516
 
 
 class SolverDesc(C.Structure):
     _fields_ = [("method", C.c_int32), ("precision", C.c_int32), ("order", C.c_int32), ("max_per_leaf", C.c_int32),
-                ("theta", C.c_double), ("order_policy", C.c_int32), ("reserved", C.c_int32)]
+                ("theta", C.c_double), ("order_policy", C.c_int32), ("reserved", C.c_int32),
+                ("tolerance", C.c_double)]
 
 
 class LpmError(RuntimeError):
@@ -84,6 +87,11 @@ SIGNATURES = {
     "lpm_treesum_eval_dev": (C.c_int, [P, P, P, P]),
     "lpm_treesum_stats": (C.c_int, [P, P]),
     "lpm_treesum_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
+    "lpm_treesum_set_mlp": (C.c_int, [P, P]),
+    "lpm_treesum_sample_labels": (C.c_int, [P, P, P, C.c_int64, C.c_int64, P, P, P, P]),
+    "lpm_mlp_train": (C.c_int, [P, P, P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_uint64, P, P]),
+    "lpm_mlp_grad": (C.c_int, [P, P, P, P, C.c_int64, P, P]),
+    "lpm_mlp_predict": (C.c_int, [P, P, P, C.c_int64, P]),
     "lpm_tree_sum_mesh": (C.c_int, [P, C.POINTER(KernelDesc), C.POINTER(SolverDesc), I64, P, P, P, I64, P, P, P, P, P,
                                     P, I64, I64, I64, I64, P, P, P, P, P, P, C.POINTER(I64)]),
     "lpm_rk4_create": (C.c_int, [P, C.POINTER(KernelDesc), C.POINTER(SolverDesc), I64, I64, C.POINTER(P)]),
@@ -96,6 +104,7 @@ SIGNATURES = {
     "lpm_rk4_velocity_dev": (C.c_int, [P, P]),
     "lpm_rk4_tree_stats": (C.c_int, [P, P]),
     "lpm_rk4_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
+    "lpm_rk4_set_mlp": (C.c_int, [P, P]),
 }
 
 _lib = None

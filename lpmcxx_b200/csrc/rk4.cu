@@ -329,6 +329,18 @@ extern "C" int lpm_rk4_tree_stats(lpm_rk4* rk, int64_t* out10) {
     return tree_stats(rk->tree, out10);
 }
 
+extern "C" int lpm_rk4_set_mlp(lpm_rk4* rk, const float* params) {
+    if (!rk || !rk->tree) {
+        set_error("lpm_rk4_set_mlp: the integrator does not use the treecode");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(rk->ctx->device));
+    LPM_CUDA_TRY(cudaStreamSynchronize(rk->ctx->stream));
+    drop_graph(rk);
+    rk->warmed = false;  // the next graph step first runs uncaptured so the lists can resize
+    return tree_set_mlp(rk->tree, params);
+}
+
 extern "C" int lpm_rk4_set_param(lpm_rk4* rk, const char* name, double value) {
     if (!rk || !rk->tree) {
         set_error("lpm_rk4_set_param: the integrator does not use the treecode");

@@ -31,6 +31,7 @@
 // pair arithmetic (|x - y|^2 form, as the FP32 direct sum) and FP64 accumulation across tiles.
 #include "treecode.h"
 
+#include "mlp.h"
 #include "octree.h"
 
 #include <algorithm>
@@ -345,10 +346,75 @@ struct TraverseArgs {
     int2* near_list;
     int64_t far_cap, near_cap;
     int32_t* flags;
-    unsigned long long* pair_counts;  // [0] target-cluster far evaluations, [1] target-source near pairs
+    unsigned long long* pair_counts;  // [0] target-cluster far evaluations, [1] target-source near pairs,
+                                      // [2] far coefficient evaluations (sum over far evaluations of E(P))
+    // learned order selection (learned != 0): the MLP picks each accepted pair's order
+    int learned;
+    int max_order;
+    double eps;
+    CutoffTable ct;
+    const float* node_feat;
+    const double* node_wabs;
+    const __nv_bfloat16* mlp_w;
+    const float* mlp_norm;
 };
 
 constexpr int kWarpStack = 1024;
+
+// ---------------------------------------------------------------------------------- learned order
+// Per node: log10 radius, log10 sum|w|, log10 of the Frobenius norms of the degree-2/4/6 moment tensors
+// about the centre, log10 count, level (8th slot unused).
+__global__ void node_feature_kernel(Octree t, int pm, const double4* __restrict__ node_ctr,
+                                    const double* __restrict__ node_wabs, const double* __restrict__ node_mom,
+                                    float* __restrict__ node_feat) {
+    const int nn = t.counters[1];
+    const int cd = cube_dim(pm);
+    for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < nn; node += gridDim.x * blockDim.x) {
+        const double* mom = node_mom + (size_t)node * cd * cd * cd;
+        double norm[3] = {0, 0, 0};
+        for (int d = 0; d < 3; ++d) {
+            const int n = 2 * (d + 1);
+            if (n > pm) continue;
+            for (int a = 0; a <= n; ++a)
+                for (int b = 0; a + b <= n; ++b) {
+                    const double v = mom[(a * cd + b) * cd + (n - a - b)];
+                    norm[d] += v * v;
+                }
+        }
+        float* f = node_feat + (size_t)node * kMlpIn;
+        f[0] = (float)log10(fmax(node_ctr[node].w, 1e-30));
+        f[1] = (float)log10(fmax(node_wabs[node], 1e-30));
+        for (int d = 0; d < 3; ++d) f[2 + d] = (float)log10(fmax(sqrt(norm[d]), 1e-30));
+        f[5] = (float)log10((double)max(t.node_end[node] - t.node_start[node], 1));
+        f[6] = (float)t.node_level[node];
+        f[7] = 0.0f;
+    }
+}
+
+// The 8 MLP inputs of a (batch, cluster) pair.  With R' = |x_batch - c| - r_batch the distance from the
+// centre to the closest point of the batch's ball and tau = eps * sum|w|_all the per-pair error budget
+// (in units of |mult|), the moment features are log10(2 |M_n| / (R'^(n+1) tau)) -- the size of the
+// degree-n term of the expansion relative to the budget -- and the monopole-like feature is
+// log10(2 sum|w|_c / (R' tau)).
+__device__ __forceinline__ void pair_features(const double4& bc, const double4& c, const float* nf, float log_s,
+                                              float* f) {
+    const double dx = bc.x - c.x, dy = bc.y - c.y, dz = bc.z - c.z;
+    const double Rp = fmax(sqrt(dx * dx + dy * dy + dz * dz) - bc.w, 1e-12);
+    const float lr = (float)log10(Rp);
+    f[0] = nf[0];
+    f[1] = nf[0] - lr;
+    f[2] = nf[2] + log_s - 3.0f * lr;
+    f[3] = nf[3] + log_s - 5.0f * lr;
+    f[4] = nf[4] + log_s - 7.0f * lr;
+    f[5] = nf[5];
+    f[6] = nf[6];
+    f[7] = nf[1] + log_s - lr;
+}
+
+// log10(2 / tau), tau = eps * sum|w| over all sources (the root's sum)
+__device__ __forceinline__ float log_budget(const double* node_wabs, double eps) {
+    return (float)log10(2.0 / fmax(eps * node_wabs[0], 1e-300));
+}
 
 // One warp per target batch walks the source tree breadth-first, up to 32 nodes per step: (batch, node)
 // pairs that pass the acceptance test go to the far list with the order to use; leaves that fail it,
@@ -356,6 +422,13 @@ constexpr int kWarpStack = 1024;
 // Entries are appended in lane order, so the lists are deterministic.
 __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
     __shared__ int sstack[4][kWarpStack];
+    __shared__ __nv_bfloat16 mw[kMlpParams];
+    __shared__ float mnorm[2 * kMlpIn];
+    if (A.learned) {  // uniform per launch
+        for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) mw[i] = A.mlp_w[i];
+        for (int i = threadIdx.x; i < 2 * kMlpIn; i += blockDim.x) mnorm[i] = A.mlp_norm[i];
+        __syncthreads();
+    }
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t b = (int64_t)blockIdx.x * 4 + w;
     if (b >= A.n_batches) return;  // uniform per warp
@@ -371,26 +444,38 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
     }
     const double4 bc = A.batch_ctr[b];
     const unsigned long long nb = (unsigned long long)(A.batch_first[b + 1] - A.batch_first[b]);
+    const float log_s = A.learned ? log_budget(A.node_wabs, A.eps) : 0.0f;
     int size = 1;
     if (lane == 0) st[0] = 0;
     __syncwarp();
     int nfar = 0, nnear = 0;
-    unsigned long long far_pairs = 0, near_pairs = 0;
+    unsigned long long far_pairs = 0, near_pairs = 0, far_terms = 0;
     const int64_t foff = A.fill ? A.far_off[b] : 0, noff = A.fill ? A.near_off[b] : 0;
     while (size > 0) {
         const int m = min(32, size);
         const int node = lane < m ? st[size - 1 - lane] : -1;
         __syncwarp();
         size -= m;
-        int kind = 0, nch = 0, lo = 0, hi = 0, cnt = 0, fc = 0;
+        int kind = 0, nch = 0, lo = 0, hi = 0, cnt = 0, fc = 0, P = A.order;
         if (node >= 0) {
             const double4 c = A.node_ctr[node];
             const int s = t.node_start[node], e = t.node_end[node];
             const double dx = bc.x - c.x, dy = bc.y - c.y, dz = bc.z - c.z;
             const double R = sqrt(dx * dx + dy * dy + dz * dz);
-            const bool far_ok = R > bc.w && c.w < A.theta * (R - bc.w);
+            bool far_ok = R > bc.w && c.w < A.theta * (R - bc.w);
             const int nc = t.node_nchild[node];
-            if (far_ok && e - s >= A.direct_below) {
+            int cut = A.direct_below;
+            if (far_ok && A.learned) {
+                // the selector's order; "no order meets the budget" opens a cluster large enough to be
+                // worth opening and sums a leaf or a small cluster directly
+                float f[kMlpIn];
+                pair_features(bc, c, A.node_feat + (size_t)node * kMlpIn, log_s, f);
+                const int cls = mlp_argmax_bf16(mw, mnorm, f);
+                P = cls == kMlpDirectClass ? 0 : min(cls + 1, A.max_order);
+                cut = P > 0 ? A.ct.direct_below[P] : 0x7fffffff;
+                if (P == 0 && nc > 0 && e - s >= A.ct.direct_below[A.max_order]) far_ok = false;
+            }
+            if (far_ok && e - s >= cut) {
                 kind = 1;
             } else if (far_ok || nc == 0) {
                 kind = 2;
@@ -406,7 +491,7 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
         const unsigned fm = __ballot_sync(full, kind == 1);
         if (kind == 1 && A.fill) {
             const int64_t at = foff + nfar + __popc(fm & lt);
-            if (at < A.far_cap) A.far_list[at] = make_int2(node, A.order);
+            if (at < A.far_cap) A.far_list[at] = make_int2(node, P);
             else atomicOr(&A.flags[0], 1);
         }
         nfar += __popc(fm);
@@ -419,8 +504,13 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
         }
         nnear += __popc(nm);
         unsigned long long np = (unsigned long long)cnt * nb;
-        for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(full, np, o);
+        unsigned long long ft = kind == 1 ? (unsigned long long)entries_for(P) * nb : 0ull;
+        for (int o = 16; o > 0; o >>= 1) {
+            np += __shfl_xor_sync(full, np, o);
+            ft += __shfl_xor_sync(full, ft, o);
+        }
         near_pairs += np;
+        far_terms += ft;
         // push the children of split nodes
         int incl = nch;
         for (int o = 1; o < 32; o <<= 1) {
@@ -442,6 +532,7 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
         A.near_cnt[b] = nnear;
         atomicAdd(&A.pair_counts[0], far_pairs);
         atomicAdd(&A.pair_counts[1], near_pairs);
+        atomicAdd(&A.pair_counts[2], far_terms);
     }
 }
 
@@ -584,6 +675,98 @@ __global__ void __launch_bounds__(kBatch) far_kernel(const double4* __restrict__
         V[q] = acc[0];
         V[n_tgt + q] = acc[1];
         V[2 * n_tgt + q] = acc[2];
+    }
+}
+
+// ---------------------------------------------------------------------------------- selector training data
+// Training pairs: every `stride`-th far entry (stride <= 0: max_pairs spread over the list) -> (batch, node).
+__global__ void sample_pairs_kernel(const int32_t* __restrict__ far_off, const int32_t* __restrict__ nbat,
+                                    const int2* __restrict__ far_list, int64_t far_cap,
+                                    const int32_t* __restrict__ totals, int64_t stride, int64_t max_pairs,
+                                    int2* __restrict__ pairs, int32_t* __restrict__ n_pairs) {
+    const int64_t total = min((int64_t)totals[0], far_cap);
+    if (stride <= 0) stride = max((int64_t)1, (total + max_pairs - 1) / max_pairs);
+    const int64_t np = min(max_pairs, (total + stride - 1) / stride);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n_pairs = (int32_t)np;
+    const int nb = *nbat;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < np; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t f = k * stride;
+        int lo = 0, hi = nb;  // last batch with far_off <= f (the one whose range holds f)
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (far_off[mid] <= f) lo = mid;
+            else hi = mid;
+        }
+        pairs[k] = make_int2(lo, far_list[f].x);
+    }
+}
+
+// One block per sampled (batch, cluster) pair: the cluster's exact FP64 contribution at the batch's
+// targets, its expansion at orders 1..max_order (FP64), the largest per-target error of each order in
+// units of |mult|, the label (smallest order within eps * sum|w|_all, else kMlpDirectClass) and the
+// pair's features.
+__global__ void __launch_bounds__(kBatch) label_kernel(Octree t, const int2* __restrict__ pairs,
+                                                       const int32_t* __restrict__ n_pairs,
+                                                       const int32_t* __restrict__ batch_first,
+                                                       const double4* __restrict__ tgt_sorted,
+                                                       const double4* __restrict__ src_sorted,
+                                                       const double4* __restrict__ batch_ctr,
+                                                       const double4* __restrict__ node_ctr,
+                                                       const float* __restrict__ node_feat,
+                                                       const double* __restrict__ node_wabs,
+                                                       const double4* __restrict__ B64, int n_ent,
+                                                       const int32_t* __restrict__ gtab, CutoffTable ct, int max_order,
+                                                       double eps, float* __restrict__ feats,
+                                                       int32_t* __restrict__ labels, float* __restrict__ errs) {
+    extern __shared__ double4 sbuf[];
+    __shared__ double red[kBatch / 32];
+    const int64_t k = blockIdx.x;
+    if (k >= *n_pairs) return;  // uniform per block
+    const int2 pr = pairs[k];
+    const int64_t q0 = batch_first[pr.x], q1 = batch_first[pr.x + 1];
+    const int64_t q = q0 + threadIdx.x;
+    const bool ok = q < q1;
+    const double4 x = ok ? tgt_sorted[q] : make_double4(0, 0, 0, 0);
+    const double4 c = node_ctr[pr.y];
+    // exact contribution sum_j w_j 2 (x cross y_j) / |x - y_j|^2 (the far field's units)
+    double ex[3] = {0, 0, 0};
+    if (ok) {
+        for (int j = t.node_start[pr.y]; j < t.node_end[pr.y]; ++j) {
+            const double4 y = src_sorted[j];
+            const double dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
+            const double s = 2.0 * y.w / (dx * dx + dy * dy + dz * dz);
+            ex[0] += s * (x.y * y.z - x.z * y.y);
+            ex[1] += s * (x.z * y.x - x.x * y.z);
+            ex[2] += s * (x.x * y.y - x.y * y.x);
+        }
+    }
+    const double budget = eps * node_wabs[0];
+    int label = kMlpDirectClass;
+    for (int P = 1; P <= max_order; ++P) {
+        const int nterm = ct.table_off[P + 1] - ct.table_off[P];
+        const int32_t* tab = gtab + ct.table_off[P];
+        const double4* src = B64 + (size_t)pr.y * n_ent;
+        __syncthreads();  // previous order's readers of sbuf / red are done
+        for (int i = threadIdx.x; i < nterm; i += kBatch) sbuf[i] = src[tab[i]];
+        __syncthreads();
+        double v[3] = {0, 0, 0};
+        far_dispatch<double, double4>(P, sbuf, x, c, v);
+        double e = 0.0;
+        if (ok)
+            e = sqrt((v[0] - ex[0]) * (v[0] - ex[0]) + (v[1] - ex[1]) * (v[1] - ex[1]) +
+                     (v[2] - ex[2]) * (v[2] - ex[2]));
+        for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+        __syncthreads();
+        double emax = 0.0;
+        for (int i = 0; i < kBatch / 32; ++i) emax = fmax(emax, red[i]);
+        if (threadIdx.x == 0 && errs) errs[k * max_order + (P - 1)] = (float)(emax / fmax(budget, 1e-300));
+        if (label == kMlpDirectClass && emax <= budget) label = P - 1;
+    }
+    if (threadIdx.x == 0) {
+        labels[k] = label;
+        pair_features(batch_ctr[pr.x], c, node_feat + (size_t)pr.y * kMlpIn, log_budget(node_wabs, eps),
+                      feats + k * kMlpIn);
     }
 }
 
@@ -783,6 +966,13 @@ struct TreeSolver {
     int2 *far_list = nullptr, *near_list = nullptr;
     int64_t far_cap = 0, near_cap = 0;
     double* V = nullptr;
+    // learned order selection
+    bool learned = false;     // order_policy == LPM_ORDER_LEARNED
+    bool mlp_loaded = false;  // weights present; without them the fixed order is the fallback
+    double eps = 2e-8;        // per-pair error budget relative to |mult| * sum|w|
+    float* node_feat = nullptr;
+    __nv_bfloat16* mlp_w = nullptr;
+    float* mlp_norm = nullptr;
     std::vector<void*> allocs;
 };
 
@@ -856,7 +1046,10 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     t->solver = solver;
     t->n_src = n_src;
     t->n_tgt = n_tgt;
-    t->pm = solver.order_policy == LPM_ORDER_LEARNED ? kPMax : solver.order;
+    t->learned = solver.order_policy == LPM_ORDER_LEARNED;
+    // the selector picks orders up to kMlpDirectClass (11); the fixed order is its fallback
+    t->pm = t->learned ? std::max(kMlpDirectClass, solver.order) : solver.order;
+    if (t->learned && solver.tolerance > 0.0) t->eps = solver.tolerance;
     // FP32 far field by default: its rounding stays ~1e-7 relative, below the truncation error of the
     // orders used; LPM_PREC_F64 evaluates every far expansion in FP64
     t->f64_from = solver.precision == LPM_PREC_F64 ? 1 : kPMax + 1;
@@ -937,8 +1130,13 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->far_off, (size_t)t->n_batches + 1));
     A(talloc(t, &t->near_off, (size_t)t->n_batches + 1));
     A(talloc(t, &t->flags, 8));
-    A(talloc(t, &t->pair_counts, 2));
+    A(talloc(t, &t->pair_counts, 3));
     A(talloc(t, &t->V, 3 * ntg));
+    if (t->learned) {
+        A(talloc(t, &t->node_feat, nn * kMlpIn));
+        A(talloc(t, &t->mlp_w, kMlpParams));
+        A(talloc(t, &t->mlp_norm, 2 * kMlpIn));
+    }
     if (e == cudaSuccess) e = cudaMemcpy(t->ent, ent.data(), ent.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(t->mono, mono.data(), mono.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !gtab.empty())
@@ -996,7 +1194,15 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     A.flags = t->flags;
     A.pair_counts = t->pair_counts;
     A.fill = 0;
-    LPM_CUDA_TRY(cudaMemsetAsync(t->pair_counts, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    A.learned = (t->learned && t->mlp_loaded) ? 1 : 0;
+    A.max_order = std::min(t->pm, kMlpDirectClass);
+    A.eps = t->eps;
+    A.ct = t->ct;
+    A.node_feat = t->node_feat;
+    A.node_wabs = t->node_wabs;
+    A.mlp_w = t->mlp_w;
+    A.mlp_norm = t->mlp_norm;
+    LPM_CUDA_TRY(cudaMemsetAsync(t->pair_counts, 0, 3 * sizeof(unsigned long long), ctx->stream));
     const unsigned g = grid_for(t->n_batches, 4);
     LPM_LAUNCH(ctx, "traverse_kernel", traverse_kernel, g, 128, 0, A);
     int rc = scan_exclusive_i32(ctx, t->far_cnt, t->far_off, t->n_batches + 1, t->flags + 2);
@@ -1057,6 +1263,9 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
                    t->node_ctr, t->node_wabs, t->node_mom);
     LPM_LAUNCH(ctx, "coeff_kernel", coeff_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->node_mom, t->B64,
                t->B32);
+    if (t->learned)
+        LPM_LAUNCH(ctx, "node_feature_kernel", node_feature_kernel, gl, 128, 0, t->st, t->pm, t->node_ctr,
+                   t->node_wabs, t->node_mom, t->node_feat);
     // targets in Morton order, cut into compact batches of at most kBatch
     LPM_CUDA_TRY(cudaMemsetAsync(t->tcount, 0, 4 * sizeof(int32_t), ctx->stream));
     rc = morton_keys(ctx, X, n_tgt, rb, t->tkeys, t->tperm, t->tcount);
@@ -1117,7 +1326,7 @@ int tree_check(TreeSolver* t) {
 
 int tree_stats(TreeSolver* t, int64_t* out8) {
     int32_t f[8], c[8];
-    unsigned long long pc[2];
+    unsigned long long pc[3];
     lpm_ctx* ctx = t->ctx;
     LPM_CUDA_TRY(cudaMemcpyAsync(pc, t->pair_counts, sizeof(pc), cudaMemcpyDeviceToHost, ctx->stream));
     LPM_CUDA_TRY(cudaMemcpyAsync(f, t->flags, sizeof(f), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1134,7 +1343,7 @@ int tree_stats(TreeSolver* t, int64_t* out8) {
     out8[6] = f[0];
     out8[7] = (int64_t)pc[0];  // far-field target-cluster evaluations
     out8[8] = (int64_t)pc[1];  // near-field target-source pairs
-    out8[9] = 0;
+    out8[9] = (int64_t)pc[2];  // far coefficient evaluations: sum of E(P) over far evaluations
     return LPM_OK;
 }
 
@@ -1150,6 +1359,8 @@ int tree_set_param(TreeSolver* t, const char* name, double value) {
     const std::string n(name);
     if (n == "theta" && value > 0.0 && value < 1.0) {
         t->solver.theta = value;
+    } else if (n == "eps" && value > 0.0) {
+        t->eps = value;
     } else if (n == "batch_level" && value >= 1.0 && value <= t->batch_level_max && value == std::floor(value)) {
         t->batch_level = (int)value;
     } else if (n == "f64_from" && value >= 1.0 && value <= kPMax + 1 && value == std::floor(value)) {
@@ -1159,6 +1370,85 @@ int tree_set_param(TreeSolver* t, const char* name, double value) {
         set_error("tree_set_param: unknown parameter or value out of range: %s = %g", name, value);
         return LPM_ERR_ARG;
     }
+    return LPM_OK;
+}
+
+}  // namespace lpm
+
+namespace lpm {
+
+int tree_set_mlp(TreeSolver* t, const float* params_host) {
+    if (!t->learned) {
+        set_error("tree solver: the order selector applies to LPM_ORDER_LEARNED solvers only");
+        return LPM_ERR_ARG;
+    }
+    if (!params_host) {
+        t->mlp_loaded = false;  // back to the fixed-order fallback
+        return LPM_OK;
+    }
+    int rc = mlp_upload_bf16(t->ctx, params_host, t->mlp_w, t->mlp_norm);
+    if (rc) return rc;
+    t->mlp_loaded = true;
+    return LPM_OK;
+}
+
+namespace {
+struct TmpBuf {
+    void* p = nullptr;
+    ~TmpBuf() {
+        if (p) cudaFree(p);
+    }
+};
+}  // namespace
+
+// One evaluation with every accepted cluster listed as a far entry (fixed-order lists, no cost cutoff),
+// then the sampled pairs are labelled against the FP64 direct sum of each cluster.  Host outputs: feats
+// (max_pairs x 8), labels (max_pairs), errs (max_pairs x 11, may be null: error / budget per order).
+int tree_sample_labels(TreeSolver* t, const double4* src, const double4* tgt, int64_t stride, int64_t max_pairs,
+                       float* feats, int32_t* labels, float* errs, int64_t* n_out) {
+    if (!t->learned || max_pairs < 1 || max_pairs > (1 << 24) || !feats || !labels || !n_out) {
+        set_error("tree_sample_labels: needs a LPM_ORDER_LEARNED solver, 1 <= max_pairs <= 2^24 and output arrays");
+        return LPM_ERR_ARG;
+    }
+    *n_out = 0;
+    if (t->n_src == 0 || t->n_tgt == 0) return LPM_OK;
+    lpm_ctx* ctx = t->ctx;
+    const int max_order = std::min(t->pm, kMlpDirectClass);
+    TmpBuf bu, bp, bf, bl, be;
+    LPM_CUDA_TRY(cudaMalloc(&bu.p, 3 * (size_t)t->n_tgt * sizeof(double)));
+    LPM_CUDA_TRY(cudaMalloc(&bp.p, (size_t)max_pairs * sizeof(int2)));
+    LPM_CUDA_TRY(cudaMalloc(&bf.p, (size_t)max_pairs * kMlpIn * sizeof(float)));
+    LPM_CUDA_TRY(cudaMalloc(&bl.p, ((size_t)max_pairs + 1) * sizeof(int32_t)));
+    LPM_CUDA_TRY(cudaMalloc(&be.p, (size_t)max_pairs * max_order * sizeof(float)));
+    const bool had = t->mlp_loaded;
+    const int32_t keep = t->ct.direct_below[t->solver.order];
+    t->mlp_loaded = false;
+    t->ct.direct_below[t->solver.order] = 1;
+    int rc = tree_velocity(t, src, t->n_src, tgt, t->n_tgt, (double*)bu.p);
+    t->ct.direct_below[t->solver.order] = keep;
+    t->mlp_loaded = had;
+    if (rc) return rc;
+    int32_t* dlab = (int32_t*)bl.p;
+    int32_t* np_dev = dlab + max_pairs;  // count stored after the labels
+    LPM_LAUNCH(ctx, "sample_pairs_kernel", sample_pairs_kernel, 64, 256, 0, t->far_off, t->tcount + 1, t->far_list,
+               t->far_cap, t->flags + 2, stride, max_pairs, (int2*)bp.p, np_dev);
+    const size_t smem = (size_t)entries_for(max_order) * sizeof(double4);
+    if (smem > 48 * 1024)
+        LPM_CUDA_TRY(cudaFuncSetAttribute(label_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LPM_LAUNCH(ctx, "label_kernel", label_kernel, (unsigned)max_pairs, kBatch, smem, t->st, (const int2*)bp.p, np_dev,
+               t->batch_first, t->tgt_sorted, t->src_sorted, t->batch_ctr, t->node_ctr, t->node_feat, t->node_wabs,
+               t->B64, t->n_ent, t->gtab, t->ct, max_order, t->eps, (float*)bf.p, dlab, (float*)be.p);
+    int32_t np = 0;
+    LPM_CUDA_TRY(cudaMemcpyAsync(&np, np_dev, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    LPM_CUDA_TRY(cudaMemcpyAsync(feats, bf.p, (size_t)np * kMlpIn * sizeof(float), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    LPM_CUDA_TRY(cudaMemcpyAsync(labels, dlab, (size_t)np * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    if (errs)
+        LPM_CUDA_TRY(cudaMemcpyAsync(errs, be.p, (size_t)np * max_order * sizeof(float), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    *n_out = np;
     return LPM_OK;
 }
 

@@ -16,11 +16,17 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
 // Synchronises and reports capacity overflows of the last evaluation (LPM_ERR_CAPACITY).
 int tree_check(TreeSolver* t);
 // nodes, leaves, depth, far (batch, cluster) pairs, near runs, batches, overflow flags,
-// far target-cluster evaluations, near target-source pairs, 0 (10 values; synchronises)
+// far target-cluster evaluations, near target-source pairs, far coefficient evaluations (sum over far
+// evaluations of the order's coefficient count) (10 values; synchronises)
 int tree_stats(TreeSolver* t, int64_t* out10);
 // Run-time parameters: "theta" (0 < theta < 1, acceptance criterion), "f64_from" (1..kPMax+1: far
-// expansions of this order and above evaluate in FP64), "batch_level" (octree level whose cells target
+// expansions of this order and above evaluate in FP64), "eps" (learned order's per-pair budget), "batch_level" (octree level whose cells target
 // batches may not straddle; 1 .. the level chosen at creation).
 int tree_set_param(TreeSolver* t, const char* name, double value);
+// Learned order: load the selector (LPM_MLP_PARAMS floats, host) or null for the fixed-order fallback.
+int tree_set_mlp(TreeSolver* t, const float* params_host);
+// Learned order: labelled training pairs from one evaluation (see lpm_treesum_sample_labels).
+int tree_sample_labels(TreeSolver* t, const double4* src, const double4* tgt, int64_t stride, int64_t max_pairs,
+                       float* feats, int32_t* labels, float* errs, int64_t* n_out);
 
 }  // namespace lpm

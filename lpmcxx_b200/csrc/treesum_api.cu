@@ -76,6 +76,27 @@ extern "C" int lpm_treesum_set_param(lpm_treesum* ts, const char* name, double v
     return tree_set_param(ts->solver, name, value);
 }
 
+extern "C" int lpm_treesum_set_mlp(lpm_treesum* ts, const float* params) {
+    if (!ts) {
+        set_error("lpm_treesum_set_mlp: null solver");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(ts->ctx->device));
+    return tree_set_mlp(ts->solver, params);
+}
+
+extern "C" int lpm_treesum_sample_labels(lpm_treesum* ts, const double* src, const double* tgt, int64_t stride,
+                                         int64_t max_pairs, float* feats, int32_t* labels, float* errs,
+                                         int64_t* n_out) {
+    if (!ts || (ts->n_src > 0 && !src) || (ts->n_tgt > 0 && !tgt)) {
+        set_error("lpm_treesum_sample_labels: null argument");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(ts->ctx->device));
+    return tree_sample_labels(ts->solver, (const double4*)src, (const double4*)tgt, stride, max_pairs, feats, labels,
+                              errs, n_out);
+}
+
 extern "C" int lpm_tree_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver,
                                  int64_t n_verts, const double* vx, const double* vy, const double* vz, int64_t n_faces,
                                  const double* fx, const double* fy, const double* fz, const double* face_area,
