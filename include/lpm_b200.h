@@ -107,9 +107,9 @@ int lpm_direct_sum_dev(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precisio
                        const double* tgt, int64_t n_tgt, int64_t n_coincident, double* out);
 
 /* Allocation-free variant of lpm_direct_sum_dev at LPM_PREC_F32 (no counterpart in the reference, which
- * has no GPU path).  For callers that cannot allocate device memory while they run: code inside a CUDA
- * graph being captured, hosts that reserve the whole device for their own pool, real-time loops that may
- * not block in the allocator.  Arguments as lpm_direct_sum_dev, device pointers, enqueued on cuda_stream
+ * has no GPU path).  For callers that cannot allocate device memory while they run: hosts that reserve
+ * the whole device for their own pool allocator, real-time loops that may not block in the allocator.
+ * Arguments as lpm_direct_sum_dev, device pointers, enqueued on cuda_stream
  * (NULL = legacy default stream) of the current device; no context.  The FP32 copies live in one
  * file-scope device array of 524,288 points (8 MiB, held by every GPU that loads the library): n_src +
  * n_tgt above that returns LPM_ERR_CAPACITY.  Calls never call cudaMalloc / cudaFree.  The first call on a

@@ -1,9 +1,9 @@
 // Allocation-free FP32 direct sum.
 //
-// Some callers cannot allocate device memory at call time: code running inside a CUDA graph that is
-// being captured (no cudaMalloc there), hosts whose memory pool is reserved up front (a solver embedded
-// in a larger simulation that owns every byte of the device), or real-time loops that may not block on
-// the allocator.  The regular FP32 entry point (lpm_direct_sum_dev with LPM_PREC_F32) converts its FP64
+// Some callers cannot allocate device memory at call time: hosts whose memory pool is reserved up front
+// (a solver embedded in a larger simulation whose own allocator owns every byte of the device, so a
+// cudaMalloc here would fail or steal from it), and real-time loops that may not block on the allocator
+// or grow the process's device footprint after start-up.  The regular FP32 entry point (lpm_direct_sum_dev with LPM_PREC_F32) converts its FP64
 // inputs into FP32 copies held in per-context scratch that it grows with cudaMalloc.  This variant keeps
 // those copies in one file-scope device array instead, so it allocates nothing: the caller passes the
 // inputs, the output and a stream, and no context is needed.

@@ -1,7 +1,8 @@
 """The allocation-free FP32 direct sum (lpm_direct_sum_f32_noalloc) through the C ABI.
 
-It serves callers that cannot allocate device memory at call time (graph capture, hosts that own the
-whole device, real-time loops): its FP32 copies live in a fixed file-scope device array instead of
+It serves callers that cannot allocate device memory at call time (hosts whose own pool allocator owns
+the whole device, real-time loops that may not block in the allocator): its FP32 copies live in a fixed
+file-scope device array instead of
 context scratch.  Its output must match the regular FP32 entry point's within the FP32 tolerance of the
 other GPU tests, on two calls in a row (the second reuses the array the first one filled).  This file is
 collected last so a failure here leaves every other test already run.
