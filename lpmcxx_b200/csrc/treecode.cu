@@ -338,13 +338,14 @@ struct TraverseArgs {
     int order;
     int direct_below;
     int fill;  // 0 = count, 1 = fill
-    int32_t* far_cnt;
+    int32_t* far_cnt;  // far lists are bucketed by order: row P (stride nb1) holds every batch's order-P entries
     int32_t* near_cnt;
     const int32_t* far_off;
     const int32_t* near_off;
     int2* far_list;
     int2* near_list;
     int64_t far_cap, near_cap;
+    int64_t nb1;  // row stride of far_cnt / far_off (n_batches + 1)
     int32_t* flags;
     unsigned long long* pair_counts;  // [0] target-cluster far evaluations, [1] target-source near pairs,
                                       // [2] far coefficient evaluations (sum over far evaluations of E(P))
@@ -422,6 +423,7 @@ __device__ __forceinline__ float log_budget(const double* node_wabs, double eps)
 // Entries are appended in lane order, so the lists are deterministic.
 __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
     __shared__ int sstack[4][kWarpStack];
+    __shared__ int pcnt[4][kPMax + 1];  // per warp: far entries of each order so far
     __shared__ __nv_bfloat16 mw[kMlpParams];
     __shared__ float mnorm[2 * kMlpIn];
     if (A.learned) {  // uniform per launch
@@ -435,10 +437,11 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
     const Octree& t = A.t;
     const unsigned full = 0xffffffffu, lt = (1u << lane) - 1u;
     int* st = sstack[w];
+    if (lane <= kPMax) pcnt[w][lane] = 0;
     if (t.counters[1] == 0 || t.counters[0] == 0 || b >= *A.nbat) {
-        if (!A.fill && lane == 0) {
-            A.far_cnt[b] = 0;
-            A.near_cnt[b] = 0;
+        if (!A.fill) {
+            if (lane <= kPMax) A.far_cnt[lane * A.nb1 + b] = 0;
+            if (lane == 0) A.near_cnt[b] = 0;
         }
         return;
     }
@@ -448,9 +451,9 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
     int size = 1;
     if (lane == 0) st[0] = 0;
     __syncwarp();
-    int nfar = 0, nnear = 0;
+    int nnear = 0;
     unsigned long long far_pairs = 0, near_pairs = 0, far_terms = 0;
-    const int64_t foff = A.fill ? A.far_off[b] : 0, noff = A.fill ? A.near_off[b] : 0;
+    const int64_t noff = A.fill ? A.near_off[b] : 0;
     while (size > 0) {
         const int m = min(32, size);
         const int node = lane < m ? st[size - 1 - lane] : -1;
@@ -489,12 +492,21 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
             }
         }
         const unsigned fm = __ballot_sync(full, kind == 1);
-        if (kind == 1 && A.fill) {
-            const int64_t at = foff + nfar + __popc(fm & lt);
-            if (at < A.far_cap) A.far_list[at] = make_int2(node, P);
-            else atomicOr(&A.flags[0], 1);
+        if (fm) {  // warp-uniform: rank each far entry among this step's entries of its order, in lane order
+            const unsigned grp = __match_any_sync(full, kind == 1 ? P : 64 + lane);
+            const int rank = __popc(grp & lt);
+            const int base = kind == 1 ? pcnt[w][P] : 0;
+            __syncwarp();
+            if (kind == 1) {
+                if (rank == 0) pcnt[w][P] = base + __popc(grp);
+                if (A.fill) {
+                    const int64_t at = A.far_off[P * A.nb1 + b] + base + rank;
+                    if (at < A.far_cap) A.far_list[at] = make_int2(node, P);
+                    else atomicOr(&A.flags[0], 1);
+                }
+            }
+            __syncwarp();
         }
-        nfar += __popc(fm);
         far_pairs += (unsigned long long)__popc(fm) * nb;
         const unsigned nm = __ballot_sync(full, kind == 2);
         if (kind == 2 && A.fill) {
@@ -527,8 +539,8 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
         __syncwarp();
         if (size + total <= kWarpStack) size += total;
     }
+    if (!A.fill && lane <= kPMax) A.far_cnt[lane * A.nb1 + b] = pcnt[w][lane];
     if (!A.fill && lane == 0) {
-        A.far_cnt[b] = nfar;
         A.near_cnt[b] = nnear;
         atomicAdd(&A.pair_counts[0], far_pairs);
         atomicAdd(&A.pair_counts[1], near_pairs);
@@ -606,75 +618,160 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
-__device__ __forceinline__ void cp_async_commit_wait() {
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <typename F, typename F4>
+__device__ __forceinline__ void fma4(F (&r)[4], F e, const F4& v) {
+    r[0] = fma(r[0], e, v.x);
+    r[1] = fma(r[1], e, v.y);
+    r[2] = fma(r[2], e, v.z);
+    r[3] = fma(r[3], e, v.w);
+}
+template <typename F>
+__device__ __forceinline__ void fma4(F (&r)[4], F e, const F (&v)[4]) {
+    r[0] = fma(r[0], e, v[0]);
+    r[1] = fma(r[1], e, v[1]);
+    r[2] = fma(r[2], e, v[2]);
+    r[3] = fma(r[3], e, v[3]);
 }
 
-// Issue the asynchronous gather of one far entry's coefficients (order-P Horner sequence) into buf.
-__device__ __forceinline__ void far_gather(int2 ent, const double4* __restrict__ B64, const float4* __restrict__ B32,
-                                           int n_ent, const int32_t* __restrict__ gtab, const CutoffTable& ct,
-                                           int f64_from, double4* buf) {
-    const int P = ent.y;
-    if (P <= 0) return;
-    const int nterm = ct.table_off[P + 1] - ct.table_off[P];
-    const int32_t* tab = gtab + ct.table_off[P];
-    if (P >= f64_from) {
-        const double4* src = B64 + (size_t)ent.x * n_ent;
-        for (int i = threadIdx.x; i < 2 * nterm; i += kBatch) {
-            const double4* g = src + tab[i >> 1];
-            cp_async16((char*)(buf + (i >> 1)) + 16 * (i & 1), (const char*)g + 16 * (i & 1));
-        }
-    } else {
-        float4* s32 = (float4*)buf;
-        const float4* src = B32 + (size_t)ent.x * n_ent;
-        for (int i = threadIdx.x; i < nterm; i += kBatch) cp_async16(s32 + i, src + tab[i]);
+// One far entry at one target in F arithmetic: acc += 2 [(x cross d) G0 + x cross G], d = c - x,
+// G = g / |d|^2, g from the order-P Horner scheme (fully unrolled for P).
+template <int P, typename F, typename F4>
+__device__ __forceinline__ void far_one_acc(const F4* __restrict__ Bc, const double4& x, double cx, double cy,
+                                            double cz, double (&acc)[3]) {
+    const F dx = (F)(cx - x.x), dy = (F)(cy - x.y), dz = (F)(cz - x.z);
+    const F inv = F(1) / (dx * dx + dy * dy + dz * dz);
+    F g0, g1, g2, g3;
+    horner<P, F, F4>(Bc, dx * inv, dy * inv, dz * inv, inv, g0, g1, g2, g3);
+    const F s = F(2) * inv;
+    const F G0 = s * g0, Gx = s * g1, Gy = s * g2, Gz = s * g3;
+    const F xx = (F)x.x, xy = (F)x.y, xz = (F)x.z;
+    acc[0] += (double)((xy * dz - xz * dy) * G0 + (xy * Gz - xz * Gy));
+    acc[1] += (double)((xz * dx - xx * dz) * G0 + (xz * Gx - xx * Gz));
+    acc[2] += (double)((xx * dy - xy * dx) * G0 + (xx * Gy - xy * Gx));
+}
+
+struct FarArgs {
+    const double4* tgt_sorted;
+    int64_t n_tgt;
+    const int32_t* batch_first;
+    const int32_t* nbat;
+    const int32_t* far_off;  // row P of the bucketed offsets / counts
+    const int32_t* far_cnt;
+    const int2* far_list;
+    int64_t far_cap;
+    const double4* node_ctr;
+    const double4* B64;
+    const float4* B32;
+    int n_ent;
+    const int32_t* gtab;  // order-P gather table: canonical index of each Horner-sequence entry
+    double* V;
+};
+
+constexpr int kFarStageUnits = 1024;  // 16-byte units gathered per stage (at least one entry)
+
+template <int P, typename F4>
+struct FarShape {
+    static constexpr int kUnits = entries_for(P) * (int)(sizeof(F4) / 16);  // per entry
+    static constexpr int kK =
+        kUnits >= kFarStageUnits ? 1 : (kFarStageUnits / kUnits > 32 ? 32 : kFarStageUnits / kUnits);
+    static constexpr int kStage = kK * kUnits;  // units per stage buffer
+    static constexpr size_t kSmem = 2 * (size_t)kStage * 16 + 2 * (size_t)kK * sizeof(double4);
+};
+
+// Issue the copies of entries [s0, s0 + n) of the batch's order-P list into one stage: coefficients by
+// cp.async, cluster centres by plain stores.
+template <int P, typename F4>
+__device__ __forceinline__ void far_stage_gather(const FarArgs& A, int64_t s0, int n, float4* buf, double4* ctr) {
+    using S = FarShape<P, F4>;
+    constexpr int kSub = (int)(sizeof(F4) / 16);
+    const F4* base = (const F4*)(kSub == 2 ? (const void*)A.B64 : (const void*)A.B32);
+    for (int i = threadIdx.x; i < n * S::kUnits; i += kBatch) {
+        const int e = i / S::kUnits, j = i - e * S::kUnits;
+        const int node = A.far_list[s0 + e].x;
+        const char* src = (const char*)(base + (size_t)node * A.n_ent + A.gtab[j / kSub]) + 16 * (j % kSub);
+        cp_async16(buf + i, src);
     }
+    if ((int)threadIdx.x < n) ctr[threadIdx.x] = A.node_ctr[A.far_list[s0 + threadIdx.x].x];
 }
 
-// One block per target batch; each thread owns one target and sweeps the batch's far list.  The next
-// entry's coefficients are gathered into the other half of a double buffer (cp.async) while the
-// current one is evaluated.  Warps past the end of a short batch only help with the gathers.
-__global__ void __launch_bounds__(kBatch) far_kernel(const double4* __restrict__ tgt_sorted, int64_t n_tgt,
-                                                     const int32_t* __restrict__ batch_first,
-                                                     const int32_t* __restrict__ nbat,
-                                                     const int32_t* __restrict__ far_off,
-                                                     const int32_t* __restrict__ far_cnt,
-                                                     const int2* __restrict__ far_list, int64_t far_cap,
-                                                     const double4* __restrict__ node_ctr,
-                                                     const double4* __restrict__ B64, const float4* __restrict__ B32,
-                                                     int n_ent, const int32_t* __restrict__ gtab, CutoffTable ct,
-                                                     int buf_terms, int f64_from, double* __restrict__ V) {
-    extern __shared__ double4 sbuf[];
+// Far field for the order-P bucket: one block per target batch, one thread per target, the order's
+// fully unrolled Horner scheme in F arithmetic.  Entries are gathered kK at a time into one half of a
+// double buffer (cp.async) while the other half is evaluated; one launch per order keeps every warp of
+// the GPU in the same compact code.  Adds to V (cleared before the first order's launch).
+template <int P, typename F, typename F4>
+__global__ void __launch_bounds__(kBatch) far_order_kernel(FarArgs A) {
+    using S = FarShape<P, F4>;
+    extern __shared__ float4 fbuf[];  // 2 stages of S::kStage units, then 2 x kK centres
+    double4* ctr = (double4*)(fbuf + 2 * S::kStage);
     const int64_t b = blockIdx.x;
-    if (b >= *nbat) return;  // uniform per block
-    const int64_t q = batch_first[b] + threadIdx.x;
-    const bool ok = q < batch_first[b + 1];
-    const bool live = batch_first[b] + (threadIdx.x & ~31) < batch_first[b + 1];  // uniform per warp
-    const double4 x = ok ? tgt_sorted[q] : make_double4(0, 0, 0, 0);
+    if (b >= *A.nbat) return;  // uniform per block
+    const int64_t f0 = A.far_off[b], f1 = min(f0 + (int64_t)A.far_cnt[b], A.far_cap);
+    if (f0 >= f1) return;  // uniform per block
+    const int64_t q0 = A.batch_first[b], qe = A.batch_first[b + 1];
+    const int64_t q = q0 + threadIdx.x;
+    const bool live = q0 + (int64_t)(threadIdx.x & ~31) < qe;  // warp-uniform
+    const double4 x = q < qe ? A.tgt_sorted[q] : make_double4(0, 0, 1, 0);
     double acc[3] = {0, 0, 0};
-    const int64_t f0 = far_off[b];
-    const int64_t f1 = min(f0 + (int64_t)far_cnt[b], far_cap);
-    if (f0 < f1) far_gather(far_list[f0], B64, B32, n_ent, gtab, ct, f64_from, sbuf);
-    for (int64_t f = f0; f < f1; ++f) {
-        cp_async_commit_wait();
-        __syncthreads();  // entry f is in buffer (f - f0) & 1; the other buffer is free
-        const int2 ent = far_list[f];
-        if (f + 1 < f1)
-            far_gather(far_list[f + 1], B64, B32, n_ent, gtab, ct, f64_from,
-                       sbuf + (size_t)((f + 1 - f0) & 1) * buf_terms);
-        const int P = ent.y;
-        if (P <= 0 || !live) continue;  // P <= 0: summed directly by the near kernel
-        const double4* cur = sbuf + (size_t)((f - f0) & 1) * buf_terms;
-        const double4 c = node_ctr[ent.x];
-        if (P >= f64_from)
-            far_dispatch<double, double4>(P, cur, x, c, acc);
-        else
-            far_dispatch<float, float4>(P, (const float4*)cur, x, c, acc);
+    far_stage_gather<P, F4>(A, f0, (int)min((int64_t)S::kK, f1 - f0), fbuf, ctr);
+    cp_async_commit();
+    int s = 0;
+    for (int64_t s0 = f0;; s ^= 1) {
+        const int n = (int)min((int64_t)S::kK, f1 - s0);
+        const int64_t s1 = s0 + n;
+        if (s1 < f1)
+            far_stage_gather<P, F4>(A, s1, (int)min((int64_t)S::kK, f1 - s1), fbuf + (size_t)(s ^ 1) * S::kStage,
+                                    ctr + (s ^ 1) * S::kK);
+        cp_async_commit();
+        cp_async_wait_prev();
+        __syncthreads();  // stage s resident
+        if (live) {
+            const F4* Bc = (const F4*)(fbuf + (size_t)s * S::kStage);
+            const double4* cs = ctr + s * S::kK;
+            for (int k = 0; k < n; ++k)
+                far_one_acc<P, F, F4>(Bc + (size_t)k * entries_for(P), x, cs[k].x, cs[k].y, cs[k].z, acc);
+        }
+        if (s1 >= f1) break;
+        __syncthreads();  // stage s consumed before it is refilled
+        s0 = s1;
     }
-    if (ok) {
-        V[q] = acc[0];
-        V[n_tgt + q] = acc[1];
-        V[2 * n_tgt + q] = acc[2];
+    if (q < qe) {
+        A.V[q] += acc[0];
+        A.V[A.n_tgt + q] += acc[1];
+        A.V[2 * A.n_tgt + q] += acc[2];
+    }
+}
+
+typedef void (*FarKernelFn)(FarArgs);
+
+template <int P>
+FarKernelFn far_kernel_for(bool f64, size_t* smem) {
+    if (f64) {
+        *smem = FarShape<P, double4>::kSmem;
+        return far_order_kernel<P, double, double4>;
+    }
+    *smem = FarShape<P, float4>::kSmem;
+    return far_order_kernel<P, float, float4>;
+}
+
+// The order-P far kernel (FP64 or FP32 arithmetic) and its dynamic shared memory.
+FarKernelFn far_kernel_select(int P, bool f64, size_t* smem) {
+    switch (P) {
+        case 1: return far_kernel_for<1>(f64, smem);
+        case 2: return far_kernel_for<2>(f64, smem);
+        case 3: return far_kernel_for<3>(f64, smem);
+        case 4: return far_kernel_for<4>(f64, smem);
+        case 5: return far_kernel_for<5>(f64, smem);
+        case 6: return far_kernel_for<6>(f64, smem);
+        case 7: return far_kernel_for<7>(f64, smem);
+        case 8: return far_kernel_for<8>(f64, smem);
+        case 9: return far_kernel_for<9>(f64, smem);
+        case 10: return far_kernel_for<10>(f64, smem);
+        case 11: return far_kernel_for<11>(f64, smem);
+        default: return far_kernel_for<12>(f64, smem);
     }
 }
 
@@ -690,7 +787,7 @@ __global__ void sample_pairs_kernel(const int32_t* __restrict__ far_off, const i
     if (blockIdx.x == 0 && threadIdx.x == 0) *n_pairs = (int32_t)np;
     const int nb = *nbat;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < np; k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t f = k * stride;
+        const int64_t f = far_off[0] + k * stride;  // far_off: the sampled order's row
         int lo = 0, hi = nb;  // last batch with far_off <= f (the one whose range holds f)
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
@@ -823,9 +920,6 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
                                                             const int32_t* __restrict__ near_off,
                                                             const int32_t* __restrict__ near_cnt,
                                                             const int2* __restrict__ near_list, int64_t near_cap,
-                                                            const int32_t* __restrict__ far_off,
-                                                            const int32_t* __restrict__ far_cnt,
-                                                            const int2* __restrict__ far_list, int64_t far_cap,
                                                             const float4* __restrict__ src32,
                                                             const double* __restrict__ V, double mult,
                                                             double* __restrict__ U) {
@@ -841,8 +935,7 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
     const float tx1 = (float)x1.x, ty1 = (float)x1.y, tz1 = (float)x1.z;
     double D0[3] = {0, 0, 0}, D1[3] = {0, 0, 0};
     const int64_t n0 = near_off[b], n1 = min(n0 + (int64_t)near_cnt[b], near_cap);
-    const int64_t f0 = far_off[b], f1 = min(f0 + (int64_t)far_cnt[b], far_cap);
-    const int64_t n_near = n1 - n0, n_all = n_near + (f1 - f0);
+    const int64_t n_all = n1 - n0;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int64_t c0 = 0; c0 < n_all; c0 += kNearRuns) {
         // resolve up to kNearRuns entries into source ranges and their prefix offsets
@@ -853,17 +946,9 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
             len[h] = 0;
             st[h] = 0;
             if (k < n_all) {
-                if (k < n_near) {
-                    const int2 r = near_list[n0 + k];
-                    st[h] = t.node_start[t.leaf_node[r.x]];
-                    len[h] = t.node_end[t.leaf_node[r.y]] - st[h];
-                } else {
-                    const int2 ent = far_list[f0 + (k - n_near)];
-                    if (ent.y <= 0) {
-                        st[h] = t.node_start[ent.x];
-                        len[h] = t.node_end[ent.x] - st[h];
-                    }
-                }
+                const int2 r = near_list[n0 + k];
+                st[h] = t.node_start[t.leaf_node[r.x]];
+                len[h] = t.node_end[t.leaf_node[r.y]] - st[h];
             }
         }
         // exclusive scan of the 2 x 64 lengths (two warps)
@@ -921,6 +1006,7 @@ void canonical_entries(int pm, std::vector<int4>& ent) {
 
 // Cost model: an order-P expansion costs ~8 E(P) + 40 flops per target (twice that in FP64), a
 // direct pair 17; a cluster with fewer sources than this is cheaper to sum directly.
+
 static int32_t direct_cutoff(int P, int f64_from) {
     return (int32_t)((P >= f64_from ? 2.0 : 1.0) * (8.0 * entries_for(P) + 40.0) / 17.0);
 }
@@ -975,6 +1061,20 @@ struct TreeSolver {
     float* mlp_norm = nullptr;
     std::vector<void*> allocs;
 };
+
+// Dynamic shared memory of every far kernel above 48 KB needs the opt-in attribute.
+static cudaError_t far_smem_attributes() {
+    for (int P = 1; P <= kPMax; ++P)
+        for (int f64 = 0; f64 < 2; ++f64) {
+            size_t smem = 0;
+            FarKernelFn fn = far_kernel_select(P, f64 != 0, &smem);
+            if (smem > 48 * 1024) {
+                const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
+            }
+        }
+    return cudaSuccess;
+}
 
 namespace {
 
@@ -1125,9 +1225,10 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->ent, ent.size()));
     A(talloc(t, &t->mono, mono.size()));
     A(talloc(t, &t->gtab, gtab.size()));
-    A(talloc(t, &t->far_cnt, (size_t)t->n_batches + 1));
+    const size_t far_rows = (size_t)(kPMax + 1) * ((size_t)t->n_batches + 1);  // order-bucketed rows
+    A(talloc(t, &t->far_cnt, far_rows));
     A(talloc(t, &t->near_cnt, (size_t)t->n_batches + 1));
-    A(talloc(t, &t->far_off, (size_t)t->n_batches + 1));
+    A(talloc(t, &t->far_off, far_rows));
     A(talloc(t, &t->near_off, (size_t)t->n_batches + 1));
     A(talloc(t, &t->flags, 8));
     A(talloc(t, &t->pair_counts, 3));
@@ -1143,20 +1244,17 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
         e = cudaMemcpy(t->gtab, gtab.data(), gtab.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(t->node_mom, 0, nn * cd * cd * cd * sizeof(double));
     // the count arrays carry one extra zero entry so that their exclusive scans also yield the totals
-    if (e == cudaSuccess) e = cudaMemset(t->far_cnt, 0, ((size_t)t->n_batches + 1) * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(t->far_cnt, 0, far_rows * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMemset(t->near_cnt, 0, ((size_t)t->n_batches + 1) * sizeof(int32_t));
     if (e != cudaSuccess) {
         tree_solver_destroy(t);
         return cuda_status(e, "tree solver allocation");
     }
     {
-        const size_t smem = 2 * (size_t)entries_for(t->pm) * sizeof(double4);
-        if (smem > 48 * 1024) {
-            cudaError_t ea = cudaFuncSetAttribute(far_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (ea != cudaSuccess) {
-                tree_solver_destroy(t);
-                return cuda_status(ea, "cudaFuncSetAttribute (far_kernel)");
-            }
+        const cudaError_t ea = far_smem_attributes();
+        if (ea != cudaSuccess) {
+            tree_solver_destroy(t);
+            return cuda_status(ea, "cudaFuncSetAttribute (far_kernel)");
         }
     }
     rc = alloc_lists(t, std::max<int64_t>(t->n_batches * 256, 1024), std::max<int64_t>(t->n_batches * 64, 1024));
@@ -1188,6 +1286,7 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     A.order = t->solver.order;
     A.direct_below = t->ct.direct_below[t->solver.order];
     A.far_cnt = t->far_cnt;
+    A.nb1 = t->n_batches + 1;
     A.near_cnt = t->near_cnt;
     A.far_off = t->far_off;
     A.near_off = t->near_off;
@@ -1205,7 +1304,7 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     LPM_CUDA_TRY(cudaMemsetAsync(t->pair_counts, 0, 3 * sizeof(unsigned long long), ctx->stream));
     const unsigned g = grid_for(t->n_batches, 4);
     LPM_LAUNCH(ctx, "traverse_kernel", traverse_kernel, g, 128, 0, A);
-    int rc = scan_exclusive_i32(ctx, t->far_cnt, t->far_off, t->n_batches + 1, t->flags + 2);
+    int rc = scan_exclusive_i32(ctx, t->far_cnt, t->far_off, (int64_t)(kPMax + 1) * (t->n_batches + 1), t->flags + 2);
     if (rc) return rc;
     rc = scan_exclusive_i32(ctx, t->near_cnt, t->near_off, t->n_batches + 1, t->flags + 3);
     if (rc) return rc;
@@ -1284,15 +1383,38 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
                t->tcount + 1, t->tgt_sorted, t->batch_ctr);
     rc = build_lists(t, can_sync);
     if (rc) return rc;
-    const int buf_terms = entries_for(t->pm);
-    const size_t smem = 2 * (size_t)buf_terms * sizeof(double4);  // attribute raised at creation
-    LPM_LAUNCH(ctx, "far_kernel", far_kernel, (unsigned)t->n_batches, kBatch, smem, t->tgt_sorted, n_tgt,
-               t->batch_first, t->tcount + 1, t->far_off, t->far_cnt, t->far_list, t->far_cap, t->node_ctr, t->B64,
-               t->B32, t->n_ent, t->gtab, t->ct, buf_terms, t->f64_from, t->V);
+    // far field: one launch per order present (only the fixed order, or the selector's orders 1..11),
+    // each adding its bucket's contributions to V
+    LPM_CUDA_TRY(cudaMemsetAsync(t->V, 0, 3 * (size_t)n_tgt * sizeof(double), ctx->stream));
+    {
+        const int64_t nb1 = t->n_batches + 1;
+        const bool sel = t->learned && t->mlp_loaded;
+        const int p_lo = sel ? 1 : t->solver.order, p_hi = sel ? std::min(t->pm, kMlpDirectClass) : t->solver.order;
+        for (int P = p_lo; P <= p_hi; ++P) {
+            FarArgs F{};
+            F.tgt_sorted = t->tgt_sorted;
+            F.n_tgt = n_tgt;
+            F.batch_first = t->batch_first;
+            F.nbat = t->tcount + 1;
+            F.far_off = t->far_off + (size_t)P * nb1;
+            F.far_cnt = t->far_cnt + (size_t)P * nb1;
+            F.far_list = t->far_list;
+            F.far_cap = t->far_cap;
+            F.node_ctr = t->node_ctr;
+            F.B64 = t->B64;
+            F.B32 = t->B32;
+            F.n_ent = t->n_ent;
+            F.gtab = t->gtab + t->ct.table_off[P];
+            F.V = t->V;
+            size_t smem = 0;
+            FarKernelFn fn = far_kernel_select(P, P >= t->f64_from, &smem);
+            LPM_LAUNCH(ctx, "far_kernel", fn, (unsigned)t->n_batches, kBatch, smem, F);
+        }
+    }
     const double mult = -1.0 / (4.0 * kPi * t->kernel.radius);
     LPM_LAUNCH(ctx, "near_kernel", near_kernel, (unsigned)t->n_batches, kNearThreads, 0, t->st, t->tgt_sorted, n_tgt,
                t->tperm, t->batch_first, t->tcount + 1, t->near_off, t->near_cnt, t->near_list, t->near_cap,
-               t->far_off, t->far_cnt, t->far_list, t->far_cap, t->src32, t->V, mult, U);
+               t->src32, t->V, mult, U);
     if (can_sync) return tree_check(t);
     return LPM_OK;
 }
@@ -1430,7 +1552,8 @@ int tree_sample_labels(TreeSolver* t, const double4* src, const double4* tgt, in
     if (rc) return rc;
     int32_t* dlab = (int32_t*)bl.p;
     int32_t* np_dev = dlab + max_pairs;  // count stored after the labels
-    LPM_LAUNCH(ctx, "sample_pairs_kernel", sample_pairs_kernel, 64, 256, 0, t->far_off, t->tcount + 1, t->far_list,
+    LPM_LAUNCH(ctx, "sample_pairs_kernel", sample_pairs_kernel, 64, 256, 0,
+               t->far_off + (size_t)t->solver.order * (t->n_batches + 1), t->tcount + 1, t->far_list,
                t->far_cap, t->flags + 2, stride, max_pairs, (int2*)bp.p, np_dev);
     const size_t smem = (size_t)entries_for(max_order) * sizeof(double4);
     if (smem > 48 * 1024)
