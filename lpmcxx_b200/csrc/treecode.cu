@@ -358,9 +358,11 @@ struct TraverseArgs {
     const double* node_wabs;
     const __nv_bfloat16* mlp_w;
     const float* mlp_norm;
+    uint8_t* decisions;  // n_batches x kDecisionCap selector classes (count pass writes, fill pass reads)
 };
 
 constexpr int kWarpStack = 1024;
+constexpr int kDecisionCap = 1024;  // cached selector decisions per batch
 
 // ---------------------------------------------------------------------------------- learned order
 // Per node: log10 radius, log10 sum|w|, log10 of the Frobenius norms of the degree-2/4/6 moment tensors
@@ -451,7 +453,7 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
     int size = 1;
     if (lane == 0) st[0] = 0;
     __syncwarp();
-    int nnear = 0;
+    int nnear = 0, ndec = 0;
     unsigned long long far_pairs = 0, near_pairs = 0, far_terms = 0;
     const int64_t noff = A.fill ? A.near_off[b] : 0;
     while (size > 0) {
@@ -460,24 +462,42 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
         __syncwarp();
         size -= m;
         int kind = 0, nch = 0, lo = 0, hi = 0, cnt = 0, fc = 0, P = A.order;
+        double4 c = make_double4(0, 0, 0, 0);
+        int s = 0, e = 0, nc = 0;
+        bool far_ok = false;
         if (node >= 0) {
-            const double4 c = A.node_ctr[node];
-            const int s = t.node_start[node], e = t.node_end[node];
+            c = A.node_ctr[node];
+            s = t.node_start[node];
+            e = t.node_end[node];
             const double dx = bc.x - c.x, dy = bc.y - c.y, dz = bc.z - c.z;
             const double R = sqrt(dx * dx + dy * dy + dz * dz);
-            bool far_ok = R > bc.w && c.w < A.theta * (R - bc.w);
-            const int nc = t.node_nchild[node];
-            int cut = A.direct_below;
-            if (far_ok && A.learned) {
-                // the selector's order; "no order meets the budget" opens a cluster large enough to be
-                // worth opening and sums a leaf or a small cluster directly
+            far_ok = R > bc.w && c.w < A.theta * (R - bc.w);
+            nc = t.node_nchild[node];
+        }
+        int cut = A.direct_below;
+        if (A.learned) {  // uniform per launch
+            // the selector's order; "no order meets the budget" opens a cluster large enough to be worth
+            // opening and sums a leaf or a small cluster directly.  The count pass caches each batch's
+            // first kDecisionCap decisions (in visiting order) for the fill pass.
+            const unsigned okm = __ballot_sync(full, far_ok);
+            const int idx = ndec + __popc(okm & lt);
+            ndec += __popc(okm);
+            uint8_t* dec = A.decisions + (size_t)b * kDecisionCap;
+            int cls = -1;
+            if (far_ok && A.fill && idx < kDecisionCap) cls = dec[idx];
+            if (far_ok && cls < 0) {
                 float f[kMlpIn];
                 pair_features(bc, c, A.node_feat + (size_t)node * kMlpIn, log_s, f);
-                const int cls = mlp_argmax_bf16(mw, mnorm, f);
+                cls = mlp_argmax_bf16(mw, mnorm, f);
+                if (!A.fill && idx < kDecisionCap) dec[idx] = (uint8_t)cls;
+            }
+            if (far_ok) {
                 P = cls == kMlpDirectClass ? 0 : min(cls + 1, A.max_order);
                 cut = P > 0 ? A.ct.direct_below[P] : 0x7fffffff;
                 if (P == 0 && nc > 0 && e - s >= A.ct.direct_below[A.max_order]) far_ok = false;
             }
+        }
+        if (node >= 0) {
             if (far_ok && e - s >= cut) {
                 kind = 1;
             } else if (far_ok || nc == 0) {
@@ -1059,6 +1079,7 @@ struct TreeSolver {
     float* node_feat = nullptr;
     __nv_bfloat16* mlp_w = nullptr;
     float* mlp_norm = nullptr;
+    uint8_t* decisions = nullptr;  // selector decisions of the count pass, reused by the fill pass
     std::vector<void*> allocs;
 };
 
@@ -1237,6 +1258,7 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
         A(talloc(t, &t->node_feat, nn * kMlpIn));
         A(talloc(t, &t->mlp_w, kMlpParams));
         A(talloc(t, &t->mlp_norm, 2 * kMlpIn));
+        A(talloc(t, &t->decisions, (size_t)t->n_batches * kDecisionCap));
     }
     if (e == cudaSuccess) e = cudaMemcpy(t->ent, ent.data(), ent.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(t->mono, mono.data(), mono.size() * sizeof(int4), cudaMemcpyHostToDevice);
@@ -1301,6 +1323,7 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     A.node_wabs = t->node_wabs;
     A.mlp_w = t->mlp_w;
     A.mlp_norm = t->mlp_norm;
+    A.decisions = t->decisions;
     LPM_CUDA_TRY(cudaMemsetAsync(t->pair_counts, 0, 3 * sizeof(unsigned long long), ctx->stream));
     const unsigned g = grid_for(t->n_batches, 4);
     LPM_LAUNCH(ctx, "traverse_kernel", traverse_kernel, g, 128, 0, A);
