@@ -181,16 +181,20 @@ typedef struct lpm_solver_desc {
     double tolerance;     /* LPM_ORDER_LEARNED: per-pair error budget relative to |mult| * sum|w| (0 = 2e-8) */
 } lpm_solver_desc;
 
-/* ---- treecode (TreeSum).  Biot-Savart on the unit sphere (radius 1, delta 0).  The far field expands
+/* ---- treecode (TreeSum).  Biot-Savart on the unit sphere (radius 1, delta 0): the far field expands
  * 1/|x-y|^2 (equal to 1/(2(1 - x.y)) on the sphere) about each cluster's centre to Taylor order p
- * (|k| < p) and accepts (target batch, cluster) pairs with rho < theta (|x_batch - c| - r_batch); see
- * treecode.cu.  A reusable solver object for fixed sizes: */
+ * (|k| < p, the reference's SumNode convention).  3D Poisson 1/(4 pi r) (LPM_KERNEL_POISSON_3D, points in
+ * [-1, 1]^3): the far field expands 1/|x-y| to order p with |k| <= p (the reference's TaylorSeries3d
+ * convention, src/LpmTaylorSeries3d.cpp:16-50), coincident pairs excluded; the learned order is
+ * Biot-Savart only.  Both accept (target batch, cluster) pairs with rho < theta (|x_batch - c| - r_batch);
+ * see treecode.cu.  A reusable solver object for fixed sizes: */
 typedef struct lpm_treesum lpm_treesum;
 int lpm_treesum_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver, int64_t n_src,
                        int64_t n_tgt, lpm_treesum** out);
 int lpm_treesum_destroy(lpm_treesum* ts);
-/* Device arrays: src n_src x 4 (x,y,z,w), tgt n_tgt x 4, out 3 x n_tgt (component-major).  Replaces
- * TreeSum::computeMeshMoments + meshSolve (src/LpmTreeSum.cpp:55-86,182-197) for device-resident data. */
+/* Device arrays: src n_src x 4 (x,y,z,w), tgt n_tgt x 4, out 3 x n_tgt (component-major; Poisson:
+ * 1 x n_tgt).  Replaces TreeSum::computeMeshMoments + meshSolve (src/LpmTreeSum.cpp:55-86,182-197) for
+ * device-resident data. */
 int lpm_treesum_eval_dev(lpm_treesum* ts, const double* src, const double* tgt, double* out);
 /* Statistics of the last evaluation, 10 values: nodes, leaves, depth, far (batch, cluster) pairs, near
  * leaf ranges, target batches, overflow flags, far-field (target, cluster) evaluations, near-field

@@ -102,12 +102,14 @@ __global__ void gather_sources_kernel(const double4* __restrict__ X, const int32
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) out[q] = X[perm[q]];
 }
 
-// Leaves: centre (mean position), radius, FP32 source copies (w pre-scaled by 2) and ordinary moments
+// Leaves: centre (mean position), radius, FP32 source copies (w scaled by wscale: 2 folds the factor of
+// 1/(1 - x.y) = 2/|x - y|^2 of the sphere kernel into the strength) and ordinary moments
 // mom[a][b][c] = sum_j w_j h^(a,b,c) for a+b+c <= pm.
 __global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* __restrict__ src, int pm,
                                                        const int4* __restrict__ mono, int n_mono,
                                                        double4* __restrict__ node_ctr, double* __restrict__ node_wabs,
-                                                       double* __restrict__ node_mom, float4* __restrict__ src32) {
+                                                       double* __restrict__ node_mom, float4* __restrict__ src32,
+                                                       double wscale) {
     __shared__ double sh[32];
     __shared__ double pw[32][3][kPMax + 1];
     __shared__ double ww[32];
@@ -129,7 +131,7 @@ __global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* 
             const double4 p = src[q];
             const double hx = p.x - cx, hy = p.y - cy, hz = p.z - cz;
             r = fmax(r, sqrt(hx * hx + hy * hy + hz * hz));
-            src32[q] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)(2.0 * p.w));
+            src32[q] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)(wscale * p.w));
         }
         r = block_max(r, sh);
         if (threadIdx.x == 0) {
@@ -275,6 +277,40 @@ __global__ void coeff_kernel(Octree t, int pm, const int4* __restrict__ ent, int
             const double4 v = make_double4(pre * n0, pre * n1, pre * n2, pre * n3);
             B64[(size_t)node * n_ent + i] = v;
             B32[(size_t)node * n_ent + i] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
+        }
+    }
+}
+
+// Scalar far-field coefficients of the 1/|x - y| kernel (Gegenbauer index 1/2), order-pm Horner layout,
+// rows padded to `stride` entries.  With d = c - x, e = d/|d|^2, s = 1/|d|^2 and r = y - c:
+//   sum_j w_j / |x - y_j| = (1/|d|) sum_{m,k} A_{m,k} e^k s^m,
+//   A_{m,k} = (-1)^(m+|k|) g(|k|+m) 2^|k| / k! sum_{|j|=m} M_{k+2j} / j!,  g(n) = Gamma(n+1/2)/Gamma(1/2),
+// from the generating function 1/sqrt(1 - 2 t u + u^2) = sum_n C_n^(1/2)(t) u^n.
+__global__ void coeff_scalar_kernel(Octree t, int pm, const int4* __restrict__ ent, int n_ent, int stride,
+                                    const double* __restrict__ node_mom, double* __restrict__ A64,
+                                    float* __restrict__ A32) {
+    const int nn = t.counters[1];
+    const int cd = cube_dim(pm);
+    for (int node = blockIdx.x; node < nn; node += gridDim.x) {
+        const double* mom = node_mom + (size_t)node * cd * cd * cd;
+        for (int i = threadIdx.x; i < stride; i += blockDim.x) {
+            double v = 0.0;
+            if (i < n_ent) {
+                const int4 mk = ent[i];  // (m, a, b, c)
+                const int m = mk.x, a = mk.y, b = mk.z, c = mk.w, q = a + b + c;
+                double n0 = 0;
+                for (int j0 = 0; j0 <= m; ++j0)
+                    for (int j1 = 0; j1 <= m - j0; ++j1) {
+                        const int j2 = m - j0 - j1;
+                        n0 += mom[((a + 2 * j0) * cd + b + 2 * j1) * cd + c + 2 * j2] /
+                              (c_fact[j0] * c_fact[j1] * c_fact[j2]);
+                    }
+                double g = 1.0;  // Gamma(q+m+1/2) / Gamma(1/2)
+                for (int k = 0; k < q + m; ++k) g *= (double)k + 0.5;
+                v = (((m + q) & 1) ? -1.0 : 1.0) * g * (double)(1ull << q) / (c_fact[a] * c_fact[b] * c_fact[c]) * n0;
+            }
+            A64[(size_t)node * stride + i] = v;
+            A32[(size_t)node * stride + i] = (float)v;
         }
     }
 }
@@ -765,6 +801,124 @@ __global__ void __launch_bounds__(kBatch) far_order_kernel(FarArgs A) {
     }
 }
 
+// The Horner scheme of `horner` with scalar coefficients.
+template <int P, typename T>
+__device__ __forceinline__ T horner1(const T* __restrict__ Bc, T e0, T e1, T e2, T s) {
+    int q = 0;
+    T G = 0;
+#pragma unroll
+    for (int m = (P - 1) / 2; m >= 0; --m) {
+        const int Q = P - 2 * m;
+        T Pp = 0;
+#pragma unroll
+        for (int a = Q - 1; a >= 0; --a) {
+            T Qq = 0;
+#pragma unroll
+            for (int b = Q - 1 - a; b >= 0; --b) {
+                T R = 0;
+#pragma unroll
+                for (int c = Q - 1 - a - b; c >= 0; --c) R = fma(R, e2, Bc[q++]);
+                Qq = fma(Qq, e1, R);
+            }
+            Pp = fma(Pp, e0, Qq);
+        }
+        G = fma(G, s, Pp);
+    }
+    return G;
+}
+
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+
+// Far field of the scalar 1/|x - y| kernel at order P (= pm; degree < P): one block per target batch,
+// one thread per target; each entry's contiguous coefficient row (stride entries, 16-byte aligned) is
+// staged with cp.async, kK entries per stage, double-buffered.  Adds sum w/|x - y| to V[q].
+template <int P, typename F>
+__global__ void __launch_bounds__(kBatch) far_scalar_kernel(FarArgs A, int stride) {
+    constexpr int kE = entries_for(P);
+    constexpr int kUnits = (kE * (int)sizeof(F) + 15) / 16;
+    constexpr int kK = kUnits >= kFarStageUnits ? 1 : (kFarStageUnits / kUnits > 32 ? 32 : kFarStageUnits / kUnits);
+    extern __shared__ float4 fbuf[];  // 2 stages of kK x kUnits units, then 2 x kK centres
+    double4* ctr = (double4*)(fbuf + 2 * kK * kUnits);
+    const int64_t b = blockIdx.x;
+    if (b >= *A.nbat) return;  // uniform per block
+    const int64_t f0 = A.far_off[b], f1 = min(f0 + (int64_t)A.far_cnt[b], A.far_cap);
+    if (f0 >= f1) return;  // uniform per block
+    const int64_t q0 = A.batch_first[b], qe = A.batch_first[b + 1];
+    const int64_t q = q0 + threadIdx.x;
+    const bool live = q0 + (int64_t)(threadIdx.x & ~31) < qe;  // warp-uniform
+    const double4 x = q < qe ? A.tgt_sorted[q] : make_double4(2, 2, 2, 0);
+    const F* base = (const F*)(sizeof(F) == 8 ? (const void*)A.B64 : (const void*)A.B32);
+    auto gather = [&](int64_t s0, int n, float4* buf, double4* cs) {
+        for (int i = threadIdx.x; i < n * kUnits; i += kBatch) {
+            const int e = i / kUnits, j = i - e * kUnits;
+            cp_async16(buf + i, (const char*)(base + (size_t)A.far_list[s0 + e].x * stride) + 16 * j);
+        }
+        if ((int)threadIdx.x < n) cs[threadIdx.x] = A.node_ctr[A.far_list[s0 + threadIdx.x].x];
+    };
+    double acc = 0.0;
+    gather(f0, (int)min((int64_t)kK, f1 - f0), fbuf, ctr);
+    cp_async_commit();
+    int sb = 0;
+    for (int64_t s0 = f0;; sb ^= 1) {
+        const int n = (int)min((int64_t)kK, f1 - s0);
+        const int64_t s1 = s0 + n;
+        if (s1 < f1) gather(s1, (int)min((int64_t)kK, f1 - s1), fbuf + (size_t)(sb ^ 1) * kK * kUnits, ctr + (sb ^ 1) * kK);
+        cp_async_commit();
+        cp_async_wait_prev();
+        __syncthreads();  // stage sb resident
+        if (live) {
+            const float4* buf = fbuf + (size_t)sb * kK * kUnits;
+            const double4* cs = ctr + sb * kK;
+            for (int k = 0; k < n; ++k) {
+                const F dx = (F)(cs[k].x - x.x), dy = (F)(cs[k].y - x.y), dz = (F)(cs[k].z - x.z);
+                const F rinv = rsqrt_t(dx * dx + dy * dy + dz * dz);
+                const F s2 = rinv * rinv;
+                acc += (double)(rinv * horner1<P, F>((const F*)(buf + (size_t)k * kUnits), dx * s2, dy * s2, dz * s2, s2));
+            }
+        }
+        if (s1 >= f1) break;
+        __syncthreads();  // stage sb consumed before it is refilled
+        s0 = s1;
+    }
+    if (q < qe) A.V[q] += acc;
+}
+
+typedef void (*FarScalarFn)(FarArgs, int);
+
+template <int P>
+FarScalarFn far_scalar_for(bool f64, size_t* smem) {
+    constexpr int kE = entries_for(P);
+    auto sm = [](int bytes) {
+        const int units = (kE * bytes + 15) / 16;
+        const int k = units >= kFarStageUnits ? 1 : (kFarStageUnits / units > 32 ? 32 : kFarStageUnits / units);
+        return 2 * (size_t)k * units * 16 + 2 * (size_t)k * sizeof(double4);
+    };
+    if (f64) {
+        *smem = sm(8);
+        return far_scalar_kernel<P, double>;
+    }
+    *smem = sm(4);
+    return far_scalar_kernel<P, float>;
+}
+
+FarScalarFn far_scalar_select(int P, bool f64, size_t* smem) {
+    switch (P) {
+        case 1: return far_scalar_for<1>(f64, smem);
+        case 2: return far_scalar_for<2>(f64, smem);
+        case 3: return far_scalar_for<3>(f64, smem);
+        case 4: return far_scalar_for<4>(f64, smem);
+        case 5: return far_scalar_for<5>(f64, smem);
+        case 6: return far_scalar_for<6>(f64, smem);
+        case 7: return far_scalar_for<7>(f64, smem);
+        case 8: return far_scalar_for<8>(f64, smem);
+        case 9: return far_scalar_for<9>(f64, smem);
+        case 10: return far_scalar_for<10>(f64, smem);
+        case 11: return far_scalar_for<11>(f64, smem);
+        default: return far_scalar_for<12>(f64, smem);
+    }
+}
+
 typedef void (*FarKernelFn)(FarArgs);
 
 template <int P>
@@ -933,6 +1087,33 @@ __device__ __forceinline__ void finish_target(int64_t q, int64_t qe, int64_t n_t
 // A batch's near work is the concatenation of its source ranges (runs of consecutive leaves, then
 // clusters whose order was set to "direct"); it is streamed through shared memory in tiles of
 // kNearStreamTile sources regardless of how short the individual ranges are.
+// One tile of the scalar 1/r stream: D += sum_j w_j / |x - y_j| (FP32 within the tile, FP64 across
+// tiles); a source at the target's own position (r = 0) contributes nothing.
+__device__ __forceinline__ void near_tile_scalar(const float4* tile, int m, float tx0, float ty0, float tz0,
+                                                 float tx1, float ty1, float tz1, double* D0, double* D1) {
+    float a = 0.f, c = 0.f;
+#pragma unroll 4
+    for (int j = 0; j < m; ++j) {
+        const float4 y = tile[j];
+        const float dx = tx0 - y.x, dy = ty0 - y.y, dz = tz0 - y.z;
+        const float rr = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        a = fmaf(y.w, rr > 0.f ? rsqrtf(rr) : 0.f, a);
+        const float ex = tx1 - y.x, ey = ty1 - y.y, ez = tz1 - y.z;
+        const float ss = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+        c = fmaf(y.w, ss > 0.f ? rsqrtf(ss) : 0.f, c);
+    }
+    D0[0] += a;
+    D1[0] += c;
+}
+
+__device__ __forceinline__ void finish_target_scalar(int64_t q, int64_t qe, const double* D,
+                                                     const int32_t* __restrict__ tperm, const double* __restrict__ V,
+                                                     double mult, double* __restrict__ U) {
+    if (q >= qe) return;
+    U[tperm[q]] = mult * (V[q] + D[0]);
+}
+
+template <bool kScalar>
 __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const double4* __restrict__ tgt_sorted,
                                                             int64_t n_tgt, const int32_t* __restrict__ tperm,
                                                             const int32_t* __restrict__ batch_first,
@@ -1004,11 +1185,19 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
                 tile[j] = src32[r_start[lo] + (p - r_pre[lo])];
             }
             __syncthreads();
-            near_tile(tile, m, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
+            if constexpr (kScalar)
+                near_tile_scalar(tile, m, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
+            else
+                near_tile(tile, m, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
         }
     }
-    finish_target(q0, qe, n_tgt, x0, D0, tperm, V, mult, U);
-    finish_target(q1, qe, n_tgt, x1, D1, tperm, V, mult, U);
+    if constexpr (kScalar) {
+        finish_target_scalar(q0, qe, D0, tperm, V, mult, U);
+        finish_target_scalar(q1, qe, D1, tperm, V, mult, U);
+    } else {
+        finish_target(q0, qe, n_tgt, x0, D0, tperm, V, mult, U);
+        finish_target(q1, qe, n_tgt, x1, D1, tperm, V, mult, U);
+    }
 }
 
 // host-side tables --------------------------------------------------------------------------------
@@ -1027,7 +1216,9 @@ void canonical_entries(int pm, std::vector<int4>& ent) {
 // Cost model: an order-P expansion costs ~8 E(P) + 40 flops per target (twice that in FP64), a
 // direct pair 17; a cluster with fewer sources than this is cheaper to sum directly.
 
-static int32_t direct_cutoff(int P, int f64_from) {
+static int32_t direct_cutoff(int P, int f64_from, bool scalar) {
+    // scalar 1/r: 2 flops per coefficient + ~12 of setup against 11 per direct pair
+    if (scalar) return (int32_t)((P >= f64_from ? 2.0 : 1.0) * (2.0 * entries_for(P) + 12.0) / 11.0);
     return (int32_t)((P >= f64_from ? 2.0 : 1.0) * (8.0 * entries_for(P) + 40.0) / 17.0);
 }
 
@@ -1042,6 +1233,11 @@ struct TreeSolver {
     int32_t* bflag = nullptr;
     int32_t* batch_first = nullptr;
     int pm = 8;
+    int order = 8;         // the fixed order in the internal convention (degree < order)
+    bool scalar = false;   // the 1/(4 pi r) kernel (else Biot-Savart on the sphere)
+    int a_stride = 0;      // scalar kernel: coefficient row length (padded to 4 entries)
+    double* A64 = nullptr;  // scalar kernel: coefficient rows (FP64, FP32)
+    float* A32 = nullptr;
     int f64_from = kF64From;  // far expansions of order >= f64_from evaluate in FP64
     Octree st;
     // target ordering
@@ -1149,13 +1345,22 @@ int upload_constants() {
 int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_solver_desc& solver, int64_t n_src,
                        int64_t n_tgt, TreeSolver** out) {
     *out = nullptr;
-    if (kernel.kind != LPM_KERNEL_BIOT_SAVART_SPHERE || kernel.radius != 1.0 || kernel.delta != 0.0) {
-        set_error("tree solver: only the singular Biot-Savart kernel on the unit sphere is supported");
+    const bool scalar = kernel.kind == LPM_KERNEL_POISSON_3D;
+    if (!scalar && (kernel.kind != LPM_KERNEL_BIOT_SAVART_SPHERE || kernel.radius != 1.0 || kernel.delta != 0.0)) {
+        set_error("tree solver: supports the singular Biot-Savart kernel on the unit sphere and the 3D Poisson kernel");
         return LPM_ERR_KERNEL;
     }
-    if (solver.order < 1 || solver.order > kPMax || solver.max_per_leaf < 1 || !(solver.theta > 0.0) ||
-        solver.theta >= 1.0 || n_src >= INT32_MAX || n_tgt >= INT32_MAX) {
-        set_error("tree solver: need 1 <= order <= %d, max_per_leaf >= 1, 0 < theta < 1", kPMax);
+    // Biot-Savart: order p = multi-indices |k| < p (the reference's SumNode); Poisson: |k| <= p (the
+    // reference's TaylorSeries3d convention), i.e. internal order p + 1
+    const int order = scalar ? solver.order + 1 : solver.order;
+    if (order < 1 || order > kPMax || solver.max_per_leaf < 1 || !(solver.theta > 0.0) || solver.theta >= 1.0 ||
+        n_src >= INT32_MAX || n_tgt >= INT32_MAX) {
+        set_error("tree solver: need 1 <= order <= %d (Poisson: 0 <= order <= %d), max_per_leaf >= 1, 0 < theta < 1",
+                  kPMax, kPMax - 1);
+        return LPM_ERR_ARG;
+    }
+    if (scalar && solver.order_policy == LPM_ORDER_LEARNED) {
+        set_error("tree solver: the learned order selector is trained for the Biot-Savart kernel only");
         return LPM_ERR_ARG;
     }
     int rc = upload_constants();
@@ -1167,23 +1372,28 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     t->solver = solver;
     t->n_src = n_src;
     t->n_tgt = n_tgt;
+    t->scalar = scalar;
+    t->order = order;
     t->learned = solver.order_policy == LPM_ORDER_LEARNED;
     // the selector picks orders up to kMlpDirectClass (11); the fixed order is its fallback
-    t->pm = t->learned ? std::max(kMlpDirectClass, solver.order) : solver.order;
+    t->pm = t->learned ? std::max(kMlpDirectClass, order) : order;
     if (t->learned && solver.tolerance > 0.0) t->eps = solver.tolerance;
     // FP32 far field by default: its rounding stays ~1e-7 relative, below the truncation error of the
     // orders used; LPM_PREC_F64 evaluates every far expansion in FP64
     t->f64_from = solver.precision == LPM_PREC_F64 ? 1 : kPMax + 1;
-    // about 4.7 * 4^L cells of level L meet the unit sphere.  L is the level whose cells hold ~kBatch
-    // targets (the capacity is sized for it); batches are cut at the cells of the next coarser level,
-    // so that the thinly populated cells the sphere only grazes merge with their Morton neighbours
-    // and batches run fuller (measured: ~20% less far + near time at 2M targets).
+    // about 4.7 * 4^L cells of level L meet the unit sphere (Biot-Savart); volume data (Poisson) fill up
+    // to 8^L.  L is the level whose cells hold ~kBatch targets (the capacity is sized for it); batches
+    // are cut at the cells of the next coarser level, so that the thinly populated cells the sphere only
+    // grazes merge with their Morton neighbours and batches run fuller (measured: ~20% less far + near
+    // time at 2M targets on the sphere).
     {
+        const double grow = scalar ? 8.0 : 4.0, occ = scalar ? 1.0 : 4.7;
         int L = 1;
-        while (L < kTreeDepth && 4.7 * std::pow(4.0, L + 1) * kBatch <= 1.5 * (double)n_tgt) ++L;
+        while (L < kTreeDepth && occ * std::pow(grow, L + 1) * kBatch <= 1.5 * (double)n_tgt) ++L;
         t->batch_level = std::max(1, L - 1);
         t->batch_level_max = L;
-        const int64_t cells = std::min<int64_t>(std::max<int64_t>(n_tgt, 1), (int64_t)(8.0 * std::pow(4.0, L)) + 64);
+        const double cells_at_l = scalar ? std::pow(8.0, L) : 8.0 * std::pow(4.0, L);
+        const int64_t cells = std::min<int64_t>(std::max<int64_t>(n_tgt, 1), (int64_t)cells_at_l + 64);
         t->n_batches = (n_tgt + kBatch - 1) / kBatch + cells;
     }
     rc = octree_alloc(t->st, std::max<int64_t>(n_src, 1), solver.max_per_leaf, kTreeDepth);
@@ -1221,7 +1431,7 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     // a cluster is cheaper to sum directly when its far-field work per target (8 flops per coefficient
     // plus ~40 of setup, at FP64 or FP32 rate) exceeds ~17 flops per direct pair at the FP32 rate
     for (int P = 0; P <= kPMax; ++P)
-        t->ct.direct_below[P] = direct_cutoff(P, t->f64_from);
+        t->ct.direct_below[P] = direct_cutoff(P, t->f64_from, t->scalar);
     cudaError_t e = cudaSuccess;
     auto A = [&](cudaError_t r) {
         if (e == cudaSuccess) e = r;
@@ -1241,8 +1451,14 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->node_ctr, nn));
     A(talloc(t, &t->node_wabs, nn));
     A(talloc(t, &t->node_mom, nn * cd * cd * cd));
-    A(talloc(t, &t->B64, nn * t->n_ent));
-    A(talloc(t, &t->B32, nn * t->n_ent));
+    if (scalar) {
+        t->a_stride = (t->n_ent + 3) & ~3;  // 16-byte aligned rows in FP32 and FP64
+        A(talloc(t, &t->A64, nn * t->a_stride));
+        A(talloc(t, &t->A32, nn * t->a_stride));
+    } else {
+        A(talloc(t, &t->B64, nn * t->n_ent));
+        A(talloc(t, &t->B32, nn * t->n_ent));
+    }
     A(talloc(t, &t->ent, ent.size()));
     A(talloc(t, &t->mono, mono.size()));
     A(talloc(t, &t->gtab, gtab.size()));
@@ -1305,8 +1521,8 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     A.nbat = t->tcount + 1;
     A.n_batches = t->n_batches;
     A.theta = t->solver.theta;
-    A.order = t->solver.order;
-    A.direct_below = t->ct.direct_below[t->solver.order];
+    A.order = t->order;
+    A.direct_below = t->ct.direct_below[t->order];
     A.far_cnt = t->far_cnt;
     A.nb1 = t->n_batches + 1;
     A.near_cnt = t->near_cnt;
@@ -1361,7 +1577,7 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     const bool can_sync = cap == cudaStreamCaptureStatusNone;
     if (n_tgt == 0) return LPM_OK;
     if (n_src == 0) {
-        LPM_CUDA_TRY(cudaMemsetAsync(U, 0, 3 * (size_t)n_tgt * sizeof(double), ctx->stream));
+        LPM_CUDA_TRY(cudaMemsetAsync(U, 0, (t->scalar ? 1 : 3) * (size_t)n_tgt * sizeof(double), ctx->stream));
         return LPM_OK;
     }
     LPM_CUDA_TRY(cudaMemsetAsync(t->flags, 0, 8 * sizeof(int32_t), ctx->stream));
@@ -1379,12 +1595,16 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
                t->src_sorted);
     const unsigned gl = (unsigned)std::max<int64_t>(1, std::min<int64_t>(t->st.node_cap, 16 * ctx->num_sms));
     LPM_LAUNCH(ctx, "leaf_p2m_kernel", leaf_p2m_kernel, gl, 128, 0, t->st, t->src_sorted, t->pm, t->mono, t->n_mono,
-               t->node_ctr, t->node_wabs, t->node_mom, t->src32);
+               t->node_ctr, t->node_wabs, t->node_mom, t->src32, t->scalar ? 1.0 : 2.0);
     for (int l = kTreeDepth - 1; l >= 0; --l)
         LPM_LAUNCH(ctx, "m2m_level_kernel", m2m_level_kernel, gl, 128, 0, t->st, l, t->pm, t->mono, t->n_mono,
                    t->node_ctr, t->node_wabs, t->node_mom);
-    LPM_LAUNCH(ctx, "coeff_kernel", coeff_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->node_mom, t->B64,
-               t->B32);
+    if (t->scalar)
+        LPM_LAUNCH(ctx, "coeff_kernel", coeff_scalar_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->a_stride,
+                   t->node_mom, t->A64, t->A32);
+    else
+        LPM_LAUNCH(ctx, "coeff_kernel", coeff_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->node_mom, t->B64,
+                   t->B32);
     if (t->learned)
         LPM_LAUNCH(ctx, "node_feature_kernel", node_feature_kernel, gl, 128, 0, t->st, t->pm, t->node_ctr,
                    t->node_wabs, t->node_mom, t->node_feat);
@@ -1412,7 +1632,7 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     {
         const int64_t nb1 = t->n_batches + 1;
         const bool sel = t->learned && t->mlp_loaded;
-        const int p_lo = sel ? 1 : t->solver.order, p_hi = sel ? std::min(t->pm, kMlpDirectClass) : t->solver.order;
+        const int p_lo = sel ? 1 : t->order, p_hi = sel ? std::min(t->pm, kMlpDirectClass) : t->order;
         for (int P = p_lo; P <= p_hi; ++P) {
             FarArgs F{};
             F.tgt_sorted = t->tgt_sorted;
@@ -1430,14 +1650,25 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
             F.gtab = t->gtab + t->ct.table_off[P];
             F.V = t->V;
             size_t smem = 0;
-            FarKernelFn fn = far_kernel_select(P, P >= t->f64_from, &smem);
-            LPM_LAUNCH(ctx, "far_kernel", fn, (unsigned)t->n_batches, kBatch, smem, F);
+            if (t->scalar) {
+                F.B64 = (const double4*)t->A64;
+                F.B32 = (const float4*)t->A32;
+                FarScalarFn fs = far_scalar_select(P, P >= t->f64_from, &smem);
+                LPM_LAUNCH(ctx, "far_kernel", fs, (unsigned)t->n_batches, kBatch, smem, F, t->a_stride);
+            } else {
+                FarKernelFn fn = far_kernel_select(P, P >= t->f64_from, &smem);
+                LPM_LAUNCH(ctx, "far_kernel", fn, (unsigned)t->n_batches, kBatch, smem, F);
+            }
         }
     }
-    const double mult = -1.0 / (4.0 * kPi * t->kernel.radius);
-    LPM_LAUNCH(ctx, "near_kernel", near_kernel, (unsigned)t->n_batches, kNearThreads, 0, t->st, t->tgt_sorted, n_tgt,
-               t->tperm, t->batch_first, t->tcount + 1, t->near_off, t->near_cnt, t->near_list, t->near_cap,
-               t->src32, t->V, mult, U);
+    if (t->scalar)
+        LPM_LAUNCH(ctx, "near_kernel", near_kernel<true>, (unsigned)t->n_batches, kNearThreads, 0, t->st, t->tgt_sorted,
+                   n_tgt, t->tperm, t->batch_first, t->tcount + 1, t->near_off, t->near_cnt, t->near_list, t->near_cap,
+                   t->src32, t->V, 1.0 / (4.0 * kPi), U);
+    else
+        LPM_LAUNCH(ctx, "near_kernel", near_kernel<false>, (unsigned)t->n_batches, kNearThreads, 0, t->st,
+                   t->tgt_sorted, n_tgt, t->tperm, t->batch_first, t->tcount + 1, t->near_off, t->near_cnt,
+                   t->near_list, t->near_cap, t->src32, t->V, -1.0 / (4.0 * kPi * t->kernel.radius), U);
     if (can_sync) return tree_check(t);
     return LPM_OK;
 }
@@ -1510,7 +1741,7 @@ int tree_set_param(TreeSolver* t, const char* name, double value) {
         t->batch_level = (int)value;
     } else if (n == "f64_from" && value >= 1.0 && value <= kPMax + 1 && value == std::floor(value)) {
         t->f64_from = (int)value;
-        for (int P = 1; P <= kPMax; ++P) t->ct.direct_below[P] = direct_cutoff(P, t->f64_from);
+        for (int P = 1; P <= kPMax; ++P) t->ct.direct_below[P] = direct_cutoff(P, t->f64_from, t->scalar);
     } else {
         set_error("tree_set_param: unknown parameter or value out of range: %s = %g", name, value);
         return LPM_ERR_ARG;
@@ -1566,17 +1797,17 @@ int tree_sample_labels(TreeSolver* t, const double4* src, const double4* tgt, in
     LPM_CUDA_TRY(cudaMalloc(&bl.p, ((size_t)max_pairs + 1) * sizeof(int32_t)));
     LPM_CUDA_TRY(cudaMalloc(&be.p, (size_t)max_pairs * max_order * sizeof(float)));
     const bool had = t->mlp_loaded;
-    const int32_t keep = t->ct.direct_below[t->solver.order];
+    const int32_t keep = t->ct.direct_below[t->order];
     t->mlp_loaded = false;
-    t->ct.direct_below[t->solver.order] = 1;
+    t->ct.direct_below[t->order] = 1;
     int rc = tree_velocity(t, src, t->n_src, tgt, t->n_tgt, (double*)bu.p);
-    t->ct.direct_below[t->solver.order] = keep;
+    t->ct.direct_below[t->order] = keep;
     t->mlp_loaded = had;
     if (rc) return rc;
     int32_t* dlab = (int32_t*)bl.p;
     int32_t* np_dev = dlab + max_pairs;  // count stored after the labels
     LPM_LAUNCH(ctx, "sample_pairs_kernel", sample_pairs_kernel, 64, 256, 0,
-               t->far_off + (size_t)t->solver.order * (t->n_batches + 1), t->tcount + 1, t->far_list,
+               t->far_off + (size_t)t->order * (t->n_batches + 1), t->tcount + 1, t->far_list,
                t->far_cap, t->flags + 2, stride, max_pairs, (int2*)bp.p, np_dev);
     const size_t smem = (size_t)entries_for(max_order) * sizeof(double4);
     if (smem > 48 * 1024)

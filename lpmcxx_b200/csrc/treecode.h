@@ -10,8 +10,9 @@ struct TreeSolver;
 int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_solver_desc& solver, int64_t n_src,
                        int64_t n_tgt, TreeSolver** out);
 void tree_solver_destroy(TreeSolver* t);
-// Velocity (3 x n_tgt, component-major) at targets tgt[0:n_tgt] from sources src[0:n_src] (x, y, z, w).
-// Targets may coincide with sources (their self pair contributes nothing).
+// Velocity (3 x n_tgt, component-major; Biot-Savart) or potential (1 x n_tgt; Poisson 1/(4 pi r)) at
+// targets tgt[0:n_tgt] from sources src[0:n_src] (x, y, z, w).  Targets may coincide with sources (their
+// self pair contributes nothing).
 int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double4* tgt, int64_t n_tgt, double* U);
 // Synchronises and reports capacity overflows of the last evaluation (LPM_ERR_CAPACITY).
 int tree_check(TreeSolver* t);

@@ -69,3 +69,22 @@ def rh_wave_mesh(kind: str, level: int):
     mesh = build_mesh(kind, level)
     p, n_src = particles(mesh, rossby_haurwitz_4(mesh.face_xyz))
     return mesh, p, n_src
+
+
+def splitmix64_uniform(n: int, seed: int) -> np.ndarray:
+    """n doubles in [0, 1) from the splitmix64 generator (Steele, Lea & Flood, OOPSLA 2014): state
+    s_i = seed + i * 0x9E3779B97F4A7C15 (i = 1, 2, ...), output mixed by two xor-shift-multiply rounds,
+    top 53 bits scaled by 2^-53."""
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + np.arange(1, n + 1, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def poisson_cube(n: int = 1_048_576, seed: int = 0x2B) -> np.ndarray:
+    """(n, 4) points uniform in [-1, 1]^3 with charges uniform in [-1, 1] (x, y, z, q consecutive draws
+    of one splitmix64 stream): the 3D Poisson workload."""
+    u = splitmix64_uniform(4 * n, seed).reshape(n, 4)
+    return 2.0 * u - 1.0

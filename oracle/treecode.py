@@ -44,3 +44,76 @@ def direct_velocity_sum(x: np.ndarray, y: np.ndarray, w: np.ndarray) -> np.ndarr
     """sum_j w_j (x cross y_j)/(1 - x.y_j) (the reference kernel, without the -1/(4 pi) multiplier)."""
     den = 1.0 - y @ x
     return (np.cross(x, y) * (w / den)[:, None]).sum(axis=0)
+
+
+# ------------------------------------------------------------------------------------------------------
+# 3D Poisson kernel 1/|x - y|.  Two independent restatements of its truncated Taylor series about a
+# cluster centre c (total degree in h = y - c at most p, the TaylorSeries3d convention |k| <= p of
+# src/LpmTaylorSeries3d.cpp:16-50):
+#   (1) the Gegenbauer form: with d = c - x, 1/|d + h| = (1/|d|) sum_n C_n^(1/2)(t) (|h|/|d|)^n,
+#       t = -(d.h)/(|d||h|), C_n^(1/2) the Legendre polynomials, expanded per term (what the CUDA
+#       coefficient kernel implements after summing over the sources);
+#   (2) the Cartesian Taylor coefficients a_k = (1/k!) D_y^k (1/|x - y|) at y = c from the recurrence of
+#       Lindsay & Krasny (J. Comput. Phys. 172, 2001) / Duan & Krasny, with R = x - c:
+#       |k| |R|^2 a_k - (2|k| - 1) sum_i R_i a_{k - e_i} + (|k| - 1) sum_i a_{k - 2 e_i} = 0, a_0 = 1/|R|,
+#       contracted with the ordinary moments M_k = sum_j w_j h_j^k.
+
+
+def _gegenbauer_half_coef(q: int, m: int) -> float:
+    """(-1)^m Gamma(q + m + 1/2) / (Gamma(1/2) m! q!) 2^q: the coefficient of t^q u^(q + 2m) in
+    1/sqrt(1 - 2 t u + u^2) = sum_n C_n^(1/2)(t) u^n."""
+    g = 1.0
+    for k in range(q + m):
+        g *= k + 0.5
+    from math import factorial
+
+    return (-1) ** m * g / (factorial(m) * factorial(q)) * 2.0 ** q
+
+
+def potential_series_gegenbauer(x: np.ndarray, y: np.ndarray, w: np.ndarray, c: np.ndarray, p: int) -> float:
+    """sum_j w_j [1/|x - y_j|]_p via the Gegenbauer (Legendre) form, term by term per source."""
+    d = c - x
+    h = y - c
+    dd = d @ d
+    dh = h @ d
+    hh = np.einsum("ij,ij->i", h, h)
+    total = np.zeros(y.shape[0])
+    for m in range(0, p // 2 + 1):
+        for q in range(0, p - 2 * m + 1):
+            # t^q u^n = (-(d.h))^q |h|^(2m) / |d|^(2q + 2m) with n = q + 2m
+            total += _gegenbauer_half_coef(q, m) * (-dh) ** q * hh ** m / dd ** (q + m)
+    return float((w * total).sum() / np.sqrt(dd))
+
+
+def _multi_indices(p: int):
+    return [(a, b, n - a - b) for n in range(p + 1) for a in range(n, -1, -1) for b in range(n - a, -1, -1)]
+
+
+def potential_series_recurrence(x: np.ndarray, y: np.ndarray, w: np.ndarray, c: np.ndarray, p: int) -> float:
+    """sum_{|k| <= p} a_k(x - c) M_k with the Lindsay-Krasny recurrence for a_k."""
+    R = x - c
+    RR = R @ R
+    a = {(0, 0, 0): 1.0 / np.sqrt(RR)}
+    for k in _multi_indices(p)[1:]:
+        n = sum(k)
+        s1 = 0.0
+        s2 = 0.0
+        for i in range(3):
+            km = list(k)
+            km[i] -= 1
+            if km[i] >= 0:
+                s1 += R[i] * a[tuple(km)]
+            km[i] -= 1
+            if km[i] >= 0:
+                s2 += a[tuple(km)]
+        a[k] = ((2 * n - 1) * s1 - (n - 1) * s2) / (n * RR)
+    h = y - c
+    total = 0.0
+    for k, ak in a.items():
+        total += ak * (w * h[:, 0] ** k[0] * h[:, 1] ** k[1] * h[:, 2] ** k[2]).sum()
+    return float(total)
+
+
+def direct_potential_sum(x: np.ndarray, y: np.ndarray, w: np.ndarray) -> float:
+    """sum_j w_j / |x - y_j| (without the 1/(4 pi) multiplier)."""
+    return float((w / np.linalg.norm(y - x, axis=1)).sum())

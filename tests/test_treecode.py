@@ -84,3 +84,60 @@ def test_tree_rejects_unsupported_kernels(ctx):
         L.TreeSum(ctx, L.biot_savart_kernel(1.0, 0.1), L.tree_solver(), 10, 10)
     with pytest.raises(L.LpmError):
         L.TreeSum(ctx, L.biot_savart_kernel(), L.tree_solver(order=13), 10, 10)
+
+
+# ---------------------------------------------------------------------------------- 3D Poisson 1/r
+def test_poisson_series_two_restatements_agree_and_converge():
+    from oracle.treecode import direct_potential_sum, potential_series_gegenbauer, potential_series_recurrence
+
+    rng = np.random.default_rng(4)
+    y = rng.uniform(-0.1, 0.1, (300, 3)) + np.array([0.3, 0.2, -0.1])
+    w = rng.uniform(-1.0, 1.0, 300)
+    c = y.mean(0)
+    x = np.array([0.9, -0.4, 0.5])
+    exact = direct_potential_sum(x, y, w)
+    errs = []
+    for p in (2, 4, 6, 8, 10):
+        g = potential_series_gegenbauer(x, y, w, c, p)
+        r = potential_series_recurrence(x, y, w, c, p)
+        assert abs(g - r) <= 1e-13 * abs(exact)
+        errs.append(abs(g - exact) / abs(exact))
+    assert all(a > b for a, b in zip(errs, errs[1:])) and errs[-1] < 1e-9
+
+
+def test_splitmix64_stream():
+    # first outputs of splitmix64 from seed 0 (0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, ...) scaled by 2^-64
+    u = W.splitmix64_uniform(2, 0)
+    assert u[0] == (0xE220A8397B1DCDAF >> 11) * 2.0 ** -53
+    assert u[1] == (0x6E789E6AA1B965F4 >> 11) * 2.0 ** -53
+    p = W.poisson_cube(1000)
+    assert p.shape == (1000, 4) and p.min() >= -1.0 and p.max() < 1.0
+
+
+def gpu_poisson_tree_vs_direct(ctx, n, order, theta, max_leaf, prec=L.LPM_PREC_F32):
+    torch = ctx.use_torch_stream()
+    p = W.poisson_cube(n)
+    d = torch.tensor(p, device="cuda")
+    ref = torch.empty((1, n), dtype=torch.float64, device="cuda")
+    ctx.direct_sum_dev(L.poisson_kernel(), L.LPM_PREC_F64, d, d, ref)
+    ts = L.TreeSum(ctx, L.poisson_kernel(), L.tree_solver(prec, order, max_leaf, theta), n, n)
+    out = torch.empty((1, n), dtype=torch.float64, device="cuda")
+    ts.eval(d, d, out)
+    st = ts.stats()
+    ts.close()
+    return float(torch.linalg.norm(out - ref) / torch.linalg.norm(ref)), st
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order,theta,tol", [(6, 0.6, 2e-4), (10, 0.5, 2e-6)])
+def test_poisson_treecode_against_fp64_direct(ctx, order, theta, tol):
+    err, st = gpu_poisson_tree_vs_direct(ctx, 200_000, order, theta, 256)
+    assert st["far_evals"] > 0 and st["near_pairs"] > 0
+    assert err < tol, err
+
+
+@pytest.mark.gpu
+def test_poisson_treecode_fp64_far_field_matches_fp32(ctx):
+    e32, _ = gpu_poisson_tree_vs_direct(ctx, 100_000, 8, 0.5, 256, L.LPM_PREC_F32)
+    e64, _ = gpu_poisson_tree_vs_direct(ctx, 100_000, 8, 0.5, 256, L.LPM_PREC_F64)
+    assert abs(e32 - e64) < 0.1 * e64 + 1e-7
