@@ -345,6 +345,64 @@ def run_gpu_poisson(args) -> None:
     print(json.dumps(out_line))
 
 
+ENSEMBLE_METRIC = "ensemble RK4 steps/s: 64 instances (icos L5/L6/L7/L8 x 16, 27.85M sources), learned treecode"
+
+
+def run_gpu_ensemble(args) -> None:
+    """The ensemble configuration: 64 Biot-Savart RK4 instances of uneven sizes; a step advances every
+    instance by one RK4 step (one replay of the ensemble's graph)."""
+    import torch
+
+    import lpmcxx_b200 as L
+    import lpmcxx_b200.workloads as W
+    from lpmcxx_b200 import learned
+
+    local = env_int("LOCAL_RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    torch.cuda.set_device(local)
+    inst = W.ensemble_instances()
+    ctx = L.Context(local)
+    p_, theta, leaf = TREE_SETTINGS["tree_learned"]
+    solver = L.tree_solver(L.LPM_PREC_F32, p_, leaf, theta, learned=True, tolerance=LEARNED_EPS)
+    ens = L.Ensemble(ctx, L.biot_savart_kernel(), solver, [n for _, _, n in inst], [p.shape[0] for _, p, _ in inst],
+                     lanes=args.lanes)
+    ens.set_mlp(learned.load()[0])
+    for i, (_, p, _) in enumerate(inst):
+        ens.instance(i).set_state(p)
+    dt = 0.01
+    ens.step(dt, args.warmup, use_graph=True)
+    torch.cuda.synchronize()
+    launches0 = ctx.launch_count
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    clocks = ClockSampler(local).start()
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ens.step(dt, 1, use_graph=True)  # synchronous: replays on the ensemble's stream, waits for it
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    launches = ctx.launch_count - launches0
+    value = world * args.steps / (sum(ms) * 1e-3)
+    n_total = int(sum(p.shape[0] for _, p, _ in inst))
+    out = {
+        "metric": ENSEMBLE_METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": float(np.mean(ms)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"64 instances: icos L5/L6/L7/L8 x 16, RH m=4 + seeded Gaussian, {n_total:,} particles",
+                   "solver": f"learned treecode theta={theta}, {leaf} per leaf, budget {LEARNED_EPS}",
+                   "lanes": args.lanes, "dt": dt, "graph": "one CUDA graph replay per ensemble step"},
+        "particle_steps_per_s": value * n_total, "gpu_launches": launches, "clocks": clk,
+    }
+    ens.close()
+    print(json.dumps(out))
+
+
 def run_gpu(args) -> None:
     import torch
     import torch.distributed as dist
@@ -546,8 +604,10 @@ def main() -> None:
     ap.add_argument("--level", type=int, default=LEVEL)
     ap.add_argument("--dt", type=float, default=DT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="sphere_rk4", choices=["sphere_rk4", "poisson_cube"],
-                    help="sphere_rk4: the Biot-Savart RK4 headline; poisson_cube: the 3D Poisson treecode")
+    ap.add_argument("--workload", default="sphere_rk4", choices=["sphere_rk4", "poisson_cube", "ensemble"],
+                    help="sphere_rk4: the Biot-Savart RK4 headline; poisson_cube: the 3D Poisson treecode; "
+                         "ensemble: 64 uneven RK4 instances")
+    ap.add_argument("--lanes", type=int, default=8, help="ensemble: streams the instances are spread over")
     ap.add_argument("--points", type=int, default=1_048_576, help="poisson_cube: number of points")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -556,6 +616,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload == "poisson_cube":
         run_gpu_poisson(args)
+    elif args.workload == "ensemble":
+        run_gpu_ensemble(args)
     else:
         run_gpu(args)
 

@@ -207,6 +207,9 @@ int lpm_treesum_stats(lpm_treesum* ts, int64_t* out10);
  * LPM_PREC_F64); "batch_level": octree level whose cells a target batch may not straddle (1 .. the
  * level chosen at creation; coarser levels give fuller batches).  Takes effect at the next evaluation. */
 int lpm_treesum_set_param(lpm_treesum* ts, const char* name, double value);
+/* Current value of a run-time parameter: those of lpm_treesum_set_param, plus "batch_level_max" (the finest
+ * batch level allowed) and "order" (the fixed order in the solver's convention: Poisson reports p + 1). */
+int lpm_treesum_get_param(const lpm_treesum* ts, const char* name, double* value);
 
 /* ---- learned Taylor-order selection (no reference counterpart: the reference's TreeSum uses one
  * fixed order).  An MLP (8 -> 64 -> 64 -> 12, GELU) maps the features of an accepted (target batch,
@@ -272,6 +275,20 @@ int lpm_rk4_tree_stats(lpm_rk4* rk, int64_t* out10);
 int lpm_rk4_set_param(lpm_rk4* rk, const char* name, double value);
 /* lpm_treesum_set_mlp for the integrator's treecode; drops a captured step graph (synchronises). */
 int lpm_rk4_set_mlp(lpm_rk4* rk, const float* params);
+
+/* ---- ensembles (no reference counterpart): n_inst independent RK4 problems of uneven sizes advanced
+ * together.  Instances are spread over `lanes` streams (each with its own internal context, assigned
+ * longest-first by an n log n size estimate); after one uncaptured step, each step of every instance is
+ * one replay of a single CUDA graph that forks onto the lanes and joins back.  Instance i is an lpm_rk4
+ * (lpm_ensemble_instance) for setting and reading its state; lpm_ensemble_step is synchronous. */
+typedef struct lpm_ensemble lpm_ensemble;
+int lpm_ensemble_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver, int n_inst,
+                        const int64_t* n_src, const int64_t* n_pts, int lanes, lpm_ensemble** out);
+int lpm_ensemble_destroy(lpm_ensemble* ens);
+int lpm_ensemble_instance(lpm_ensemble* ens, int i, lpm_rk4** rk);
+int lpm_ensemble_lane_of(const lpm_ensemble* ens, int i, int* lane);
+int lpm_ensemble_set_mlp(lpm_ensemble* ens, const float* params);
+int lpm_ensemble_step(lpm_ensemble* ens, double dt, int nsteps, int use_graph);
 
 #ifdef __cplusplus
 }

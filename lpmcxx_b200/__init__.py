@@ -238,6 +238,61 @@ class RK4:
         check(lib().lpm_rk4_set_mlp(self.h, ptr(p)), "lpm_rk4_set_mlp")
 
 
+class _RK4View(RK4):
+    """An ensemble instance: an RK4 whose lifetime the ensemble owns."""
+
+    def __init__(self, ctx, h, n_src, n_pts):
+        self.h, self.ctx, self.n_src, self.n = h, ctx, n_src, n_pts
+
+    def close(self) -> None:
+        self.h = None
+
+
+class Ensemble:
+    """lpm_ensemble: independent RK4 problems of uneven sizes, advanced together by one CUDA graph per
+    step spread over `lanes` streams.  `instance(i)` gives an RK4 handle for states."""
+
+    def __init__(self, ctx: Context, kernel: KernelDesc, solver: _capi.SolverDesc, n_src, n_pts, lanes: int = 8):
+        n_src = np.ascontiguousarray(n_src, dtype=np.int64)
+        n_pts = np.ascontiguousarray(n_pts, dtype=np.int64)
+        h = C.c_void_p()
+        check(lib().lpm_ensemble_create(ctx.h, C.byref(kernel), C.byref(solver), len(n_src), ptr(n_src), ptr(n_pts),
+                                        lanes, C.byref(h)), "lpm_ensemble_create")
+        self.h, self.ctx = h, ctx
+        self.n_src, self.n_pts = n_src, n_pts
+
+    def close(self) -> None:
+        if self.h:
+            lib().lpm_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        return len(self.n_src)
+
+    def instance(self, i: int) -> RK4:
+        r = C.c_void_p()
+        check(lib().lpm_ensemble_instance(self.h, i, C.byref(r)), "lpm_ensemble_instance")
+        return _RK4View(self.ctx, r, int(self.n_src[i]), int(self.n_pts[i]))
+
+    def lane_of(self, i: int) -> int:
+        v = C.c_int()
+        check(lib().lpm_ensemble_lane_of(self.h, i, C.byref(v)), "lpm_ensemble_lane_of")
+        return v.value
+
+    def set_mlp(self, params) -> None:
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        check(lib().lpm_ensemble_set_mlp(self.h, ptr(p)), "lpm_ensemble_set_mlp")
+
+    def step(self, dt: float, nsteps: int = 1, use_graph: bool = True) -> None:
+        check(lib().lpm_ensemble_step(self.h, dt, nsteps, 1 if use_graph else 0), "lpm_ensemble_step")
+
+
 class Tree:
     """Device octree (lpm_tree) over a (n, 4) float64 CUDA tensor of points."""
 
@@ -319,6 +374,12 @@ class TreeSum:
     def set_param(self, name: str, value: float) -> None:
         """Run-time parameter (lpm_treesum_set_param): "theta", "f64_from", "eps" or "batch_level"."""
         check(lib().lpm_treesum_set_param(self.h, name.encode(), float(value)), "lpm_treesum_set_param")
+
+    def get_param(self, name: str) -> float:
+        """Current run-time parameter: as set_param, plus "batch_level_max" and "order"."""
+        v = C.c_double()
+        check(lib().lpm_treesum_get_param(self.h, name.encode(), C.byref(v)), "lpm_treesum_get_param")
+        return v.value
 
     def set_mlp(self, params) -> None:
         """Load the order selector (MLP_PARAMS floats), or None for the fixed-order fallback."""

@@ -1,0 +1,150 @@
+"""Autotuner for the treecode: picks the fastest (leaf size, acceptance theta, batch cell level, and the
+fixed order or the learned selector's per-pair budget) that meets a relative L2 tolerance on a workload.
+
+Accuracy is judged on a random sample of targets against the FP64 direct sum (the library's own
+`lpm_direct_sum_dev`, which is parity-tested against the reference); time is the median of CUDA-event
+timed evaluations on the GPU.  Candidates sharing a leaf size reuse one solver and switch the run-time
+parameters (`TreeSum.set_param`), so a sweep costs one octree allocation per leaf size.
+
+    best = autotune(ctx, L.biot_savart_kernel(), src, tgt, tol=1e-6)
+    solver = tuned_solver(best)            # an lpm_solver_desc for TreeSum / RK4
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import (LPM_KERNEL_POISSON_3D, LPM_PREC_F32, LPM_PREC_F64, Context, KernelDesc, TreeSum, tree_solver)
+from . import learned as _learned  # noqa: F401  (shipped selector weights)
+
+
+@dataclass
+class Candidate:
+    max_per_leaf: int
+    theta: float
+    knob: float            # learned: per-pair budget eps; fixed: Taylor order
+    batch_level: int | None = None
+    ms: float | None = None
+    rel_err: float | None = None
+
+
+@dataclass
+class TuneResult:
+    learned: bool
+    kernel_kind: int
+    best: Candidate | None
+    tried: list = field(default_factory=list)
+
+    def as_dict(self) -> dict:
+        b = self.best
+        return {"learned": self.learned, "max_per_leaf": b.max_per_leaf, "theta": b.theta,
+                ("eps" if self.learned else "order"): b.knob, "batch_level": b.batch_level, "ms": b.ms,
+                "rel_err": b.rel_err}
+
+
+def default_grid(learned: bool, kernel_kind: int):
+    thetas = (0.4, 0.5, 0.6, 0.7)
+    leaves = (256, 512, 1024)
+    if learned:
+        knobs = (1e-8, 2e-8, 4e-8)
+    elif kernel_kind == LPM_KERNEL_POISSON_3D:
+        knobs = (4, 6, 8, 10)
+    else:
+        knobs = (8, 10, 11)
+    return leaves, thetas, knobs
+
+
+def _timed_eval(ctx, ts, src, tgt, out, reps):
+    import torch
+
+    ts.eval(src, tgt, out)  # sizes the interaction lists
+    ms = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ts.eval(src, tgt, out)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return float(np.median(ms))
+
+
+def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bool = True, params=None,
+             grid=None, batch_levels=(0, -1), sample: int = 4096, reps: int = 3, seed: int = 0,
+             safety: float = 0.8) -> TuneResult:
+    """Sweep the grid on device-resident src (n_src, 4) / tgt (n_tgt, 4) float64 tensors.
+
+    tol: relative L2 tolerance over the sampled targets (a candidate must reach safety * tol).
+    learned: tune the learned selector's budget (Biot-Savart only) instead of the fixed order.
+    batch_levels: offsets from each solver's default batch cell level to try (0 = default).
+    """
+    import torch
+
+    kind = int(kernel.kind)
+    if learned and kind == LPM_KERNEL_POISSON_3D:
+        raise ValueError("the learned selector applies to the Biot-Savart kernel only")
+    if learned and params is None:
+        params, _ = _learned.load()
+        if params is None:
+            raise FileNotFoundError("no selector weights shipped; pass params")
+    leaves, thetas, knobs = grid if grid is not None else default_grid(learned, kind)
+    n_src, n_tgt = src.shape[0], tgt.shape[0]
+    comps = 1 if kind == LPM_KERNEL_POISSON_3D else 3
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(n_tgt, size=min(sample, n_tgt), replace=False))
+    idx_t = torch.as_tensor(idx, device=tgt.device)
+    ref = torch.empty((comps, idx.size), dtype=torch.float64, device=tgt.device)
+    ctx.direct_sum_dev(kernel, LPM_PREC_F64, src, tgt[idx_t].contiguous(), ref)
+    ref_norm = float(torch.linalg.norm(ref))
+    out = torch.empty((comps, n_tgt), dtype=torch.float64, device=tgt.device)
+    res = TuneResult(learned=learned, kernel_kind=kind, best=None)
+    for leaf in leaves:
+        base_knob = 10 if learned else int(knobs[0])
+        ts = TreeSum(ctx, kernel, tree_solver(LPM_PREC_F32, base_knob, leaf, thetas[0], learned=learned),
+                     n_src, n_tgt)
+        try:
+            if learned:
+                ts.set_mlp(params)
+            level0 = None
+            for knob in knobs:
+                if not learned and int(knob) != base_knob:
+                    ts.close()
+                    ts = TreeSum(ctx, kernel, tree_solver(LPM_PREC_F32, int(knob), leaf, thetas[0]), n_src, n_tgt)
+                    base_knob = int(knob)
+                for theta in thetas:
+                    ts.set_param("theta", theta)
+                    if learned:
+                        ts.set_param("eps", knob)
+                    for off in batch_levels:
+                        if level0 is None:
+                            level0 = int(ts.get_param("batch_level"))
+                        lvl = level0 + off
+                        if lvl < 1:
+                            continue
+                        ts.set_param("batch_level", lvl)
+                        ms = _timed_eval(ctx, ts, src, tgt, out, reps)
+                        err = float(torch.linalg.norm(out[:, idx_t] - ref)) / ref_norm
+                        c = Candidate(leaf, theta, knob, lvl, ms, err)
+                        res.tried.append(c)
+                        if err <= safety * tol and (res.best is None or ms < res.best.ms):
+                            res.best = c
+                    ts.set_param("batch_level", level0)
+        finally:
+            ts.close()
+    return res
+
+
+def tuned_solver(result: TuneResult, precision: int = LPM_PREC_F32):
+    """lpm_solver_desc of the tuned setting (the batch level is a run-time parameter: apply it with
+    set_param("batch_level", result.best.batch_level) on the TreeSum / RK4 made from this descriptor)."""
+    b = result.best
+    if b is None:
+        raise ValueError("no candidate met the tolerance")
+    if result.learned:
+        return tree_solver(precision, 10, b.max_per_leaf, b.theta, learned=True, tolerance=b.knob)
+    return tree_solver(precision, int(b.knob), b.max_per_leaf, b.theta)
+
+
+__all__ = ["autotune", "tuned_solver", "TuneResult", "Candidate", "default_grid", "LPM_PREC_F64"]

@@ -1,0 +1,257 @@
+// Ensembles: many independent RK4 problems of uneven sizes advanced together.
+//
+// The instances are spread over `lanes` streams, each with its own library context (so concurrently
+// running instances never share scratch memory); a lane runs its instances one after the other.  The
+// assignment is longest-processing-time-first by an n log n size estimate, so that the lanes finish
+// together.  After one uncaptured step (which sizes every buffer), one RK4 step of every instance is
+// captured into a single CUDA graph that forks onto the lanes and joins back, and the graph is replayed
+// once per step: small instances (20k particles) that cannot fill a B200 alone overlap with each other
+// and with the large ones.
+#include "lpm_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <numeric>
+#include <vector>
+
+namespace lpm {
+int rk4_step_enqueue(lpm_rk4* rk, double dt);
+lpm_ctx* rk4_context(lpm_rk4* rk);
+int rk4_tree_check(lpm_rk4* rk);
+int rk4_set_mlp_internal(lpm_rk4* rk, const float* params);
+}  // namespace lpm
+
+using namespace lpm;
+
+struct lpm_ensemble {
+    lpm_ctx* ctx = nullptr;            // the caller's context: its own stream carries the graph
+    std::vector<lpm_ctx*> lanes;       // one context (and stream) per lane
+    std::vector<lpm_rk4*> inst;
+    std::vector<int> lane_of;
+    std::vector<cudaEvent_t> join;     // per lane
+    cudaEvent_t fork = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double graph_dt = 0.0;
+    int64_t graph_nodes = 0;
+    bool warmed = false;
+};
+
+static void ens_drop_graph(lpm_ensemble* e) {
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->exec = nullptr;
+    e->graph = nullptr;
+    e->graph_nodes = 0;
+}
+
+extern "C" int lpm_ensemble_destroy(lpm_ensemble* e) {
+    if (!e) return LPM_OK;
+    cudaSetDevice(e->ctx->device);
+    for (lpm_ctx* c : e->lanes) cudaStreamSynchronize(c->stream);
+    ens_drop_graph(e);
+    for (lpm_rk4* r : e->inst) lpm_rk4_destroy(r);
+    for (cudaEvent_t ev : e->join) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    for (lpm_ctx* c : e->lanes) lpm_ctx_destroy(c);
+    delete e;
+    return LPM_OK;
+}
+
+extern "C" int lpm_ensemble_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver,
+                                   int n_inst, const int64_t* n_src, const int64_t* n_pts, int lanes,
+                                   lpm_ensemble** out) {
+    if (!ctx || !kernel || !solver || !n_src || !n_pts || !out || n_inst < 1 || lanes < 1 || lanes > 64) {
+        set_error("lpm_ensemble_create: bad argument (1 <= lanes <= 64, n_inst >= 1)");
+        return LPM_ERR_ARG;
+    }
+    *out = nullptr;
+    LPM_CUDA_TRY(cudaSetDevice(ctx->device));
+    lpm_ensemble* e = new (std::nothrow) lpm_ensemble();
+    if (!e) return LPM_ERR_OOM;
+    e->ctx = ctx;
+    lanes = std::min(lanes, n_inst);
+    for (int l = 0; l < lanes; ++l) {
+        lpm_ctx* c = nullptr;
+        int rc = lpm_ctx_create(ctx->device, &c);
+        if (rc) {
+            lpm_ensemble_destroy(e);
+            return rc;
+        }
+        e->lanes.push_back(c);
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            lpm_ensemble_destroy(e);
+            return cuda_status(cudaGetLastError(), "cudaEventCreate");
+        }
+        e->join.push_back(ev);
+    }
+    if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) {
+        lpm_ensemble_destroy(e);
+        return cuda_status(cudaGetLastError(), "cudaEventCreate");
+    }
+    // longest processing time first onto the least loaded lane
+    std::vector<int> order(n_inst);
+    std::iota(order.begin(), order.end(), 0);
+    auto cost = [&](int i) { return (double)n_pts[i] * std::log2(2.0 + (double)n_pts[i]); };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    std::vector<double> load(lanes, 0.0);
+    e->lane_of.assign(n_inst, 0);
+    for (int i : order) {
+        const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        e->lane_of[i] = l;
+        load[l] += cost(i);
+    }
+    e->inst.assign(n_inst, nullptr);
+    for (int i = 0; i < n_inst; ++i) {
+        int rc = lpm_rk4_create(e->lanes[e->lane_of[i]], kernel, solver, n_src[i], n_pts[i], &e->inst[i]);
+        if (rc) {
+            lpm_ensemble_destroy(e);
+            return rc;
+        }
+    }
+    *out = e;
+    return LPM_OK;
+}
+
+static int ens_check(lpm_ensemble* e, int i) {
+    if (i < 0 || i >= (int)e->inst.size()) {
+        set_error("ensemble: instance %d out of range", i);
+        return LPM_ERR_ARG;
+    }
+    return LPM_OK;
+}
+
+extern "C" int lpm_ensemble_instance(lpm_ensemble* e, int i, lpm_rk4** rk) {
+    if (!e || !rk) {
+        set_error("lpm_ensemble_instance: null argument");
+        return LPM_ERR_ARG;
+    }
+    int rc = ens_check(e, i);
+    if (rc) return rc;
+    *rk = e->inst[i];
+    return LPM_OK;
+}
+
+extern "C" int lpm_ensemble_set_mlp(lpm_ensemble* e, const float* params) {
+    if (!e) {
+        set_error("lpm_ensemble_set_mlp: null ensemble");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(e->ctx->device));
+    for (lpm_ctx* c : e->lanes) LPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    ens_drop_graph(e);
+    e->warmed = false;
+    for (lpm_rk4* r : e->inst) {
+        int rc = rk4_set_mlp_internal(r, params);
+        if (rc) return rc;
+    }
+    return LPM_OK;
+}
+
+// One step of every instance, each on its lane's current stream.
+static int ens_enqueue(lpm_ensemble* e, double dt) {
+    for (size_t i = 0; i < e->inst.size(); ++i) {
+        int rc = rk4_step_enqueue(e->inst[i], dt);
+        if (rc) return rc;
+    }
+    return LPM_OK;
+}
+
+static int ens_capture(lpm_ensemble* e, double dt) {
+    ens_drop_graph(e);
+    cudaStream_t origin = e->ctx->own_stream;
+    for (lpm_ctx* c : e->lanes) LPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    LPM_CUDA_TRY(cudaStreamSynchronize(origin));
+    std::vector<cudaStream_t> user(e->lanes.size());
+    std::vector<int64_t> before(e->lanes.size());
+    for (size_t l = 0; l < e->lanes.size(); ++l) {
+        user[l] = e->lanes[l]->stream;
+        e->lanes[l]->stream = e->lanes[l]->own_stream;
+        before[l] = e->lanes[l]->launches;
+    }
+    auto restore = [&]() {
+        for (size_t l = 0; l < e->lanes.size(); ++l) {
+            e->lanes[l]->stream = user[l];
+            e->lanes[l]->launches = before[l];
+        }
+    };
+    cudaError_t err = cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal);
+    if (err != cudaSuccess) {
+        restore();
+        return cuda_status(err, "cudaStreamBeginCapture");
+    }
+    int rc = LPM_OK;
+    err = cudaEventRecord(e->fork, origin);
+    for (size_t l = 0; l < e->lanes.size() && err == cudaSuccess; ++l)
+        err = cudaStreamWaitEvent(e->lanes[l]->stream, e->fork, 0);
+    if (err == cudaSuccess) rc = ens_enqueue(e, dt);
+    for (size_t l = 0; l < e->lanes.size() && err == cudaSuccess; ++l) {
+        err = cudaEventRecord(e->join[l], e->lanes[l]->stream);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(origin, e->join[l], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(origin, &g);
+    restore();
+    if (rc || err != cudaSuccess || end != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (rc) return rc;
+        return cuda_status(err != cudaSuccess ? err : end, "ensemble graph capture");
+    }
+    e->graph = g;
+    size_t nodes = 0;
+    LPM_CUDA_TRY(cudaGraphGetNodes(g, nullptr, &nodes));
+    e->graph_nodes = (int64_t)nodes;
+    LPM_CUDA_TRY(cudaGraphInstantiate(&e->exec, g, 0));
+    e->graph_dt = dt;
+    return LPM_OK;
+}
+
+extern "C" int lpm_ensemble_step(lpm_ensemble* e, double dt, int nsteps, int use_graph) {
+    if (!e || nsteps < 0 || !std::isfinite(dt)) {
+        set_error("lpm_ensemble_step: bad argument");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(e->ctx->device));
+    int s = 0;
+    // work the caller enqueued on its stream (states) comes first
+    LPM_CUDA_TRY(cudaStreamSynchronize(e->ctx->stream));
+    if (!use_graph || !e->warmed) {
+        const int n_plain = use_graph ? std::min(nsteps, 1) : nsteps;
+        for (; s < n_plain; ++s) {
+            int rc = ens_enqueue(e, dt);
+            if (rc) return rc;
+        }
+        if (n_plain > 0) e->warmed = true;
+    }
+    if (s < nsteps) {
+        if (!e->exec || e->graph_dt != dt) {
+            int rc = ens_capture(e, dt);
+            if (rc) return rc;
+        }
+        for (lpm_ctx* c : e->lanes) LPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        for (; s < nsteps; ++s) {
+            LPM_CUDA_TRY(cudaGraphLaunch(e->exec, e->ctx->own_stream));
+            e->ctx->launches += e->graph_nodes;
+        }
+        LPM_CUDA_TRY(cudaStreamSynchronize(e->ctx->own_stream));
+    } else {
+        for (lpm_ctx* c : e->lanes) LPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    }
+    // replays cannot grow the treecode's buffers: report an overflow instead of returning wrong data
+    for (lpm_rk4* r : e->inst) {
+        int rc = rk4_tree_check(r);
+        if (rc) return rc;
+    }
+    return LPM_OK;
+}
+
+extern "C" int lpm_ensemble_lane_of(const lpm_ensemble* e, int i, int* lane) {
+    if (!e || !lane || i < 0 || i >= (int)e->inst.size()) {
+        set_error("lpm_ensemble_lane_of: bad argument");
+        return LPM_ERR_ARG;
+    }
+    *lane = e->lane_of[i];
+    return LPM_OK;
+}

@@ -107,6 +107,18 @@ static int rk4_one_step(lpm_rk4* rk, double dt) {
     return LPM_OK;
 }
 
+// One uncaptured-or-captured RK4 step of rk on its context's current stream (for the ensemble).
+int rk4_step_enqueue(lpm_rk4* rk, double dt) { return rk4_one_step(rk, dt); }
+lpm_ctx* rk4_context(lpm_rk4* rk) { return rk->ctx; }
+int rk4_tree_check(lpm_rk4* rk) { return rk->tree ? tree_check(rk->tree) : LPM_OK; }
+int rk4_set_mlp_internal(lpm_rk4* rk, const float* params) {
+    if (!rk->tree) {
+        set_error("ensemble: the instances do not use the treecode");
+        return LPM_ERR_ARG;
+    }
+    return tree_set_mlp(rk->tree, params);
+}
+
 static void drop_graph(lpm_rk4* rk) {
     if (rk->graph_exec) cudaGraphExecDestroy(rk->graph_exec);
     if (rk->graph) cudaGraphDestroy(rk->graph);

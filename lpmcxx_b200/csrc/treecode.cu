@@ -1727,6 +1727,25 @@ int tree_stats(TreeSolver* t, int64_t* out8) {
 
 namespace lpm {
 
+int tree_get_param(const TreeSolver* t, const char* name, double* value) {
+    if (!name || !value) {
+        set_error("tree_get_param: null argument");
+        return LPM_ERR_ARG;
+    }
+    const std::string n(name);
+    if (n == "theta") *value = t->solver.theta;
+    else if (n == "eps") *value = t->eps;
+    else if (n == "f64_from") *value = t->f64_from;
+    else if (n == "batch_level") *value = t->batch_level;
+    else if (n == "batch_level_max") *value = t->batch_level_max;
+    else if (n == "order") *value = t->order;
+    else {
+        set_error("tree_get_param: unknown parameter %s", name);
+        return LPM_ERR_ARG;
+    }
+    return LPM_OK;
+}
+
 int tree_set_param(TreeSolver* t, const char* name, double value) {
     if (!name) {
         set_error("tree_set_param: null name");

@@ -24,6 +24,8 @@ int tree_stats(TreeSolver* t, int64_t* out10);
 // expansions of this order and above evaluate in FP64), "eps" (learned order's per-pair budget), "batch_level" (octree level whose cells target
 // batches may not straddle; 1 .. the level chosen at creation).
 int tree_set_param(TreeSolver* t, const char* name, double value);
+// Current value of a run-time parameter (as tree_set_param, plus "batch_level_max" and "order").
+int tree_get_param(const TreeSolver* t, const char* name, double* value);
 // Learned order: load the selector (LPM_MLP_PARAMS floats, host) or null for the fixed-order fallback.
 int tree_set_mlp(TreeSolver* t, const float* params_host);
 // Learned order: labelled training pairs from one evaluation (see lpm_treesum_sample_labels).

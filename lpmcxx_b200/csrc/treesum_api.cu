@@ -97,6 +97,14 @@ extern "C" int lpm_treesum_sample_labels(lpm_treesum* ts, const double* src, con
                               errs, n_out);
 }
 
+extern "C" int lpm_treesum_get_param(const lpm_treesum* ts, const char* name, double* value) {
+    if (!ts) {
+        set_error("lpm_treesum_get_param: null solver");
+        return LPM_ERR_ARG;
+    }
+    return tree_get_param(ts->solver, name, value);
+}
+
 extern "C" int lpm_tree_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver,
                                  int64_t n_verts, const double* vx, const double* vy, const double* vz, int64_t n_faces,
                                  const double* fx, const double* fy, const double* fz, const double* face_area,

@@ -88,3 +88,26 @@ def poisson_cube(n: int = 1_048_576, seed: int = 0x2B) -> np.ndarray:
     of one splitmix64 stream): the 3D Poisson workload."""
     u = splitmix64_uniform(4 * n, seed).reshape(n, 4)
     return 2.0 * u - 1.0
+
+
+def ensemble_instances(levels=(5, 6, 7, 8), per_level: int = 16, seed: int = 4000):
+    """The ensemble workload: per_level instances on each icosahedral level, each a Rossby-Haurwitz m=4
+    wave plus a Gaussian vortex (amplitude U(0.5, 2) 4 pi, width as gaussian_vortex) at a seeded random
+    centre, minus its area-weighted mean.  Returns [(level, particles (n, 4), n_src)]."""
+    out = []
+    k = 0
+    for level in levels:
+        mesh = build_mesh("icos", level)
+        leaf = mesh.leaf
+        rh = rossby_haurwitz_4(mesh.face_xyz)
+        for _ in range(per_level):
+            rng = np.random.default_rng(seed + k)
+            x0 = rng.normal(size=3)
+            x0 /= np.linalg.norm(x0)
+            amp = rng.uniform(0.5, 2.0) * 4.0 * np.pi
+            zeta = rh + gaussian_vortex(mesh.face_xyz, x0, amp=amp)
+            zeta = zeta - (zeta[leaf] * mesh.face_area[leaf]).sum() / mesh.face_area[leaf].sum()
+            p, n_src = particles(mesh, zeta)
+            out.append((level, p, n_src))
+            k += 1
+    return out

@@ -1,0 +1,53 @@
+"""Autotuner: the chosen setting meets the tolerance against the FP64 direct sum and is the fastest
+candidate that does."""
+import numpy as np
+import pytest
+
+import lpmcxx_b200 as L
+import lpmcxx_b200.workloads as W
+from lpmcxx_b200.autotune import autotune, default_grid, tuned_solver
+
+
+def test_default_grids():
+    leaves, thetas, knobs = default_grid(True, L.LPM_KERNEL_BIOT_SAVART_SPHERE)
+    assert all(0 < t < 1 for t in thetas) and all(k > 0 for k in knobs) and min(leaves) >= 1
+    _, _, orders = default_grid(False, L.LPM_KERNEL_POISSON_3D)
+    assert all(isinstance(o, int) for o in orders)
+
+
+def check(res, tol):
+    ok = [c for c in res.tried if c.rel_err <= 0.8 * tol]
+    assert res.best is not None and res.best in ok
+    assert res.best.ms == min(c.ms for c in ok)
+
+
+@pytest.mark.gpu
+def test_autotune_learned_sphere(ctx):
+    torch = ctx.use_torch_stream()
+    _, p, n_src = W.gaussian_vortex_mesh("icos", 6)
+    d = torch.tensor(p, device="cuda")
+    tol = 1e-6
+    res = autotune(ctx, L.biot_savart_kernel(), d[:n_src], d, tol, learned=True,
+                   grid=((128, 256), (0.5, 0.6), (1e-8, 3e-8)), sample=2048)
+    check(res, tol)
+    # the tuned descriptor reproduces the accuracy on all targets
+    ts = L.TreeSum(ctx, L.biot_savart_kernel(), tuned_solver(res), n_src, p.shape[0])
+    ts.set_mlp(L.learned.load()[0])
+    ts.set_param("batch_level", res.best.batch_level)
+    out = torch.empty((3, p.shape[0]), dtype=torch.float64, device="cuda")
+    ts.eval(d[:n_src], d, out)
+    ts.close()
+    ref = torch.empty_like(out)
+    ctx.direct_sum_dev(L.biot_savart_kernel(), L.LPM_PREC_F64, d[:n_src], d, ref)
+    assert float(torch.linalg.norm(out - ref) / torch.linalg.norm(ref)) < tol
+
+
+@pytest.mark.gpu
+def test_autotune_fixed_poisson(ctx):
+    torch = ctx.use_torch_stream()
+    p = W.poisson_cube(60_000)
+    d = torch.tensor(p, device="cuda")
+    tol = 1e-4
+    res = autotune(ctx, L.poisson_kernel(), d, d, tol, learned=False, grid=((128, 256), (0.5, 0.7), (4, 6)),
+                   batch_levels=(0,), sample=2048)
+    check(res, tol)
