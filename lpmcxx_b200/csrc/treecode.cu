@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* 
                                                        const int4* __restrict__ mono, int n_mono,
                                                        double4* __restrict__ node_ctr, double* __restrict__ node_wabs,
                                                        double* __restrict__ node_mom, float4* __restrict__ src32,
-                                                       double wscale) {
+                                                       double wscale, int heavy_cap) {
     __shared__ double sh[32];
     __shared__ double pw[32][3][kPMax + 1];
     __shared__ double ww[32];
@@ -138,7 +138,9 @@ __global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* 
             node_ctr[node] = make_double4(cx, cy, cz, r);
             node_wabs[node] = wabs;
         }
-        // moments, 32 particles at a time with their power tables in shared memory
+        // moments, 32 particles at a time with their power tables in shared memory (nodes past the
+        // moment capacity get none: the traversal never accepts them as far clusters)
+        if (node >= heavy_cap) continue;  // uniform per block
         double acc[4] = {0, 0, 0, 0};
         for (int q0 = s; q0 < e; q0 += 32) {
             __syncthreads();
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* 
 __global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm, const int4* __restrict__ mono,
                                                         int n_mono, double4* __restrict__ node_ctr,
                                                         double* __restrict__ node_wabs,
-                                                        double* __restrict__ node_mom) {
+                                                        double* __restrict__ node_mom, int heavy_cap) {
     __shared__ double dp[8][3][kPMax + 1];
     const int lb = t.level_range[2 * l], le = t.level_range[2 * l + 1];
     const int cd = cube_dim(pm);
@@ -212,6 +214,11 @@ __global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm,
             const double dx = cc.x - cx, dy = cc.y - cy, dz = cc.z - cz;
             r = fmax(r, sqrt(dx * dx + dy * dy + dz * dz) + cc.w);
         }
+        if (threadIdx.x == 0) {
+            node_ctr[node] = make_double4(cx, cy, cz, r);
+            node_wabs[node] = wabs;
+        }
+        if (fc + nc > heavy_cap) continue;  // uniform per block: a child (numbered after node) has no moments
         __syncthreads();
         if (threadIdx.x < nc * 3) {
             const int k = threadIdx.x / 3, a = threadIdx.x % 3;
@@ -224,10 +231,6 @@ __global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm,
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            node_ctr[node] = make_double4(cx, cy, cz, r);
-            node_wabs[node] = wabs;
-        }
         double* mout = node_mom + (size_t)node * cd * cd * cd;
         for (int term = threadIdx.x; term < n_mono; term += blockDim.x) {
             const int4 kk = mono[term];
@@ -252,8 +255,8 @@ __global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm,
 // Far-field coefficients B^{0..3}_{m,k} of every node in canonical (order-pm Horner) layout.
 __global__ void coeff_kernel(Octree t, int pm, const int4* __restrict__ ent, int n_ent,
                              const double* __restrict__ node_mom, double4* __restrict__ B64,
-                             float4* __restrict__ B32) {
-    const int nn = t.counters[1];
+                             float4* __restrict__ B32, int heavy_cap) {
+    const int nn = min(t.counters[1], heavy_cap);
     const int cd = cube_dim(pm);
     for (int node = blockIdx.x; node < nn; node += gridDim.x) {
         const double* mom = node_mom + (size_t)node * cd * cd * cd;
@@ -288,8 +291,8 @@ __global__ void coeff_kernel(Octree t, int pm, const int4* __restrict__ ent, int
 // from the generating function 1/sqrt(1 - 2 t u + u^2) = sum_n C_n^(1/2)(t) u^n.
 __global__ void coeff_scalar_kernel(Octree t, int pm, const int4* __restrict__ ent, int n_ent, int stride,
                                     const double* __restrict__ node_mom, double* __restrict__ A64,
-                                    float* __restrict__ A32) {
-    const int nn = t.counters[1];
+                                    float* __restrict__ A32, int heavy_cap) {
+    const int nn = min(t.counters[1], heavy_cap);
     const int cd = cube_dim(pm);
     for (int node = blockIdx.x; node < nn; node += gridDim.x) {
         const double* mom = node_mom + (size_t)node * cd * cd * cd;
@@ -395,6 +398,7 @@ struct TraverseArgs {
     const __nv_bfloat16* mlp_w;
     const float* mlp_norm;
     uint8_t* decisions;  // n_batches x kDecisionCap selector classes (count pass writes, fill pass reads)
+    int heavy_cap;       // nodes with moments / coefficients: only these can be far clusters
 };
 
 constexpr int kWarpStack = 1024;
@@ -405,8 +409,8 @@ constexpr int kDecisionCap = 1024;  // cached selector decisions per batch
 // about the centre, log10 count, level (8th slot unused).
 __global__ void node_feature_kernel(Octree t, int pm, const double4* __restrict__ node_ctr,
                                     const double* __restrict__ node_wabs, const double* __restrict__ node_mom,
-                                    float* __restrict__ node_feat) {
-    const int nn = t.counters[1];
+                                    float* __restrict__ node_feat, int heavy_cap) {
+    const int nn = min(t.counters[1], heavy_cap);
     const int cd = cube_dim(pm);
     for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < nn; node += gridDim.x * blockDim.x) {
         const double* mom = node_mom + (size_t)node * cd * cd * cd;
@@ -471,6 +475,7 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
     }
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t b = (int64_t)blockIdx.x * 4 + w;
+    if (A.fill && b == 0 && lane == 0 && A.t.counters[1] > A.heavy_cap) atomicOr(&A.flags[0], 16);
     if (b >= A.n_batches) return;  // uniform per warp
     const Octree& t = A.t;
     const unsigned full = 0xffffffffu, lt = (1u << lane) - 1u;
@@ -507,7 +512,7 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
             e = t.node_end[node];
             const double dx = bc.x - c.x, dy = bc.y - c.y, dz = bc.z - c.z;
             const double R = sqrt(dx * dx + dy * dy + dz * dz);
-            far_ok = R > bc.w && c.w < A.theta * (R - bc.w);
+            far_ok = R > bc.w && c.w < A.theta * (R - bc.w) && node < A.heavy_cap;
             nc = t.node_nchild[node];
         }
         int cut = A.direct_below;
@@ -1239,6 +1244,7 @@ struct TreeSolver {
     double* A64 = nullptr;  // scalar kernel: coefficient rows (FP64, FP32)
     float* A32 = nullptr;
     int f64_from = kF64From;  // far expansions of order >= f64_from evaluate in FP64
+    int heavy_cap = 0;        // nodes the moment / coefficient / feature arrays hold (grown on demand)
     Octree st;
     // target ordering
     uint64_t* tkeys = nullptr;
@@ -1315,6 +1321,29 @@ int alloc_lists(TreeSolver* t, int64_t far_cap, int64_t near_cap) {
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc (interaction lists)");
     t->far_cap = far_cap;
     t->near_cap = near_cap;
+    return LPM_OK;
+}
+
+// Regrow the per-node moment / coefficient / feature arrays to hold `need` nodes (with headroom).
+int heavy_alloc(TreeSolver* t, int64_t need) {
+    const int64_t cap = std::min<int64_t>(t->st.node_cap, need + need / 2 + 256);
+    const int cd = cube_dim(t->pm);
+    auto regrow = [&](auto** p, size_t per_node) -> cudaError_t {
+        if (*p) {
+            cudaFree(*p);
+            t->allocs.erase(std::find(t->allocs.begin(), t->allocs.end(), (void*)*p));
+            *p = nullptr;
+        }
+        return talloc(t, p, (size_t)cap * per_node);
+    };
+    cudaError_t e = regrow(&t->node_mom, (size_t)cd * cd * cd);
+    if (e == cudaSuccess && t->scalar) e = regrow(&t->A64, (size_t)t->a_stride);
+    if (e == cudaSuccess && t->scalar) e = regrow(&t->A32, (size_t)t->a_stride);
+    if (e == cudaSuccess && !t->scalar) e = regrow(&t->B64, (size_t)t->n_ent);
+    if (e == cudaSuccess && !t->scalar) e = regrow(&t->B32, (size_t)t->n_ent);
+    if (e == cudaSuccess && t->learned) e = regrow(&t->node_feat, (size_t)kMlpIn);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc (node moments)");
+    t->heavy_cap = (int)cap;
     return LPM_OK;
 }
 
@@ -1450,14 +1479,18 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->src32, ns));
     A(talloc(t, &t->node_ctr, nn));
     A(talloc(t, &t->node_wabs, nn));
-    A(talloc(t, &t->node_mom, nn * cd * cd * cd));
+    // moments, coefficients and features (~40 KB per node at order 11) are sized for a realistic node
+    // count, not the octree's worst case, and grown by uncaptured evaluations (heavy_alloc)
+    t->heavy_cap = (int)std::min<int64_t>((int64_t)nn, 6 * (std::max<int64_t>(n_src, 1) / solver.max_per_leaf) + 1024);
+    const size_t nh = (size_t)t->heavy_cap;
+    A(talloc(t, &t->node_mom, nh * cd * cd * cd));
     if (scalar) {
         t->a_stride = (t->n_ent + 3) & ~3;  // 16-byte aligned rows in FP32 and FP64
-        A(talloc(t, &t->A64, nn * t->a_stride));
-        A(talloc(t, &t->A32, nn * t->a_stride));
+        A(talloc(t, &t->A64, nh * t->a_stride));
+        A(talloc(t, &t->A32, nh * t->a_stride));
     } else {
-        A(talloc(t, &t->B64, nn * t->n_ent));
-        A(talloc(t, &t->B32, nn * t->n_ent));
+        A(talloc(t, &t->B64, nh * t->n_ent));
+        A(talloc(t, &t->B32, nh * t->n_ent));
     }
     A(talloc(t, &t->ent, ent.size()));
     A(talloc(t, &t->mono, mono.size()));
@@ -1471,7 +1504,7 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->pair_counts, 3));
     A(talloc(t, &t->V, 3 * ntg));
     if (t->learned) {
-        A(talloc(t, &t->node_feat, nn * kMlpIn));
+        A(talloc(t, &t->node_feat, nh * kMlpIn));
         A(talloc(t, &t->mlp_w, kMlpParams));
         A(talloc(t, &t->mlp_norm, 2 * kMlpIn));
         A(talloc(t, &t->decisions, (size_t)t->n_batches * kDecisionCap));
@@ -1480,7 +1513,7 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     if (e == cudaSuccess) e = cudaMemcpy(t->mono, mono.data(), mono.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !gtab.empty())
         e = cudaMemcpy(t->gtab, gtab.data(), gtab.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(t->node_mom, 0, nn * cd * cd * cd * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(t->node_mom, 0, nh * cd * cd * cd * sizeof(double));
     // the count arrays carry one extra zero entry so that their exclusive scans also yield the totals
     if (e == cudaSuccess) e = cudaMemset(t->far_cnt, 0, far_rows * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMemset(t->near_cnt, 0, ((size_t)t->n_batches + 1) * sizeof(int32_t));
@@ -1540,6 +1573,7 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     A.mlp_w = t->mlp_w;
     A.mlp_norm = t->mlp_norm;
     A.decisions = t->decisions;
+    A.heavy_cap = t->heavy_cap;
     LPM_CUDA_TRY(cudaMemsetAsync(t->pair_counts, 0, 3 * sizeof(unsigned long long), ctx->stream));
     const unsigned g = grid_for(t->n_batches, 4);
     LPM_LAUNCH(ctx, "traverse_kernel", traverse_kernel, g, 128, 0, A);
@@ -1590,24 +1624,34 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     }
     int rc = octree_build(ctx, t->st, src, n_src, rb);
     if (rc) return rc;
+    if (can_sync) {  // grow the per-node arrays to this tree (a captured replay can only flag an overflow)
+        int32_t nodes = 0;
+        LPM_CUDA_TRY(cudaMemcpyAsync(&nodes, t->st.counters + 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+        LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (nodes > t->heavy_cap) {
+            rc = heavy_alloc(t, nodes);
+            if (rc) return rc;
+        }
+    }
     const unsigned gs = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(n_src, 256), 8 * ctx->num_sms));
     LPM_LAUNCH(ctx, "gather_sources_kernel", gather_sources_kernel, gs, 256, 0, src, t->st.perm, t->st.counters,
                t->src_sorted);
     const unsigned gl = (unsigned)std::max<int64_t>(1, std::min<int64_t>(t->st.node_cap, 16 * ctx->num_sms));
     LPM_LAUNCH(ctx, "leaf_p2m_kernel", leaf_p2m_kernel, gl, 128, 0, t->st, t->src_sorted, t->pm, t->mono, t->n_mono,
-               t->node_ctr, t->node_wabs, t->node_mom, t->src32, t->scalar ? 1.0 : 2.0);
+               t->node_ctr, t->node_wabs, t->node_mom, t->src32, t->scalar ? 1.0 : 2.0, t->heavy_cap);
     for (int l = kTreeDepth - 1; l >= 0; --l)
         LPM_LAUNCH(ctx, "m2m_level_kernel", m2m_level_kernel, gl, 128, 0, t->st, l, t->pm, t->mono, t->n_mono,
-                   t->node_ctr, t->node_wabs, t->node_mom);
+                   t->node_ctr, t->node_wabs, t->node_mom, t->heavy_cap);
     if (t->scalar)
         LPM_LAUNCH(ctx, "coeff_kernel", coeff_scalar_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->a_stride,
-                   t->node_mom, t->A64, t->A32);
+                   t->node_mom, t->A64, t->A32, t->heavy_cap);
     else
         LPM_LAUNCH(ctx, "coeff_kernel", coeff_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->node_mom, t->B64,
-                   t->B32);
+                   t->B32, t->heavy_cap);
     if (t->learned)
         LPM_LAUNCH(ctx, "node_feature_kernel", node_feature_kernel, gl, 128, 0, t->st, t->pm, t->node_ctr,
-                   t->node_wabs, t->node_mom, t->node_feat);
+                   t->node_wabs, t->node_mom, t->node_feat, t->heavy_cap);
     // targets in Morton order, cut into compact batches of at most kBatch
     LPM_CUDA_TRY(cudaMemsetAsync(t->tcount, 0, 4 * sizeof(int32_t), ctx->stream));
     rc = morton_keys(ctx, X, n_tgt, rb, t->tkeys, t->tperm, t->tcount);
@@ -1681,7 +1725,8 @@ int tree_check(TreeSolver* t) {
     LPM_CUDA_TRY(cudaMemcpyAsync(tc, t->tcount, sizeof(tc), cudaMemcpyDeviceToHost, ctx->stream));
     LPM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (f[0]) {
-        set_error("tree solver: interaction list capacity exceeded (flags %d)", f[0]);
+        set_error("tree solver: capacity exceeded in a captured evaluation (flags %d: 1 far list, 2 near list, "
+                  "4 traversal stack, 16 node moments); run one uncaptured evaluation to regrow", f[0]);
         return LPM_ERR_CAPACITY;
     }
     if (tc[1] > t->n_batches) {
