@@ -1,0 +1,94 @@
+// Lpm::TreeSum (declared by the reference's src/LpmTreeSum.h) on the GPU: replaces src/LpmTreeSum.cpp
+// for the mesh path (src/LpmTreeSum.cpp:55-86,182-197,221-238).  No CPU tree is built: each meshSolve
+// builds the octree, moments and interaction lists on the GPU (lpm_tree_sum_mesh) with the object's
+// series order (|k| < order), leaf capacity and the caller's acceptance parameter; macCounter grows by
+// the number of accepted far-field (target, cluster) evaluations.  computeMeshMoments and
+// computeMoments are kept as calls but do no work: moments are formed inside each solve from the source
+// field's current values.  The mesh constructor initialises the smoothing and shrink flags the
+// reference leaves unset (src/LpmTreeSum.cpp:221-226).
+#include "LpmTreeSum.h"
+
+#include "LpmB200Dropin.h"
+
+#include <stdexcept>
+#include <vector>
+
+namespace Lpm {
+
+TreeSum::TreeSum(const std::shared_ptr<Coords> crds, const int max_series_order, const int max_particles_per_box,
+                 const scalar_type smoother, const bool do_shrink)
+    : Tree(crds),
+      _maxSeriesOrder(max_series_order),
+      _maxParticlesPerNode(max_particles_per_box),
+      _smooth(smoother),
+      _shrink(do_shrink),
+      sKern(NULL),
+      vKern(NULL) {}
+
+TreeSum::TreeSum(const int max_series_order, const int max_particles_per_box, std::shared_ptr<MeshedParticles> pmesh,
+                 const std::shared_ptr<VectorKernel> kernel, const std::string tgtFieldName,
+                 const std::string srcFieldName)
+    : Tree(),
+      _maxSeriesOrder(max_series_order),
+      _maxParticlesPerNode(max_particles_per_box),
+      _smooth(0.0),
+      _shrink(false),
+      sKern(NULL),
+      vKern(kernel.get()),
+      _mesh(pmesh),
+      _vertTgt(pmesh->getVertexFieldPtr(tgtFieldName)),
+      _faceSrc(pmesh->getFaceFieldPtr(srcFieldName)),
+      _faceTgt(pmesh->getFaceFieldPtr(tgtFieldName)) {}
+
+void TreeSum::computeMoments(const std::shared_ptr<Field>) {}
+void TreeSum::computeMeshMoments() {}
+
+void TreeSum::meshSolve(const MPIReplicatedData& mpiVerts, const MPIReplicatedData& mpiFaces, const scalar_type mp_tol,
+                        int& macCounter) {
+    const int rank = mpiVerts.getRank();
+    std::shared_ptr<MeshedParticles> pm = _mesh.lock();
+    std::shared_ptr<Field> src = _faceSrc.lock(), vtgt = _vertTgt.lock(), ftgt = _faceTgt.lock();
+    if (!pm || !src || !vtgt || !ftgt) throw std::runtime_error("TreeSum::meshSolve: mesh or field expired");
+    if (!vKern) throw std::logic_error("invalid kernel");
+    const lpm_kernel_desc kd = b200::describe(*vKern);
+    const index_type nv = pm->nVertices(), nf = pm->nFaces();
+    std::vector<double> vx(nv), vy(nv), vz(nv), fx(nf), fy(nf), fz(nf), area(nf), s(nf);
+    std::vector<uint8_t> divided(nf);
+    for (index_type i = 0; i < nv; ++i) {
+        const XyzVector v = pm->getVertex(i);
+        vx[i] = v.x;
+        vy[i] = v.y;
+        vz[i] = v.z;
+    }
+    for (index_type j = 0; j < nf; ++j) {
+        divided[j] = pm->faceIsDivided(j) ? 1 : 0;
+        if (divided[j]) continue;
+        const XyzVector c = pm->getFaceCentroid(j);
+        fx[j] = c.x;
+        fy[j] = c.y;
+        fz[j] = c.z;
+        area[j] = pm->getFaceArea(j);
+        s[j] = src->getScalar(j);
+    }
+    lpm_solver_desc sd{};
+    sd.method = LPM_METHOD_TREE;
+    sd.precision = LPM_PREC_F32;
+    sd.order = _maxSeriesOrder;
+    sd.max_per_leaf = _maxParticlesPerNode;
+    sd.theta = mp_tol;
+    sd.order_policy = LPM_ORDER_FIXED;
+    int64_t mac = 0;
+    b200::check(lpm_tree_sum_mesh(b200::context(), &kd, &sd, nv, vx.data(), vy.data(), vz.data(), nf, fx.data(),
+                                  fy.data(), fz.data(), area.data(), divided.data(), s.data(),
+                                  mpiVerts.startIndex(rank), mpiVerts.endIndex(rank), mpiFaces.startIndex(rank),
+                                  mpiFaces.endIndex(rank), vtgt->getPtrToData(0), vtgt->getPtrToData(1),
+                                  vtgt->getPtrToData(2), ftgt->getPtrToData(0), ftgt->getPtrToData(1),
+                                  ftgt->getPtrToData(2), &mac),
+                "lpm_tree_sum_mesh");
+    macCounter += (int)mac;
+}
+
+// One GPU computes every target of the calling rank; the slices of other ranks are theirs to compute.
+void TreeSum::meshBroadcast(const MPIReplicatedData&, const MPIReplicatedData&) const {}
+
+}  // namespace Lpm
