@@ -85,6 +85,7 @@ int lpm_ctx_profile_report(lpm_ctx* ctx, char* buf, size_t len);
 /* Measured FMA-pipe peak (TFLOP/s, FMA = 2 flops) of this device for LPM_PREC_F32 or LPM_PREC_F64: the
  * roofline denominator of the pairwise and far-field kernels.  Synchronous; takes ~100 ms. */
 int lpm_fma_peak(lpm_ctx* ctx, int precision, double* tflops);
+#define LPM_PEAK_F32X2 2 /* lpm_fma_peak: FP32 issued as packed pairs (fma.rn.f32x2) */
 
 /* ---- mesh generation (host).  The reference's PolyMesh2d(seed, level) constructor
  * (src/LpmPolyMesh2d.cpp:20-93) in the same vertex / face index order.  Arrays are caller-owned:

@@ -9,7 +9,8 @@ import ctypes as C
 import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "liblpm_b200.so"
+# LPM_B200_LIB selects another build of the library (e.g. one compiled with different tuning constants)
+LIB_PATH = Path(os.environ.get("LPM_B200_LIB", str(Path(__file__).resolve().parent / "liblpm_b200.so")))
 
 LPM_OK = 0
 LPM_ERR_ARG = 1

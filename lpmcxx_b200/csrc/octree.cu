@@ -190,8 +190,15 @@ int radix_sort_impl(lpm_ctx* ctx, K* keys, int32_t* vals, K* tk, int32_t* tv, in
     for (int shift = bit_lo; shift < bit_hi; shift += 8) {
         LPM_LAUNCH(ctx, "radix_hist_kernel", radix_hist_kernel<K>, nblocks, kSortThreads, 0, src_k, n, shift, counts,
                    nblocks);
-        LPM_LAUNCH(ctx, "scan_single_block_kernel", scan_single_block_kernel, 1, 1024, 0, counts,
-                   (int64_t)256 * nblocks, (int32_t*)nullptr);
+        // digit-major counts -> global offsets; a single block suffices for small arrays, the three-pass
+        // scan takes the large ones (1.3M keys: 256 x 1280 counts)
+        if ((int64_t)256 * nblocks <= 16 * 1024) {
+            LPM_LAUNCH(ctx, "scan_single_block_kernel", scan_single_block_kernel, 1, 1024, 0, counts,
+                       (int64_t)256 * nblocks, (int32_t*)nullptr);
+        } else {
+            const int rc = scan_exclusive_i32(ctx, counts, counts, (int64_t)256 * nblocks, nullptr);
+            if (rc) return rc;
+        }
         LPM_LAUNCH(ctx, "radix_scatter_kernel", radix_scatter_kernel<K>, nblocks, kSortThreads, 0, src_k, src_v, dst_k,
                    dst_v, n, shift, counts, nblocks);
         std::swap(src_k, dst_k);

@@ -20,19 +20,49 @@ __global__ void __launch_bounds__(256) fma_chain_kernel(T* out, int iters, T a, 
     if (s == (T)-1.2345) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// The same with packed FP32 pairs (fma.rn.f32x2, sm_100): 8 chains of two lanes each per thread.
+__device__ __forceinline__ unsigned long long fma_f32x2(unsigned long long a, unsigned long long b,
+                                                         unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    return ((unsigned long long)__float_as_uint(hi) << 32) | (unsigned long long)__float_as_uint(lo);
+}
+
+__global__ void __launch_bounds__(256) fma2_chain_kernel(float* out, int iters, float a, float b) {
+    const float t = (float)threadIdx.x;
+    unsigned long long x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = pack2(t + k, t - k);
+    const unsigned long long A = pack2(a, a), B = pack2(b, b);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) x[k] = fma_f32x2(x[k], A, B);
+        }
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += __uint_as_float((unsigned)x[k]) + __uint_as_float((unsigned)(x[k] >> 32));
+    if (s == -1.2345f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace
 }  // namespace lpm
 
 using namespace lpm;
 
 extern "C" int lpm_fma_peak(lpm_ctx* ctx, int precision, double* tflops) {
-    if (!ctx || !tflops || (precision != LPM_PREC_F32 && precision != LPM_PREC_F64)) {
+    if (!ctx || !tflops || (precision != LPM_PREC_F32 && precision != LPM_PREC_F64 && precision != LPM_PEAK_F32X2)) {
         set_error("lpm_fma_peak: bad argument");
         return LPM_ERR_ARG;
     }
     LPM_CUDA_TRY(cudaSetDevice(ctx->device));
     const int blocks = ctx->num_sms * 8, threads = 256;
-    const int iters = precision == LPM_PREC_F32 ? 4096 : 1024;
+    const int iters = precision == LPM_PREC_F64 ? 1024 : 4096;
     void* out = scratch(ctx, kSlotMisc3, (size_t)blocks * threads * sizeof(double));
     if (!out) return LPM_ERR_OOM;
     cudaEvent_t e0, e1;
@@ -41,7 +71,9 @@ extern "C" int lpm_fma_peak(lpm_ctx* ctx, int precision, double* tflops) {
     float best = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
         cudaEventRecord(e0, ctx->stream);
-        if (precision == LPM_PREC_F32)
+        if (precision == LPM_PEAK_F32X2)
+            fma2_chain_kernel<<<blocks, threads, 0, ctx->stream>>>((float*)out, iters, 0.999999f, 1e-7f);
+        else if (precision == LPM_PREC_F32)
             fma_chain_kernel<float><<<blocks, threads, 0, ctx->stream>>>((float*)out, iters, 0.999999f, 1e-7f);
         else
             fma_chain_kernel<double><<<blocks, threads, 0, ctx->stream>>>((double*)out, iters, 0.999999, 1e-7);
@@ -54,7 +86,7 @@ extern "C" int lpm_fma_peak(lpm_ctx* ctx, int precision, double* tflops) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    const double flops = 2.0 * 8.0 * 16.0 * (double)iters * blocks * threads;
+    const double flops = (precision == LPM_PEAK_F32X2 ? 2.0 : 1.0) * 2.0 * 8.0 * 16.0 * (double)iters * blocks * threads;
     *tflops = flops / (best * 1e-3) * 1e-12;
     return LPM_OK;
 }

@@ -732,7 +732,14 @@ struct FarArgs {
     double* V;
 };
 
-constexpr int kFarStageUnits = 1024;  // 16-byte units gathered per stage (at least one entry)
+#ifndef LPM_FAR_STAGE_UNITS
+#define LPM_FAR_STAGE_UNITS 1024
+#endif
+#ifndef LPM_FAR_MIN_BLOCKS
+#define LPM_FAR_MIN_BLOCKS 6
+#endif
+constexpr int kFarStageUnits = LPM_FAR_STAGE_UNITS;  // 16-byte units gathered per stage (at least one entry)
+constexpr int kFarMinBlocks = LPM_FAR_MIN_BLOCKS;    // resident blocks per SM the far kernels are built for
 
 template <int P, typename F4>
 struct FarShape {
@@ -764,7 +771,7 @@ __device__ __forceinline__ void far_stage_gather(const FarArgs& A, int64_t s0, i
 // double buffer (cp.async) while the other half is evaluated; one launch per order keeps every warp of
 // the GPU in the same compact code.  Adds to V (cleared before the first order's launch).
 template <int P, typename F, typename F4>
-__global__ void __launch_bounds__(kBatch) far_order_kernel(FarArgs A) {
+__global__ void __launch_bounds__(kBatch, kFarMinBlocks) far_order_kernel(FarArgs A) {
     using S = FarShape<P, F4>;
     extern __shared__ float4 fbuf[];  // 2 stages of S::kStage units, then 2 x kK centres
     double4* ctr = (double4*)(fbuf + 2 * S::kStage);
