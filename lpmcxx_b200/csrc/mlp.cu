@@ -166,13 +166,19 @@ __global__ void mlp_to_bf16_kernel(const float* __restrict__ params, __nv_bfloat
     if (p < kMlpParams) w[p] = __float2bfloat16_rn(params[p]);
 }
 
-__global__ void mlp_predict_bf16_kernel(const __nv_bfloat16* __restrict__ w, const float* __restrict__ norm,
-                                        const float* __restrict__ feats, int64_t n, int32_t* __restrict__ cls) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+// The treecode's inference path (mlp_warp_argmax): 32 samples per warp on the tensor cores.
+__global__ void __launch_bounds__(128) mlp_predict_bf16_kernel(const __nv_bfloat16* __restrict__ w,
+                                                               const float* __restrict__ norm,
+                                                               const float* __restrict__ feats, int64_t n,
+                                                               int32_t* __restrict__ cls) {
+    __shared__ __align__(16) __nv_bfloat16 xs[4][32 * 16];
+    const int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    if (base >= n) return;  // uniform per warp
+    const int64_t i = base + (threadIdx.x & 31);
     float f[kMlpIn];
-    for (int k = 0; k < kMlpIn; ++k) f[k] = feats[i * kMlpIn + k];
-    cls[i] = mlp_argmax_bf16(w, norm, f);
+    for (int k = 0; k < kMlpIn; ++k) f[k] = i < n ? feats[i * kMlpIn + k] : norm[k];
+    const int c = mlp_warp_argmax(w, norm, f, xs[threadIdx.x >> 5]);
+    if (i < n) cls[i] = c;
 }
 
 int train_smem_bytes() { return kTrainSmemFloats * (int)sizeof(float); }

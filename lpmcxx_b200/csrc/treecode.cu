@@ -466,7 +466,8 @@ __device__ __forceinline__ float log_budget(const double* node_wabs, double eps)
 __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
     __shared__ int sstack[4][kWarpStack];
     __shared__ int pcnt[4][kPMax + 1];  // per warp: far entries of each order so far
-    __shared__ __nv_bfloat16 mw[kMlpParams];
+    __shared__ __align__(16) __nv_bfloat16 mw[kMlpParams];
+    __shared__ __align__(16) __nv_bfloat16 mxs[4][32 * 16];  // per warp: the selector's input rows
     __shared__ float mnorm[2 * kMlpIn];
     if (A.learned) {  // uniform per launch
         for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) mw[i] = A.mlp_w[i];
@@ -526,11 +527,17 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
             uint8_t* dec = A.decisions + (size_t)b * kDecisionCap;
             int cls = -1;
             if (far_ok && A.fill && idx < kDecisionCap) cls = dec[idx];
-            if (far_ok && cls < 0) {
+            const bool need = far_ok && cls < 0;
+            if (__any_sync(full, need)) {  // the whole warp runs the selector on the tensor cores
                 float f[kMlpIn];
-                pair_features(bc, c, A.node_feat + (size_t)node * kMlpIn, log_s, f);
-                cls = mlp_argmax_bf16(mw, mnorm, f);
-                if (!A.fill && idx < kDecisionCap) dec[idx] = (uint8_t)cls;
+#pragma unroll
+                for (int i = 0; i < kMlpIn; ++i) f[i] = mnorm[i];  // finite filler for lanes without a pair
+                if (need) pair_features(bc, c, A.node_feat + (size_t)node * kMlpIn, log_s, f);
+                const int c2 = mlp_warp_argmax(mw, mnorm, f, mxs[w]);
+                if (need) {
+                    cls = c2;
+                    if (!A.fill && idx < kDecisionCap) dec[idx] = (uint8_t)cls;
+                }
             }
             if (far_ok) {
                 P = cls == kMlpDirectClass ? 0 : min(cls + 1, A.max_order);

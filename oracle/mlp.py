@@ -87,9 +87,14 @@ def predict(p: np.ndarray, feats: np.ndarray) -> np.ndarray:
 
 
 def predict_bf16(p: np.ndarray, feats: np.ndarray):
-    """Classes with BF16-rounded weights (standardisation kept in FP32) and the top-2 logit margin."""
+    """Classes of the BF16 inference path (BF16 weights; standardised inputs and hidden activations
+    rounded to BF16 between layers; FP32-or-better accumulation) and the top-2 logit margin."""
     q = np.asarray(p, np.float32).copy()
     q[:N_TRAINABLE] = round_bf16(q[:N_TRAINABLE])
-    z = logits(q, feats)
+    (w1, b1, w2, b2, w3, b3), mean, inv_std = unpack(q)
+    x = round_bf16(((np.asarray(feats, np.float32) - mean.astype(np.float32)) * inv_std.astype(np.float32)))
+    h1 = round_bf16(gelu(x.astype(np.float64) @ w1.T + b1))
+    h2 = round_bf16(gelu(h1.astype(np.float64) @ w2.T + b2))
+    z = h2.astype(np.float64) @ w3.T + b3
     s = np.sort(z, axis=1)
     return z.argmax(axis=1), s[:, -1] - s[:, -2]
