@@ -189,13 +189,26 @@ __global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* 
 // Internal nodes of level l: centre = count-weighted mean of the children's centres, radius bound
 // max(|c_child - c| + r_child), moments shifted from the children:
 // m_k(c) = sum_child sum_{j <= k} C(k, j) (c_child - c)^(k-j) m_j(c_child).
+// The children's moments (packed in monomial order), their shift powers and the binomial table are
+// staged in shared memory, so the inner loops read no global or constant memory.
+
 __global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm, const int4* __restrict__ mono,
                                                         int n_mono, double4* __restrict__ node_ctr,
                                                         double* __restrict__ node_wabs,
                                                         double* __restrict__ node_mom, int heavy_cap) {
+    extern __shared__ double m2m_sh[];  // 2 x 8 x n_mono: child moments and their partial shifts
     __shared__ double dp[8][3][kPMax + 1];
+    __shared__ double bin[kPMax + 1][kPMax + 1];
+    __shared__ int mono_idx[kPMax + 1][kPMax + 1][kPMax + 1];  // (a, b, c) -> position in the monomial list
     const int lb = t.level_range[2 * l], le = t.level_range[2 * l + 1];
     const int cd = cube_dim(pm);
+    for (int i = threadIdx.x; i < (kPMax + 1) * (kPMax + 1); i += blockDim.x)
+        bin[i / (kPMax + 1)][i % (kPMax + 1)] = c_binom[i / (kPMax + 1)][i % (kPMax + 1)];
+    for (int i = threadIdx.x; i < n_mono; i += blockDim.x) {
+        const int4 k = mono[i];
+        mono_idx[k.x][k.y][k.z] = i;
+    }
+    __syncthreads();
     for (int node = lb + blockIdx.x; node < le; node += gridDim.x) {
         const int nc = t.node_nchild[node];
         if (nc == 0) continue;  // a leaf: done by leaf_p2m_kernel
@@ -219,7 +232,7 @@ __global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm,
             node_wabs[node] = wabs;
         }
         if (fc + nc > heavy_cap) continue;  // uniform per block: a child (numbered after node) has no moments
-        __syncthreads();
+        __syncthreads();  // the previous node's readers of dp / m2m_sh are done
         if (threadIdx.x < nc * 3) {
             const int k = threadIdx.x / 3, a = threadIdx.x % 3;
             const double4 cc = node_ctr[fc + k];
@@ -230,23 +243,41 @@ __global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm,
                 v *= d;
             }
         }
+        double* S0 = m2m_sh;                  // nc x n_mono
+        double* S1 = m2m_sh + 8 * n_mono;     // nc x n_mono
+        for (int i = threadIdx.x; i < nc * n_mono; i += blockDim.x) {
+            const int k = i / n_mono, term = i - k * n_mono;
+            const int4 j = mono[term];
+            S0[i] = node_mom[(size_t)(fc + k) * cd * cd * cd + (j.x * cd + j.y) * cd + j.z];
+        }
+        __syncthreads();
+        // the shift factorises by axis: three 1D binomial shifts (x, then y, then z with the sum over
+        // children), (k_x + 1) + (k_y + 1) + (k_z + 1) terms per monomial instead of their product
+        for (int i = threadIdx.x; i < nc * n_mono; i += blockDim.x) {
+            const int k = i / n_mono, term = i - k * n_mono;
+            const int4 kk = mono[term];
+            double acc = 0;
+            for (int j0 = 0; j0 <= kk.x; ++j0)
+                acc = fma(bin[kk.x][j0] * dp[k][0][kk.x - j0], S0[k * n_mono + mono_idx[j0][kk.y][kk.z]], acc);
+            S1[i] = acc;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nc * n_mono; i += blockDim.x) {
+            const int k = i / n_mono, term = i - k * n_mono;
+            const int4 kk = mono[term];
+            double acc = 0;
+            for (int j1 = 0; j1 <= kk.y; ++j1)
+                acc = fma(bin[kk.y][j1] * dp[k][1][kk.y - j1], S1[k * n_mono + mono_idx[kk.x][j1][kk.z]], acc);
+            S0[i] = acc;
+        }
         __syncthreads();
         double* mout = node_mom + (size_t)node * cd * cd * cd;
         for (int term = threadIdx.x; term < n_mono; term += blockDim.x) {
             const int4 kk = mono[term];
             double acc = 0;
-            for (int k = 0; k < nc; ++k) {
-                const double* mc = node_mom + (size_t)(fc + k) * cd * cd * cd;
-                for (int j0 = 0; j0 <= kk.x; ++j0) {
-                    const double f0 = c_binom[kk.x][j0] * dp[k][0][kk.x - j0];
-                    for (int j1 = 0; j1 <= kk.y; ++j1) {
-                        const double f1 = f0 * c_binom[kk.y][j1] * dp[k][1][kk.y - j1];
-                        const double* row = mc + (j0 * cd + j1) * cd;
-                        for (int j2 = 0; j2 <= kk.z; ++j2)
-                            acc = fma(f1 * c_binom[kk.z][j2] * dp[k][2][kk.z - j2], row[j2], acc);
-                    }
-                }
-            }
+            for (int k = 0; k < nc; ++k)
+                for (int j2 = 0; j2 <= kk.z; ++j2)
+                    acc = fma(bin[kk.z][j2] * dp[k][2][kk.z - j2], S0[k * n_mono + mono_idx[kk.x][kk.y][j2]], acc);
             mout[(kk.x * cd + kk.y) * cd + kk.z] = acc;
         }
     }
@@ -1536,7 +1567,12 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
         return cuda_status(e, "tree solver allocation");
     }
     {
-        const cudaError_t ea = far_smem_attributes();
+        cudaError_t ea = far_smem_attributes();
+        // M2M stages two 8-child copies of the moments: opt in for the largest order any solver may use
+        const int mono_max = (kPMax + 1) * (kPMax + 2) * (kPMax + 3) / 6;
+        if (ea == cudaSuccess)
+            ea = cudaFuncSetAttribute(m2m_level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(16 * mono_max * sizeof(double)));
         if (ea != cudaSuccess) {
             tree_solver_destroy(t);
             return cuda_status(ea, "cudaFuncSetAttribute (far_kernel)");
@@ -1655,8 +1691,8 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     LPM_LAUNCH(ctx, "leaf_p2m_kernel", leaf_p2m_kernel, gl, 128, 0, t->st, t->src_sorted, t->pm, t->mono, t->n_mono,
                t->node_ctr, t->node_wabs, t->node_mom, t->src32, t->scalar ? 1.0 : 2.0, t->heavy_cap);
     for (int l = kTreeDepth - 1; l >= 0; --l)
-        LPM_LAUNCH(ctx, "m2m_level_kernel", m2m_level_kernel, gl, 128, 0, t->st, l, t->pm, t->mono, t->n_mono,
-                   t->node_ctr, t->node_wabs, t->node_mom, t->heavy_cap);
+        LPM_LAUNCH(ctx, "m2m_level_kernel", m2m_level_kernel, gl, 128, (size_t)16 * t->n_mono * sizeof(double), t->st,
+                   l, t->pm, t->mono, t->n_mono, t->node_ctr, t->node_wabs, t->node_mom, t->heavy_cap);
     if (t->scalar)
         LPM_LAUNCH(ctx, "coeff_kernel", coeff_scalar_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->a_stride,
                    t->node_mom, t->A64, t->A32, t->heavy_cap);
