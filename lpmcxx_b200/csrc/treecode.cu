@@ -677,6 +677,60 @@ __device__ __forceinline__ void horner(const T4* __restrict__ Bc, T e0, T e1, T 
     g0 = G0; g1 = G1; g2 = G2; g3 = G3;
 }
 
+// FP32 Horner scheme with the four components in two packed pairs (fma.rn.f32x2, sm_100): half the FMA
+// instructions per coefficient for the same lane work and the same rounding (measured: far field 17-19%
+// faster).
+__device__ __forceinline__ void fma2p(float& d0, float& d1, float a0, float a1, float b, float c0, float c1) {
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %4};\n\tmov.b64 rc, {%5, %6};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d0), "=f"(d1)
+        : "f"(a0), "f"(a1), "f"(b), "f"(c0), "f"(c1));
+}
+
+// (d0, d1) = (a0 b0 + c0, a1 b1 + c1) as one packed FMA.
+__device__ __forceinline__ void fma2v(float& d0, float& d1, float a0, float a1, float b0, float b1, float c0,
+                                      float c1) {
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d0), "=f"(d1)
+        : "f"(a0), "f"(a1), "f"(b0), "f"(b1), "f"(c0), "f"(c1));
+}
+
+template <int P>
+__device__ __forceinline__ void horner_f32x2(const float4* __restrict__ Bc, float e0, float e1, float e2, float s,
+                                             float& g0, float& g1, float& g2, float& g3) {
+    int q = 0;
+    float G0 = 0, G1 = 0, G2 = 0, G3 = 0;
+#pragma unroll
+    for (int m = (P - 1) / 2; m >= 0; --m) {
+        const int Q = P - 2 * m;
+        float P0 = 0, P1 = 0, P2 = 0, P3 = 0;
+#pragma unroll
+        for (int a = Q - 1; a >= 0; --a) {
+            float Q0 = 0, Q1 = 0, Q2 = 0, Q3 = 0;
+#pragma unroll
+            for (int b = Q - 1 - a; b >= 0; --b) {
+                float R0 = 0, R1 = 0, R2 = 0, R3 = 0;
+#pragma unroll
+                for (int c = Q - 1 - a - b; c >= 0; --c) {
+                    const float4 v = Bc[q++];
+                    fma2p(R0, R1, R0, R1, e2, v.x, v.y);
+                    fma2p(R2, R3, R2, R3, e2, v.z, v.w);
+                }
+                fma2p(Q0, Q1, Q0, Q1, e1, R0, R1);
+                fma2p(Q2, Q3, Q2, Q3, e1, R2, R3);
+            }
+            fma2p(P0, P1, P0, P1, e0, Q0, Q1);
+            fma2p(P2, P3, P2, P3, e0, Q2, Q3);
+        }
+        fma2p(G0, G1, G0, G1, s, P0, P1);
+        fma2p(G2, G3, G2, G3, s, P2, P3);
+    }
+    g0 = G0; g1 = G1; g2 = G2; g3 = G3;
+}
+
 // Adds 2 [(x cross d) G0 + x cross G] of one cluster to V, d = c - x.
 template <int P, typename T, typename T4>
 __device__ __forceinline__ void far_one(const T4* Bc, const double4& x, const double4& c, double* V) {
@@ -744,7 +798,10 @@ __device__ __forceinline__ void far_one_acc(const F4* __restrict__ Bc, const dou
     const F dx = (F)(cx - x.x), dy = (F)(cy - x.y), dz = (F)(cz - x.z);
     const F inv = F(1) / (dx * dx + dy * dy + dz * dz);
     F g0, g1, g2, g3;
-    horner<P, F, F4>(Bc, dx * inv, dy * inv, dz * inv, inv, g0, g1, g2, g3);
+    if constexpr (sizeof(F) == 4)
+        horner_f32x2<P>((const float4*)Bc, dx * inv, dy * inv, dz * inv, inv, g0, g1, g2, g3);
+    else
+        horner<P, F, F4>(Bc, dx * inv, dy * inv, dz * inv, inv, g0, g1, g2, g3);
     const F s = F(2) * inv;
     const F G0 = s * g0, Gx = s * g1, Gy = s * g2, Gz = s * g3;
     const F xx = (F)x.x, xy = (F)x.y, xz = (F)x.z;
@@ -1102,22 +1159,22 @@ constexpr int kNearRuns = 128;        // source ranges resolved per chunk
 // FP64 across tiles.  A target's own source (d = 0) contributes 0 through the clamped denominator.
 __device__ __forceinline__ void near_tile(const float4* tile, int m, float tx0, float ty0, float tz0, float tx1,
                                           float ty1, float tz1, double* D0, double* D1) {
+    // the two targets travel as packed pairs (fma.rn.f32x2): d = t - y, rr = |d|^2 + 1e-30, f = w / rr
     float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
 #pragma unroll 4
     for (int j = 0; j < m; ++j) {
         const float4 y = tile[j];
-        const float dx = tx0 - y.x, dy = ty0 - y.y, dz = tz0 - y.z;
-        const float rr = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1e-30f);
-        const float f = y.w * rcp32(rr);
-        a0 = fmaf(f, dx, a0);
-        a1 = fmaf(f, dy, a1);
-        a2 = fmaf(f, dz, a2);
-        const float ex = tx1 - y.x, ey = ty1 - y.y, ez = tz1 - y.z;
-        const float ss = fmaxf(fmaf(ez, ez, fmaf(ey, ey, ex * ex)), 1e-30f);
-        const float g = y.w * rcp32(ss);
-        b0 = fmaf(g, ex, b0);
-        b1 = fmaf(g, ey, b1);
-        b2 = fmaf(g, ez, b2);
+        float dx0, dx1, dy0, dy1, dz0, dz1, r0, r1;
+        fma2p(dx0, dx1, y.x, y.x, -1.0f, tx0, tx1);
+        fma2p(dy0, dy1, y.y, y.y, -1.0f, ty0, ty1);
+        fma2p(dz0, dz1, y.z, y.z, -1.0f, tz0, tz1);
+        fma2v(r0, r1, dx0, dx1, dx0, dx1, 1e-30f, 1e-30f);
+        fma2v(r0, r1, dy0, dy1, dy0, dy1, r0, r1);
+        fma2v(r0, r1, dz0, dz1, dz0, dz1, r0, r1);
+        const float f = y.w * rcp32(r0), g = y.w * rcp32(r1);
+        fma2v(a0, b0, f, g, dx0, dx1, a0, b0);
+        fma2v(a1, b1, f, g, dy0, dy1, a1, b1);
+        fma2v(a2, b2, f, g, dz0, dz1, a2, b2);
     }
     D0[0] += a0; D0[1] += a1; D0[2] += a2;
     D1[0] += b0; D1[1] += b1; D1[2] += b2;
