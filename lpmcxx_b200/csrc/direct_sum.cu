@@ -167,20 +167,32 @@ __global__ void __launch_bounds__(kThreads) poisson_f64_kernel(const double4* __
 template <bool kGuard, bool kDelta>
 __device__ __forceinline__ void bs_f32_tile(const float4* tile, int m, const float* tx, const float* ty,
                                             const float* tz, float* ax, float* ay, float* az, float d2x2) {
+    // Targets go in pairs through packed FMAs (fma.rn.f32x2); each lane rounds as the scalar form
+    // d = t - s, rr = fma(dz, dz, fma(dy, dy, dx dx)), f = w / rr, a += f d:  t - s is fma(s, -1, t) and
+    // a product is fma(a, b, -0), both exact restatements of the single-rounded operation.
+    static_assert(kTpt32 % 2 == 0, "targets are processed in pairs");
 #pragma unroll 4
     for (int k = 0; k < m; ++k) {
         const float4 s = tile[k];
 #pragma unroll
-        for (int t = 0; t < kTpt32; ++t) {
-            const float dx = tx[t] - s.x, dy = ty[t] - s.y, dz = tz[t] - s.z;
-            float rr = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            if (kDelta) rr += d2x2;
-            float inv = rcp32(rr);
-            if (kGuard) inv = rr > 2.0e-13f ? inv : 0.0f;
-            const float f = s.w * inv;
-            ax[t] = fmaf(f, dx, ax[t]);
-            ay[t] = fmaf(f, dy, ay[t]);
-            az[t] = fmaf(f, dz, az[t]);
+        for (int t = 0; t < kTpt32; t += 2) {
+            float dx0, dx1, dy0, dy1, dz0, dz1, r0, r1, f0, f1;
+            fma2p(dx0, dx1, s.x, s.x, -1.0f, tx[t], tx[t + 1]);
+            fma2p(dy0, dy1, s.y, s.y, -1.0f, ty[t], ty[t + 1]);
+            fma2p(dz0, dz1, s.z, s.z, -1.0f, tz[t], tz[t + 1]);
+            fma2v(r0, r1, dx0, dx1, dx0, dx1, -0.0f, -0.0f);
+            fma2v(r0, r1, dy0, dy1, dy0, dy1, r0, r1);
+            fma2v(r0, r1, dz0, dz1, dz0, dz1, r0, r1);
+            if (kDelta) { r0 += d2x2; r1 += d2x2; }
+            float i0 = rcp32(r0), i1 = rcp32(r1);
+            if (kGuard) {
+                i0 = r0 > 2.0e-13f ? i0 : 0.0f;
+                i1 = r1 > 2.0e-13f ? i1 : 0.0f;
+            }
+            fma2p(f0, f1, i0, i1, s.w, -0.0f, -0.0f);
+            fma2v(ax[t], ax[t + 1], f0, f1, dx0, dx1, ax[t], ax[t + 1]);
+            fma2v(ay[t], ay[t + 1], f0, f1, dy0, dy1, ay[t], ay[t + 1]);
+            fma2v(az[t], az[t + 1], f0, f1, dz0, dz1, az[t], az[t + 1]);
         }
     }
 }

@@ -134,6 +134,26 @@ int direct_sum_any(lpm_ctx* ctx, const lpm_kernel_desc& k, int precision, const 
 int pack_f32(lpm_ctx* ctx, const double4* in, int64_t n, float4* out, bool scale_w2);
 int check_kernel_desc(const lpm_kernel_desc* k);
 
+// Packed FP32 (fma.rn.f32x2, sm_100): two FP32 FMAs in one instruction, each lane rounded like fmaf.
+// (d0, d1) = (a0 b + c0, a1 b + c1).
+__device__ __forceinline__ void fma2p(float& d0, float& d1, float a0, float a1, float b, float c0, float c1) {
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %4};\n\tmov.b64 rc, {%5, %6};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d0), "=f"(d1)
+        : "f"(a0), "f"(a1), "f"(b), "f"(c0), "f"(c1));
+}
+
+// (d0, d1) = (a0 b0 + c0, a1 b1 + c1).
+__device__ __forceinline__ void fma2v(float& d0, float& d1, float a0, float a1, float b0, float b1, float c0,
+                                      float c1) {
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d0), "=f"(d1)
+        : "f"(a0), "f"(a1), "f"(b0), "f"(b1), "f"(c0), "f"(c1));
+}
+
 }  // namespace lpm
 
 #endif  // __CUDACC__

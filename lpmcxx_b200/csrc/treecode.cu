@@ -680,24 +680,6 @@ __device__ __forceinline__ void horner(const T4* __restrict__ Bc, T e0, T e1, T 
 // FP32 Horner scheme with the four components in two packed pairs (fma.rn.f32x2, sm_100): half the FMA
 // instructions per coefficient for the same lane work and the same rounding (measured: far field 17-19%
 // faster).
-__device__ __forceinline__ void fma2p(float& d0, float& d1, float a0, float a1, float b, float c0, float c1) {
-    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
-        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %4};\n\tmov.b64 rc, {%5, %6};\n\t"
-        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(d0), "=f"(d1)
-        : "f"(a0), "f"(a1), "f"(b), "f"(c0), "f"(c1));
-}
-
-// (d0, d1) = (a0 b0 + c0, a1 b1 + c1) as one packed FMA.
-__device__ __forceinline__ void fma2v(float& d0, float& d1, float a0, float a1, float b0, float b1, float c0,
-                                      float c1) {
-    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
-        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
-        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(d0), "=f"(d1)
-        : "f"(a0), "f"(a1), "f"(b0), "f"(b1), "f"(c0), "f"(c1));
-}
-
 template <int P>
 __device__ __forceinline__ void horner_f32x2(const float4* __restrict__ Bc, float e0, float e1, float e2, float s,
                                              float& g0, float& g1, float& g2, float& g3) {
