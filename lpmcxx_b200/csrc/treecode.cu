@@ -651,6 +651,8 @@ __global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
 template <int P, typename T, typename T4>
 __device__ __forceinline__ void horner(const T4* __restrict__ Bc, T e0, T e1, T e2, T s, T& g0, T& g1, T& g2,
                                        T& g3) {
+    // Each chain starts from its leading term (an FMA onto a zero accumulator cannot be folded away by
+    // the compiler, since 0 * e is not 0 for infinite e): one FMA per coefficient after the first.
     int q = 0;
     T G0 = 0, G1 = 0, G2 = 0, G3 = 0;
 #pragma unroll
@@ -666,13 +668,29 @@ __device__ __forceinline__ void horner(const T4* __restrict__ Bc, T e0, T e1, T 
 #pragma unroll
                 for (int c = Q - 1 - a - b; c >= 0; --c) {
                     const T4 v = Bc[q++];
-                    R0 = fma(R0, e2, v.x); R1 = fma(R1, e2, v.y); R2 = fma(R2, e2, v.z); R3 = fma(R3, e2, v.w);
+                    if (c == Q - 1 - a - b) {
+                        R0 = v.x; R1 = v.y; R2 = v.z; R3 = v.w;
+                    } else {
+                        R0 = fma(R0, e2, v.x); R1 = fma(R1, e2, v.y); R2 = fma(R2, e2, v.z); R3 = fma(R3, e2, v.w);
+                    }
                 }
-                Q0 = fma(Q0, e1, R0); Q1 = fma(Q1, e1, R1); Q2 = fma(Q2, e1, R2); Q3 = fma(Q3, e1, R3);
+                if (b == Q - 1 - a) {
+                    Q0 = R0; Q1 = R1; Q2 = R2; Q3 = R3;
+                } else {
+                    Q0 = fma(Q0, e1, R0); Q1 = fma(Q1, e1, R1); Q2 = fma(Q2, e1, R2); Q3 = fma(Q3, e1, R3);
+                }
             }
-            P0 = fma(P0, e0, Q0); P1 = fma(P1, e0, Q1); P2 = fma(P2, e0, Q2); P3 = fma(P3, e0, Q3);
+            if (a == Q - 1) {
+                P0 = Q0; P1 = Q1; P2 = Q2; P3 = Q3;
+            } else {
+                P0 = fma(P0, e0, Q0); P1 = fma(P1, e0, Q1); P2 = fma(P2, e0, Q2); P3 = fma(P3, e0, Q3);
+            }
         }
-        G0 = fma(G0, s, P0); G1 = fma(G1, s, P1); G2 = fma(G2, s, P2); G3 = fma(G3, s, P3);
+        if (m == (P - 1) / 2) {
+            G0 = P0; G1 = P1; G2 = P2; G3 = P3;
+        } else {
+            G0 = fma(G0, s, P0); G1 = fma(G1, s, P1); G2 = fma(G2, s, P2); G3 = fma(G3, s, P3);
+        }
     }
     g0 = G0; g1 = G1; g2 = G2; g3 = G3;
 }
@@ -698,17 +716,33 @@ __device__ __forceinline__ void horner_f32x2(const float4* __restrict__ Bc, floa
 #pragma unroll
                 for (int c = Q - 1 - a - b; c >= 0; --c) {
                     const float4 v = Bc[q++];
-                    fma2p(R0, R1, R0, R1, e2, v.x, v.y);
-                    fma2p(R2, R3, R2, R3, e2, v.z, v.w);
+                    if (c == Q - 1 - a - b) {  // leading term: no FMA (see horner)
+                        R0 = v.x; R1 = v.y; R2 = v.z; R3 = v.w;
+                    } else {
+                        fma2p(R0, R1, R0, R1, e2, v.x, v.y);
+                        fma2p(R2, R3, R2, R3, e2, v.z, v.w);
+                    }
                 }
-                fma2p(Q0, Q1, Q0, Q1, e1, R0, R1);
-                fma2p(Q2, Q3, Q2, Q3, e1, R2, R3);
+                if (b == Q - 1 - a) {
+                    Q0 = R0; Q1 = R1; Q2 = R2; Q3 = R3;
+                } else {
+                    fma2p(Q0, Q1, Q0, Q1, e1, R0, R1);
+                    fma2p(Q2, Q3, Q2, Q3, e1, R2, R3);
+                }
             }
-            fma2p(P0, P1, P0, P1, e0, Q0, Q1);
-            fma2p(P2, P3, P2, P3, e0, Q2, Q3);
+            if (a == Q - 1) {
+                P0 = Q0; P1 = Q1; P2 = Q2; P3 = Q3;
+            } else {
+                fma2p(P0, P1, P0, P1, e0, Q0, Q1);
+                fma2p(P2, P3, P2, P3, e0, Q2, Q3);
+            }
         }
-        fma2p(G0, G1, G0, G1, s, P0, P1);
-        fma2p(G2, G3, G2, G3, s, P2, P3);
+        if (m == (P - 1) / 2) {
+            G0 = P0; G1 = P1; G2 = P2; G3 = P3;
+        } else {
+            fma2p(G0, G1, G0, G1, s, P0, P1);
+            fma2p(G2, G3, G2, G3, s, P2, P3);
+        }
     }
     g0 = G0; g1 = G1; g2 = G2; g3 = G3;
 }
@@ -818,24 +852,23 @@ struct FarArgs {
 constexpr int kFarStageUnits = LPM_FAR_STAGE_UNITS;  // 16-byte units gathered per stage (at least one entry)
 constexpr int kFarMinBlocks = LPM_FAR_MIN_BLOCKS;    // resident blocks per SM the far kernels are built for
 
-template <int P, typename F4>
+template <int P, typename F4, int U = kFarStageUnits>
 struct FarShape {
     static constexpr int kUnits = entries_for(P) * (int)(sizeof(F4) / 16);  // per entry
-    static constexpr int kK =
-        kUnits >= kFarStageUnits ? 1 : (kFarStageUnits / kUnits > 32 ? 32 : kFarStageUnits / kUnits);
+    static constexpr int kK = kUnits >= U ? 1 : (U / kUnits > 32 ? 32 : U / kUnits);
     static constexpr int kStage = kK * kUnits;  // units per stage buffer
     static constexpr size_t kSmem = 2 * (size_t)kStage * 16 + 2 * (size_t)kK * sizeof(double4);
 };
 
 // Issue the copies of entries [s0, s0 + n) of the batch's order-P list into one stage: coefficients by
 // cp.async, cluster centres by plain stores.
-template <int P, typename F4>
+template <int P, typename F4, int NT = kBatch>
 __device__ __forceinline__ void far_stage_gather(const FarArgs& A, int64_t s0, int n, float4* buf, double4* ctr) {
-    using S = FarShape<P, F4>;
+    constexpr int kUnits = FarShape<P, F4>::kUnits;
     constexpr int kSub = (int)(sizeof(F4) / 16);
     const F4* base = (const F4*)(kSub == 2 ? (const void*)A.B64 : (const void*)A.B32);
-    for (int i = threadIdx.x; i < n * S::kUnits; i += kBatch) {
-        const int e = i / S::kUnits, j = i - e * S::kUnits;
+    for (int i = threadIdx.x; i < n * kUnits; i += NT) {
+        const int e = i / kUnits, j = i - e * kUnits;
         const int node = A.far_list[s0 + e].x;
         const char* src = (const char*)(base + (size_t)node * A.n_ent + A.gtab[j / kSub]) + 16 * (j % kSub);
         cp_async16(buf + i, src);
@@ -890,6 +923,165 @@ __global__ void __launch_bounds__(kBatch, kFarMinBlocks) far_order_kernel(FarArg
     }
 }
 
+// ---- two targets per thread (FP32, low and middle orders)
+// The Horner scheme of horner_f32x2 for two targets at once: every coefficient read from shared memory
+// feeds both targets' chains (four packed FMAs per load instead of two) and each thread carries two
+// independent dependency chains.  e[t] = (e0, e1, e2, s) of target t; same arithmetic per target as
+// horner_f32x2.
+template <int P>
+__device__ __forceinline__ void horner2_f32x2(const float4* __restrict__ Bc, const float (&e)[2][4],
+                                              float (&g)[2][4]) {
+    int q = 0;
+    float G[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll
+    for (int m = (P - 1) / 2; m >= 0; --m) {
+        const int Q = P - 2 * m;
+        float Pa[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll
+        for (int a = Q - 1; a >= 0; --a) {
+            float Qa[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll
+            for (int b = Q - 1 - a; b >= 0; --b) {
+                float R[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll
+                for (int c = Q - 1 - a - b; c >= 0; --c) {
+                    const float4 v = Bc[q++];
+#pragma unroll
+                    for (int t = 0; t < 2; ++t) {
+                        if (c == Q - 1 - a - b) {  // leading term: no FMA (see horner)
+                            R[t][0] = v.x; R[t][1] = v.y; R[t][2] = v.z; R[t][3] = v.w;
+                        } else {
+                            fma2p(R[t][0], R[t][1], R[t][0], R[t][1], e[t][2], v.x, v.y);
+                            fma2p(R[t][2], R[t][3], R[t][2], R[t][3], e[t][2], v.z, v.w);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    if (b == Q - 1 - a) {
+                        Qa[t][0] = R[t][0]; Qa[t][1] = R[t][1]; Qa[t][2] = R[t][2]; Qa[t][3] = R[t][3];
+                    } else {
+                        fma2p(Qa[t][0], Qa[t][1], Qa[t][0], Qa[t][1], e[t][1], R[t][0], R[t][1]);
+                        fma2p(Qa[t][2], Qa[t][3], Qa[t][2], Qa[t][3], e[t][1], R[t][2], R[t][3]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                if (a == Q - 1) {
+                    Pa[t][0] = Qa[t][0]; Pa[t][1] = Qa[t][1]; Pa[t][2] = Qa[t][2]; Pa[t][3] = Qa[t][3];
+                } else {
+                    fma2p(Pa[t][0], Pa[t][1], Pa[t][0], Pa[t][1], e[t][0], Qa[t][0], Qa[t][1]);
+                    fma2p(Pa[t][2], Pa[t][3], Pa[t][2], Pa[t][3], e[t][0], Qa[t][2], Qa[t][3]);
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            if (m == (P - 1) / 2) {
+                G[t][0] = Pa[t][0]; G[t][1] = Pa[t][1]; G[t][2] = Pa[t][2]; G[t][3] = Pa[t][3];
+            } else {
+                fma2p(G[t][0], G[t][1], G[t][0], G[t][1], e[t][3], Pa[t][0], Pa[t][1]);
+                fma2p(G[t][2], G[t][3], G[t][2], G[t][3], e[t][3], Pa[t][2], Pa[t][3]);
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) g[t][c] = G[t][c];
+}
+
+// far_one_acc<P, float, float4> for two targets (identical arithmetic per target).
+template <int P>
+__device__ __forceinline__ void far_one_acc2(const float4* __restrict__ Bc, const double4 (&x)[2], double cx,
+                                             double cy, double cz, double (&acc)[2][3]) {
+    float d[2][3], e[2][4], g[2][4];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const float dx = (float)(cx - x[t].x), dy = (float)(cy - x[t].y), dz = (float)(cz - x[t].z);
+        const float inv = 1.0f / (dx * dx + dy * dy + dz * dz);
+        d[t][0] = dx; d[t][1] = dy; d[t][2] = dz;
+        e[t][0] = dx * inv; e[t][1] = dy * inv; e[t][2] = dz * inv; e[t][3] = inv;
+    }
+    horner2_f32x2<P>(Bc, e, g);
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const float dx = d[t][0], dy = d[t][1], dz = d[t][2];
+        const float s = 2.0f * e[t][3];
+        const float G0 = s * g[t][0], Gx = s * g[t][1], Gy = s * g[t][2], Gz = s * g[t][3];
+        const float xx = (float)x[t].x, xy = (float)x[t].y, xz = (float)x[t].z;
+        acc[t][0] += (double)((xy * dz - xz * dy) * G0 + (xy * Gz - xz * Gy));
+        acc[t][1] += (double)((xz * dx - xx * dz) * G0 + (xz * Gx - xx * Gz));
+        acc[t][2] += (double)((xx * dy - xy * dx) * G0 + (xx * Gy - xy * Gx));
+    }
+}
+
+#ifndef LPM_FAR2_MAX_ORDER
+#define LPM_FAR2_MAX_ORDER 9
+#endif
+#ifndef LPM_FAR2_STAGE_UNITS
+#define LPM_FAR2_STAGE_UNITS 512
+#endif
+#ifndef LPM_FAR2_MIN_BLOCKS
+#define LPM_FAR2_MIN_BLOCKS 10
+#endif
+constexpr int kFar2MaxOrder = LPM_FAR2_MAX_ORDER;  // FP32 orders up to this run two targets per thread
+constexpr int kFar2Threads = kBatch / 2;
+constexpr int kFar2StageUnits = LPM_FAR2_STAGE_UNITS;
+constexpr int kFar2MinBlocks = LPM_FAR2_MIN_BLOCKS;
+
+// far_order_kernel<P, float, float4> with two targets per thread (targets i and i + 64 of the batch):
+// 64 threads per block, stages of kFar2StageUnits, same double buffering and the same sums.
+template <int P>
+__global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kernel(FarArgs A) {
+    using S = FarShape<P, float4, kFar2StageUnits>;
+    extern __shared__ float4 fbuf[];  // 2 stages of S::kStage units, then 2 x kK centres
+    double4* ctr = (double4*)(fbuf + 2 * S::kStage);
+    const int64_t b = blockIdx.x;
+    if (b >= *A.nbat) return;  // uniform per block
+    const int64_t f0 = A.far_off[b], f1 = min(f0 + (int64_t)A.far_cnt[b], A.far_cap);
+    if (f0 >= f1) return;  // uniform per block
+    const int64_t q0 = A.batch_first[b], qe = A.batch_first[b + 1];
+    const int64_t qa = q0 + threadIdx.x, qb = qa + kFar2Threads;
+    const bool live = q0 + (int64_t)(threadIdx.x & ~31) < qe;  // warp-uniform (second targets lie further on)
+    const double4 x[2] = {qa < qe ? A.tgt_sorted[qa] : make_double4(0, 0, 1, 0),
+                          qb < qe ? A.tgt_sorted[qb] : make_double4(0, 0, 1, 0)};
+    double acc[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    far_stage_gather<P, float4, kFar2Threads>(A, f0, (int)min((int64_t)S::kK, f1 - f0), fbuf, ctr);
+    cp_async_commit();
+    int s = 0;
+    for (int64_t s0 = f0;; s ^= 1) {
+        const int n = (int)min((int64_t)S::kK, f1 - s0);
+        const int64_t s1 = s0 + n;
+        if (s1 < f1)
+            far_stage_gather<P, float4, kFar2Threads>(A, s1, (int)min((int64_t)S::kK, f1 - s1),
+                                                      fbuf + (size_t)(s ^ 1) * S::kStage, ctr + (s ^ 1) * S::kK);
+        cp_async_commit();
+        cp_async_wait_prev();
+        __syncthreads();  // stage s resident
+        if (live) {
+            const float4* Bc = fbuf + (size_t)s * S::kStage;
+            const double4* cs = ctr + s * S::kK;
+            for (int k = 0; k < n; ++k)
+                far_one_acc2<P>(Bc + (size_t)k * entries_for(P), x, cs[k].x, cs[k].y, cs[k].z, acc);
+        }
+        if (s1 >= f1) break;
+        __syncthreads();  // stage s consumed before it is refilled
+        s0 = s1;
+    }
+    if (qa < qe) {
+        A.V[qa] += acc[0][0];
+        A.V[A.n_tgt + qa] += acc[0][1];
+        A.V[2 * A.n_tgt + qa] += acc[0][2];
+    }
+    if (qb < qe) {
+        A.V[qb] += acc[1][0];
+        A.V[A.n_tgt + qb] += acc[1][1];
+        A.V[2 * A.n_tgt + qb] += acc[1][2];
+    }
+}
+
 // The Horner scheme of `horner` with scalar coefficients.
 template <int P, typename T>
 __device__ __forceinline__ T horner1(const T* __restrict__ Bc, T e0, T e1, T e2, T s) {
@@ -906,12 +1098,15 @@ __device__ __forceinline__ T horner1(const T* __restrict__ Bc, T e0, T e1, T e2,
             for (int b = Q - 1 - a; b >= 0; --b) {
                 T R = 0;
 #pragma unroll
-                for (int c = Q - 1 - a - b; c >= 0; --c) R = fma(R, e2, Bc[q++]);
-                Qq = fma(Qq, e1, R);
+                for (int c = Q - 1 - a - b; c >= 0; --c) {
+                    const T v = Bc[q++];
+                    R = c == Q - 1 - a - b ? v : fma(R, e2, v);  // leading term: no FMA (see horner)
+                }
+                Qq = b == Q - 1 - a ? R : fma(Qq, e1, R);
             }
-            Pp = fma(Pp, e0, Qq);
+            Pp = a == Q - 1 ? Qq : fma(Pp, e0, Qq);
         }
-        G = fma(G, s, Pp);
+        G = m == (P - 1) / 2 ? Pp : fma(G, s, Pp);
     }
     return G;
 }
@@ -1011,30 +1206,36 @@ FarScalarFn far_scalar_select(int P, bool f64, size_t* smem) {
 typedef void (*FarKernelFn)(FarArgs);
 
 template <int P>
-FarKernelFn far_kernel_for(bool f64, size_t* smem) {
+FarKernelFn far_kernel_for(bool f64, size_t* smem, int* threads) {
+    *threads = kBatch;
     if (f64) {
         *smem = FarShape<P, double4>::kSmem;
         return far_order_kernel<P, double, double4>;
+    }
+    if constexpr (P <= kFar2MaxOrder) {
+        *threads = kFar2Threads;
+        *smem = FarShape<P, float4, kFar2StageUnits>::kSmem;
+        return far_order2_kernel<P>;
     }
     *smem = FarShape<P, float4>::kSmem;
     return far_order_kernel<P, float, float4>;
 }
 
 // The order-P far kernel (FP64 or FP32 arithmetic) and its dynamic shared memory.
-FarKernelFn far_kernel_select(int P, bool f64, size_t* smem) {
+FarKernelFn far_kernel_select(int P, bool f64, size_t* smem, int* threads) {
     switch (P) {
-        case 1: return far_kernel_for<1>(f64, smem);
-        case 2: return far_kernel_for<2>(f64, smem);
-        case 3: return far_kernel_for<3>(f64, smem);
-        case 4: return far_kernel_for<4>(f64, smem);
-        case 5: return far_kernel_for<5>(f64, smem);
-        case 6: return far_kernel_for<6>(f64, smem);
-        case 7: return far_kernel_for<7>(f64, smem);
-        case 8: return far_kernel_for<8>(f64, smem);
-        case 9: return far_kernel_for<9>(f64, smem);
-        case 10: return far_kernel_for<10>(f64, smem);
-        case 11: return far_kernel_for<11>(f64, smem);
-        default: return far_kernel_for<12>(f64, smem);
+        case 1: return far_kernel_for<1>(f64, smem, threads);
+        case 2: return far_kernel_for<2>(f64, smem, threads);
+        case 3: return far_kernel_for<3>(f64, smem, threads);
+        case 4: return far_kernel_for<4>(f64, smem, threads);
+        case 5: return far_kernel_for<5>(f64, smem, threads);
+        case 6: return far_kernel_for<6>(f64, smem, threads);
+        case 7: return far_kernel_for<7>(f64, smem, threads);
+        case 8: return far_kernel_for<8>(f64, smem, threads);
+        case 9: return far_kernel_for<9>(f64, smem, threads);
+        case 10: return far_kernel_for<10>(f64, smem, threads);
+        case 11: return far_kernel_for<11>(f64, smem, threads);
+        default: return far_kernel_for<12>(f64, smem, threads);
     }
 }
 
@@ -1374,7 +1575,8 @@ static cudaError_t far_smem_attributes() {
     for (int P = 1; P <= kPMax; ++P)
         for (int f64 = 0; f64 < 2; ++f64) {
             size_t smem = 0;
-            FarKernelFn fn = far_kernel_select(P, f64 != 0, &smem);
+            int threads = 0;
+            FarKernelFn fn = far_kernel_select(P, f64 != 0, &smem, &threads);
             if (smem > 48 * 1024) {
                 const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 if (e != cudaSuccess) return e;
@@ -1789,8 +1991,9 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
                 FarScalarFn fs = far_scalar_select(P, P >= t->f64_from, &smem);
                 LPM_LAUNCH(ctx, "far_kernel", fs, (unsigned)t->n_batches, kBatch, smem, F, t->a_stride);
             } else {
-                FarKernelFn fn = far_kernel_select(P, P >= t->f64_from, &smem);
-                LPM_LAUNCH(ctx, "far_kernel", fn, (unsigned)t->n_batches, kBatch, smem, F);
+                int threads = 0;
+                FarKernelFn fn = far_kernel_select(P, P >= t->f64_from, &smem, &threads);
+                LPM_LAUNCH(ctx, "far_kernel", fn, (unsigned)t->n_batches, threads, smem, F);
             }
         }
     }
