@@ -250,16 +250,25 @@ __global__ void __launch_bounds__(kThreads) bs_f32_kernel(const float4* __restri
 template <bool kGuard>
 __device__ __forceinline__ void poisson_f32_tile(const float4* tile, int m, const float* tx, const float* ty,
                                                  const float* tz, float* acc) {
+    // targets in pairs through packed FMAs, rounded as the scalar form (see bs_f32_tile)
 #pragma unroll 4
     for (int k = 0; k < m; ++k) {
         const float4 s = tile[k];
 #pragma unroll
-        for (int t = 0; t < kTpt32; ++t) {
-            const float dx = tx[t] - s.x, dy = ty[t] - s.y, dz = tz[t] - s.z;
-            const float rr = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            float inv = rsqrt32(rr);
-            if (kGuard) inv = rr > 0.0f ? inv : 0.0f;
-            acc[t] = fmaf(s.w, inv, acc[t]);
+        for (int t = 0; t < kTpt32; t += 2) {
+            float dx0, dx1, dy0, dy1, dz0, dz1, r0, r1;
+            fma2p(dx0, dx1, s.x, s.x, -1.0f, tx[t], tx[t + 1]);
+            fma2p(dy0, dy1, s.y, s.y, -1.0f, ty[t], ty[t + 1]);
+            fma2p(dz0, dz1, s.z, s.z, -1.0f, tz[t], tz[t + 1]);
+            fma2v(r0, r1, dx0, dx1, dx0, dx1, -0.0f, -0.0f);
+            fma2v(r0, r1, dy0, dy1, dy0, dy1, r0, r1);
+            fma2v(r0, r1, dz0, dz1, dz0, dz1, r0, r1);
+            float i0 = rsqrt32(r0), i1 = rsqrt32(r1);
+            if (kGuard) {
+                i0 = r0 > 0.0f ? i0 : 0.0f;
+                i1 = r1 > 0.0f ? i1 : 0.0f;
+            }
+            fma2p(acc[t], acc[t + 1], i0, i1, s.w, acc[t], acc[t + 1]);
         }
     }
 }

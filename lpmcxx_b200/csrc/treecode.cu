@@ -94,6 +94,11 @@ __device__ __forceinline__ float rcp32(float x) {
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
+__device__ __forceinline__ float rsqrt32(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 // ---------------------------------------------------------------------------------- per-evaluation kernels
 __global__ void gather_sources_kernel(const double4* __restrict__ X, const int32_t* __restrict__ perm,
@@ -1381,16 +1386,20 @@ __device__ __forceinline__ void finish_target(int64_t q, int64_t qe, int64_t n_t
 // tiles); a source at the target's own position (r = 0) contributes nothing.
 __device__ __forceinline__ void near_tile_scalar(const float4* tile, int m, float tx0, float ty0, float tz0,
                                                  float tx1, float ty1, float tz1, double* D0, double* D1) {
+    // the two targets travel as packed pairs (fma.rn.f32x2): d = t - y, rr = |d|^2, a += w / sqrt(rr)
     float a = 0.f, c = 0.f;
 #pragma unroll 4
     for (int j = 0; j < m; ++j) {
         const float4 y = tile[j];
-        const float dx = tx0 - y.x, dy = ty0 - y.y, dz = tz0 - y.z;
-        const float rr = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        a = fmaf(y.w, rr > 0.f ? rsqrtf(rr) : 0.f, a);
-        const float ex = tx1 - y.x, ey = ty1 - y.y, ez = tz1 - y.z;
-        const float ss = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-        c = fmaf(y.w, ss > 0.f ? rsqrtf(ss) : 0.f, c);
+        float dx0, dx1, dy0, dy1, dz0, dz1, r0, r1;
+        fma2p(dx0, dx1, y.x, y.x, -1.0f, tx0, tx1);
+        fma2p(dy0, dy1, y.y, y.y, -1.0f, ty0, ty1);
+        fma2p(dz0, dz1, y.z, y.z, -1.0f, tz0, tz1);
+        fma2v(r0, r1, dx0, dx1, dx0, dx1, -0.0f, -0.0f);
+        fma2v(r0, r1, dy0, dy1, dy0, dy1, r0, r1);
+        fma2v(r0, r1, dz0, dz1, dz0, dz1, r0, r1);
+        const float i0 = r0 > 0.f ? rsqrt32(r0) : 0.f, i1 = r1 > 0.f ? rsqrt32(r1) : 0.f;
+        fma2p(a, c, i0, i1, y.w, a, c);
     }
     D0[0] += a;
     D1[0] += c;
