@@ -928,7 +928,7 @@ __global__ void __launch_bounds__(kBatch, kFarMinBlocks) far_order_kernel(FarArg
     }
 }
 
-// ---- two targets per thread (FP32, low and middle orders)
+// ---- two targets per thread (FP32)
 // The Horner scheme of horner_f32x2 for two targets at once: every coefficient read from shared memory
 // feeds both targets' chains (four packed FMAs per load instead of two) and each thread carries two
 // independent dependency chains.  e[t] = (e0, e1, e2, s) of target t; same arithmetic per target as
@@ -1023,7 +1023,7 @@ __device__ __forceinline__ void far_one_acc2(const float4* __restrict__ Bc, cons
 }
 
 #ifndef LPM_FAR2_MAX_ORDER
-#define LPM_FAR2_MAX_ORDER 9
+#define LPM_FAR2_MAX_ORDER 11
 #endif
 #ifndef LPM_FAR2_STAGE_UNITS
 #define LPM_FAR2_STAGE_UNITS 512
@@ -1031,7 +1031,7 @@ __device__ __forceinline__ void far_one_acc2(const float4* __restrict__ Bc, cons
 #ifndef LPM_FAR2_MIN_BLOCKS
 #define LPM_FAR2_MIN_BLOCKS 10
 #endif
-constexpr int kFar2MaxOrder = LPM_FAR2_MAX_ORDER;  // FP32 orders up to this run two targets per thread
+constexpr int kFar2MaxOrder = LPM_FAR2_MAX_ORDER;  // FP32 orders up to this run two targets per thread (all used)
 constexpr int kFar2Threads = kBatch / 2;
 constexpr int kFar2StageUnits = LPM_FAR2_STAGE_UNITS;
 constexpr int kFar2MinBlocks = LPM_FAR2_MIN_BLOCKS;
@@ -1119,14 +1119,71 @@ __device__ __forceinline__ T horner1(const T* __restrict__ Bc, T e0, T e1, T e2,
 __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 
+// horner1 for two targets at once, packed across the targets (fma.rn.f32x2 with each target's own
+// variable): one FMA instruction per coefficient for both targets, the same rounding per target as
+// horner1.  e[t] = (e0, e1, e2, s) of target t.
+template <int P>
+__device__ __forceinline__ void horner1x2(const float* __restrict__ Bc, const float (&e)[2][4], float (&g)[2]) {
+    int q = 0;
+    float G0 = 0, G1 = 0;
+#pragma unroll
+    for (int m = (P - 1) / 2; m >= 0; --m) {
+        const int Q = P - 2 * m;
+        float P0 = 0, P1 = 0;
+#pragma unroll
+        for (int a = Q - 1; a >= 0; --a) {
+            float Q0 = 0, Q1 = 0;
+#pragma unroll
+            for (int b = Q - 1 - a; b >= 0; --b) {
+                float R0 = 0, R1 = 0;
+#pragma unroll
+                for (int c = Q - 1 - a - b; c >= 0; --c) {
+                    const float v = Bc[q++];
+                    if (c == Q - 1 - a - b) {
+                        R0 = v; R1 = v;
+                    } else {
+                        fma2v(R0, R1, R0, R1, e[0][2], e[1][2], v, v);
+                    }
+                }
+                if (b == Q - 1 - a) {
+                    Q0 = R0; Q1 = R1;
+                } else {
+                    fma2v(Q0, Q1, Q0, Q1, e[0][1], e[1][1], R0, R1);
+                }
+            }
+            if (a == Q - 1) {
+                P0 = Q0; P1 = Q1;
+            } else {
+                fma2v(P0, P1, P0, P1, e[0][0], e[1][0], Q0, Q1);
+            }
+        }
+        if (m == (P - 1) / 2) {
+            G0 = P0; G1 = P1;
+        } else {
+            fma2v(G0, G1, G0, G1, e[0][3], e[1][3], P0, P1);
+        }
+    }
+    g[0] = G0;
+    g[1] = G1;
+}
+
+#ifndef LPM_FAR2_SCALAR_MAX_ORDER
+#define LPM_FAR2_SCALAR_MAX_ORDER 12
+#endif
+constexpr int kFar2ScalarMaxOrder = LPM_FAR2_SCALAR_MAX_ORDER;  // FP32 scalar orders up to this: 2 targets/thread
+
 // Far field of the scalar 1/|x - y| kernel at order P (= pm; degree < P): one block per target batch,
-// one thread per target; each entry's contiguous coefficient row (stride entries, 16-byte aligned) is
-// staged with cp.async, kK entries per stage, double-buffered.  Adds sum w/|x - y| to V[q].
-template <int P, typename F>
-__global__ void __launch_bounds__(kBatch) far_scalar_kernel(FarArgs A, int stride) {
+// T targets per thread (targets i, i + 128/T, ...; T = 2 only in FP32); each entry's contiguous
+// coefficient row (stride entries, 16-byte aligned) is staged with cp.async, kK entries per stage,
+// double-buffered.  Adds sum w/|x - y| to V[q].
+template <int P, typename F, int T>
+__global__ void __launch_bounds__(kBatch / T) far_scalar_kernel(FarArgs A, int stride) {
+    constexpr int kNT = kBatch / T;
+    constexpr int kU = T == 2 ? kFar2StageUnits : kFarStageUnits;
     constexpr int kE = entries_for(P);
     constexpr int kUnits = (kE * (int)sizeof(F) + 15) / 16;
-    constexpr int kK = kUnits >= kFarStageUnits ? 1 : (kFarStageUnits / kUnits > 32 ? 32 : kFarStageUnits / kUnits);
+    constexpr int kK = kUnits >= kU ? 1 : (kU / kUnits > 32 ? 32 : kU / kUnits);
+    static_assert(T == 1 || (T == 2 && sizeof(F) == 4), "two targets per thread in FP32 only");
     extern __shared__ float4 fbuf[];  // 2 stages of kK x kUnits units, then 2 x kK centres
     double4* ctr = (double4*)(fbuf + 2 * kK * kUnits);
     const int64_t b = blockIdx.x;
@@ -1135,17 +1192,21 @@ __global__ void __launch_bounds__(kBatch) far_scalar_kernel(FarArgs A, int strid
     if (f0 >= f1) return;  // uniform per block
     const int64_t q0 = A.batch_first[b], qe = A.batch_first[b + 1];
     const int64_t q = q0 + threadIdx.x;
-    const bool live = q0 + (int64_t)(threadIdx.x & ~31) < qe;  // warp-uniform
-    const double4 x = q < qe ? A.tgt_sorted[q] : make_double4(2, 2, 2, 0);
+    const bool live = q0 + (int64_t)(threadIdx.x & ~31) < qe;  // warp-uniform (later targets lie further on)
+    double4 x[T];
+#pragma unroll
+    for (int t = 0; t < T; ++t) x[t] = q + t * kNT < qe ? A.tgt_sorted[q + t * kNT] : make_double4(2, 2, 2, 0);
     const F* base = (const F*)(sizeof(F) == 8 ? (const void*)A.B64 : (const void*)A.B32);
     auto gather = [&](int64_t s0, int n, float4* buf, double4* cs) {
-        for (int i = threadIdx.x; i < n * kUnits; i += kBatch) {
+        for (int i = threadIdx.x; i < n * kUnits; i += kNT) {
             const int e = i / kUnits, j = i - e * kUnits;
             cp_async16(buf + i, (const char*)(base + (size_t)A.far_list[s0 + e].x * stride) + 16 * j);
         }
         if ((int)threadIdx.x < n) cs[threadIdx.x] = A.node_ctr[A.far_list[s0 + threadIdx.x].x];
     };
-    double acc = 0.0;
+    double acc[T];
+#pragma unroll
+    for (int t = 0; t < T; ++t) acc[t] = 0.0;
     gather(f0, (int)min((int64_t)kK, f1 - f0), fbuf, ctr);
     cp_async_commit();
     int sb = 0;
@@ -1160,51 +1221,72 @@ __global__ void __launch_bounds__(kBatch) far_scalar_kernel(FarArgs A, int strid
             const float4* buf = fbuf + (size_t)sb * kK * kUnits;
             const double4* cs = ctr + sb * kK;
             for (int k = 0; k < n; ++k) {
-                const F dx = (F)(cs[k].x - x.x), dy = (F)(cs[k].y - x.y), dz = (F)(cs[k].z - x.z);
-                const F rinv = rsqrt_t(dx * dx + dy * dy + dz * dz);
-                const F s2 = rinv * rinv;
-                acc += (double)(rinv * horner1<P, F>((const F*)(buf + (size_t)k * kUnits), dx * s2, dy * s2, dz * s2, s2));
+                F rinv[T], e[T][4];
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    const F dx = (F)(cs[k].x - x[t].x), dy = (F)(cs[k].y - x[t].y), dz = (F)(cs[k].z - x[t].z);
+                    rinv[t] = rsqrt_t(dx * dx + dy * dy + dz * dz);
+                    const F s2 = rinv[t] * rinv[t];
+                    e[t][0] = dx * s2; e[t][1] = dy * s2; e[t][2] = dz * s2; e[t][3] = s2;
+                }
+                const F* row = (const F*)(buf + (size_t)k * kUnits);
+                if constexpr (T == 2) {
+                    float g[2];
+                    horner1x2<P>(row, e, g);
+                    acc[0] += (double)(rinv[0] * g[0]);
+                    acc[1] += (double)(rinv[1] * g[1]);
+                } else {
+                    acc[0] += (double)(rinv[0] * horner1<P, F>(row, e[0][0], e[0][1], e[0][2], e[0][3]));
+                }
             }
         }
         if (s1 >= f1) break;
         __syncthreads();  // stage sb consumed before it is refilled
         s0 = s1;
     }
-    if (q < qe) A.V[q] += acc;
+#pragma unroll
+    for (int t = 0; t < T; ++t)
+        if (q + t * kNT < qe) A.V[q + t * kNT] += acc[t];
 }
 
 typedef void (*FarScalarFn)(FarArgs, int);
 
 template <int P>
-FarScalarFn far_scalar_for(bool f64, size_t* smem) {
+FarScalarFn far_scalar_for(bool f64, size_t* smem, int* threads) {
     constexpr int kE = entries_for(P);
-    auto sm = [](int bytes) {
+    auto sm = [](int bytes, int U) {
         const int units = (kE * bytes + 15) / 16;
-        const int k = units >= kFarStageUnits ? 1 : (kFarStageUnits / units > 32 ? 32 : kFarStageUnits / units);
+        const int k = units >= U ? 1 : (U / units > 32 ? 32 : U / units);
         return 2 * (size_t)k * units * 16 + 2 * (size_t)k * sizeof(double4);
     };
+    *threads = kBatch;
     if (f64) {
-        *smem = sm(8);
-        return far_scalar_kernel<P, double>;
+        *smem = sm(8, kFarStageUnits);
+        return far_scalar_kernel<P, double, 1>;
     }
-    *smem = sm(4);
-    return far_scalar_kernel<P, float>;
+    if constexpr (P <= kFar2ScalarMaxOrder) {
+        *threads = kBatch / 2;
+        *smem = sm(4, kFar2StageUnits);
+        return far_scalar_kernel<P, float, 2>;
+    }
+    *smem = sm(4, kFarStageUnits);
+    return far_scalar_kernel<P, float, 1>;
 }
 
-FarScalarFn far_scalar_select(int P, bool f64, size_t* smem) {
+FarScalarFn far_scalar_select(int P, bool f64, size_t* smem, int* threads) {
     switch (P) {
-        case 1: return far_scalar_for<1>(f64, smem);
-        case 2: return far_scalar_for<2>(f64, smem);
-        case 3: return far_scalar_for<3>(f64, smem);
-        case 4: return far_scalar_for<4>(f64, smem);
-        case 5: return far_scalar_for<5>(f64, smem);
-        case 6: return far_scalar_for<6>(f64, smem);
-        case 7: return far_scalar_for<7>(f64, smem);
-        case 8: return far_scalar_for<8>(f64, smem);
-        case 9: return far_scalar_for<9>(f64, smem);
-        case 10: return far_scalar_for<10>(f64, smem);
-        case 11: return far_scalar_for<11>(f64, smem);
-        default: return far_scalar_for<12>(f64, smem);
+        case 1: return far_scalar_for<1>(f64, smem, threads);
+        case 2: return far_scalar_for<2>(f64, smem, threads);
+        case 3: return far_scalar_for<3>(f64, smem, threads);
+        case 4: return far_scalar_for<4>(f64, smem, threads);
+        case 5: return far_scalar_for<5>(f64, smem, threads);
+        case 6: return far_scalar_for<6>(f64, smem, threads);
+        case 7: return far_scalar_for<7>(f64, smem, threads);
+        case 8: return far_scalar_for<8>(f64, smem, threads);
+        case 9: return far_scalar_for<9>(f64, smem, threads);
+        case 10: return far_scalar_for<10>(f64, smem, threads);
+        case 11: return far_scalar_for<11>(f64, smem, threads);
+        default: return far_scalar_for<12>(f64, smem, threads);
     }
 }
 
@@ -1997,8 +2079,9 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
             if (t->scalar) {
                 F.B64 = (const double4*)t->A64;
                 F.B32 = (const float4*)t->A32;
-                FarScalarFn fs = far_scalar_select(P, P >= t->f64_from, &smem);
-                LPM_LAUNCH(ctx, "far_kernel", fs, (unsigned)t->n_batches, kBatch, smem, F, t->a_stride);
+                int threads = 0;
+                FarScalarFn fs = far_scalar_select(P, P >= t->f64_from, &smem, &threads);
+                LPM_LAUNCH(ctx, "far_kernel", fs, (unsigned)t->n_batches, threads, smem, F, t->a_stride);
             } else {
                 int threads = 0;
                 FarKernelFn fn = far_kernel_select(P, P >= t->f64_from, &smem, &threads);
