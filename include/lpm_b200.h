@@ -48,6 +48,10 @@ extern "C" {
 
 #define LPM_KERNEL_BIOT_SAVART_SPHERE 1 /* BiotSavartSphere (src/LpmVectorKernel.h:19-39) */
 #define LPM_KERNEL_POISSON_3D 2         /* 1/(4 pi |x-y|): the ScalarKernel subclass the reference lacks */
+#define LPM_KERNEL_SPHERE_GREENS 3      /* SphereGreensFn (src/LpmScalarKernel.h:31-45) */
+#define LPM_KERNEL_PLANAR_LOG 4         /* PlanarGreensFnFreeBoundaries (src/LpmScalarKernel.h:19-29) */
+#define LPM_KERNEL_DELTA_3D 5           /* SecondOrderDelta3d (src/LpmScalarKernel.h:47-62) */
+#define LPM_KERNEL_SPHERE_DELTA 6       /* SphereDelta (src/LpmScalarKernel.h:64-78) */
 
 #define LPM_PREC_F64 0 /* FP64 throughout: parity path against the reference */
 #define LPM_PREC_F32 1 /* FP32 pairwise arithmetic, FP64 accumulation of per-tile FP32 partial sums */
@@ -55,7 +59,15 @@ extern "C" {
 /* Kernel descriptor: the data behind the reference's ScalarKernel / VectorKernel plugin objects.
  * BIOT_SAVART_SPHERE: K(x,y) = (x cross y)/(radius^2 - x.y + delta^2), 0 when |den| <= 1e-13,
  *   sum multiplier -1/(4 pi radius), singular iff delta == 0 (src/LpmVectorKernel.h:24-34).
- * POISSON_3D: K(x,y) = 1/(4 pi |x-y|), 0 at x == y. */
+ * POISSON_3D: K(x,y) = 1/(4 pi |x-y|), 0 at x == y.
+ * The rest of the reference's ScalarKernel family (direct sums in FP64 only; not in the treecode):
+ * SPHERE_GREENS: K = -log(radius^2 - x.y)/(4 pi radius), singular.
+ * PLANAR_LOG: K = log(|x-y|^2)/(4 pi), singular.
+ * DELTA_3D: K = 3 exp(-(|x-y|/eps)^3)/(4 pi eps^3) with eps in `delta`, not singular.
+ * SPHERE_DELTA: K = (2 eps^2 d - (1-d)^2)/(4 pi (1 - d + eps^2)^2) - 1/(4 pi), d = x.y, eps in `delta`,
+ *   not singular.
+ * A singular kernel's self pair (a face-centroid target and its own source; in the meshfree sum, point i
+ * and itself) is skipped by index, as the reference skips j == i (src/LpmDirectSum.cpp:49-68). */
 typedef struct lpm_kernel_desc {
     int32_t kind;
     int32_t reserved;
@@ -126,7 +138,9 @@ int lpm_direct_sum_f32_noalloc(const lpm_kernel_desc* kernel, const double* src,
  * vertices vert_begin..vert_end and undivided faces face_begin..face_end (inclusive); sources are all
  * undivided faces with strength src*area.  Outputs (host, caller-owned) are written only at target
  * indices: vert_out0..2 (n_verts) and face_out0..2 (n_faces); divided faces are left untouched.
- * Only vector kernels (Biot-Savart) are accepted here. */
+ * Scalar kernels (DirectSum::meshSolve's scalar branch, src/LpmDirectSum.cpp:29-93) write vert_out0 and
+ * face_out0 only (the other outputs may be NULL); a singular kernel skips each face target's own source,
+ * a non-singular one includes it.  FP32 takes the Biot-Savart and 3D Poisson kernels only. */
 int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precision, int64_t n_verts,
                         const double* vx, const double* vy, const double* vz, int64_t n_faces, const double* fx,
                         const double* fy, const double* fz, const double* face_area, const uint8_t* face_divided,
@@ -135,8 +149,10 @@ int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precisi
                         double* face_out1, double* face_out2);
 
 /* Host-facing meshfree scalar direct sum: DirectSum::meshfreeSolve (src/LpmDirectSum.cpp:175-254)
- * for the 3D Poisson kernel.  x/y/z/src(/weights, may be NULL) are host arrays of n points; targets are
- * points begin..end; out (host, n) is written at target indices. */
+ * for the scalar kernels.  x/y/z/src(/weights, may be NULL) are host arrays of n points; targets are
+ * points begin..end; out (host, n) is written at target indices.  A singular kernel skips j == i for
+ * every target (the reference's singular loops stop at endIndex(i) instead of endIndex(rank),
+ * src/LpmDirectSum.cpp:188,222, and run past the slice for i > 0: not restated). */
 int lpm_direct_sum_meshfree(lpm_ctx* ctx, const lpm_kernel_desc* kernel, int precision, int64_t n, const double* x,
                             const double* y, const double* z, const double* src, const double* weights, int64_t begin,
                             int64_t end, double* out);

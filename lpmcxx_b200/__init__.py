@@ -12,11 +12,13 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _capi
-from ._capi import (LPM_KERNEL_BIOT_SAVART_SPHERE, LPM_KERNEL_POISSON_3D, LPM_MESH_CUBED_SPHERE,
+from ._capi import (LPM_KERNEL_BIOT_SAVART_SPHERE, LPM_KERNEL_DELTA_3D, LPM_KERNEL_PLANAR_LOG,
+                    LPM_KERNEL_POISSON_3D, LPM_KERNEL_SPHERE_DELTA, LPM_KERNEL_SPHERE_GREENS, LPM_MESH_CUBED_SPHERE,
                     LPM_MESH_ICOS_TRI, LPM_PREC_F32, LPM_PREC_F64, KernelDesc, LpmError, check, lib, ptr)
 
 __all__ = [
-    "Context", "SphereMesh", "build_mesh", "mesh_counts", "biot_savart_kernel", "poisson_kernel", "LpmError",
+    "Context", "SphereMesh", "build_mesh", "mesh_counts", "biot_savart_kernel", "poisson_kernel",
+    "sphere_greens_kernel", "planar_log_kernel", "delta3d_kernel", "sphere_delta_kernel", "LpmError",
     "LPM_MESH_ICOS_TRI", "LPM_MESH_CUBED_SPHERE", "LPM_PREC_F64", "LPM_PREC_F32",
 ]
 
@@ -31,6 +33,26 @@ def biot_savart_kernel(radius: float = 1.0, delta: float = 0.0) -> KernelDesc:
 def poisson_kernel() -> KernelDesc:
     """1/(4 pi |x - y|), zero at x == y."""
     return KernelDesc(LPM_KERNEL_POISSON_3D, 0, 1.0, 0.0)
+
+
+def sphere_greens_kernel(radius: float = 1.0) -> KernelDesc:
+    """SphereGreensFn(r): -log(r^2 - x.y) / (4 pi r) (src/LpmScalarKernel.h:31-45); singular."""
+    return KernelDesc(LPM_KERNEL_SPHERE_GREENS, 0, float(radius), 0.0)
+
+
+def planar_log_kernel() -> KernelDesc:
+    """PlanarGreensFnFreeBoundaries: log(|x - y|^2) / (4 pi) (src/LpmScalarKernel.h:19-29); singular."""
+    return KernelDesc(LPM_KERNEL_PLANAR_LOG, 0, 1.0, 0.0)
+
+
+def delta3d_kernel(eps: float) -> KernelDesc:
+    """SecondOrderDelta3d(eps): 3 exp(-(|x - y|/eps)^3) / (4 pi eps^3) (src/LpmScalarKernel.h:47-62)."""
+    return KernelDesc(LPM_KERNEL_DELTA_3D, 0, 1.0, float(eps))
+
+
+def sphere_delta_kernel(eps: float) -> KernelDesc:
+    """SphereDelta(eps) (src/LpmScalarKernel.h:64-78)."""
+    return KernelDesc(LPM_KERNEL_SPHERE_DELTA, 0, 1.0, float(eps))
 
 
 @dataclass
@@ -142,19 +164,22 @@ class Context:
 
     def direct_sum_mesh(self, kernel: KernelDesc, precision: int, mesh: SphereMesh, face_src: np.ndarray,
                         vert_range=None, face_range=None, vert_out=None, face_out=None):
-        """DirectSum::meshSolve on host arrays; returns (vert_out (3,nv), face_out (3,nf))."""
+        """DirectSum::meshSolve on host arrays; returns (vert_out (c,nv), face_out (c,nf)) with c = 3 for
+        the Biot-Savart kernel and 1 for the scalar kernels."""
         nv, nf = mesh.n_verts, mesh.n_faces
+        comps = 3 if kernel.kind == LPM_KERNEL_BIOT_SAVART_SPHERE else 1
         vb, ve = vert_range if vert_range is not None else (0, nv - 1)
         fb, fe = face_range if face_range is not None else (0, nf - 1)
         vx, vy, vz = (np.ascontiguousarray(mesh.vert_xyz[:, c]) for c in range(3))
         fx, fy, fz = (np.ascontiguousarray(mesh.face_xyz[:, c]) for c in range(3))
-        vo = np.zeros((3, nv)) if vert_out is None else vert_out
-        fo = np.zeros((3, nf)) if face_out is None else face_out
+        vo = np.zeros((comps, nv)) if vert_out is None else vert_out
+        fo = np.zeros((comps, nf)) if face_out is None else face_out
         src = np.ascontiguousarray(face_src, dtype=np.float64)
+        rest = lambda a, c: ptr(a[c]) if comps == 3 else None  # noqa: E731
         check(lib().lpm_direct_sum_mesh(self.h, C.byref(kernel), precision, nv, ptr(vx), ptr(vy), ptr(vz), nf,
                                         ptr(fx), ptr(fy), ptr(fz), ptr(mesh.face_area), ptr(mesh.face_divided),
-                                        ptr(src), vb, ve, fb, fe, ptr(vo[0]), ptr(vo[1]), ptr(vo[2]),
-                                        ptr(fo[0]), ptr(fo[1]), ptr(fo[2])), "lpm_direct_sum_mesh")
+                                        ptr(src), vb, ve, fb, fe, ptr(vo[0]), rest(vo, 1), rest(vo, 2),
+                                        ptr(fo[0]), rest(fo, 1), rest(fo, 2)), "lpm_direct_sum_mesh")
         return vo, fo
 
     def direct_sum_meshfree(self, kernel: KernelDesc, precision: int, xyz: np.ndarray, src: np.ndarray,

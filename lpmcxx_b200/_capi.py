@@ -26,6 +26,10 @@ LPM_MESH_ICOS_TRI = 1
 LPM_MESH_CUBED_SPHERE = 2
 LPM_KERNEL_BIOT_SAVART_SPHERE = 1
 LPM_KERNEL_POISSON_3D = 2
+LPM_KERNEL_SPHERE_GREENS = 3
+LPM_KERNEL_PLANAR_LOG = 4
+LPM_KERNEL_DELTA_3D = 5
+LPM_KERNEL_SPHERE_DELTA = 6
 LPM_PREC_F64 = 0
 LPM_PREC_F32 = 1
 

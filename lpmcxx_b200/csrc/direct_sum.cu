@@ -160,6 +160,100 @@ __global__ void __launch_bounds__(kThreads) poisson_f64_kernel(const double4* __
     }
 }
 
+// ------------------------------------------------------------------ FP64 scalar kernels of the ScalarKernel family
+// Pair values without the constant factor (applied once per target as `mult`), each formed as the
+// reference forms it (products and sums without contraction where the reference has no FMA):
+//   SphereGreensFn        -log(R^2 - y.x) / (4 pi R)           (src/LpmScalarKernel.h:31-45)
+//   PlanarGreens...       log(|x - y|^2) / (4 pi)              (src/LpmScalarKernel.h:19-29)
+//   SecondOrderDelta3d    3 exp(-(|x - y|/eps)^3) / (4 pi eps^3) (src/LpmScalarKernel.h:47-62)
+//   SphereDelta           (2 eps^2 d - (1 - d)^2) / (4 pi (1 - d + eps^2)^2) - 1/(4 pi), d = x.y
+//                                                               (src/LpmScalarKernel.h:64-78)
+struct SphereGreensPair {
+    double r2;
+    __device__ double operator()(double tx, double ty, double tz, double sx, double sy, double sz) const {
+        const double dot = __dadd_rn(__dadd_rn(__dmul_rn(sx, tx), __dmul_rn(sy, ty)), __dmul_rn(sz, tz));
+        return log(r2 - dot);
+    }
+};
+struct PlanarLogPair {
+    __device__ double operator()(double tx, double ty, double tz, double sx, double sy, double sz) const {
+        const double dx = tx - sx, dy = ty - sy, dz = tz - sz;
+        return log(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    }
+};
+struct Delta3dPair {
+    double inv_eps;
+    __device__ double operator()(double tx, double ty, double tz, double sx, double sy, double sz) const {
+        const double dx = tx - sx, dy = ty - sy, dz = tz - sz;
+        const double q = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz))) * inv_eps;
+        return exp(-(q * q * q));
+    }
+};
+struct SphereDeltaPair {
+    double eps2;
+    __device__ double operator()(double tx, double ty, double tz, double sx, double sy, double sz) const {
+        const double d = __dadd_rn(__dadd_rn(__dmul_rn(tx, sx), __dmul_rn(ty, sy)), __dmul_rn(tz, sz));
+        const double numer = 2.0 * eps2 * d - (1.0 - d) * (1.0 - d);
+        const double den = 1.0 - d + eps2;
+        return numer / (den * den) - 1.0;
+    }
+};
+
+// out[i] = mult * sum_j w_j K(x_i, y_j), skipping j == coinc_off + i for targets i < coinc_n when
+// kSkipSelf (the singular kernels' self pair, excluded by index as the reference does).
+template <class K, bool kSkipSelf>
+__global__ void __launch_bounds__(kThreads) scalar_f64_kernel(const double4* __restrict__ src, int64_t n_src,
+                                                              const double4* __restrict__ tgt, int64_t n_tgt, K kern,
+                                                              double mult, double* __restrict__ out, int64_t coinc_n,
+                                                              int64_t coinc_off) {
+    __shared__ double4 tile[kTile];
+    const int64_t base = (int64_t)blockIdx.x * (kThreads * kTpt64) + threadIdx.x;
+    double tx[kTpt64], ty[kTpt64], tz[kTpt64], phi[kTpt64];
+    int64_t self[kTpt64];
+#pragma unroll
+    for (int t = 0; t < kTpt64; ++t) {
+        const int64_t i = base + t * kThreads;
+        const double4 p = i < n_tgt ? tgt[i] : make_double4(0.0, 0.0, 2.0, 0.0);
+        tx[t] = p.x; ty[t] = p.y; tz[t] = p.z;
+        phi[t] = 0.0;
+        self[t] = kSkipSelf && i < coinc_n ? coinc_off + i : -1;
+    }
+    for (int64_t j0 = 0; j0 < n_src; j0 += kTile) {
+        __syncthreads();
+        const int64_t j = j0 + threadIdx.x;
+        tile[threadIdx.x] = j < n_src ? src[j] : make_double4(0.0, 0.0, 0.0, 0.0);
+        __syncthreads();
+        const int m = (int)min((int64_t)kTile, n_src - j0);
+        for (int k = 0; k < m; ++k) {
+            const double4 s = tile[k];
+#pragma unroll
+            for (int t = 0; t < kTpt64; ++t) {
+                if (kSkipSelf && j0 + k == self[t]) continue;
+                phi[t] = fma(s.w, kern(tx[t], ty[t], tz[t], s.x, s.y, s.z), phi[t]);
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < kTpt64; ++t) {
+        const int64_t i = base + t * kThreads;
+        if (i < n_tgt) out[i] = mult * phi[t];
+    }
+}
+
+template <class K>
+int launch_scalar_f64(lpm_ctx* ctx, const char* name, K kern, bool skip_self, const double4* src, int64_t n_src,
+                      const double4* tgt, int64_t n_tgt, double mult, double* out, int64_t coinc_n,
+                      int64_t coinc_off) {
+    const unsigned grid = grid_for(n_tgt, kThreads * kTpt64);
+    if (skip_self)
+        LPM_LAUNCH(ctx, name, (scalar_f64_kernel<K, true>), grid, kThreads, 0, src, n_src, tgt, n_tgt, kern, mult, out,
+                   coinc_n, coinc_off);
+    else
+        LPM_LAUNCH(ctx, name, (scalar_f64_kernel<K, false>), grid, kThreads, 0, src, n_src, tgt, n_tgt, kern, mult, out,
+                   coinc_n, coinc_off);
+    return LPM_OK;
+}
+
 // ------------------------------------------------------------------ FP32 Biot-Savart
 // src.w holds 2*strength.  Coincident (target, source) pairs -- a face-centroid target and its
 // own source -- can only sit at equal indices (see coinc_* arguments); tiles that may contain one
@@ -331,7 +425,7 @@ int pack_f32(lpm_ctx* ctx, const double4* in, int64_t n, float4* out, bool scale
 }
 
 int direct_sum_f64(lpm_ctx* ctx, const lpm_kernel_desc& k, const double4* src, int64_t n_src, const double4* tgt,
-                   int64_t n_tgt, double* out, int64_t out_stride) {
+                   int64_t n_tgt, double* out, int64_t out_stride, int64_t coinc_n, int64_t coinc_off) {
     if (n_tgt <= 0) return LPM_OK;
     const unsigned grid = grid_for(n_tgt, kThreads * kTpt64);
     if (k.kind == LPM_KERNEL_BIOT_SAVART_SPHERE) {
@@ -345,6 +439,19 @@ int direct_sum_f64(lpm_ctx* ctx, const lpm_kernel_desc& k, const double4* src, i
                                                                      out_stride);
     } else if (k.kind == LPM_KERNEL_POISSON_3D) {
         LPM_LAUNCH(ctx, "poisson_f64_kernel", poisson_f64_kernel, grid, kThreads, 0, src, n_src, tgt, n_tgt, 1.0 / (4.0 * kPi), out);
+    } else if (k.kind == LPM_KERNEL_SPHERE_GREENS) {
+        return launch_scalar_f64(ctx, "scalar_f64_kernel", SphereGreensPair{k.radius * k.radius}, true, src, n_src, tgt,
+                                 n_tgt, -1.0 / (4.0 * kPi * k.radius), out, coinc_n, coinc_off);
+    } else if (k.kind == LPM_KERNEL_PLANAR_LOG) {
+        return launch_scalar_f64(ctx, "scalar_f64_kernel", PlanarLogPair{}, true, src, n_src, tgt, n_tgt,
+                                 1.0 / (4.0 * kPi), out, coinc_n, coinc_off);
+    } else if (k.kind == LPM_KERNEL_DELTA_3D) {
+        const double e3 = k.delta * k.delta * k.delta;
+        return launch_scalar_f64(ctx, "scalar_f64_kernel", Delta3dPair{1.0 / k.delta}, false, src, n_src, tgt, n_tgt,
+                                 3.0 / (4.0 * kPi * e3), out, 0, 0);
+    } else if (k.kind == LPM_KERNEL_SPHERE_DELTA) {
+        return launch_scalar_f64(ctx, "scalar_f64_kernel", SphereDeltaPair{k.delta * k.delta}, false, src, n_src, tgt,
+                                 n_tgt, 1.0 / (4.0 * kPi), out, 0, 0);
     } else {
         set_error("invalid kernel");
         return LPM_ERR_KERNEL;
@@ -384,12 +491,16 @@ int check_kernel_desc(const lpm_kernel_desc* k) {
         set_error("null kernel descriptor");
         return LPM_ERR_ARG;
     }
-    if (k->kind != LPM_KERNEL_BIOT_SAVART_SPHERE && k->kind != LPM_KERNEL_POISSON_3D) {
+    if (k->kind < LPM_KERNEL_BIOT_SAVART_SPHERE || k->kind > LPM_KERNEL_SPHERE_DELTA) {
         set_error("invalid kernel");
         return LPM_ERR_KERNEL;
     }
-    if (k->kind == LPM_KERNEL_BIOT_SAVART_SPHERE && !(k->radius > 0.0)) {
-        set_error("Biot-Savart kernel needs radius > 0");
+    if ((k->kind == LPM_KERNEL_BIOT_SAVART_SPHERE || k->kind == LPM_KERNEL_SPHERE_GREENS) && !(k->radius > 0.0)) {
+        set_error("sphere kernels need radius > 0");
+        return LPM_ERR_ARG;
+    }
+    if ((k->kind == LPM_KERNEL_DELTA_3D || k->kind == LPM_KERNEL_SPHERE_DELTA) && !(k->delta > 0.0)) {
+        set_error("delta kernels need eps (the delta field) > 0");
         return LPM_ERR_ARG;
     }
     return LPM_OK;
@@ -398,10 +509,14 @@ int check_kernel_desc(const lpm_kernel_desc* k) {
 // Device entry shared by the C ABI: FP64 or FP32 (FP32 copies go to scratch slots).
 int direct_sum_any(lpm_ctx* ctx, const lpm_kernel_desc& k, int precision, const double4* src, int64_t n_src,
                    const double4* tgt, int64_t n_tgt, double* out, int64_t coinc_n, int64_t coinc_off) {
-    if (precision == LPM_PREC_F64) return direct_sum_f64(ctx, k, src, n_src, tgt, n_tgt, out, n_tgt);
+    if (precision == LPM_PREC_F64) return direct_sum_f64(ctx, k, src, n_src, tgt, n_tgt, out, n_tgt, coinc_n, coinc_off);
     if (precision != LPM_PREC_F32) {
         set_error("unknown precision %d", precision);
         return LPM_ERR_ARG;
+    }
+    if (k.kind != LPM_KERNEL_BIOT_SAVART_SPHERE && k.kind != LPM_KERNEL_POISSON_3D) {
+        set_error("invalid kernel: the FP32 direct sum takes the Biot-Savart and 3D Poisson kernels (use LPM_PREC_F64)");
+        return LPM_ERR_KERNEL;
     }
     float4* s32 = (float4*)scratch(ctx, kSlotSrc32, sizeof(float4) * (size_t)std::max<int64_t>(n_src, 1));
     float4* t32 = (float4*)scratch(ctx, kSlotTgt32, sizeof(float4) * (size_t)std::max<int64_t>(n_tgt, 1));
@@ -449,10 +564,8 @@ extern "C" int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, 
     }
     int rc = check_kernel_desc(kernel);
     if (rc) return rc;
-    if (kernel->kind != LPM_KERNEL_BIOT_SAVART_SPHERE) {
-        set_error("invalid kernel: lpm_direct_sum_mesh takes a vector kernel");
-        return LPM_ERR_KERNEL;
-    }
+    const bool vec = kernel->kind == LPM_KERNEL_BIOT_SAVART_SPHERE;
+    const int comps = vec ? 3 : 1;
     if (n_verts < 0 || n_faces < 0 || (n_verts > 0 && (!vx || !vy || !vz)) ||
         (n_faces > 0 && (!fx || !fy || !fz || !face_area || !face_divided || !face_src))) {
         set_error("lpm_direct_sum_mesh: null input arrays");
@@ -460,8 +573,8 @@ extern "C" int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, 
     }
     // empty ranges (end < begin) are allowed, as for a rank with no items
     const bool do_v = vert_end >= vert_begin, do_f = face_end >= face_begin;
-    if ((do_v && (vert_begin < 0 || vert_end >= n_verts || !vert_out0 || !vert_out1 || !vert_out2)) ||
-        (do_f && (face_begin < 0 || face_end >= n_faces || !face_out0 || !face_out1 || !face_out2))) {
+    if ((do_v && (vert_begin < 0 || vert_end >= n_verts || !vert_out0 || (vec && (!vert_out1 || !vert_out2)))) ||
+        (do_f && (face_begin < 0 || face_end >= n_faces || !face_out0 || (vec && (!face_out1 || !face_out2))))) {
         set_error("lpm_direct_sum_mesh: target range out of bounds or null outputs");
         return LPM_ERR_ARG;
     }
@@ -478,7 +591,7 @@ extern "C" int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, 
     const int64_t n_vt = do_v ? vert_end - vert_begin + 1 : 0;
     const int64_t n_tgt = n_ft + n_vt;
     const size_t in_bytes = sizeof(double4) * (size_t)(n_src + n_tgt);
-    const size_t out_bytes = sizeof(double) * 3 * (size_t)n_tgt;
+    const size_t out_bytes = sizeof(double) * comps * (size_t)n_tgt;
     double* host = (double*)pinned(ctx, in_bytes + out_bytes);
     if (!host) return LPM_ERR_OOM;
     double4* hsrc = (double4*)host;
@@ -503,6 +616,8 @@ extern "C" int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, 
             LPM_CUDA_TRY(cudaMemcpyAsync(dsrc, hsrc, sizeof(double4) * (size_t)n_src, cudaMemcpyHostToDevice,
                                          ctx->stream));
         LPM_CUDA_TRY(cudaMemcpyAsync(dtgt, htgt, sizeof(double4) * (size_t)n_tgt, cudaMemcpyHostToDevice, ctx->stream));
+        // face targets come first and sit on sources src_before_fb.. in order: the self pairs a singular
+        // scalar kernel skips (the FP32 paths use the same indices to guard coincident pairs)
         rc = direct_sum_any(ctx, *kernel, precision, dsrc, n_src, dtgt, n_tgt, dout, n_ft, src_before_fb);
         if (rc) return rc;
         LPM_CUDA_TRY(cudaMemcpyAsync(hout, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
@@ -512,14 +627,18 @@ extern "C" int lpm_direct_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, 
     for (int64_t i = face_begin; do_f && i <= face_end; ++i) {
         if (face_divided[i]) continue;
         face_out0[i] = hout[t];
-        face_out1[i] = hout[n_tgt + t];
-        face_out2[i] = hout[2 * n_tgt + t];
+        if (vec) {
+            face_out1[i] = hout[n_tgt + t];
+            face_out2[i] = hout[2 * n_tgt + t];
+        }
         ++t;
     }
     for (int64_t i = 0; i < n_vt; ++i, ++t) {
         vert_out0[vert_begin + i] = hout[t];
-        vert_out1[vert_begin + i] = hout[n_tgt + t];
-        vert_out2[vert_begin + i] = hout[2 * n_tgt + t];
+        if (vec) {
+            vert_out1[vert_begin + i] = hout[n_tgt + t];
+            vert_out2[vert_begin + i] = hout[2 * n_tgt + t];
+        }
     }
     return LPM_OK;
 }
@@ -533,7 +652,7 @@ extern "C" int lpm_direct_sum_meshfree(lpm_ctx* ctx, const lpm_kernel_desc* kern
     }
     int rc = check_kernel_desc(kernel);
     if (rc) return rc;
-    if (kernel->kind != LPM_KERNEL_POISSON_3D) {
+    if (kernel->kind == LPM_KERNEL_BIOT_SAVART_SPHERE) {
         set_error("invalid kernel: lpm_direct_sum_meshfree takes a scalar kernel");
         return LPM_ERR_KERNEL;
     }

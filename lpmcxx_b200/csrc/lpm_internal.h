@@ -123,8 +123,9 @@ void prof_end(lpm_ctx* ctx, LpmProfRecord& r);
 inline unsigned grid_for(int64_t n, int per_block) { return (unsigned)((n + per_block - 1) / per_block); }
 
 // direct sums (direct_sum.cu)
+// FP64 sums; a singular scalar kernel skips source coinc_off + i for target i < coinc_n.
 int direct_sum_f64(lpm_ctx* ctx, const lpm_kernel_desc& k, const double4* src, int64_t n_src, const double4* tgt,
-                   int64_t n_tgt, double* out, int64_t out_stride);
+                   int64_t n_tgt, double* out, int64_t out_stride, int64_t coinc_n = 0, int64_t coinc_off = 0);
 // FP32 sums: src.w = 2*strength for Biot-Savart; targets 0..coinc_n-1 sit on sources coinc_off.. .
 int direct_sum_f32_impl(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* src, int64_t n_src, const float4* tgt,
                         const double4* tgt64, int64_t n_tgt, double* out, int64_t out_stride, int64_t coinc_n,

@@ -22,6 +22,10 @@ extern "C" int lpm_treesum_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, c
     *out = nullptr;
     int rc = check_kernel_desc(kernel);
     if (rc) return rc;
+    if (kernel->kind != LPM_KERNEL_BIOT_SAVART_SPHERE && kernel->kind != LPM_KERNEL_POISSON_3D) {
+        set_error("invalid kernel: the treecode takes the Biot-Savart and 3D Poisson kernels");
+        return LPM_ERR_KERNEL;
+    }
     if (solver->method != LPM_METHOD_TREE) {
         set_error("lpm_treesum_create: solver method must be LPM_METHOD_TREE");
         return LPM_ERR_ARG;

@@ -13,8 +13,11 @@
  * the calling rank, and ranks that need the other slices exchange them exactly as before by calling
  * the reference's broadcast on their own (single-GPU runs have one rank).
  *
- * Kernel mapping (lpm_kernel_desc): BiotSavartSphere(delta, R) (src/LpmVectorKernel.h:19-39) through
- * its public interface, and PoissonGreensFn3d below, the 3D Poisson kernel the reference lacks.
+ * Kernel mapping (lpm_kernel_desc): BiotSavartSphere(delta, R) (src/LpmVectorKernel.h:19-39) and the
+ * ScalarKernel family (SphereGreensFn, PlanarGreensFnFreeBoundaries, SecondOrderDelta3d, SphereDelta;
+ * src/LpmScalarKernel.h:19-78), whose parameters are recovered through their public interface, and
+ * PoissonGreensFn3d below, the 3D Poisson kernel the reference lacks.  The ScalarKernel family runs in
+ * FP64 only (LPM_B200_PRECISION=f32 applies to Biot-Savart and PoissonGreensFn3d).
  */
 #ifndef LPM_B200_DROPIN_H
 #define LPM_B200_DROPIN_H
@@ -54,7 +57,7 @@ void check(int status, const char* where);
 /// lpm_kernel_desc of a reference vector kernel; throws std::logic_error("invalid kernel") for kernels
 /// the GPU path does not implement.
 lpm_kernel_desc describe(const VectorKernel& k);
-/// lpm_kernel_desc of a scalar kernel (PoissonGreensFn3d only).
+/// lpm_kernel_desc of a scalar kernel (the reference's ScalarKernel subclasses and PoissonGreensFn3d).
 lpm_kernel_desc describe(const ScalarKernel& k);
 
 }  // namespace b200

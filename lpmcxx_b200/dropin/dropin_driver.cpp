@@ -8,9 +8,13 @@
  *   direct KIND LEVEL DELTA ZETA.bin OUTDIR          DirectSum(pmesh, BiotSavartSphere(DELTA)).meshSolve
  *   tree   KIND LEVEL ORDER LEAF THETA ZETA.bin OUTDIR TreeSum(ORDER, LEAF, pmesh, kernel).meshSolve(THETA)
  *   poisson N XYZQ.bin OUTDIR                          DirectSum(particles, PoissonGreensFn3d).meshfreeSolve
+ *   scalar KIND LEVEL KERNEL PARAM ZETA.bin OUTDIR     DirectSum(pmesh, ScalarKernel).meshSolve with the reference's
+ *                                                      SphereGreensFn(PARAM) | PlanarGreensFnFreeBoundaries |
+ *                                                      SecondOrderDelta3d(PARAM) | SphereDelta(PARAM)
+ *                                                      (KERNEL = spheregreens|planarlog|delta3d|spheredelta)
  * KIND is icos|cube.  ZETA.bin holds one value per face (divided faces included, as the face field);
- * XYZQ.bin holds N x 4 (x, y, z, charge).  OUTDIR receives vert_vel.bin / face_vel.bin (n x 3) or
- * potential.bin (N), and the driver prints one JSON line.
+ * XYZQ.bin holds N x 4 (x, y, z, charge).  OUTDIR receives vert_vel.bin / face_vel.bin (n x 3),
+ * vert_phi.bin / face_phi.bin (n) or potential.bin (N), and the driver prints one JSON line.
  */
 #include "LpmB200Dropin.h"
 #include "LpmDirectSum.h"
@@ -108,6 +112,28 @@ int main(int argc, char** argv) {
             write_f64(out + "/vert_vel.bin", rows3(pm->getVertexFieldPtr("velocity"), pm->nVertices()));
             write_f64(out + "/face_vel.bin", rows3(pm->getFaceFieldPtr("velocity"), pm->nFaces()));
             std::printf("{\"cmd\": \"tree\", \"mac_count\": %d}\n", mac);
+        } else if (cmd == "scalar" && argc == 8) {
+            auto pm = mesh_with_zeta(argv[2], std::atoi(argv[3]), argv[6]);
+            pm->createVertexField("potential", "n/a", 1);
+            pm->createFaceField("potential", "n/a", 1);
+            const std::string kname = argv[4];
+            const double param = std::atof(argv[5]);
+            std::shared_ptr<ScalarKernel> kernel;
+            if (kname == "spheregreens") kernel = std::make_shared<SphereGreensFn>(param);
+            else if (kname == "planarlog") kernel = std::make_shared<PlanarGreensFnFreeBoundaries>();
+            else if (kname == "delta3d") kernel = std::make_shared<SecondOrderDelta3d>(param);
+            else if (kname == "spheredelta") kernel = std::make_shared<SphereDelta>(param);
+            else throw std::invalid_argument("KERNEL must be spheregreens, planarlog, delta3d or spheredelta");
+            MPIReplicatedData mv(pm->nVertices(), 0, 1), mf(pm->nFaces(), 0, 1);
+            DirectSum solver(pm, kernel, "potential", "vorticity");
+            solver.meshSolve(mv, mf);
+            const std::string out = argv[7];
+            std::vector<double> vp(pm->nVertices()), fp(pm->nFaces());
+            for (index_type i = 0; i < pm->nVertices(); ++i) vp[i] = pm->getVertexFieldPtr("potential")->getScalar(i);
+            for (index_type i = 0; i < pm->nFaces(); ++i) fp[i] = pm->getFaceFieldPtr("potential")->getScalar(i);
+            write_f64(out + "/vert_phi.bin", vp);
+            write_f64(out + "/face_phi.bin", fp);
+            std::printf("{\"cmd\": \"scalar\", \"kernel\": \"%s\"}\n", kname.c_str());
         } else if (cmd == "poisson" && argc == 5) {
             const long n = std::atol(argv[2]);
             const std::vector<double> p = read_f64(argv[3]);

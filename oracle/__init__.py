@@ -39,6 +39,7 @@ def lib() -> C.CDLL:
         P, I, D = C.c_void_p, C.c_int64, C.c_double
         h.oracle_bs_direct.argtypes = [P, I, P, I, D, D, P]
         h.oracle_poisson_direct.argtypes = [P, I, P, I, P]
+        h.oracle_scalar_direct.argtypes = [C.c_int, D, P, I, P, I, P, P]
         h.oracle_rk4_direct.argtypes = [P, I, I, D, D, D, C.c_int]
         h.oracle_tree_build.argtypes = [P, I, P, C.c_int, C.c_int, P, P, P, P, P, P, P, P, I, P]
         _lib = h
@@ -63,6 +64,17 @@ def bs_direct(src4: np.ndarray, tgt4: np.ndarray, radius: float = 1.0, delta: fl
     out = np.zeros((3, tgt4.shape[0]))
     lib().oracle_bs_direct(src4.ctypes.data, src4.shape[0], tgt4.ctypes.data, tgt4.shape[0], radius, delta,
                            out.ctypes.data)
+    return out
+
+
+def scalar_direct(kind: int, param: float, src4: np.ndarray, tgt4: np.ndarray, self_idx=None) -> np.ndarray:
+    """ScalarKernel-family direct sum (kind 3..6 as LPM_KERNEL_*); self_idx[i] >= 0 is a source index
+    target i skips (a singular kernel's own face)."""
+    src4, tgt4 = _c(src4), _c(tgt4)
+    out = np.zeros(tgt4.shape[0])
+    si = None if self_idx is None else np.ascontiguousarray(self_idx, dtype=np.int64)
+    lib().oracle_scalar_direct(int(kind), float(param), src4.ctypes.data, src4.shape[0], tgt4.ctypes.data,
+                               tgt4.shape[0], None if si is None else si.ctypes.data, out.ctypes.data)
     return out
 
 

@@ -129,6 +129,67 @@ void oracle_poisson_direct(const double* src, int64_t n_src, const double* tgt, 
     parallel_range(n_tgt, poisson_direct_range, &a);
 }
 
+/* The rest of the ScalarKernel family (src/LpmScalarKernel.h:19-78), each value formed as the reference
+ * forms it, summed as DirectSum::meshSolve's scalar branch does (src/LpmDirectSum.cpp:36-88):
+ * tgtVal += kval * strength over sources j, skipping j == self[i] when self[i] >= 0. */
+typedef struct {
+    const double* src;
+    const double* tgt;
+    int64_t n_src, n_tgt;
+    int kind;
+    double param;
+    const int64_t* self;
+    double* out;
+} scalar_args;
+
+static double scalar_kernel_value(int kind, double param, const double* t, const double* s) {
+    switch (kind) {
+        case 3: { /* SphereGreensFn(radius) (src/LpmScalarKernel.h:35-38) */
+            const double inarg = param * param - (s[0] * t[0] + s[1] * t[1] + s[2] * t[2]);
+            return -log(inarg) / (4.0 * kPi * param);
+        }
+        case 4: { /* PlanarGreensFnFreeBoundaries (src/LpmScalarKernel.h:23-26) */
+            const double dx = t[0] - s[0], dy = t[1] - s[1], dz = t[2] - s[2];
+            return log(dx * dx + dy * dy + dz * dz) / (4.0 * kPi);
+        }
+        case 5: { /* SecondOrderDelta3d(eps) (src/LpmScalarKernel.h:51-57) */
+            const double dx = t[0] - s[0], dy = t[1] - s[1], dz = t[2] - s[2];
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            const double expfactor = exp(-pow(r / param, 3));
+            const double eps3 = pow(param, 3);
+            return 3.0 * expfactor / (4.0 * kPi * eps3);
+        }
+        case 6: { /* SphereDelta(eps) (src/LpmScalarKernel.h:68-74) */
+            const double bkgrnd = 1.0 / (4.0 * kPi);
+            const double d = t[0] * s[0] + t[1] * s[1] + t[2] * s[2];
+            const double numer = 2.0 * param * param * d - (1.0 - d) * (1.0 - d);
+            const double denom = 4.0 * kPi * (1.0 - d + param * param) * (1.0 - d + param * param);
+            return numer / denom - bkgrnd;
+        }
+        default: return 0.0;
+    }
+}
+
+static void scalar_direct_range(void* p, int64_t i0, int64_t i1) {
+    const scalar_args* a = (const scalar_args*)p;
+    for (int64_t i = i0; i < i1; ++i) {
+        const int64_t skip = a->self ? a->self[i] : -1;
+        double v = 0.0;
+        for (int64_t j = 0; j < a->n_src; ++j) {
+            if (j == skip) continue;
+            const double kval = scalar_kernel_value(a->kind, a->param, a->tgt + 4 * i, a->src + 4 * j);
+            v += kval * a->src[4 * j + 3];
+        }
+        a->out[i] = v;
+    }
+}
+
+void oracle_scalar_direct(int kind, double param, const double* src, int64_t n_src, const double* tgt, int64_t n_tgt,
+                          const int64_t* self, double* out) {
+    scalar_args a = {src, tgt, n_src, n_tgt, kind, param, self, out};
+    parallel_range(n_tgt, scalar_direct_range, &a);
+}
+
 /* RK4 of Lagrangian particles on the sphere with the FP64 direct-sum velocity.  The reference's C++
  * tree has no integrator (README.md:75 describes the Fortran one); these are the library's stated
  * semantics: classical RK4, stage positions and the new position re-projected x <- R x/|x|,

@@ -20,6 +20,13 @@ void oracle_bs_direct(const double* src, int64_t n_src, const double* tgt, int64
 /* 1/(4 pi |x-y|) direct sum, zero at x == y (DirectSum::meshfreeSolve, src/LpmDirectSum.cpp:240-252). */
 void oracle_poisson_direct(const double* src, int64_t n_src, const double* tgt, int64_t n_tgt, double* out);
 
+/* The ScalarKernel family (src/LpmScalarKernel.h:19-78) summed as DirectSum::meshSolve's scalar branch
+ * (src/LpmDirectSum.cpp:36-88): out[i] = sum_j w_j K(t_i, s_j) over j != self[i] (self may be NULL; -1 =
+ * skip nothing).  kind 3 SphereGreensFn (param = radius), 4 PlanarGreensFnFreeBoundaries, 5
+ * SecondOrderDelta3d (param = eps), 6 SphereDelta (param = eps). */
+void oracle_scalar_direct(int kind, double param, const double* src, int64_t n_src, const double* tgt, int64_t n_tgt,
+                          const int64_t* self, double* out);
+
 /* nsteps classical RK4 steps of the particles state (n x 4: x,y,z,w; the first n_src are sources) with
  * the Biot-Savart direct-sum velocity, stage and final positions re-projected onto the sphere. */
 void oracle_rk4_direct(double* state, int64_t n_src, int64_t n, double radius, double delta, double dt, int nsteps);

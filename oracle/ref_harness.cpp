@@ -11,6 +11,9 @@
  *   tree     KIND LEVEL MAXLEAF OUTDIR             TreeSum mesh ctor + tree (src/LpmTreeSum.cpp:221-238,266-290)
  *   treesum  KIND LEVEL ZETA P MAXLEAF THETA OUTDIR  TreeSum::computeMeshMoments + meshSolve
  *                                                  (src/LpmTreeSum.cpp:55-86,106-197)
+ *   scalar   KIND LEVEL ZETA KERNEL PARAM OUTDIR   DirectSum::meshSolve, scalar branch (src/LpmDirectSum.cpp:29-93)
+ *                                                  with the reference's ScalarKernel KERNEL: spheregreens (PARAM =
+ *                                                  radius), planarlog, delta3d / spheredelta (PARAM = eps)
  *   poisson  NPTS SEED OUTDIR                      DirectSum::meshfreeSolve (src/LpmDirectSum.cpp:240-252)
  *                                                  with a 1/(4 pi r) ScalarKernel subclass
  *   pointtree NPTS SEED MAXLEAF OUTDIR             TreeSum(coords,...) meshfree ctor (src/LpmTreeSum.cpp:208-219)
@@ -246,7 +249,7 @@ static uint64_t splitmix64(uint64_t& s) {
 static double uniform_pm1(uint64_t& s) { return 2.0 * ((splitmix64(s) >> 11) * (1.0 / 9007199254740992.0)) - 1.0; }
 
 static int usage() {
-    fprintf(stderr, "usage: ref_harness mesh|direct|tree|treesum|poisson|pointtree ...\n");
+    fprintf(stderr, "usage: ref_harness mesh|direct|scalar|tree|treesum|poisson|pointtree ...\n");
     return 2;
 }
 
@@ -350,6 +353,35 @@ int main(int argc, char** argv) {
             printf("{\"cmd\": \"treesum\", \"mac\": %d, \"seconds\": %.6f}\n", mac, secs);
             tree->~TreeProbe();
             ::operator delete(tree);
+        } else if (cmd == "scalar" && argc == 8) {
+            auto seed = make_seed(argv[2]);
+            const std::string out = argv[7], kname = argv[5];
+            const double param = atof(argv[6]);
+            auto pm = std::make_shared<MeshedParticles>(*seed, atoi(argv[3]), false, 1.0, rank);
+            init_vorticity(*pm, argv[4]);
+            pm->createVertexField("potential", "n/a", 1);
+            pm->createFaceField("potential", "n/a", 1);
+            std::shared_ptr<ScalarKernel> kernel;
+            if (kname == "spheregreens") kernel.reset(new SphereGreensFn(param));
+            else if (kname == "planarlog") kernel.reset(new PlanarGreensFnFreeBoundaries());
+            else if (kname == "delta3d") kernel.reset(new SecondOrderDelta3d(param));
+            else if (kname == "spheredelta") kernel.reset(new SphereDelta(param));
+            else throw std::invalid_argument("KERNEL must be spheregreens, planarlog, delta3d or spheredelta");
+            MPIReplicatedData mv(pm->nVertices(), rank, size), mf(pm->nFaces(), rank, size);
+            DirectSum solver(pm, kernel, "potential", "vorticity");
+            const auto t0 = std::chrono::steady_clock::now();
+            solver.meshSolve(mv, mf);
+            const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            std::vector<double> fz(pm->nFaces()), vp(pm->nVertices()), fp(pm->nFaces());
+            for (index_type i = 0; i < pm->nFaces(); ++i) {
+                fz[i] = pm->getFaceFieldPtr("vorticity")->getScalar(i);
+                fp[i] = pm->getFaceFieldPtr("potential")->getScalar(i);
+            }
+            for (index_type i = 0; i < pm->nVertices(); ++i) vp[i] = pm->getVertexFieldPtr("potential")->getScalar(i);
+            npy_f64(out, "face_zeta", fz);
+            npy_f64(out, "vert_phi", vp);
+            npy_f64(out, "face_phi", fp);
+            printf("{\"cmd\": \"scalar\", \"kernel\": \"%s\", \"seconds\": %.6f}\n", kname.c_str(), secs);
         } else if (cmd == "poisson" && argc == 5) {
             const index_type n = atol(argv[2]);
             uint64_t s = strtoull(argv[3], nullptr, 0);

@@ -14,6 +14,10 @@ Fixtures
                              cube level 3, Gaussian vortex
   direct_icos3_rh_r2.npz     MPIReplicatedData rank 1 of 3: only that rank's target slice is written
   poisson_2000.npz           DirectSum::meshfreeSolve with a 1/(4 pi r) ScalarKernel, 2000 points
+  scalar_icos3_harm.npz      DirectSum::meshSolve, scalar branch, with the reference's SphereGreensFn(1),
+                             PlanarGreensFnFreeBoundaries, SecondOrderDelta3d(0.1) and SphereDelta(0.1);
+                             icos level 3, zeta = sphereHarmonic54 (`python make_golden.py scalar` makes
+                             only this one)
 """
 from __future__ import annotations
 
@@ -41,7 +45,25 @@ def load(d: Path, *names) -> dict:
     return {n: np.load(d / f"{n}.npy") for n in names}
 
 
+SCALAR_KERNELS = (("spheregreens", 1.0), ("planarlog", 0.0), ("delta3d", 0.1), ("spheredelta", 0.1))
+
+
+def scalar_fixture() -> None:
+    z = {}
+    for name, param in SCALAR_KERNELS:
+        d = harness("scalar", "icos", 3, "harm", name, param)
+        z["face_zeta"] = np.load(d / "face_zeta.npy")
+        z[f"{name}_vert_phi"] = np.load(d / "vert_phi.npy")
+        z[f"{name}_face_phi"] = np.load(d / "face_phi.npy")
+        z[f"{name}_param"] = np.array(param)
+    np.savez_compressed(HERE / "scalar_icos3_harm.npz", **z)
+
+
 def main() -> None:
+    if sys.argv[1:] == ["scalar"]:
+        scalar_fixture()
+        return
+    scalar_fixture()
     for kind in ("icos", "cube"):
         d = harness("mesh", kind, 3)
         np.savez_compressed(HERE / f"mesh_{kind}3.npz",

@@ -174,8 +174,8 @@ def test_invalid_kernel_and_ranges(ctx):
     with pytest.raises(L.LpmError) as e:
         ctx.direct_sum_mesh(bad, L.LPM_PREC_F64, m, zeta)
     assert e.value.code == L._capi.LPM_ERR_KERNEL
-    with pytest.raises(L.LpmError) as e:
-        ctx.direct_sum_mesh(L.poisson_kernel(), L.LPM_PREC_F64, m, zeta)
+    with pytest.raises(L.LpmError) as e:  # the FP32 path takes Biot-Savart and 3D Poisson only
+        ctx.direct_sum_mesh(L.sphere_greens_kernel(), L.LPM_PREC_F32, m, zeta)
     assert e.value.code == L._capi.LPM_ERR_KERNEL
     with pytest.raises(L.LpmError) as e:
         ctx.direct_sum_mesh(BS, L.LPM_PREC_F64, m, zeta, vert_range=(0, m.n_verts))

@@ -60,6 +60,22 @@ def test_dropin_direct_sum_nonsingular_kernel_cube3():
 
 @pytest.mark.gpu
 @needs_driver
+@pytest.mark.parametrize("name", ["spheregreens", "planarlog", "delta3d", "spheredelta"])
+def test_dropin_scalar_kernels_match_reference(name):
+    # the reference's own ScalarKernel objects through the drop-in DirectSum::meshSolve (scalar branch);
+    # their protected parameters are recovered through the public interface
+    g = golden("scalar_icos3_harm.npz")
+    with tempfile.TemporaryDirectory() as d:
+        g["face_zeta"].astype("<f8").tofile(f"{d}/zeta.bin")
+        run("scalar", "icos", 3, name, float(g[f"{name}_param"]), f"{d}/zeta.bin", d)
+        vp = np.fromfile(f"{d}/vert_phi.bin")
+        fp = np.fromfile(f"{d}/face_phi.bin")
+    assert rel_linf(vp, g[f"{name}_vert_phi"]) < 1e-12
+    assert rel_linf(fp, g[f"{name}_face_phi"]) < 1e-12
+
+
+@pytest.mark.gpu
+@needs_driver
 def test_dropin_meshfree_poisson_matches_reference():
     g = golden("poisson_2000.npz")
     n = g["xyz"].shape[0]
