@@ -106,6 +106,38 @@ int lpm_fma_peak(lpm_ctx* ctx, int precision, double* tflops);
 int lpm_mesh_counts(int kind, int level, int64_t* n_verts, int64_t* n_faces, int64_t* n_leaves);
 int lpm_mesh_build(int kind, int level, double radius, double* vert_xyz, double* face_xyz, double* face_area,
                    uint8_t* face_divided);
+/* Vertex indices of every face (n_faces x 3 for LPM_MESH_ICOS_TRI, x 4 for LPM_MESH_CUBED_SPHERE), in
+ * the order of Faces::vertexIndices (src/LpmFaces.cpp:63-69): the connectivity lpm_write_vtk writes. */
+int lpm_mesh_face_vertices(int kind, int level, int64_t* face_verts);
+
+/* ---- field output in the reference's file formats (host; fields may be device-resident) */
+typedef struct lpm_field_desc {
+    const char* name;   /* Field::name() */
+    const char* units;  /* Field::units() */
+    int32_t ndim;       /* 1, 2 or 3 components */
+    int32_t on_device;  /* nonzero: data is device memory (copied to the host after a device synchronize) */
+    const double* data; /* component-major: component c of item i at data[c * n + i] */
+} lpm_field_desc;
+
+/* Legacy ASCII VTK POLYDATA of a mesh and its fields, byte for byte the file
+ * MeshedParticles::writeToVtkFile writes (src/LpmMeshedParticles.cpp:131-153, VtkWriter in
+ * src/LpmVtkFileIO.cpp:12-118,195-236): title line, POINTS (n_verts points, xyz_stride doubles apart:
+ * 3 for n x 3 arrays, 4 for the RK4 state), POLYGONS of the undivided faces (nsides vertices each from
+ * face_verts, n_faces x nsides), POINT_DATA (lag_xyz, if not NULL, as "lagrangian_coords", then the
+ * vertex fields, n_verts items), CELL_DATA (the face fields, n_faces items, written at undivided faces).
+ * Fields are written in the order given; the reference's MeshedParticles writes them in name order.
+ * Doubles print as printf "%.19g" (the reference's setprecision(digits10 of long double + 1)). */
+int lpm_write_vtk(const char* path, const char* title, int64_t n_verts, const double* vert_xyz, int32_t xyz_stride,
+                  int32_t xyz_on_device, const double* lag_xyz, int64_t n_faces, int32_t nsides,
+                  const int64_t* face_verts, const uint8_t* face_divided, int32_t n_vert_fields,
+                  const lpm_field_desc* vert_fields, int32_t n_face_fields, const lpm_field_desc* face_fields);
+
+/* Points and fields as CSV: VtkWriter::writePointsAndFieldsToCSV (src/LpmVtkFileIO.cpp:117-193): header
+ * "x,y,z" plus name (1 component) or name0,name1[,name2], one row per point, "%g" (a fresh stream's
+ * precision).  The reference prints 0 for the third component of the last field when it has 3 (it reads
+ * that field through get2dVector, src/LpmVtkFileIO.cpp:186-188); this writes the component's value. */
+int lpm_write_csv(const char* path, int64_t n, const double* xyz, int32_t xyz_stride, int32_t xyz_on_device,
+                  int32_t n_fields, const lpm_field_desc* fields);
 
 /* ---- direct sums */
 

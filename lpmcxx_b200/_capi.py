@@ -46,6 +46,11 @@ LPM_MLP_PARAMS = 5532
 LPM_MLP_TRAINABLE = 5516
 
 
+class FieldDesc(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("units", C.c_char_p), ("ndim", C.c_int32), ("on_device", C.c_int32),
+                ("data", C.c_void_p)]
+
+
 class SolverDesc(C.Structure):
     _fields_ = [("method", C.c_int32), ("precision", C.c_int32), ("order", C.c_int32), ("max_per_leaf", C.c_int32),
                 ("theta", C.c_double), ("order_policy", C.c_int32), ("reserved", C.c_int32),
@@ -77,6 +82,10 @@ SIGNATURES = {
     "lpm_ctx_profile_report": (C.c_int, [P, C.c_char_p, C.c_size_t]),
     "lpm_mesh_counts": (C.c_int, [C.c_int, C.c_int, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
     "lpm_mesh_build": (C.c_int, [C.c_int, C.c_int, D, P, P, P, P]),
+    "lpm_mesh_face_vertices": (C.c_int, [C.c_int, C.c_int, P]),
+    "lpm_write_vtk": (C.c_int, [C.c_char_p, C.c_char_p, I64, P, C.c_int32, C.c_int32, P, I64, C.c_int32, P, P,
+                                C.c_int32, C.POINTER(FieldDesc), C.c_int32, C.POINTER(FieldDesc)]),
+    "lpm_write_csv": (C.c_int, [C.c_char_p, I64, P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(FieldDesc)]),
     "lpm_direct_sum_dev": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, P, I64, P, I64, I64, P]),
     "lpm_direct_sum_f32_noalloc": (C.c_int, [C.POINTER(KernelDesc), P, I64, P, I64, I64, P, P]),
     "lpm_direct_sum_mesh": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, I64, P, P, P, I64, P, P, P, P, P, P,

@@ -225,12 +225,12 @@ extern "C" int lpm_mesh_counts(int kind, int level, int64_t* n_verts, int64_t* n
     return LPM_OK;
 }
 
-extern "C" int lpm_mesh_build(int kind, int level, double radius, double* vert_xyz, double* face_xyz,
-                              double* face_area, uint8_t* face_divided) {
+// Builds the mesh and fills whichever outputs are not NULL.
+static int mesh_build_into(int kind, int level, double radius, double* vert_xyz, double* face_xyz,
+                           double* face_area, uint8_t* face_divided, int64_t* face_verts) {
     int64_t nv, nf, nl;
     int rc = lpm_mesh_counts(kind, level, &nv, &nf, &nl);
     if (rc != LPM_OK) return rc;
-    if (!vert_xyz || !face_xyz || !face_area || !face_divided || !(radius > 0.0)) return LPM_ERR_ARG;
     try {
         const bool icos = kind == LPM_MESH_ICOS_TRI;
         MeshBuilder mb(icos ? 3 : 4, radius);
@@ -263,21 +263,35 @@ extern "C" int lpm_mesh_build(int kind, int level, double radius, double* vert_x
                 if (!mb.divided(f)) mb.divide(f);
         }
         if ((int64_t)mb.vx_.size() != nv || mb.nfaces() != nf) return LPM_ERR_INTERNAL;
-        for (int64_t i = 0; i < nv; ++i) {
+        for (int64_t i = 0; vert_xyz && i < nv; ++i) {
             vert_xyz[3 * i] = mb.vx_[i].x;
             vert_xyz[3 * i + 1] = mb.vx_[i].y;
             vert_xyz[3 * i + 2] = mb.vx_[i].z;
         }
         for (int64_t f = 0; f < nf; ++f) {
-            const V3 c = mb.centroid(f);
-            face_xyz[3 * f] = c.x;
-            face_xyz[3 * f + 1] = c.y;
-            face_xyz[3 * f + 2] = c.z;
-            face_area[f] = mb.farea_[f];
-            face_divided[f] = mb.fdiv_[f];
+            if (face_xyz) {
+                const V3 c = mb.centroid(f);
+                face_xyz[3 * f] = c.x;
+                face_xyz[3 * f + 1] = c.y;
+                face_xyz[3 * f + 2] = c.z;
+            }
+            if (face_area) face_area[f] = mb.farea_[f];
+            if (face_divided) face_divided[f] = mb.fdiv_[f];
+            if (face_verts) mb.face_vertices(f, face_verts + f * (icos ? 3 : 4));
         }
     } catch (...) {
         return LPM_ERR_OOM;
     }
     return LPM_OK;
+}
+
+extern "C" int lpm_mesh_build(int kind, int level, double radius, double* vert_xyz, double* face_xyz,
+                              double* face_area, uint8_t* face_divided) {
+    if (!vert_xyz || !face_xyz || !face_area || !face_divided || !(radius > 0.0)) return LPM_ERR_ARG;
+    return mesh_build_into(kind, level, radius, vert_xyz, face_xyz, face_area, face_divided, nullptr);
+}
+
+extern "C" int lpm_mesh_face_vertices(int kind, int level, int64_t* face_verts) {
+    if (!face_verts) return LPM_ERR_ARG;
+    return mesh_build_into(kind, level, 1.0, nullptr, nullptr, nullptr, nullptr, face_verts);
 }

@@ -14,6 +14,13 @@
  *   scalar   KIND LEVEL ZETA KERNEL PARAM OUTDIR   DirectSum::meshSolve, scalar branch (src/LpmDirectSum.cpp:29-93)
  *                                                  with the reference's ScalarKernel KERNEL: spheregreens (PARAM =
  *                                                  radius), planarlog, delta3d / spheredelta (PARAM = eps)
+ *   vtk      KIND LEVEL ZETA LAG OUTDIR            MeshedParticles::writeToVtkFile (src/LpmMeshedParticles.cpp:131-153)
+ *                                                  of a mesh (Lagrangian if LAG is 1) with the vorticity and its
+ *                                                  DirectSum velocity as vertex and face fields -> OUTDIR/mesh.vtk;
+ *                                                  VtkWriter::writePointsAndFieldsToCSV of the vertices with
+ *                                                  (velocity, vorticity) -> OUTDIR/points.csv
+ *   vtktime  KIND LEVEL OUTDIR                     times writeToVtkFile of the mesh with vorticity (rh) and a zero
+ *                                                  velocity field (no solve) -> OUTDIR/mesh.vtk
  *   poisson  NPTS SEED OUTDIR                      DirectSum::meshfreeSolve (src/LpmDirectSum.cpp:240-252)
  *                                                  with a 1/(4 pi r) ScalarKernel subclass
  *   pointtree NPTS SEED MAXLEAF OUTDIR             TreeSum(coords,...) meshfree ctor (src/LpmTreeSum.cpp:208-219)
@@ -31,6 +38,8 @@
 #include "LpmMPIReplicatedData.h"
 #include "LpmDirectSum.h"
 #include "LpmTreeSum.h"
+#include "LpmVtkFileIO.h"
+#include <fstream>
 #include "LpmEuclideanCoords.h"
 #include "LpmParticles.h"
 #include <mpi.h>
@@ -249,7 +258,7 @@ static uint64_t splitmix64(uint64_t& s) {
 static double uniform_pm1(uint64_t& s) { return 2.0 * ((splitmix64(s) >> 11) * (1.0 / 9007199254740992.0)) - 1.0; }
 
 static int usage() {
-    fprintf(stderr, "usage: ref_harness mesh|direct|scalar|tree|treesum|poisson|pointtree ...\n");
+    fprintf(stderr, "usage: ref_harness mesh|direct|scalar|vtk|tree|treesum|poisson|pointtree ...\n");
     return 2;
 }
 
@@ -382,6 +391,42 @@ int main(int argc, char** argv) {
             npy_f64(out, "vert_phi", vp);
             npy_f64(out, "face_phi", fp);
             printf("{\"cmd\": \"scalar\", \"kernel\": \"%s\", \"seconds\": %.6f}\n", kname.c_str(), secs);
+        } else if (cmd == "vtk" && argc == 7) {
+            auto seed = make_seed(argv[2]);
+            const std::string out = argv[6];
+            auto pm = std::make_shared<MeshedParticles>(*seed, atoi(argv[3]), atoi(argv[5]) != 0, 1.0, rank);
+            init_vorticity(*pm, argv[4]);
+            pm->createVertexField("velocity", "length/time", 3);
+            pm->createFaceField("velocity", "length/time", 3);
+            std::shared_ptr<VectorKernel> kernel(new BiotSavartSphere());
+            MPIReplicatedData mv(pm->nVertices(), rank, size), mf(pm->nFaces(), rank, size);
+            DirectSum solver(pm, kernel, "velocity", "vorticity");
+            solver.meshSolve(mv, mf);
+            pm->writeToVtkFile(out + "/mesh.vtk", "lpm vtk test");
+            {
+                VtkWriter writer;
+                std::ofstream fs(out + "/points.csv");
+                writer.writePointsAndFieldsToCSV(fs, pm->getCoordPtr(false),
+                                                 {pm->getVertexFieldPtr("velocity"), pm->getVertexFieldPtr("vorticity")});
+            }
+            std::vector<double> vz(pm->nVertices()), fz(pm->nFaces());
+            for (index_type i = 0; i < pm->nVertices(); ++i) vz[i] = pm->getVertexFieldPtr("vorticity")->getScalar(i);
+            for (index_type i = 0; i < pm->nFaces(); ++i) fz[i] = pm->getFaceFieldPtr("vorticity")->getScalar(i);
+            npy_f64(out, "vert_zeta", vz);
+            npy_f64(out, "face_zeta", fz);
+            npy_f64(out, "vert_vel", field3(pm->getVertexFieldPtr("velocity"), pm->nVertices()), 3);
+            npy_f64(out, "face_vel", field3(pm->getFaceFieldPtr("velocity"), pm->nFaces()), 3);
+        } else if (cmd == "vtktime" && argc == 5) {
+            auto seed = make_seed(argv[2]);
+            const std::string out = argv[4];
+            auto pm = std::make_shared<MeshedParticles>(*seed, atoi(argv[3]), false, 1.0, rank);
+            init_vorticity(*pm, "rh");
+            pm->createVertexField("velocity", "length/time", 3);
+            pm->createFaceField("velocity", "length/time", 3);
+            const auto t0 = std::chrono::steady_clock::now();
+            pm->writeToVtkFile(out + "/mesh.vtk", "lpm vtk test");
+            const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            printf("{\"cmd\": \"vtktime\", \"seconds\": %.6f}\n", secs);
         } else if (cmd == "poisson" && argc == 5) {
             const index_type n = atol(argv[2]);
             uint64_t s = strtoull(argv[3], nullptr, 0);

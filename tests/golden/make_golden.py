@@ -16,8 +16,12 @@ Fixtures
   poisson_2000.npz           DirectSum::meshfreeSolve with a 1/(4 pi r) ScalarKernel, 2000 points
   scalar_icos3_harm.npz      DirectSum::meshSolve, scalar branch, with the reference's SphereGreensFn(1),
                              PlanarGreensFnFreeBoundaries, SecondOrderDelta3d(0.1) and SphereDelta(0.1);
-                             icos level 3, zeta = sphereHarmonic54 (`python make_golden.py scalar` makes
-                             only this one)
+                             icos level 3, zeta = sphereHarmonic54
+  vtk_icos2_rh.npz,          MeshedParticles::writeToVtkFile (non-Lagrangian icos level 2 / Lagrangian cube
+  vtk_cube2_gauss_lag.npz    level 2) with vorticity and DirectSum velocity fields, and
+                             VtkWriter::writePointsAndFieldsToCSV of the vertices: the files' bytes and the
+                             field values written
+`python make_golden.py scalar vtk` remakes only the named groups.
 """
 from __future__ import annotations
 
@@ -59,11 +63,23 @@ def scalar_fixture() -> None:
     np.savez_compressed(HERE / "scalar_icos3_harm.npz", **z)
 
 
+def vtk_fixtures() -> None:
+    for kind, level, zeta, lag, name in (("icos", 2, "rh", 0, "vtk_icos2_rh"), ("cube", 2, "gauss", 1, "vtk_cube2_gauss_lag")):
+        d = harness("vtk", kind, level, zeta, lag)
+        z = load(d, "vert_zeta", "face_zeta", "vert_vel", "face_vel")
+        z["vtk"] = np.frombuffer((d / "mesh.vtk").read_bytes(), dtype=np.uint8)
+        z["csv"] = np.frombuffer((d / "points.csv").read_bytes(), dtype=np.uint8)
+        np.savez_compressed(HERE / f"{name}.npz", **z)
+
+
 def main() -> None:
-    if sys.argv[1:] == ["scalar"]:
-        scalar_fixture()
+    groups = {"scalar": scalar_fixture, "vtk": vtk_fixtures}
+    if sys.argv[1:]:
+        for g in sys.argv[1:]:
+            groups[g]()
         return
     scalar_fixture()
+    vtk_fixtures()
     for kind in ("icos", "cube"):
         d = harness("mesh", kind, 3)
         np.savez_compressed(HERE / f"mesh_{kind}3.npz",
