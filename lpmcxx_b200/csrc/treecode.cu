@@ -1026,10 +1026,10 @@ __device__ __forceinline__ void far_one_acc2(const float4* __restrict__ Bc, cons
 #define LPM_FAR2_MAX_ORDER 11
 #endif
 #ifndef LPM_FAR2_STAGE_UNITS
-#define LPM_FAR2_STAGE_UNITS 512
+#define LPM_FAR2_STAGE_UNITS 768
 #endif
 #ifndef LPM_FAR2_MIN_BLOCKS
-#define LPM_FAR2_MIN_BLOCKS 10
+#define LPM_FAR2_MIN_BLOCKS 8
 #endif
 constexpr int kFar2MaxOrder = LPM_FAR2_MAX_ORDER;  // FP32 orders up to this run two targets per thread (all used)
 constexpr int kFar2Threads = kBatch / 2;
@@ -1037,7 +1037,9 @@ constexpr int kFar2StageUnits = LPM_FAR2_STAGE_UNITS;
 constexpr int kFar2MinBlocks = LPM_FAR2_MIN_BLOCKS;
 
 // far_order_kernel<P, float, float4> with two targets per thread (targets i and i + 64 of the batch):
-// 64 threads per block, stages of kFar2StageUnits, same double buffering and the same sums.
+// 64 threads per block, stages of kFar2StageUnits, same double buffering and the same sums.  Built for 8
+// blocks per SM with 768-unit stages: measured faster than more resident blocks with smaller stages
+// (fewer block barriers per coefficient) and than fewer blocks with larger ones.
 template <int P>
 __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kernel(FarArgs A) {
     using S = FarShape<P, float4, kFar2StageUnits>;
@@ -1419,35 +1421,53 @@ __global__ void __launch_bounds__(kBatch) label_kernel(Octree t, const int2* __r
 }
 
 // ---------------------------------------------------------------------------------- near field
-constexpr int kNearThreads = 64;  // 2 targets per thread, kBatch targets per block
+#ifndef LPM_NEAR_TARGETS
+#define LPM_NEAR_TARGETS 2
+#endif
+constexpr int kNearTargets = LPM_NEAR_TARGETS;       // targets per thread (even; 4 measured slower than 2)
+constexpr int kNearThreads = kBatch / kNearTargets;  // kBatch targets per block
 
 constexpr int kNearStreamTile = 512;  // sources staged per tile
 constexpr int kNearRuns = 128;        // source ranges resolved per chunk
 
 // One tile of the stream: m tree-ordered sources (FP32 absolute coordinates, w pre-scaled by 2)
-// against the thread's two targets: D += sum_j (2 w_j / |x - y_j|^2) (x - y_j), FP32 within the tile,
+// against the thread's 2 NP targets: D += sum_j (2 w_j / |x - y_j|^2) (x - y_j), FP32 within the tile,
 // FP64 across tiles.  A target's own source (d = 0) contributes 0 through the clamped denominator.
-__device__ __forceinline__ void near_tile(const float4* tile, int m, float tx0, float ty0, float tz0, float tx1,
-                                          float ty1, float tz1, double* D0, double* D1) {
-    // the two targets travel as packed pairs (fma.rn.f32x2): d = t - y, rr = |d|^2 + 1e-30, f = w / rr
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
+// Targets travel as packed pairs (fma.rn.f32x2): d = t - y, rr = |d|^2 + 1e-30, f = w / rr; every
+// source read from shared memory serves all 2 NP targets.
+template <int NP>
+__device__ __forceinline__ void near_tile(const float4* tile, int m, const float (&tx)[2 * NP],
+                                          const float (&ty)[2 * NP], const float (&tz)[2 * NP],
+                                          double (&D)[2 * NP][3]) {
+    float a[2 * NP][3];
+#pragma unroll
+    for (int t = 0; t < 2 * NP; ++t) a[t][0] = a[t][1] = a[t][2] = 0.f;
 #pragma unroll 4
     for (int j = 0; j < m; ++j) {
         const float4 y = tile[j];
-        float dx0, dx1, dy0, dy1, dz0, dz1, r0, r1;
-        fma2p(dx0, dx1, y.x, y.x, -1.0f, tx0, tx1);
-        fma2p(dy0, dy1, y.y, y.y, -1.0f, ty0, ty1);
-        fma2p(dz0, dz1, y.z, y.z, -1.0f, tz0, tz1);
-        fma2v(r0, r1, dx0, dx1, dx0, dx1, 1e-30f, 1e-30f);
-        fma2v(r0, r1, dy0, dy1, dy0, dy1, r0, r1);
-        fma2v(r0, r1, dz0, dz1, dz0, dz1, r0, r1);
-        const float f = y.w * rcp32(r0), g = y.w * rcp32(r1);
-        fma2v(a0, b0, f, g, dx0, dx1, a0, b0);
-        fma2v(a1, b1, f, g, dy0, dy1, a1, b1);
-        fma2v(a2, b2, f, g, dz0, dz1, a2, b2);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            const int t = 2 * q;
+            float dx0, dx1, dy0, dy1, dz0, dz1, r0, r1;
+            fma2p(dx0, dx1, y.x, y.x, -1.0f, tx[t], tx[t + 1]);
+            fma2p(dy0, dy1, y.y, y.y, -1.0f, ty[t], ty[t + 1]);
+            fma2p(dz0, dz1, y.z, y.z, -1.0f, tz[t], tz[t + 1]);
+            fma2v(r0, r1, dx0, dx1, dx0, dx1, 1e-30f, 1e-30f);
+            fma2v(r0, r1, dy0, dy1, dy0, dy1, r0, r1);
+            fma2v(r0, r1, dz0, dz1, dz0, dz1, r0, r1);
+            float f, g;
+            fma2p(f, g, rcp32(r0), rcp32(r1), y.w, -0.0f, -0.0f);  // w / rr for both targets in one instruction
+            fma2v(a[t][0], a[t + 1][0], f, g, dx0, dx1, a[t][0], a[t + 1][0]);
+            fma2v(a[t][1], a[t + 1][1], f, g, dy0, dy1, a[t][1], a[t + 1][1]);
+            fma2v(a[t][2], a[t + 1][2], f, g, dz0, dz1, a[t][2], a[t + 1][2]);
+        }
     }
-    D0[0] += a0; D0[1] += a1; D0[2] += a2;
-    D1[0] += b0; D1[1] += b1; D1[2] += b2;
+#pragma unroll
+    for (int t = 0; t < 2 * NP; ++t) {
+        D[t][0] += a[t][0];
+        D[t][1] += a[t][1];
+        D[t][2] += a[t][2];
+    }
 }
 
 __device__ __forceinline__ void finish_target(int64_t q, int64_t qe, int64_t n_tgt, const double4& x,
@@ -1465,26 +1485,34 @@ __device__ __forceinline__ void finish_target(int64_t q, int64_t qe, int64_t n_t
 // clusters whose order was set to "direct"); it is streamed through shared memory in tiles of
 // kNearStreamTile sources regardless of how short the individual ranges are.
 // One tile of the scalar 1/r stream: D += sum_j w_j / |x - y_j| (FP32 within the tile, FP64 across
-// tiles); a source at the target's own position (r = 0) contributes nothing.
-__device__ __forceinline__ void near_tile_scalar(const float4* tile, int m, float tx0, float ty0, float tz0,
-                                                 float tx1, float ty1, float tz1, double* D0, double* D1) {
-    // the two targets travel as packed pairs (fma.rn.f32x2): d = t - y, rr = |d|^2, a += w / sqrt(rr)
-    float a = 0.f, c = 0.f;
+// tiles); a source at the target's own position (r = 0) contributes nothing.  Pairs of targets packed as
+// in near_tile.
+template <int NP>
+__device__ __forceinline__ void near_tile_scalar(const float4* tile, int m, const float (&tx)[2 * NP],
+                                                 const float (&ty)[2 * NP], const float (&tz)[2 * NP],
+                                                 double (&D)[2 * NP][3]) {
+    float a[2 * NP];
+#pragma unroll
+    for (int t = 0; t < 2 * NP; ++t) a[t] = 0.f;
 #pragma unroll 4
     for (int j = 0; j < m; ++j) {
         const float4 y = tile[j];
-        float dx0, dx1, dy0, dy1, dz0, dz1, r0, r1;
-        fma2p(dx0, dx1, y.x, y.x, -1.0f, tx0, tx1);
-        fma2p(dy0, dy1, y.y, y.y, -1.0f, ty0, ty1);
-        fma2p(dz0, dz1, y.z, y.z, -1.0f, tz0, tz1);
-        fma2v(r0, r1, dx0, dx1, dx0, dx1, -0.0f, -0.0f);
-        fma2v(r0, r1, dy0, dy1, dy0, dy1, r0, r1);
-        fma2v(r0, r1, dz0, dz1, dz0, dz1, r0, r1);
-        const float i0 = r0 > 0.f ? rsqrt32(r0) : 0.f, i1 = r1 > 0.f ? rsqrt32(r1) : 0.f;
-        fma2p(a, c, i0, i1, y.w, a, c);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            const int t = 2 * q;
+            float dx0, dx1, dy0, dy1, dz0, dz1, r0, r1;
+            fma2p(dx0, dx1, y.x, y.x, -1.0f, tx[t], tx[t + 1]);
+            fma2p(dy0, dy1, y.y, y.y, -1.0f, ty[t], ty[t + 1]);
+            fma2p(dz0, dz1, y.z, y.z, -1.0f, tz[t], tz[t + 1]);
+            fma2v(r0, r1, dx0, dx1, dx0, dx1, -0.0f, -0.0f);
+            fma2v(r0, r1, dy0, dy1, dy0, dy1, r0, r1);
+            fma2v(r0, r1, dz0, dz1, dz0, dz1, r0, r1);
+            const float i0 = r0 > 0.f ? rsqrt32(r0) : 0.f, i1 = r1 > 0.f ? rsqrt32(r1) : 0.f;
+            fma2p(a[t], a[t + 1], i0, i1, y.w, a[t], a[t + 1]);
+        }
     }
-    D0[0] += a;
-    D1[0] += c;
+#pragma unroll
+    for (int t = 0; t < 2 * NP; ++t) D[t][0] += a[t];
 }
 
 __device__ __forceinline__ void finish_target_scalar(int64_t q, int64_t qe, const double* D,
@@ -1505,26 +1533,36 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
                                                             const float4* __restrict__ src32,
                                                             const double* __restrict__ V, double mult,
                                                             double* __restrict__ U) {
+    constexpr int kT = kNearTargets, kNW = kNearThreads / 32, kRPT = kNearRuns / kNearThreads;
+    static_assert(kT % 2 == 0 && kNearThreads % 32 == 0 && kNearRuns % kNearThreads == 0, "near kernel shape");
     __shared__ float4 tile[kNearStreamTile];
     __shared__ int r_start[kNearRuns], r_pre[kNearRuns + 1];
+    __shared__ int warp_tot[kNW];
     const int64_t b = blockIdx.x;
     if (b >= *nbat) return;  // uniform per block
     const int64_t qe = batch_first[b + 1];
-    const int64_t q0 = batch_first[b] + threadIdx.x, q1 = q0 + kNearThreads;
-    const double4 x0 = q0 < qe ? tgt_sorted[q0] : make_double4(2, 2, 2, 0);
-    const double4 x1 = q1 < qe ? tgt_sorted[q1] : make_double4(2, 2, 2, 0);
-    const float tx0 = (float)x0.x, ty0 = (float)x0.y, tz0 = (float)x0.z;
-    const float tx1 = (float)x1.x, ty1 = (float)x1.y, tz1 = (float)x1.z;
-    double D0[3] = {0, 0, 0}, D1[3] = {0, 0, 0};
+    // targets i, i + kNearThreads, ... of the batch
+    float tx[kT], ty[kT], tz[kT];
+    double D[kT][3];
+#pragma unroll
+    for (int u = 0; u < kT; ++u) {
+        const int64_t q = batch_first[b] + threadIdx.x + u * kNearThreads;
+        const double4 x = q < qe ? tgt_sorted[q] : make_double4(2, 2, 2, 0);
+        tx[u] = (float)x.x;
+        ty[u] = (float)x.y;
+        tz[u] = (float)x.z;
+        D[u][0] = D[u][1] = D[u][2] = 0.0;
+    }
     const int64_t n0 = near_off[b], n1 = min(n0 + (int64_t)near_cnt[b], near_cap);
     const int64_t n_all = n1 - n0;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int64_t c0 = 0; c0 < n_all; c0 += kNearRuns) {
         // resolve up to kNearRuns entries into source ranges and their prefix offsets
-        int len[2], st[2];
+        int len[kRPT], st[kRPT];
+        int v = 0;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int64_t k = c0 + threadIdx.x * 2 + h;
+        for (int h = 0; h < kRPT; ++h) {
+            const int64_t k = c0 + threadIdx.x * kRPT + h;
             len[h] = 0;
             st[h] = 0;
             if (k < n_all) {
@@ -1532,24 +1570,29 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
                 st[h] = t.node_start[t.leaf_node[r.x]];
                 len[h] = t.node_end[t.leaf_node[r.y]] - st[h];
             }
+            v += len[h];
         }
-        // exclusive scan of the 2 x 64 lengths (two warps)
-        int v = len[0] + len[1];
+        // exclusive scan of the kNearRuns lengths (kNW warps)
         int incl = v;
         for (int o = 1; o < 32; o <<= 1) {
             const int u = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += u;
         }
         __syncthreads();  // previous chunk's readers of r_pre / r_start / tile are done
-        __shared__ int warp_tot[2];
         if (lane == 31) warp_tot[w] = incl;
         __syncthreads();
-        const int base = (w ? warp_tot[0] : 0) + incl - v;
-        r_pre[threadIdx.x * 2] = base;
-        r_pre[threadIdx.x * 2 + 1] = base + len[0];
-        r_start[threadIdx.x * 2] = st[0];
-        r_start[threadIdx.x * 2 + 1] = st[1];
-        const int total = warp_tot[0] + warp_tot[1];
+        int base = incl - v, total = 0;
+#pragma unroll
+        for (int k = 0; k < kNW; ++k) {
+            if (k < w) base += warp_tot[k];
+            total += warp_tot[k];
+        }
+#pragma unroll
+        for (int h = 0; h < kRPT; ++h) {
+            r_pre[threadIdx.x * kRPT + h] = base;
+            r_start[threadIdx.x * kRPT + h] = st[h];
+            base += len[h];
+        }
         if (threadIdx.x == 0) r_pre[kNearRuns] = total;
         __syncthreads();
         for (int p0 = 0; p0 < total; p0 += kNearStreamTile) {
@@ -1567,17 +1610,18 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
             }
             __syncthreads();
             if constexpr (kScalar)
-                near_tile_scalar(tile, m, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
+                near_tile_scalar<kT / 2>(tile, m, tx, ty, tz, D);
             else
-                near_tile(tile, m, tx0, ty0, tz0, tx1, ty1, tz1, D0, D1);
+                near_tile<kT / 2>(tile, m, tx, ty, tz, D);
         }
     }
-    if constexpr (kScalar) {
-        finish_target_scalar(q0, qe, D0, tperm, V, mult, U);
-        finish_target_scalar(q1, qe, D1, tperm, V, mult, U);
-    } else {
-        finish_target(q0, qe, n_tgt, x0, D0, tperm, V, mult, U);
-        finish_target(q1, qe, n_tgt, x1, D1, tperm, V, mult, U);
+#pragma unroll
+    for (int u = 0; u < kT; ++u) {
+        const int64_t q = batch_first[b] + threadIdx.x + u * kNearThreads;
+        if constexpr (kScalar)
+            finish_target_scalar(q, qe, D[u], tperm, V, mult, U);
+        else if (q < qe)
+            finish_target(q, qe, n_tgt, tgt_sorted[q], D[u], tperm, V, mult, U);  // FP64 position re-read
     }
 }
 
