@@ -357,12 +357,18 @@ __global__ void coeff_scalar_kernel(Octree t, int pm, const int4* __restrict__ e
 // Target batches.  Targets sorted by Morton key are cut into batches of at most kBatch consecutive
 // targets that also share one octree cell of level `level` (cells of edge 2/2^level): consecutive
 // Morton positions can be far apart across a cell boundary, and a batch's radius decides how many
-// clusters it can accept.  bflag[q] = 1 where a batch starts; one thread per cell walks its cell.
+// clusters it can accept.  bflag[q] = 1 where a batch starts: one thread per target finds the first
+// target of its cell by binary search in the sorted keys (batches start every kBatch targets from there).
 __global__ void batch_flags_kernel(const uint64_t* __restrict__ keys, int64_t n, int shift, int32_t* __restrict__ bflag) {
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
         const uint64_t cell = keys[q] >> shift;
-        if (q > 0 && (keys[q - 1] >> shift) == cell) continue;
-        for (int64_t j = q; j < n && (j == q || (keys[j] >> shift) == cell); ++j) bflag[j] = ((j - q) % kBatch) == 0;
+        int64_t lo = 0, hi = q;  // smallest j <= q in the same cell
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if ((keys[mid] >> shift) < cell) lo = mid + 1;
+            else hi = mid;
+        }
+        bflag[q] = ((q - lo) % kBatch) == 0;
     }
 }
 
@@ -499,7 +505,12 @@ __device__ __forceinline__ float log_budget(const double* node_wabs, double eps)
 // pairs that pass the acceptance test go to the far list with the order to use; leaves that fail it,
 // and accepted clusters too small to be worth an expansion, go to the near list as leaf-id ranges.
 // Entries are appended in lane order, so the lists are deterministic.
-__global__ void __launch_bounds__(128) traverse_kernel(TraverseArgs A) {
+// Registers capped for 4 resident blocks per SM (16 warps): the count pass, which runs the selector MLP,
+// is latency-bound, and at its natural 140 registers only 3 blocks fit (measured 1.52 -> 1.43 ms at icos L8).
+#ifndef LPM_TRAVERSE_MIN_BLOCKS
+#define LPM_TRAVERSE_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(128, LPM_TRAVERSE_MIN_BLOCKS) traverse_kernel(TraverseArgs A) {
     __shared__ int sstack[4][kWarpStack];
     __shared__ int pcnt[4][kPMax + 1];  // per warp: far entries of each order so far
     __shared__ __align__(16) __nv_bfloat16 mw[kMlpParams];
