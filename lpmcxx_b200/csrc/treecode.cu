@@ -1008,15 +1008,32 @@ __device__ __forceinline__ void horner2_f32x2(const float4* __restrict__ Bc, con
         for (int c = 0; c < 4; ++c) g[t][c] = G[t][c];
 }
 
-// far_one_acc<P, float, float4> for two targets (identical arithmetic per target).
+#ifndef LPM_FAR2_MAX_ORDER
+#define LPM_FAR2_MAX_ORDER 11
+#endif
+#ifndef LPM_FAR2_STAGE_UNITS
+#define LPM_FAR2_STAGE_UNITS 768
+#endif
+#ifndef LPM_FAR2_MIN_BLOCKS
+#define LPM_FAR2_MIN_BLOCKS 7
+#endif
+constexpr int kFar2MaxOrder = LPM_FAR2_MAX_ORDER;  // FP32 orders up to this run two targets per thread (all used)
+constexpr int kFar2Threads = kBatch / 2;
+constexpr int kFar2StageUnits = LPM_FAR2_STAGE_UNITS;
+constexpr int kFar2MinBlocks = LPM_FAR2_MIN_BLOCKS;
+
+// The far2 kernel's per-entry work in FP32 throughout: centres and targets are offsets from a point of the
+// batch (its first target), so d = c - x is one FP32 subtraction; 1/|d|^2 by the approximate reciprocal
+// (1 ulp); contributions summed in FP32 over a stage (acc32) and folded into FP64 once per stage.  x holds
+// the targets' absolute FP32 coordinates (for x cross d), xo their offsets, c the centre's offset.
 template <int P>
-__device__ __forceinline__ void far_one_acc2(const float4* __restrict__ Bc, const double4 (&x)[2], double cx,
-                                             double cy, double cz, double (&acc)[2][3]) {
+__device__ __forceinline__ void far_one_acc2_f32(const float4* __restrict__ Bc, const float (&x)[2][3],
+                                                 const float (&xo)[2][3], const float4 c, float (&acc32)[2][3]) {
     float d[2][3], e[2][4], g[2][4];
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
-        const float dx = (float)(cx - x[t].x), dy = (float)(cy - x[t].y), dz = (float)(cz - x[t].z);
-        const float inv = 1.0f / (dx * dx + dy * dy + dz * dz);
+        const float dx = c.x - xo[t][0], dy = c.y - xo[t][1], dz = c.z - xo[t][2];
+        const float inv = rcp32(dx * dx + dy * dy + dz * dz);
         d[t][0] = dx; d[t][1] = dy; d[t][2] = dz;
         e[t][0] = dx * inv; e[t][1] = dy * inv; e[t][2] = dz * inv; e[t][3] = inv;
     }
@@ -1026,36 +1043,40 @@ __device__ __forceinline__ void far_one_acc2(const float4* __restrict__ Bc, cons
         const float dx = d[t][0], dy = d[t][1], dz = d[t][2];
         const float s = 2.0f * e[t][3];
         const float G0 = s * g[t][0], Gx = s * g[t][1], Gy = s * g[t][2], Gz = s * g[t][3];
-        const float xx = (float)x[t].x, xy = (float)x[t].y, xz = (float)x[t].z;
-        acc[t][0] += (double)((xy * dz - xz * dy) * G0 + (xy * Gz - xz * Gy));
-        acc[t][1] += (double)((xz * dx - xx * dz) * G0 + (xz * Gx - xx * Gz));
-        acc[t][2] += (double)((xx * dy - xy * dx) * G0 + (xx * Gy - xy * Gx));
+        const float xx = x[t][0], xy = x[t][1], xz = x[t][2];
+        acc32[t][0] += (xy * dz - xz * dy) * G0 + (xy * Gz - xz * Gy);
+        acc32[t][1] += (xz * dx - xx * dz) * G0 + (xz * Gx - xx * Gz);
+        acc32[t][2] += (xx * dy - xy * dx) * G0 + (xx * Gy - xy * Gx);
     }
 }
 
-#ifndef LPM_FAR2_MAX_ORDER
-#define LPM_FAR2_MAX_ORDER 11
-#endif
-#ifndef LPM_FAR2_STAGE_UNITS
-#define LPM_FAR2_STAGE_UNITS 768
-#endif
-#ifndef LPM_FAR2_MIN_BLOCKS
-#define LPM_FAR2_MIN_BLOCKS 8
-#endif
-constexpr int kFar2MaxOrder = LPM_FAR2_MAX_ORDER;  // FP32 orders up to this run two targets per thread (all used)
-constexpr int kFar2Threads = kBatch / 2;
-constexpr int kFar2StageUnits = LPM_FAR2_STAGE_UNITS;
-constexpr int kFar2MinBlocks = LPM_FAR2_MIN_BLOCKS;
+// Stage gather of the far2 kernel: coefficients by cp.async as far_stage_gather, cluster centres as FP32
+// offsets from the block's origin o.
+template <int P>
+__device__ __forceinline__ void far2_stage_gather(const FarArgs& A, int64_t s0, int n, float4* buf, float4* ctr,
+                                                  const double4& o) {
+    constexpr int kUnits = FarShape<P, float4>::kUnits;
+    for (int i = threadIdx.x; i < n * kUnits; i += kFar2Threads) {
+        const int e = i / kUnits, j = i - e * kUnits;
+        const int node = A.far_list[s0 + e].x;
+        cp_async16(buf + i, A.B32 + (size_t)node * A.n_ent + A.gtab[j]);
+    }
+    if ((int)threadIdx.x < n) {
+        const double4 c = A.node_ctr[A.far_list[s0 + threadIdx.x].x];
+        ctr[threadIdx.x] = make_float4((float)(c.x - o.x), (float)(c.y - o.y), (float)(c.z - o.z), 0.0f);
+    }
+}
 
 // far_order_kernel<P, float, float4> with two targets per thread (targets i and i + 64 of the batch):
-// 64 threads per block, stages of kFar2StageUnits, same double buffering and the same sums.  Built for 8
-// blocks per SM with 768-unit stages: measured faster than more resident blocks with smaller stages
-// (fewer block barriers per coefficient) and than fewer blocks with larger ones.
+// 64 threads per block, stages of kFar2StageUnits, the same double buffering.  Built for 7 blocks per SM
+// (128 registers; the odd orders spill up to 128 bytes to L1) with 768-unit stages: measured faster than
+// 6 blocks without spills, than more resident blocks with smaller stages (fewer block barriers per
+// coefficient) and than fewer blocks with larger ones.
 template <int P>
 __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kernel(FarArgs A) {
     using S = FarShape<P, float4, kFar2StageUnits>;
-    extern __shared__ float4 fbuf[];  // 2 stages of S::kStage units, then 2 x kK centres
-    double4* ctr = (double4*)(fbuf + 2 * S::kStage);
+    extern __shared__ float4 fbuf[];  // 2 stages of S::kStage units, then 2 x kK centres (FP32 offsets)
+    float4* ctr = fbuf + 2 * S::kStage;
     const int64_t b = blockIdx.x;
     if (b >= *A.nbat) return;  // uniform per block
     const int64_t f0 = A.far_off[b], f1 = min(f0 + (int64_t)A.far_cnt[b], A.far_cap);
@@ -1063,26 +1084,37 @@ __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kerne
     const int64_t q0 = A.batch_first[b], qe = A.batch_first[b + 1];
     const int64_t qa = q0 + threadIdx.x, qb = qa + kFar2Threads;
     const bool live = q0 + (int64_t)(threadIdx.x & ~31) < qe;  // warp-uniform (second targets lie further on)
-    const double4 x[2] = {qa < qe ? A.tgt_sorted[qa] : make_double4(0, 0, 1, 0),
-                          qb < qe ? A.tgt_sorted[qb] : make_double4(0, 0, 1, 0)};
+    const double4 o = A.tgt_sorted[q0];  // the block's origin for FP32 offsets
+    float x[2][3], xo[2][3];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const int64_t q = t ? qb : qa;
+        const double4 p = q < qe ? A.tgt_sorted[q] : make_double4(0, 0, 1, 0);
+        x[t][0] = (float)p.x; x[t][1] = (float)p.y; x[t][2] = (float)p.z;
+        xo[t][0] = (float)(p.x - o.x); xo[t][1] = (float)(p.y - o.y); xo[t][2] = (float)(p.z - o.z);
+    }
     double acc[2][3] = {{0, 0, 0}, {0, 0, 0}};
-    far_stage_gather<P, float4, kFar2Threads>(A, f0, (int)min((int64_t)S::kK, f1 - f0), fbuf, ctr);
+    far2_stage_gather<P>(A, f0, (int)min((int64_t)S::kK, f1 - f0), fbuf, ctr, o);
     cp_async_commit();
     int s = 0;
     for (int64_t s0 = f0;; s ^= 1) {
         const int n = (int)min((int64_t)S::kK, f1 - s0);
         const int64_t s1 = s0 + n;
         if (s1 < f1)
-            far_stage_gather<P, float4, kFar2Threads>(A, s1, (int)min((int64_t)S::kK, f1 - s1),
-                                                      fbuf + (size_t)(s ^ 1) * S::kStage, ctr + (s ^ 1) * S::kK);
+            far2_stage_gather<P>(A, s1, (int)min((int64_t)S::kK, f1 - s1), fbuf + (size_t)(s ^ 1) * S::kStage,
+                                 ctr + (s ^ 1) * S::kK, o);
         cp_async_commit();
         cp_async_wait_prev();
         __syncthreads();  // stage s resident
         if (live) {
             const float4* Bc = fbuf + (size_t)s * S::kStage;
-            const double4* cs = ctr + s * S::kK;
-            for (int k = 0; k < n; ++k)
-                far_one_acc2<P>(Bc + (size_t)k * entries_for(P), x, cs[k].x, cs[k].y, cs[k].z, acc);
+            const float4* cs = ctr + s * S::kK;
+            float acc32[2][3] = {{0, 0, 0}, {0, 0, 0}};
+            for (int k = 0; k < n; ++k) far_one_acc2_f32<P>(Bc + (size_t)k * entries_for(P), x, xo, cs[k], acc32);
+#pragma unroll
+            for (int t = 0; t < 2; ++t)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) acc[t][c] += (double)acc32[t][c];
         }
         if (s1 >= f1) break;
         __syncthreads();  // stage s consumed before it is refilled
