@@ -201,6 +201,10 @@ typedef struct lpm_tree lpm_tree;
  * LPM_ERR_CAPACITY (tree still created) if a leaf at max_depth holds more than max_per_leaf points. */
 int lpm_tree_build(lpm_ctx* ctx, const double* pts, int64_t n, const double* box, int max_per_leaf, int max_depth,
                    lpm_tree** out);
+/* lpm_tree_build from host coordinates xyz (n x 3): the tree TreeSum's mesh constructor builds
+ * (src/LpmTreeSum.cpp:221-238), for callers without device buffers (the drop-in TreeSum's node count). */
+int lpm_tree_build_host(lpm_ctx* ctx, const double* xyz, int64_t n, const double* box, int max_per_leaf, int max_depth,
+                        lpm_tree** out);
 int lpm_tree_destroy(lpm_tree* tree);
 int lpm_tree_counts(const lpm_tree* tree, int64_t* n_in_tree, int64_t* n_nodes, int64_t* n_leaves, int* depth);
 /* Leaf membership as the reference holds it: members (host, n_in_tree) lists the point indices of every

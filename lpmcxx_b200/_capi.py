@@ -92,6 +92,7 @@ SIGNATURES = {
                                       I64, I64, I64, I64, P, P, P, P, P, P]),
     "lpm_direct_sum_meshfree": (C.c_int, [P, C.POINTER(KernelDesc), C.c_int, I64, P, P, P, P, P, I64, I64, P]),
     "lpm_tree_build": (C.c_int, [P, P, I64, P, C.c_int, C.c_int, C.POINTER(P)]),
+    "lpm_tree_build_host": (C.c_int, [P, P, I64, P, C.c_int, C.c_int, C.POINTER(P)]),
     "lpm_tree_destroy": (C.c_int, [P]),
     "lpm_tree_counts": (C.c_int, [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(C.c_int)]),
     "lpm_tree_leaf_membership": (C.c_int, [P, P, P]),

@@ -90,6 +90,22 @@ extern "C" int lpm_tree_build(lpm_ctx* ctx, const double* pts, int64_t n, const 
     return LPM_OK;
 }
 
+extern "C" int lpm_tree_build_host(lpm_ctx* ctx, const double* xyz, int64_t n, const double* box, int max_per_leaf,
+                                   int max_depth, lpm_tree** out) {
+    if (!ctx || !out || (n > 0 && !xyz) || n < 0) {
+        set_error("lpm_tree_build_host: bad argument");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t bytes = sizeof(double4) * (size_t)std::max<int64_t>(n, 1);
+    double4* h = (double4*)pinned(ctx, bytes);
+    double4* d = (double4*)scratch(ctx, kSlotSrcPack, bytes);
+    if (!h || !d) return LPM_ERR_OOM;
+    for (int64_t i = 0; i < n; ++i) h[i] = make_double4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.0);
+    if (n > 0) LPM_CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(double4) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    return lpm_tree_build(ctx, (const double*)d, n, box, max_per_leaf, max_depth, out);
+}
+
 extern "C" int lpm_tree_destroy(lpm_tree* tr) {
     if (!tr) return LPM_OK;
     cudaSetDevice(tr->ctx->device);

@@ -38,7 +38,34 @@ TreeSum::TreeSum(const int max_series_order, const int max_particles_per_box, st
       _mesh(pmesh),
       _vertTgt(pmesh->getVertexFieldPtr(tgtFieldName)),
       _faceSrc(pmesh->getFaceFieldPtr(srcFieldName)),
-      _faceTgt(pmesh->getFaceFieldPtr(tgtFieldName)) {}
+      _faceTgt(pmesh->getFaceFieldPtr(tgtFieldName)) {
+    // The reference's constructor builds the tree over the leaf-face centroids under Box3d(maxR) and counts
+    // its nodes (nNodes()); it never computes a depth (depth() stays 0).  The same tree is built here on the
+    // GPU for its node count.
+    const Box3d rbox(pmesh->maxR());
+    std::vector<double> xyz;
+    xyz.reserve(3 * (size_t)pmesh->nFaces());
+    for (index_type i = 0; i < pmesh->nFaces(); ++i) {
+        if (pmesh->faceIsDivided(i)) continue;
+        const XyzVector c = pmesh->getFaceCentroid(i);
+        xyz.push_back(c.x);
+        xyz.push_back(c.y);
+        xyz.push_back(c.z);
+    }
+    const double box[6] = {rbox.xmin, rbox.xmax, rbox.ymin, rbox.ymax, rbox.zmin, rbox.zmax};
+    lpm_tree* tr = nullptr;
+    const int rc = lpm_tree_build_host(b200::context(), xyz.data(), (int64_t)(xyz.size() / 3), box,
+                                       _maxParticlesPerNode, 0, &tr);
+    if (tr) {
+        int64_t n_in = 0, n_nodes = 0, n_leaves = 0;
+        int depth = 0;
+        const int rc2 = lpm_tree_counts(tr, &n_in, &n_nodes, &n_leaves, &depth);
+        lpm_tree_destroy(tr);
+        b200::check(rc2, "lpm_tree_counts");
+        _nnodes = (index_type)n_nodes;
+    }
+    if (rc != LPM_ERR_CAPACITY) b200::check(rc, "lpm_tree_build_host");
+}
 
 void TreeSum::computeMoments(const std::shared_ptr<Field>) {}
 void TreeSum::computeMeshMoments() {}

@@ -111,7 +111,8 @@ int main(int argc, char** argv) {
             const std::string out = argv[8];
             write_f64(out + "/vert_vel.bin", rows3(pm->getVertexFieldPtr("velocity"), pm->nVertices()));
             write_f64(out + "/face_vel.bin", rows3(pm->getFaceFieldPtr("velocity"), pm->nFaces()));
-            std::printf("{\"cmd\": \"tree\", \"mac_count\": %d}\n", mac);
+            std::printf("{\"cmd\": \"tree\", \"mac_count\": %d, \"n_nodes\": %ld, \"depth\": %d}\n", mac,
+                        (long)ts.nNodes(), ts.depth());
         } else if (cmd == "scalar" && argc == 8) {
             auto pm = mesh_with_zeta(argv[2], std::atoi(argv[3]), argv[6]);
             pm->createVertexField("potential", "n/a", 1);

@@ -1,6 +1,7 @@
 """The drop-in C++ classes: the reference's Lpm::DirectSum / Lpm::TreeSum API (its own headers and
 callers) with the GPU implementations linked in place of src/LpmDirectSum.cpp / src/LpmTreeSum.cpp,
 checked against fixtures produced by the unmodified reference."""
+import json
 import os
 import subprocess
 import tempfile
@@ -95,8 +96,21 @@ def test_dropin_treesum_against_reference_direct_sum():
         out = run("tree", "icos", 4, 6, 32, 0.5, f"{d}/zeta.bin", d)
         vv = np.fromfile(f"{d}/vert_vel.bin").reshape(-1, 3)
         fv = np.fromfile(f"{d}/face_vel.bin").reshape(-1, 3)
-    assert '"mac_count"' in out and int(out.split('"mac_count": ')[1].split("}")[0]) > 0
+    assert json.loads(out.strip().splitlines()[-1])["mac_count"] > 0
     leaf = np.any(g["face_vel"] != 0, axis=1)
     # order 6 (|k| < 6) at theta 0.5: the accuracy class of the host-API treecode test
     assert rel_l2(vv, g["vert_vel"]) < 2e-3
     assert rel_l2(fv[leaf], g["face_vel"][leaf]) < 2e-3
+
+
+@pytest.mark.gpu
+@needs_driver
+def test_dropin_treesum_node_count_matches_reference_tree():
+    # the reference's mesh constructor counts the nodes of its tree (nNodes()) and leaves depth() at 0
+    ref = golden("tree_icos4_m64.npz")
+    g = golden("direct_icos4_rh.npz")
+    with tempfile.TemporaryDirectory() as d:
+        g["face_zeta"].astype("<f8").tofile(f"{d}/zeta.bin")
+        out = json.loads(run("tree", "icos", 4, 6, 64, 0.5, f"{d}/zeta.bin", d).strip().splitlines()[-1])
+    assert out["n_nodes"] == ref["node_level"].shape[0]
+    assert out["depth"] == 0
