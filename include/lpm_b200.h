@@ -258,7 +258,8 @@ int lpm_treesum_stats(lpm_treesum* ts, int64_t* out10);
  * construction).  "theta": acceptance criterion, 0 < theta < 1; "f64_from": far expansions of this
  * order and above evaluate in FP64 (1..13; default 13 = all FP32 for LPM_PREC_F32 solvers, 1 for
  * LPM_PREC_F64); "batch_level": octree level whose cells a target batch may not straddle (1 .. the
- * level chosen at creation; coarser levels give fuller batches).  Takes effect at the next evaluation. */
+ * level chosen at creation; coarser levels give fuller batches); "order_bias" (learned selector only): 0..3
+ * orders added to every order the selector picks, capped at 11.  Takes effect at the next evaluation. */
 int lpm_treesum_set_param(lpm_treesum* ts, const char* name, double value);
 /* Current value of a run-time parameter: those of lpm_treesum_set_param, plus "batch_level_max" (the finest
  * batch level allowed) and "order" (the fixed order in the solver's convention: Poisson reports p + 1). */

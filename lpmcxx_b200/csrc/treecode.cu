@@ -433,6 +433,7 @@ struct TraverseArgs {
     // learned order selection (learned != 0): the MLP picks each accepted pair's order
     int learned;
     int max_order;
+    int order_bias;  // added to every order the selector picks (capped at max_order)
     double eps;
     CutoffTable ct;
     const float* node_feat;
@@ -587,7 +588,7 @@ __global__ void __launch_bounds__(128, LPM_TRAVERSE_MIN_BLOCKS) traverse_kernel(
                 }
             }
             if (far_ok) {
-                P = cls == kMlpDirectClass ? 0 : min(cls + 1, A.max_order);
+                P = cls == kMlpDirectClass ? 0 : min(cls + 1 + A.order_bias, A.max_order);
                 cut = P > 0 ? A.ct.direct_below[P] : 0x7fffffff;
                 if (P == 0 && nc > 0 && e - s >= A.ct.direct_below[A.max_order]) far_ok = false;
             }
@@ -1741,6 +1742,7 @@ struct TreeSolver {
     bool learned = false;     // order_policy == LPM_ORDER_LEARNED
     bool mlp_loaded = false;  // weights present; without them the fixed order is the fallback
     double eps = 2e-8;        // per-pair error budget relative to |mult| * sum|w|
+    int order_bias = 0;       // orders added to the selector's choice
     float* node_feat = nullptr;
     __nv_bfloat16* mlp_w = nullptr;
     float* mlp_norm = nullptr;
@@ -2035,6 +2037,7 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     A.fill = 0;
     A.learned = (t->learned && t->mlp_loaded) ? 1 : 0;
     A.max_order = std::min(t->pm, kMlpDirectClass);
+    A.order_bias = t->order_bias;
     A.eps = t->eps;
     A.ct = t->ct;
     A.node_feat = t->node_feat;
@@ -2252,6 +2255,7 @@ int tree_get_param(const TreeSolver* t, const char* name, double* value) {
     if (n == "theta") *value = t->solver.theta;
     else if (n == "eps") *value = t->eps;
     else if (n == "f64_from") *value = t->f64_from;
+    else if (n == "order_bias") *value = t->order_bias;
     else if (n == "batch_level") *value = t->batch_level;
     else if (n == "batch_level_max") *value = t->batch_level_max;
     else if (n == "order") *value = t->order;
@@ -2272,6 +2276,8 @@ int tree_set_param(TreeSolver* t, const char* name, double value) {
         t->solver.theta = value;
     } else if (n == "eps" && value > 0.0) {
         t->eps = value;
+    } else if (n == "order_bias" && value >= 0.0 && value <= 3.0 && value == std::floor(value)) {
+        t->order_bias = (int)value;
     } else if (n == "batch_level" && value >= 1.0 && value <= t->batch_level_max && value == std::floor(value)) {
         t->batch_level = (int)value;
     } else if (n == "f64_from" && value >= 1.0 && value <= kPMax + 1 && value == std::floor(value)) {

@@ -191,3 +191,33 @@ def test_learned_rk4_graph_matches_uncaptured(ctx):
         out.append(rk.get_state())
         rk.close()
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.gpu
+def test_order_bias_raises_orders_and_accuracy(ctx):
+    """order_bias adds orders to every selector choice: more far-field terms, smaller error; values outside
+    0..3 are rejected."""
+    params, _ = learned.load()
+    torch = ctx.use_torch_stream()
+    _, p, n_src = field(6)
+    n = p.shape[0]
+    d = torch.tensor(p, device="cuda")
+    u64 = torch.empty((3, n), dtype=torch.float64, device="cuda")
+    ctx.direct_sum_dev(L.biot_savart_kernel(), L.LPM_PREC_F64, d[:n_src], d, u64, n_coincident=n_src)
+    res = {}
+    for bias in (0, 2):
+        ts = L.TreeSum(ctx, L.biot_savart_kernel(), L.tree_solver(L.LPM_PREC_F32, 10, 256, 0.5, learned=True,
+                                                                  tolerance=1e-7), n_src, n)
+        ts.set_mlp(params)
+        ts.set_param("order_bias", bias)
+        assert ts.get_param("order_bias") == bias
+        u = torch.empty((3, n), dtype=torch.float64, device="cuda")
+        ts.eval(d[:n_src], d, u)
+        torch.cuda.synchronize()
+        res[bias] = (float(torch.linalg.norm(u - u64) / torch.linalg.norm(u64)), ts.stats()["far_terms"])
+        for bad in (-1, 4, 1.5):
+            with pytest.raises(L.LpmError):
+                ts.set_param("order_bias", bad)
+        ts.close()
+    assert res[2][1] > res[0][1]
+    assert res[2][0] < res[0][0]
