@@ -1,13 +1,15 @@
 """Autotuner for the treecode: picks the fastest (leaf size, acceptance theta, batch cell level, and the
-fixed order or the learned selector's per-pair budget) that meets a relative L2 tolerance on a workload.
+fixed order or the learned selector's per-pair budget and order bias) that meets a relative L2 tolerance on
+a workload.
 
 Accuracy is judged on a random sample of targets against the FP64 direct sum (the library's own
 `lpm_direct_sum_dev`, which is parity-tested against the reference); time is the median of CUDA-event
 timed evaluations on the GPU.  Candidates sharing a leaf size reuse one solver and switch the run-time
 parameters (`TreeSum.set_param`), so a sweep costs one octree allocation per leaf size.
 
-    best = autotune(ctx, L.biot_savart_kernel(), src, tgt, tol=1e-6)
+    best = autotune(ctx, L.biot_savart_kernel(), src, tgt, tol=1e-6, order_biases=(0, 2))
     solver = tuned_solver(best)            # an lpm_solver_desc for TreeSum / RK4
+    # then set_param("batch_level", best.best.batch_level) and set_param("order_bias", best.best.bias)
 """
 from __future__ import annotations
 
@@ -25,6 +27,7 @@ class Candidate:
     theta: float
     knob: float            # learned: per-pair budget eps; fixed: Taylor order
     batch_level: int | None = None
+    bias: int = 0           # learned: orders added to every selector choice
     ms: float | None = None
     rel_err: float | None = None
 
@@ -39,8 +42,8 @@ class TuneResult:
     def as_dict(self) -> dict:
         b = self.best
         return {"learned": self.learned, "max_per_leaf": b.max_per_leaf, "theta": b.theta,
-                ("eps" if self.learned else "order"): b.knob, "batch_level": b.batch_level, "ms": b.ms,
-                "rel_err": b.rel_err}
+                ("eps" if self.learned else "order"): b.knob, "batch_level": b.batch_level,
+                "order_bias": b.bias, "ms": b.ms, "rel_err": b.rel_err}
 
 
 def default_grid(learned: bool, kernel_kind: int):
@@ -73,12 +76,13 @@ def _timed_eval(ctx, ts, src, tgt, out, reps):
 
 def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bool = True, params=None,
              grid=None, batch_levels=(0, -1), sample: int = 4096, reps: int = 3, seed: int = 0,
-             safety: float = 0.8) -> TuneResult:
+             safety: float = 0.8, order_biases=(0,)) -> TuneResult:
     """Sweep the grid on device-resident src (n_src, 4) / tgt (n_tgt, 4) float64 tensors.
 
     tol: relative L2 tolerance over the sampled targets (a candidate must reach safety * tol).
     learned: tune the learned selector's budget (Biot-Savart only) instead of the fixed order.
     batch_levels: offsets from each solver's default batch cell level to try (0 = default).
+    order_biases: learned only, the selector order biases to try (set_param "order_bias").
     """
     import torch
 
@@ -113,10 +117,11 @@ def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bo
                     ts.close()
                     ts = TreeSum(ctx, kernel, tree_solver(LPM_PREC_F32, int(knob), leaf, thetas[0]), n_src, n_tgt)
                     base_knob = int(knob)
-                for theta in thetas:
+                for theta, bias in [(t, b) for t in thetas for b in (order_biases if learned else (0,))]:
                     ts.set_param("theta", theta)
                     if learned:
                         ts.set_param("eps", knob)
+                        ts.set_param("order_bias", bias)
                     for off in batch_levels:
                         if level0 is None:
                             level0 = int(ts.get_param("batch_level"))
@@ -126,7 +131,7 @@ def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bo
                         ts.set_param("batch_level", lvl)
                         ms = _timed_eval(ctx, ts, src, tgt, out, reps)
                         err = float(torch.linalg.norm(out[:, idx_t] - ref)) / ref_norm
-                        c = Candidate(leaf, theta, knob, lvl, ms, err)
+                        c = Candidate(leaf, theta, knob, lvl, bias, ms, err)
                         res.tried.append(c)
                         if err <= safety * tol and (res.best is None or ms < res.best.ms):
                             res.best = c
@@ -137,8 +142,9 @@ def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bo
 
 
 def tuned_solver(result: TuneResult, precision: int = LPM_PREC_F32):
-    """lpm_solver_desc of the tuned setting (the batch level is a run-time parameter: apply it with
-    set_param("batch_level", result.best.batch_level) on the TreeSum / RK4 made from this descriptor)."""
+    """lpm_solver_desc of the tuned setting (the batch level and the order bias are run-time parameters:
+    apply them with set_param("batch_level", result.best.batch_level) and set_param("order_bias",
+    result.best.bias) on the TreeSum / RK4 made from this descriptor)."""
     b = result.best
     if b is None:
         raise ValueError("no candidate met the tolerance")

@@ -28,12 +28,14 @@ def test_autotune_learned_sphere(ctx):
     d = torch.tensor(p, device="cuda")
     tol = 1e-6
     res = autotune(ctx, L.biot_savart_kernel(), d[:n_src], d, tol, learned=True,
-                   grid=((128, 256), (0.5, 0.6), (1e-8, 3e-8)), sample=2048)
+                   grid=((128, 256), (0.5, 0.6), (1e-8, 3e-8, 3e-7)), sample=2048, order_biases=(0, 2))
     check(res, tol)
+    assert {c.bias for c in res.tried} == {0, 2}
     # the tuned descriptor reproduces the accuracy on all targets
     ts = L.TreeSum(ctx, L.biot_savart_kernel(), tuned_solver(res), n_src, p.shape[0])
     ts.set_mlp(L.learned.load()[0])
     ts.set_param("batch_level", res.best.batch_level)
+    ts.set_param("order_bias", res.best.bias)
     out = torch.empty((3, p.shape[0]), dtype=torch.float64, device="cuda")
     ts.eval(d[:n_src], d, out)
     ts.close()
