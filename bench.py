@@ -231,7 +231,8 @@ def far_entries(p: int) -> int:
 
 
 def kernel_work(kernel: str, n_src: int, n_tgt: int, stats: dict | None, order: int) -> tuple[float, str] | None:
-    """Algorithmic flops of one launch of `kernel` (see the work conventions in DESIGN.md)."""
+    """Algorithmic flops of one launch of `kernel`: 17 per Biot-Savart pair (direct and near field), 8 per
+    far-field expansion coefficient plus 40 per (target, cluster) evaluation."""
     if kernel in ("bs_f32_kernel", "bs_f64_kernel"):
         return FLOPS_PER_BS_PAIR * float(n_src) * float(n_tgt), "TFLOP/s"
     if kernel == "near_kernel" and stats:
@@ -408,6 +409,85 @@ def run_gpu_ensemble(args) -> None:
     print(json.dumps(out))
 
 
+def pairwise_direct_f32(ctx, kern, state0, n_src: int, fp32_peak: float, u64, stream) -> dict:
+    """The FP32 direct-sum kernel (bs_f32_kernel) on the headline workload: one warm-up evaluation, then
+    one evaluation timed by the library's per-launch CUDA events; its TFLOP/s at 17 flops per pair
+    against the measured FP32 FMA peak, and its error against the FP64 direct sum."""
+    import torch
+
+    import lpmcxx_b200 as L
+
+    n = state0.shape[0]
+    out = torch.empty((3, n), dtype=torch.float64, device="cuda")
+    ctx.direct_sum_dev(kern, L.LPM_PREC_F32, state0[:n_src], state0, out, n_coincident=n_src)
+    ctx.set_profiling(True)
+    ctx.direct_sum_dev(kern, L.LPM_PREC_F32, state0[:n_src], state0, out, n_coincident=n_src)
+    prof = ctx.profile_report()
+    ctx.set_profiling(False)
+    ms = prof["bs_f32_kernel"]["ms"]
+    tflops = FLOPS_PER_BS_PAIR * float(n_src) * float(n) / (ms * 1e-3) * 1e-12
+    return {"kernel": "bs_f32_kernel", "ms": ms, "pairs": n_src * n, "achieved_tflops": tflops,
+            "peak_tflops": fp32_peak, "frac": tflops / fp32_peak,
+            "rel_l2_vs_fp64_direct": float(torch.linalg.norm(out - u64) / torch.linalg.norm(u64)),
+            "timing": "one evaluation after one warm-up, CUDA events around the launch"}
+
+
+def poisson_summary(ctx, device: int, n: int = 1_048_576, reps: int = 5) -> dict:
+    """The 3D Poisson treecode configuration inside the headline run: evaluations/s at n points (median
+    of `reps` evaluations after 3 warm-up ones), its error against the FP64 direct sum, the dominant
+    kernel's roofline and the near / far split."""
+    import torch
+
+    import lpmcxx_b200 as L
+    import lpmcxx_b200.workloads as W
+
+    pts = torch.tensor(W.poisson_cube(n), device="cuda")
+    kern = L.poisson_kernel()
+    order, theta, leaf = POISSON_SETTINGS
+    ts = L.TreeSum(ctx, kern, L.tree_solver(L.LPM_PREC_F32, order, leaf, theta), n, n)
+    out = torch.empty((1, n), dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        ts.eval(pts, pts, out)
+    stream = torch.cuda.current_stream()
+    ms = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ts.eval(pts, pts, out)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    ctx.set_profiling(True)
+    ts.eval(pts, pts, out)
+    prof = ctx.profile_report()
+    ctx.set_profiling(False)
+    st = ts.stats()
+    ts.close()
+    ref = torch.empty_like(out)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.direct_sum_dev(kern, L.LPM_PREC_F64, pts, pts, ref)
+    e1.record(stream)
+    e1.synchronize()
+    fp32_peak = ctx.fma_peak_tflops(L.LPM_PREC_F32)
+    near_ms = prof.get("near_kernel", {}).get("ms", float("nan"))
+    far_ms = prof.get("far_kernel", {}).get("ms", float("nan"))
+    near_tf = FLOPS_PER_POISSON_PAIR * float(st["near_pairs"]) / (near_ms * 1e-3) * 1e-12
+    far_tf = (2.0 * float(st["far_terms"]) + 12.0 * float(st["far_evals"])) / (far_ms * 1e-3) * 1e-12
+    med = float(np.median(ms))
+    return {"workload": f"{n:,} points uniform in [-1,1]^3, charges U(-1,1), splitmix64 seed 0x2B",
+            "solver": f"Poisson treecode p={order} (|k|<=p), theta={theta}, {leaf} per leaf",
+            "evaluations_per_s": 1e3 / med, "ms_per_evaluation": med,
+            "rel_l2_vs_fp64_direct": float(torch.linalg.norm(out - ref) / torch.linalg.norm(ref)),
+            "fp64_direct_ms": e0.elapsed_time(e1), "speedup_vs_fp64_direct": e0.elapsed_time(e1) / med,
+            "near_kernel": {"ms": near_ms, "tflops": near_tf, "frac": near_tf / fp32_peak},
+            "far_kernel": {"ms": far_ms, "tflops": far_tf, "frac": far_tf / fp32_peak,
+                           "launches": prof.get("far_kernel", {}).get("launches")},
+            "peak_tflops_fp32": fp32_peak, "tree_stats": st}
+
+
 def run_gpu(args) -> None:
     import torch
     import torch.distributed as dist
@@ -466,6 +546,9 @@ def run_gpu(args) -> None:
         clk = clocks.stop()
         launches = ctx.launch_count - launches0
         total_ms = float(sum(step_ms))
+        # the state after the warm-up and timed steps, for the accuracy check at the final state
+        state_final = torch.empty_like(state0)
+        rk.get_state(state_final)
         if world > 1:
             t = torch.tensor([total_ms], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -490,7 +573,8 @@ def run_gpu(args) -> None:
         state_bytes = n * 4 * 8
 
         # ---- accuracy of the headline velocity against the FP64 direct sum at the initial state
-        # (one uncaptured evaluation, with per-kernel CUDA-event timing for the roofline)
+        # (one uncaptured evaluation, with per-kernel CUDA-event timing for the roofline) and at the state
+        # the timed steps reached
         rk.set_state(state0)
         u_head = torch.empty((3, n), dtype=torch.float64, device="cuda")
         ctx.set_profiling(True)
@@ -498,13 +582,20 @@ def run_gpu(args) -> None:
         prof = ctx.profile_report()
         ctx.set_profiling(False)
         tstats = rk.tree_stats() if head.startswith("tree") else None
+        rk.set_state(state_final)
+        u_head_final = torch.empty((3, n), dtype=torch.float64, device="cuda")
+        rk.velocity(u_head_final)
         rk.close()
 
-        # ---- FP64 GPU direct sum on the same workload (one RK4 step)
+        # ---- FP64 GPU direct sum on the same workload (one RK4 step), its velocity at the initial and the
+        # final state, and the FP64-pipe share of its kernel
         u64 = torch.empty((3, n), dtype=torch.float64, device="cuda")
+        u64_final = torch.empty((3, n), dtype=torch.float64, device="cuda")
         fp64_sps = None
         if head != "direct_f64":
             rk64 = L.RK4(ctx, kern, solver_desc("direct_f64"), n_src, n)
+            rk64.set_state(state_final)
+            rk64.velocity(u64_final)
             rk64.set_state(state0)
             rk64.velocity(u64)
             torch.cuda.synchronize()
@@ -518,11 +609,16 @@ def run_gpu(args) -> None:
             rk64.close()
         else:
             u64.copy_(u_head)
+            u64_final.copy_(u_head_final)
             fp64_sps = value / world
         rel_l2 = float(torch.linalg.norm(u_head - u64) / torch.linalg.norm(u64))
+        rel_l2_final = float(torch.linalg.norm(u_head_final - u64_final) / torch.linalg.norm(u64_final))
+        rel_linf = float((u_head - u64).abs().max() / u64.abs().max())
         fp32_peak = ctx.fma_peak_tflops(L.LPM_PREC_F32)
         fp64_peak = ctx.fma_peak_tflops(L.LPM_PREC_F64)
+        pairwise = None if args.no_extras else pairwise_direct_f32(ctx, kern, state0, n_src, fp32_peak, u64, stream)
     torch.cuda.synchronize()
+    poisson = None if (args.no_extras or world > 1) else poisson_summary(ctx, local)
 
     # dominant kernel of the headline step
     dom = max(prof.items(), key=lambda kv: kv[1]["ms"]) if prof else (None, None)
@@ -557,6 +653,11 @@ def run_gpu(args) -> None:
                    "l2": "flushed (256 MiB write) before every timed step, outside the timed events",
                    "graph": "one CUDA graph replay per RK4 step"},
         "rel_l2_vs_fp64_direct": rel_l2,
+        "rel_l2_t0": rel_l2,
+        "rel_l2_final": rel_l2_final,
+        "rel_linf_t0": rel_linf,
+        "accuracy_states": f"t0 = the initial state; final = after the {args.warmup} warm-up and {args.steps} timed "
+                           f"steps (dt {args.dt:g}); FP64 GPU direct sum at each",
         "fp64_direct_steps_per_s": fp64_sps,
         "speedup_vs_fp64_direct": (value / world) / fp64_sps if fp64_sps else None,
         "roofline": roof,
@@ -567,6 +668,8 @@ def run_gpu(args) -> None:
                 "d2h_bytes_per_step": state_bytes},
         "gpu_launches": launches,
         "clocks": clk,
+        "pairwise_direct_f32": pairwise,
+        "poisson_treecode": poisson,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(reps=2)
@@ -613,6 +716,8 @@ def main() -> None:
     ap.add_argument("--level", type=int, default=LEVEL)
     ap.add_argument("--dt", type=float, default=DT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the extra keys of the headline line (FP32 direct-sum kernel, Poisson treecode)")
     ap.add_argument("--workload", default="sphere_rk4", choices=["sphere_rk4", "poisson_cube", "ensemble"],
                     help="sphere_rk4: the Biot-Savart RK4 headline; poisson_cube: the 3D Poisson treecode; "
                          "ensemble: 64 uneven RK4 instances")

@@ -258,12 +258,25 @@ int lpm_treesum_stats(lpm_treesum* ts, int64_t* out10);
  * construction).  "theta": acceptance criterion, 0 < theta < 1; "f64_from": far expansions of this
  * order and above evaluate in FP64 (1..13; default 13 = all FP32 for LPM_PREC_F32 solvers, 1 for
  * LPM_PREC_F64); "batch_level": octree level whose cells a target batch may not straddle (1 .. the
- * level chosen at creation; coarser levels give fuller batches); "order_bias" (learned selector only): 0..3
- * orders added to every order the selector picks, capped at 11.  Takes effect at the next evaluation. */
+ * level chosen at creation; coarser levels give fuller batches); "order_bias" (LPM_ORDER_LEARNED solvers
+ * only, LPM_ERR_ARG otherwise; acts while selector weights are loaded): 0..3 orders added to every order the
+ * selector picks, capped at 11.
+ * The source octree's root box is the reference's Box3d(R) with its 1e-5 padding (src/LpmBox3d.h:21-33), so
+ * that its leaves are the reference TreeSum's (src/LpmTreeSum.cpp:221-238).  Biot-Savart: R = "root_maxr"
+ * when positive (default 0), else maxR (Coords::maxR, src/LpmCoords.cpp:136-143) of the targets from index
+ * "root_first" on (default 0; an RK4 integrator sets it to its first vertex particle, since the reference
+ * takes maxR of the mesh vertices), computed on the device at every evaluation, or of the sources when that
+ * range is empty.  Poisson: R = the largest |coordinate| of the sources.  Sources outside the box make the
+ * evaluation fail with LPM_ERR_ARG.  Parameters take effect at the next evaluation. */
 int lpm_treesum_set_param(lpm_treesum* ts, const char* name, double value);
 /* Current value of a run-time parameter: those of lpm_treesum_set_param, plus "batch_level_max" (the finest
  * batch level allowed) and "order" (the fixed order in the solver's convention: Poisson reports p + 1). */
 int lpm_treesum_get_param(const lpm_treesum* ts, const char* name, double* value);
+/* The source octree of the solver's last evaluation as a read-only lpm_tree (lpm_tree_counts,
+ * lpm_tree_leaf_membership and lpm_tree_nodes apply; member indices refer to the evaluation's source array):
+ * the tree TreeSum's constructor builds (src/LpmTreeSum.cpp:221-290), for checking it against the
+ * reference's.  Valid until the solver's next evaluation or destruction; lpm_tree_destroy frees the view. */
+int lpm_treesum_source_tree(lpm_treesum* ts, lpm_tree** out);
 
 /* ---- learned Taylor-order selection (no reference counterpart: the reference's TreeSum uses one
  * fixed order).  An MLP (8 -> 64 -> 64 -> 12, GELU) maps the features of an accepted (target batch,
@@ -325,9 +338,14 @@ int lpm_rk4_step(lpm_rk4* rk, double dt, int nsteps, int use_graph);
 int lpm_rk4_velocity_dev(lpm_rk4* rk, double* out);
 /* Treecode statistics of the last velocity evaluation (the 10 values of lpm_treesum_stats). */
 int lpm_rk4_tree_stats(lpm_rk4* rk, int64_t* out10);
-/* lpm_treesum_set_param for the integrator's treecode; drops a captured step graph (synchronises). */
+/* lpm_treesum_set_param for the integrator's treecode; drops a captured step graph (synchronises).  On an
+ * ensemble instance it also drops the ensemble's captured step, whose launches carry the old values. */
 int lpm_rk4_set_param(lpm_rk4* rk, const char* name, double value);
-/* lpm_treesum_set_mlp for the integrator's treecode; drops a captured step graph (synchronises). */
+int lpm_rk4_get_param(const lpm_rk4* rk, const char* name, double* value);
+/* lpm_treesum_source_tree for the integrator's treecode: the octree of its last velocity evaluation. */
+int lpm_rk4_source_tree(lpm_rk4* rk, lpm_tree** out);
+/* lpm_treesum_set_mlp for the integrator's treecode; drops a captured step graph (synchronises), and the
+ * owning ensemble's captured step for an ensemble instance. */
 int lpm_rk4_set_mlp(lpm_rk4* rk, const float* params);
 
 /* ---- ensembles (no reference counterpart): n_inst independent RK4 problems of uneven sizes advanced
@@ -342,6 +360,8 @@ int lpm_ensemble_destroy(lpm_ensemble* ens);
 int lpm_ensemble_instance(lpm_ensemble* ens, int i, lpm_rk4** rk);
 int lpm_ensemble_lane_of(const lpm_ensemble* ens, int i, int* lane);
 int lpm_ensemble_set_mlp(lpm_ensemble* ens, const float* params);
+/* lpm_rk4_set_param on every instance; drops the captured step (the next graph step first runs uncaptured). */
+int lpm_ensemble_set_param(lpm_ensemble* ens, const char* name, double value);
 int lpm_ensemble_step(lpm_ensemble* ens, double dt, int nsteps, int use_graph);
 
 #ifdef __cplusplus

@@ -258,6 +258,17 @@ class RK4:
     def set_param(self, name: str, value: float) -> None:
         check(lib().lpm_rk4_set_param(self.h, name.encode(), float(value)), "lpm_rk4_set_param")
 
+    def get_param(self, name: str) -> float:
+        v = C.c_double()
+        check(lib().lpm_rk4_get_param(self.h, name.encode(), C.byref(v)), "lpm_rk4_get_param")
+        return v.value
+
+    def source_tree(self) -> "Tree":
+        """The treecode's source octree of the last velocity evaluation (a read-only view)."""
+        h = C.c_void_p()
+        check(lib().lpm_rk4_source_tree(self.h, C.byref(h)), "lpm_rk4_source_tree")
+        return Tree._view(h)
+
     def set_mlp(self, params) -> None:
         p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
         check(lib().lpm_rk4_set_mlp(self.h, ptr(p)), "lpm_rk4_set_mlp")
@@ -314,6 +325,10 @@ class Ensemble:
         p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
         check(lib().lpm_ensemble_set_mlp(self.h, ptr(p)), "lpm_ensemble_set_mlp")
 
+    def set_param(self, name: str, value: float) -> None:
+        """lpm_ensemble_set_param: one run-time treecode parameter for every instance."""
+        check(lib().lpm_ensemble_set_param(self.h, name.encode(), float(value)), "lpm_ensemble_set_param")
+
     def step(self, dt: float, nsteps: int = 1, use_graph: bool = True) -> None:
         check(lib().lpm_ensemble_step(self.h, dt, nsteps, 1 if use_graph else 0), "lpm_ensemble_step")
 
@@ -332,6 +347,12 @@ class Tree:
                 self.h = None
             check(rc, "lpm_tree_build")
         self.overflow = rc == _capi.LPM_ERR_CAPACITY
+
+    @classmethod
+    def _view(cls, h) -> "Tree":
+        t = cls.__new__(cls)
+        t.h, t.overflow = h, False
+        return t
 
     def close(self):
         if self.h:
@@ -397,8 +418,15 @@ class TreeSum:
         return dict(zip(self.STAT_KEYS, (int(v) for v in o)))
 
     def set_param(self, name: str, value: float) -> None:
-        """Run-time parameter (lpm_treesum_set_param): "theta", "f64_from", "eps" or "batch_level"."""
+        """Run-time parameter (lpm_treesum_set_param): "theta", "f64_from", "eps", "batch_level",
+        "order_bias", "root_maxr" or "root_first"."""
         check(lib().lpm_treesum_set_param(self.h, name.encode(), float(value)), "lpm_treesum_set_param")
+
+    def source_tree(self) -> "Tree":
+        """The source octree of the last evaluation (a read-only view, valid until the next one)."""
+        h = C.c_void_p()
+        check(lib().lpm_treesum_source_tree(self.h, C.byref(h)), "lpm_treesum_source_tree")
+        return Tree._view(h)
 
     def get_param(self, name: str) -> float:
         """Current run-time parameter: as set_param, plus "batch_level_max" and "order"."""

@@ -103,6 +103,7 @@ SIGNATURES = {
     "lpm_treesum_stats": (C.c_int, [P, P]),
     "lpm_treesum_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
     "lpm_treesum_get_param": (C.c_int, [P, C.c_char_p, P]),
+    "lpm_treesum_source_tree": (C.c_int, [P, C.POINTER(P)]),
     "lpm_treesum_set_mlp": (C.c_int, [P, P]),
     "lpm_treesum_sample_labels": (C.c_int, [P, P, P, C.c_int64, C.c_int64, P, P, P, P]),
     "lpm_mlp_train": (C.c_int, [P, P, P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_uint64, P, P]),
@@ -120,12 +121,15 @@ SIGNATURES = {
     "lpm_rk4_velocity_dev": (C.c_int, [P, P]),
     "lpm_rk4_tree_stats": (C.c_int, [P, P]),
     "lpm_rk4_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
+    "lpm_rk4_get_param": (C.c_int, [P, C.c_char_p, P]),
+    "lpm_rk4_source_tree": (C.c_int, [P, C.POINTER(P)]),
     "lpm_rk4_set_mlp": (C.c_int, [P, P]),
     "lpm_ensemble_create": (C.c_int, [P, P, P, C.c_int, P, P, C.c_int, P]),
     "lpm_ensemble_destroy": (C.c_int, [P]),
     "lpm_ensemble_instance": (C.c_int, [P, C.c_int, P]),
     "lpm_ensemble_lane_of": (C.c_int, [P, C.c_int, P]),
     "lpm_ensemble_set_mlp": (C.c_int, [P, P]),
+    "lpm_ensemble_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
     "lpm_ensemble_step": (C.c_int, [P, C.c_double, C.c_int, C.c_int]),
 }
 

@@ -20,6 +20,9 @@ int rk4_step_enqueue(lpm_rk4* rk, double dt);
 lpm_ctx* rk4_context(lpm_rk4* rk);
 int rk4_tree_check(lpm_rk4* rk);
 int rk4_set_mlp_internal(lpm_rk4* rk, const float* params);
+int rk4_set_param_internal(lpm_rk4* rk, const char* name, double value);
+void rk4_set_owner(lpm_rk4* rk, lpm_ensemble* e);
+int ensemble_invalidate(lpm_ensemble* e);
 }  // namespace lpm
 
 using namespace lpm;
@@ -45,6 +48,19 @@ static void ens_drop_graph(lpm_ensemble* e) {
     e->graph = nullptr;
     e->graph_nodes = 0;
 }
+
+namespace lpm {
+// An instance's parameters or selector changed: the captured step holds launches with the old ones (and
+// lists sized for them), so drop it; the next graph step first runs uncaptured to resize the lists.
+int ensemble_invalidate(lpm_ensemble* e) {
+    LPM_CUDA_TRY(cudaSetDevice(e->ctx->device));
+    for (lpm_ctx* c : e->lanes) LPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    LPM_CUDA_TRY(cudaStreamSynchronize(e->ctx->own_stream));
+    ens_drop_graph(e);
+    e->warmed = false;
+    return LPM_OK;
+}
+}  // namespace lpm
 
 extern "C" int lpm_ensemble_destroy(lpm_ensemble* e) {
     if (!e) return LPM_OK;
@@ -110,6 +126,7 @@ extern "C" int lpm_ensemble_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, 
             lpm_ensemble_destroy(e);
             return rc;
         }
+        rk4_set_owner(e->inst[i], e);
     }
     *out = e;
     return LPM_OK;
@@ -139,12 +156,24 @@ extern "C" int lpm_ensemble_set_mlp(lpm_ensemble* e, const float* params) {
         set_error("lpm_ensemble_set_mlp: null ensemble");
         return LPM_ERR_ARG;
     }
-    LPM_CUDA_TRY(cudaSetDevice(e->ctx->device));
-    for (lpm_ctx* c : e->lanes) LPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    ens_drop_graph(e);
-    e->warmed = false;
+    int rc = ensemble_invalidate(e);
+    if (rc) return rc;
     for (lpm_rk4* r : e->inst) {
-        int rc = rk4_set_mlp_internal(r, params);
+        rc = rk4_set_mlp_internal(r, params);
+        if (rc) return rc;
+    }
+    return LPM_OK;
+}
+
+extern "C" int lpm_ensemble_set_param(lpm_ensemble* e, const char* name, double value) {
+    if (!e || !name) {
+        set_error("lpm_ensemble_set_param: null argument");
+        return LPM_ERR_ARG;
+    }
+    int rc = ensemble_invalidate(e);
+    if (rc) return rc;
+    for (lpm_rk4* r : e->inst) {
+        rc = rk4_set_param_internal(r, name, value);
         if (rc) return rc;
     }
     return LPM_OK;

@@ -216,6 +216,7 @@ __global__ void morton_keys_kernel(const double4* __restrict__ pts, int64_t n, R
                                    uint64_t* __restrict__ keys, int32_t* __restrict__ vals,
                                    int32_t* __restrict__ counters) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    root = resolve_root(root);
     bool in = false;
     if (i < n) {
         const double4 p = pts[i];
@@ -249,6 +250,25 @@ __global__ void morton_keys_kernel(const double4* __restrict__ pts, int64_t n, R
     if ((threadIdx.x & 31) == 0 && b) atomicAdd(&counters[0], __popc(b));
 }
 
+__global__ void root_extent_kernel(const double4* __restrict__ pts, int64_t first, int64_t n, int mode,
+                                   unsigned long long* __restrict__ r_dev) {
+    unsigned long long m = 0;  // non-negative doubles order like their bit patterns
+    for (int64_t i = first + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double4 p = pts[i];
+        const double v = mode == kRootMaxNorm ? fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z)))
+                                              : __dadd_rn(__dadd_rn(__dmul_rn(p.x, p.x), __dmul_rn(p.y, p.y)),
+                                                          __dmul_rn(p.z, p.z));
+        const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+        m = b > m ? b : m;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long u = __shfl_xor_sync(0xffffffffu, m, o);
+        m = u > m ? u : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(r_dev, m);
+}
+
 __device__ __forceinline__ int level_digit(uint64_t key, int level) {
     return (int)((key >> (3 * (kKeyLevels - level))) & 7ull);
 }
@@ -260,9 +280,10 @@ __global__ void tree_init_kernel(Octree t) {
     t.node_first_child[0] = -1;
     t.node_nchild[0] = 0;
     t.node_level[0] = 0;
+    const RootBox root = resolve_root(t.root);
     for (int a = 0; a < 3; ++a) {
-        t.node_box[2 * a] = t.root.lo[a];
-        t.node_box[2 * a + 1] = t.root.hi[a];
+        t.node_box[2 * a] = root.lo[a];
+        t.node_box[2 * a + 1] = root.hi[a];
     }
     t.level_range[0] = 0;
     t.level_range[1] = 1;
@@ -406,6 +427,14 @@ int morton_keys(lpm_ctx* ctx, const double4* pts, int64_t n, const RootBox& root
     if (n <= 0) return LPM_OK;
     LPM_LAUNCH(ctx, "morton_keys_kernel", morton_keys_kernel, grid_for(n, 256), 256, 0, pts, n, root, keys, vals,
                counter);
+    return LPM_OK;
+}
+
+int root_extent(lpm_ctx* ctx, const double4* pts, int64_t first, int64_t n, int mode, unsigned long long* r_dev) {
+    LPM_CUDA_TRY(cudaMemsetAsync(r_dev, 0, sizeof(unsigned long long), ctx->stream));
+    if (n <= first) return LPM_OK;
+    const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(n - first, 256), 2 * ctx->num_sms));
+    LPM_LAUNCH(ctx, "root_extent_kernel", root_extent_kernel, g, 256, 0, pts, first, n, mode, r_dev);
     return LPM_OK;
 }
 

@@ -19,9 +19,36 @@ int radix_sort_u64(lpm_ctx* ctx, uint64_t* keys, int32_t* vals, uint64_t* tmp_ke
 int radix_sort_u32(lpm_ctx* ctx, uint32_t* keys, int32_t* vals, uint32_t* tmp_keys, int32_t* tmp_vals, int64_t n,
                    int bits);
 
+// Root box of a build.  With r_dev set, the box is computed on the device when the build runs (so a
+// captured graph follows the points): r_dev holds the bit pattern of a non-negative double r (written by
+// root_extent) and the box is Box3d(R) with its padding, [-R - 1e-5, R + 1e-5]^3 (src/LpmBox3d.h:21-33),
+// R = sqrt(r) for kRootEuclid (Coords::maxR, src/LpmCoords.cpp:136-143) or R = r for kRootMaxNorm.
+constexpr int kRootEuclid = 0;
+constexpr int kRootMaxNorm = 1;
 struct RootBox {
     double lo[3], hi[3];
+    const unsigned long long* r_dev = nullptr;
+    int mode = kRootEuclid;
 };
+
+#ifdef __CUDACC__
+__device__ __forceinline__ RootBox resolve_root(const RootBox& r) {
+    if (!r.r_dev) return r;
+    RootBox b = r;
+    const double v = __longlong_as_double((long long)*r.r_dev);
+    const double R = r.mode == kRootMaxNorm ? v : sqrt(v);
+    for (int a = 0; a < 3; ++a) {
+        b.lo[a] = -R - 1e-5;
+        b.hi[a] = R + 1e-5;
+    }
+    b.r_dev = nullptr;
+    return b;
+}
+#endif
+
+// *r_dev = max over pts[first:n] of (x x + y y) + z z (rounded as Coords::maxR: no fused multiply-add) for
+// kRootEuclid, or of max(|x|, |y|, |z|) for kRootMaxNorm, as the bit pattern of the double.  Capturable.
+int root_extent(lpm_ctx* ctx, const double4* pts, int64_t first, int64_t n, int mode, unsigned long long* r_dev);
 
 // Octree over points (double4, xyz used).  All arrays device-resident; sizes are capacities.
 struct Octree {

@@ -36,9 +36,13 @@ struct lpm_rk4 {
     double graph_dt = 0.0;
     int64_t graph_nodes = 0;
     bool warmed = false;
+    lpm_ensemble* owner = nullptr;  // the ensemble whose captured step replays this instance, if any
 };
 
 namespace lpm {
+// Drops the owning ensemble's captured step (its launches hold this instance's parameters); ensemble.cu.
+int ensemble_invalidate(lpm_ensemble* e);
+
 namespace {
 
 __global__ void rk4_update_kernel(double4* __restrict__ X, double4* __restrict__ Xs, float4* __restrict__ Xs32,
@@ -111,6 +115,14 @@ static int rk4_one_step(lpm_rk4* rk, double dt) {
 int rk4_step_enqueue(lpm_rk4* rk, double dt) { return rk4_one_step(rk, dt); }
 lpm_ctx* rk4_context(lpm_rk4* rk) { return rk->ctx; }
 int rk4_tree_check(lpm_rk4* rk) { return rk->tree ? tree_check(rk->tree) : LPM_OK; }
+void rk4_set_owner(lpm_rk4* rk, lpm_ensemble* e) { rk->owner = e; }
+int rk4_set_param_internal(lpm_rk4* rk, const char* name, double value) {
+    if (!rk->tree) {
+        set_error("ensemble: the instances do not use the treecode");
+        return LPM_ERR_ARG;
+    }
+    return tree_set_param(rk->tree, name, value);
+}
 int rk4_set_mlp_internal(lpm_rk4* rk, const float* params) {
     if (!rk->tree) {
         set_error("ensemble: the instances do not use the treecode");
@@ -213,6 +225,9 @@ extern "C" int lpm_rk4_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const
     }
     if (solver->method == LPM_METHOD_TREE) {
         rc = tree_solver_create(ctx, *kernel, *solver, n_src, n_pts, &rk->tree);
+        // the source octree's root is Box3d(maxR) of the vertex particles, as TreeSum's mesh constructor
+        // (src/LpmTreeSum.cpp:221-238) takes maxR of the mesh vertices
+        if (!rc && n_pts > n_src) rc = tree_set_param(rk->tree, "root_first", (double)n_src);
         if (rc) {
             lpm_rk4_destroy(rk);
             return rc;
@@ -348,6 +363,10 @@ extern "C" int lpm_rk4_set_mlp(lpm_rk4* rk, const float* params) {
     }
     LPM_CUDA_TRY(cudaSetDevice(rk->ctx->device));
     LPM_CUDA_TRY(cudaStreamSynchronize(rk->ctx->stream));
+    if (rk->owner) {
+        int rc = ensemble_invalidate(rk->owner);
+        if (rc) return rc;
+    }
     drop_graph(rk);
     rk->warmed = false;  // the next graph step first runs uncaptured so the lists can resize
     return tree_set_mlp(rk->tree, params);
@@ -360,9 +379,32 @@ extern "C" int lpm_rk4_set_param(lpm_rk4* rk, const char* name, double value) {
     }
     LPM_CUDA_TRY(cudaSetDevice(rk->ctx->device));
     LPM_CUDA_TRY(cudaStreamSynchronize(rk->ctx->stream));
+    if (rk->owner) {
+        int rc = ensemble_invalidate(rk->owner);
+        if (rc) return rc;
+    }
     drop_graph(rk);
     rk->warmed = false;  // the next graph step first runs uncaptured so the lists can resize
     return tree_set_param(rk->tree, name, value);
+}
+
+extern "C" int lpm_rk4_get_param(const lpm_rk4* rk, const char* name, double* value) {
+    if (!rk || !rk->tree) {
+        set_error("lpm_rk4_get_param: the integrator does not use the treecode");
+        return LPM_ERR_ARG;
+    }
+    return tree_get_param(rk->tree, name, value);
+}
+
+extern "C" int lpm_rk4_source_tree(lpm_rk4* rk, lpm_tree** out) {
+    if (!rk || !out || !rk->tree) {
+        set_error("lpm_rk4_source_tree: null argument, or the integrator does not use the treecode");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(rk->ctx->device));
+    int64_t n = 0;
+    const Octree& t = tree_source_octree(rk->tree, &n);
+    return tree_view_create(rk->ctx, t, n, out);
 }
 
 extern "C" int lpm_rk4_velocity_dev(lpm_rk4* rk, double* out) {

@@ -3,6 +3,7 @@
 // the coordsContained index lists of its leaves, depth first, each in increasing point index
 // (src/LpmTreeSum.cpp:266-290 keeps the parent's order when filtering into children).
 #include "octree.h"
+#include "treecode.h"
 
 #include <algorithm>
 #include <new>
@@ -14,6 +15,7 @@ struct lpm_tree {
     lpm::Octree t;
     int64_t n = 0, n_valid = 0, n_nodes = 0, n_leaves = 0;
     int depth = 0, flags = 0;
+    bool view = false;  // the octree belongs to a tree solver (lpm_treesum_source_tree / lpm_rk4_source_tree)
 };
 
 namespace lpm {
@@ -33,6 +35,8 @@ __global__ void leaf_of_point_kernel(const int32_t* __restrict__ perm, const int
 }  // namespace lpm
 
 using namespace lpm;
+
+static int read_counts(lpm_tree* tr);
 
 extern "C" int lpm_tree_build(lpm_ctx* ctx, const double* pts, int64_t n, const double* box, int max_per_leaf,
                               int max_depth, lpm_tree** out) {
@@ -62,14 +66,47 @@ extern "C" int lpm_tree_build(lpm_ctx* ctx, const double* pts, int64_t n, const 
         delete tr;
         return rc;
     }
+    rc = read_counts(tr);
+    if (rc) {
+        octree_free(tr->t);
+        delete tr;
+        return rc;
+    }
+    *out = tr;
+    if (tr->flags) {
+        set_error("lpm_tree_build: %s", (tr->flags & 2) ? "node capacity exhausted"
+                                                         : "a leaf at the depth limit exceeds max_per_leaf");
+        return LPM_ERR_CAPACITY;
+    }
+    return LPM_OK;
+}
+
+namespace lpm {
+int tree_view_create(lpm_ctx* ctx, const Octree& t, int64_t n, lpm_tree** out) {
+    *out = nullptr;
+    lpm_tree* tr = new (std::nothrow) lpm_tree();
+    if (!tr) return LPM_ERR_OOM;
+    tr->ctx = ctx;
+    tr->n = n;
+    tr->t = t;
+    tr->view = true;
+    int rc = read_counts(tr);
+    if (rc) {
+        delete tr;
+        return rc;
+    }
+    *out = tr;
+    return LPM_OK;
+}
+}  // namespace lpm
+
+static int read_counts(lpm_tree* tr) {
+    lpm_ctx* ctx = tr->ctx;
+    const int64_t n = tr->n;
     int32_t c[8];
     cudaError_t e = cudaMemcpyAsync(c, tr->t.counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) {
-        octree_free(tr->t);
-        delete tr;
-        return cuda_status(e, "lpm_tree_build");
-    }
+    if (e != cudaSuccess) return cuda_status(e, "lpm_tree counts");
     tr->n_valid = c[0];
     tr->n_nodes = c[1];
     tr->flags = c[2];
@@ -80,12 +117,6 @@ extern "C" int lpm_tree_build(lpm_ctx* ctx, const double* pts, int64_t n, const 
     if (tr->n_nodes == 1) {
         tr->n_valid = n;
         tr->n_leaves = n > 0 ? 1 : tr->n_leaves;
-    }
-    *out = tr;
-    if (tr->flags) {
-        set_error("lpm_tree_build: %s", (tr->flags & 2) ? "node capacity exhausted"
-                                                         : "a leaf at the depth limit exceeds max_per_leaf");
-        return LPM_ERR_CAPACITY;
     }
     return LPM_OK;
 }
@@ -110,7 +141,7 @@ extern "C" int lpm_tree_destroy(lpm_tree* tr) {
     if (!tr) return LPM_OK;
     cudaSetDevice(tr->ctx->device);
     cudaStreamSynchronize(tr->ctx->stream);
-    octree_free(tr->t);
+    if (!tr->view) octree_free(tr->t);
     delete tr;
     return LPM_OK;
 }

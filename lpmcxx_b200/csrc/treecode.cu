@@ -1709,6 +1709,14 @@ struct TreeSolver {
     float* A32 = nullptr;
     int f64_from = kF64From;  // far expansions of order >= f64_from evaluate in FP64
     int heavy_cap = 0;        // nodes the moment / coefficient / feature arrays hold (grown on demand)
+    // root box of the source octree: Box3d(R) padded by 1e-5 (src/LpmBox3d.h:21-33).  Biot-Savart: R is
+    // root_maxr when positive, else maxR (src/LpmCoords.cpp:136-143) of targets[root_first:n_tgt] computed on
+    // the device (TreeSum's mesh constructor takes maxR of the mesh vertices, src/LpmTreeSum.cpp:227; the RK4
+    // integrator points root_first at its vertex particles), or of the sources when that range is empty.
+    // Poisson: R is the largest |coordinate| of the sources (the smallest such cube holding them).
+    double root_maxr = 0.0;
+    int64_t root_first = 0;
+    unsigned long long* root_r = nullptr;
     Octree st;
     // target ordering
     uint64_t* tkeys = nullptr;
@@ -1967,6 +1975,7 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->far_off, far_rows));
     A(talloc(t, &t->near_off, (size_t)t->n_batches + 1));
     A(talloc(t, &t->flags, 8));
+    A(talloc(t, &t->root_r, 1));
     A(talloc(t, &t->pair_counts, 3));
     A(talloc(t, &t->V, 3 * ntg));
     if (t->learned) {
@@ -2087,14 +2096,23 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
         return LPM_OK;
     }
     LPM_CUDA_TRY(cudaMemsetAsync(t->flags, 0, 8 * sizeof(int32_t), ctx->stream));
-    // unit-sphere particles: a fixed root box |x| <= 1 (+1e-12), padded like Box3d(maxR)
-    const double maxr = 1.0 + 1e-12;
     RootBox rb;
-    for (int a = 0; a < 3; ++a) {
-        rb.lo[a] = -maxr - 1e-5;
-        rb.hi[a] = maxr + 1e-5;
+    int rc = LPM_OK;
+    if (!t->scalar && t->root_maxr > 0.0) {
+        for (int a = 0; a < 3; ++a) {
+            rb.lo[a] = -t->root_maxr - 1e-5;
+            rb.hi[a] = t->root_maxr + 1e-5;
+        }
+    } else {
+        rb.r_dev = t->root_r;
+        rb.mode = t->scalar ? kRootMaxNorm : kRootEuclid;
+        if (!t->scalar && t->root_first < n_tgt)
+            rc = root_extent(ctx, X, t->root_first, n_tgt, kRootEuclid, t->root_r);
+        else
+            rc = root_extent(ctx, src, 0, n_src, rb.mode, t->root_r);
+        if (rc) return rc;
     }
-    int rc = octree_build(ctx, t->st, src, n_src, rb);
+    rc = octree_build(ctx, t->st, src, n_src, rb);
     if (rc) return rc;
     if (can_sync) {  // grow the per-node arrays to this tree (a captured replay can only flag an overflow)
         int32_t nodes = 0;
@@ -2212,11 +2230,16 @@ int tree_check(TreeSolver* t) {
         return LPM_ERR_CAPACITY;
     }
     if (c[0] != t->n_src) {
-        set_error("tree solver: %d of %lld sources lie outside the unit-sphere root box", (int)(t->n_src - c[0]),
-                  (long long)t->n_src);
+        set_error("tree solver: %d of %lld sources lie outside the root box (non-finite coordinates, or sources "
+                  "beyond the targets' maxR)", (int)(t->n_src - c[0]), (long long)t->n_src);
         return LPM_ERR_ARG;
     }
     return LPM_OK;
+}
+
+const Octree& tree_source_octree(const TreeSolver* t, int64_t* n_points) {
+    *n_points = t->n_src;
+    return t->st;
 }
 
 int tree_stats(TreeSolver* t, int64_t* out8) {
@@ -2258,6 +2281,8 @@ int tree_get_param(const TreeSolver* t, const char* name, double* value) {
     else if (n == "order_bias") *value = t->order_bias;
     else if (n == "batch_level") *value = t->batch_level;
     else if (n == "batch_level_max") *value = t->batch_level_max;
+    else if (n == "root_maxr") *value = t->root_maxr;
+    else if (n == "root_first") *value = (double)t->root_first;
     else if (n == "order") *value = t->order;
     else {
         set_error("tree_get_param: unknown parameter %s", name);
@@ -2277,7 +2302,15 @@ int tree_set_param(TreeSolver* t, const char* name, double value) {
     } else if (n == "eps" && value > 0.0) {
         t->eps = value;
     } else if (n == "order_bias" && value >= 0.0 && value <= 3.0 && value == std::floor(value)) {
+        if (!t->learned) {
+            set_error("tree_set_param: order_bias applies to LPM_ORDER_LEARNED solvers only");
+            return LPM_ERR_ARG;
+        }
         t->order_bias = (int)value;
+    } else if (n == "root_maxr" && value >= 0.0 && std::isfinite(value)) {
+        t->root_maxr = value;
+    } else if (n == "root_first" && value >= 0.0 && value <= (double)t->n_tgt && value == std::floor(value)) {
+        t->root_first = (int64_t)value;
     } else if (n == "batch_level" && value >= 1.0 && value <= t->batch_level_max && value == std::floor(value)) {
         t->batch_level = (int)value;
     } else if (n == "f64_from" && value >= 1.0 && value <= kPMax + 1 && value == std::floor(value)) {

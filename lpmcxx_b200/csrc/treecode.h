@@ -2,10 +2,16 @@
 #pragma once
 
 #include "lpm_internal.h"
+#include "octree.h"
 
 namespace lpm {
 
 struct TreeSolver;
+
+// The source octree of the solver's last evaluation (valid until the next one) and its point count.
+const Octree& tree_source_octree(const TreeSolver* t, int64_t* n_points);
+// A read-only lpm_tree over an octree owned elsewhere (lpm_tree_destroy frees the view only).
+int tree_view_create(lpm_ctx* ctx, const Octree& t, int64_t n, lpm_tree** out);
 
 int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_solver_desc& solver, int64_t n_src,
                        int64_t n_tgt, TreeSolver** out);
@@ -21,8 +27,9 @@ int tree_check(TreeSolver* t);
 // evaluations of the order's coefficient count) (10 values; synchronises)
 int tree_stats(TreeSolver* t, int64_t* out10);
 // Run-time parameters: "theta" (0 < theta < 1, acceptance criterion), "f64_from" (1..kPMax+1: far
-// expansions of this order and above evaluate in FP64), "eps" (learned order's per-pair budget), "batch_level" (octree level whose cells target
-// batches may not straddle; 1 .. the level chosen at creation).
+// expansions of this order and above evaluate in FP64), "eps" (learned order's per-pair budget), "batch_level"
+// (octree level whose cells target batches may not straddle; 1 .. the level chosen at creation), "order_bias"
+// (learned solvers only), "root_maxr" / "root_first" (the root box of the source octree, see TreeSolver).
 int tree_set_param(TreeSolver* t, const char* name, double value);
 // Current value of a run-time parameter (as tree_set_param, plus "batch_level_max" and "order").
 int tree_get_param(const TreeSolver* t, const char* name, double* value);

@@ -3,6 +3,7 @@
 #include "treecode.h"
 
 #include <algorithm>
+#include <cmath>
 #include <new>
 
 struct lpm_treesum {
@@ -101,6 +102,17 @@ extern "C" int lpm_treesum_sample_labels(lpm_treesum* ts, const double* src, con
                               errs, n_out);
 }
 
+extern "C" int lpm_treesum_source_tree(lpm_treesum* ts, lpm_tree** out) {
+    if (!ts || !out) {
+        set_error("lpm_treesum_source_tree: null argument");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaSetDevice(ts->ctx->device));
+    int64_t n = 0;
+    const Octree& t = tree_source_octree(ts->solver, &n);
+    return tree_view_create(ts->ctx, t, n, out);
+}
+
 extern "C" int lpm_treesum_get_param(const lpm_treesum* ts, const char* name, double* value) {
     if (!ts) {
         set_error("lpm_treesum_get_param: null solver");
@@ -169,6 +181,23 @@ extern "C" int lpm_tree_sum_mesh(lpm_ctx* ctx, const lpm_kernel_desc* kernel, co
     lpm::TreeSolver* ts = nullptr;
     rc = tree_solver_create(ctx, *kernel, *solver, n_src, n_tgt, &ts);
     if (rc) return rc;
+    {
+        // root box Box3d(maxR) over every mesh vertex, as TreeSum's mesh constructor (src/LpmTreeSum.cpp:227,
+        // Coords::maxR at src/LpmCoords.cpp:136-143: (x x + y y) + z z, largest, then the square root)
+        double r2 = 0.0;
+        for (int64_t i = 0; i < n_verts; ++i) {
+            const double xx = vx[i] * vx[i];
+            const double yy = vy[i] * vy[i];
+            const double zz = vz[i] * vz[i];
+            const double t2 = (xx + yy) + zz;
+            if (t2 > r2) r2 = t2;
+        }
+        if (n_verts > 0) rc = tree_set_param(ts, "root_maxr", std::sqrt(r2));
+        if (rc) {
+            tree_solver_destroy(ts);
+            return rc;
+        }
+    }
     cudaError_t e = cudaSuccess;
     if (n_src > 0)
         e = cudaMemcpyAsync(dsrc, hsrc, sizeof(double4) * (size_t)n_src, cudaMemcpyHostToDevice, ctx->stream);

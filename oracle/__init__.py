@@ -113,6 +113,22 @@ def tree_build(pts4: np.ndarray, box, max_per_leaf: int, max_depth: int = 21) ->
             "node_parent": par[:k], "node_count": cnt[:k], "node_box": nbox[:k], "flags": flags}
 
 
+def leaf_hashes(members: np.ndarray, leaf_offsets: np.ndarray) -> np.ndarray:
+    """Per-leaf digest of an ordered member list: sum over the leaf's k-th member m of
+    splitmix64(m) * (2k + 1) mod 2^64 (test infrastructure: lets a fixture hold a large tree's leaf
+    membership in 8 bytes per leaf)."""
+    m = np.asarray(members, dtype=np.uint64)
+    off = np.asarray(leaf_offsets, dtype=np.int64)
+    with np.errstate(over="ignore"):
+        z = m + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+        pos = np.arange(m.size, dtype=np.int64) - np.repeat(off[:-1], np.diff(off))
+        z = z * (2 * pos.astype(np.uint64) + np.uint64(1))
+        return np.add.reduceat(z, off[:-1]) if m.size else np.zeros(0, np.uint64)
+
+
 def mesh_root_box(vert_xyz: np.ndarray) -> np.ndarray:
     """Box3d(maxR) with its 1e-5 padding (src/LpmBox3d.h:21-33), maxR over the vertices
     (Coords::maxR, src/LpmCoords.cpp:136-143) -- the root of TreeSum's mesh constructor."""

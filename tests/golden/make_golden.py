@@ -17,11 +17,14 @@ Fixtures
   scalar_icos3_harm.npz      DirectSum::meshSolve, scalar branch, with the reference's SphereGreensFn(1),
                              PlanarGreensFnFreeBoundaries, SecondOrderDelta3d(0.1) and SphereDelta(0.1);
                              icos level 3, zeta = sphereHarmonic54
+  tree_icos8_m512.npz        TreeSum's mesh constructor at the treecode's full size (icos level 8, 512 per
+                             leaf): node levels, parents, counts, boxes, leaf offsets and a digest of each
+                             leaf's members (oracle.leaf_hashes) instead of the 1.3M member indices
   vtk_icos2_rh.npz,          MeshedParticles::writeToVtkFile (non-Lagrangian icos level 2 / Lagrangian cube
   vtk_cube2_gauss_lag.npz    level 2) with vorticity and DirectSum velocity fields, and
                              VtkWriter::writePointsAndFieldsToCSV of the vertices: the files' bytes and the
                              field values written
-`python make_golden.py scalar vtk` remakes only the named groups.
+`python make_golden.py scalar vtk tree8` remakes only the named groups.
 """
 from __future__ import annotations
 
@@ -72,14 +75,26 @@ def vtk_fixtures() -> None:
         np.savez_compressed(HERE / f"{name}.npz", **z)
 
 
+def tree8_fixture() -> None:
+    d = harness("tree", "icos", 8, 512)
+    z = load(d, "node_level", "node_parent", "node_nkids", "node_ncoords", "node_box", "leaf_offsets",
+             "leaf_members", "maxr")
+    np.savez_compressed(HERE / "tree_icos8_m512.npz", maxr=z["maxr"], node_level=z["node_level"].astype(np.int8),
+                        node_parent=z["node_parent"].astype(np.int32), node_nkids=z["node_nkids"].astype(np.int8),
+                        node_ncoords=z["node_ncoords"].astype(np.int32), node_box=z["node_box"][:, :6],
+                        leaf_offsets=z["leaf_offsets"].astype(np.int32),
+                        leaf_hash=oracle.leaf_hashes(z["leaf_members"], z["leaf_offsets"]))
+
+
 def main() -> None:
-    groups = {"scalar": scalar_fixture, "vtk": vtk_fixtures}
+    groups = {"scalar": scalar_fixture, "vtk": vtk_fixtures, "tree8": tree8_fixture}
     if sys.argv[1:]:
         for g in sys.argv[1:]:
             groups[g]()
         return
     scalar_fixture()
     vtk_fixtures()
+    tree8_fixture()
     for kind in ("icos", "cube"):
         d = harness("mesh", kind, 3)
         np.savez_compressed(HERE / f"mesh_{kind}3.npz",

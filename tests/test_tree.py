@@ -102,3 +102,69 @@ def test_gpu_tree_duplicate_points_hit_depth_limit(ctx):
     assert tree.counts()["depth"] == 6
     with pytest.raises(L.LpmError):
         L.Tree(ctx, torch.tensor(pts, device="cuda"), [-1, 1, -1, 1, -1, 1], 4, max_depth=6)
+
+
+def check_against_digest(g, members, offsets, nodes, to_ref_index):
+    """Large trees: the fixture holds per-leaf digests of the member lists (oracle.leaf_hashes)."""
+    assert np.array_equal(offsets, g["leaf_offsets"])
+    assert np.array_equal(oracle.leaf_hashes(to_ref_index(members), offsets), g["leaf_hash"])
+    assert np.array_equal(nodes["node_level"], g["node_level"])
+    assert np.array_equal(nodes["node_parent"], g["node_parent"])
+    assert np.array_equal(nodes["node_count"], g["node_ncoords"])
+    assert np.array_equal(nodes["node_box"], g["node_box"])
+
+
+def test_oracle_tree_icos8_m512_matches_reference():
+    # the treecode's full-size configuration: 1,310,720 leaf faces, 512 per leaf
+    g = golden("tree_icos8_m512.npz")
+    m, leaf_faces, pts = mesh_points("icos", 8)
+    box = oracle.mesh_root_box(m.vert_xyz)
+    assert box[1] == g["maxr"][0] + 1e-5
+    t = oracle.tree_build(pts, box, 512)
+    assert t["flags"] == 0
+    check_against_digest(g, t["members"], t["leaf_offsets"], t, lambda idx: leaf_faces[idx])
+
+
+@pytest.mark.gpu
+def test_gpu_treecode_source_tree_is_reference_tree_icos8(ctx):
+    """The octree the treecode builds inside its RK4 step (root Box3d(maxR) of the vertex particles,
+    computed on the device) has the reference TreeSum's leaves at icos L8 / 512 per leaf."""
+    import lpmcxx_b200.workloads as W
+
+    torch = ctx.use_torch_stream()
+    g = golden("tree_icos8_m512.npz")
+    mesh, p, n_src = W.gaussian_vortex_mesh("icos", 8)
+    leaf_faces = np.nonzero(mesh.leaf)[0]
+    assert n_src == leaf_faces.size
+    rk = L.RK4(ctx, L.biot_savart_kernel(), L.tree_solver(L.LPM_PREC_F32, 8, 512, 0.7), n_src, p.shape[0])
+    assert rk.get_param("root_first") == n_src
+    rk.set_state(torch.tensor(p, device="cuda"))
+    u = torch.empty((3, p.shape[0]), dtype=torch.float64, device="cuda")
+    rk.velocity(u)
+    tree = rk.source_tree()
+    members, offsets = tree.leaf_membership()
+    assert tree.counts()["n_in_tree"] == n_src
+    check_against_digest(g, members, offsets, tree.nodes(), lambda idx: leaf_faces[idx])
+    tree.close()
+    rk.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,level,max_leaf", MESH_TREES)
+def test_gpu_treesum_source_tree_matches_reference(ctx, kind, level, max_leaf):
+    """A TreeSum evaluation over the mesh (targets: leaf faces, then vertices) with the root taken from
+    the vertex targets builds the reference's tree."""
+    torch = ctx.use_torch_stream()
+    g = golden(f"tree_{kind}{level}_m{max_leaf}.npz")
+    m, leaf_faces, pts = mesh_points(kind, level)
+    tgt = np.concatenate([pts, oracle.pack4(m.vert_xyz)])
+    ts = L.TreeSum(ctx, L.biot_savart_kernel(), L.tree_solver(L.LPM_PREC_F32, 6, max_leaf, 0.5), pts.shape[0],
+                   tgt.shape[0])
+    ts.set_param("root_first", pts.shape[0])
+    out = torch.empty((3, tgt.shape[0]), dtype=torch.float64, device="cuda")
+    ts.eval(torch.tensor(pts, device="cuda"), torch.tensor(tgt, device="cuda"), out)
+    tree = ts.source_tree()
+    members, offsets = tree.leaf_membership()
+    check_against_reference(g, members, offsets, tree.nodes(), lambda idx: leaf_faces[idx])
+    tree.close()
+    ts.close()
