@@ -221,3 +221,8 @@ def test_order_bias_raises_orders_and_accuracy(ctx):
         ts.close()
     assert res[2][1] > res[0][1]
     assert res[2][0] < res[0][0]
+    # the bias belongs to the learned selector: a fixed-order solver refuses it
+    fixed = L.TreeSum(ctx, L.biot_savart_kernel(), L.tree_solver(L.LPM_PREC_F32, 10, 256, 0.5), n_src, n)
+    with pytest.raises(L.LpmError):
+        fixed.set_param("order_bias", 1)
+    fixed.close()
