@@ -148,6 +148,42 @@ def time_reference_direct(reps: int, procs: int, targets_per_proc: int = 3) -> d
             "targets_per_rep": sum(r["vert_targets"] + r["face_targets"] for r in results), "procs": procs}
 
 
+def time_reference_poisson(reps: int, procs: int, n: int, targets_per_proc: int = 4) -> dict:
+    """The reference's DirectSum::meshfreeSolve with the 1/(4 pi r) kernel on the n-point cube: `procs`
+    processes each timing a MPIReplicatedData slice of ~targets_per_proc targets, `reps` times."""
+    exe = reference_harness()
+    size = max(procs, n // targets_per_proc)
+    jobs = []
+    for r in range(procs):
+        e = dict(os.environ, LPM_STUB_RANK=str(r), LPM_STUB_SIZE=str(size))
+        jobs.append(subprocess.Popen([str(exe), "time_poisson", str(n), "0x2B", str(reps)], stdout=subprocess.PIPE,
+                                     stderr=subprocess.DEVNULL, text=True, env=e))
+    results = []
+    for j in jobs:
+        out, _ = j.communicate()
+        line = [ln for ln in out.splitlines() if ln.startswith('{"cmd"')]
+        if j.returncode != 0 or not line:
+            raise RuntimeError("reference harness failed")
+        results.append(json.loads(line[-1]))
+    pairs = sum(r["targets"] * r["sources"] for r in results)
+    rep_s = [max(r["seconds"][k] for r in results) for k in range(reps)]
+    return {"rep_seconds": rep_s, "pairs_per_rep": pairs, "targets_per_rep": sum(r["targets"] for r in results)}
+
+
+def poisson_cpu_baseline(n: int, reps: int = 2) -> dict | None:
+    """evaluations/s of the reference's own FP64 meshfree direct sum on the host cores (bounded target
+    slice, extrapolated to all n targets); None without the reference build."""
+    if reference_harness() is None:
+        return None
+    procs = max(1, min(os.cpu_count() or 1, 32))
+    r = time_reference_poisson(reps, procs, n)
+    pps = float(np.median([r["pairs_per_rep"] / t for t in r["rep_seconds"]]))
+    return {"value": pps / (float(n) * float(n)), "unit": "evaluations/s", "cores": procs, "kind": "reference",
+            "sample": f"reference DirectSum::meshfreeSolve (FP64, 1/(4 pi r) ScalarKernel), {procs} processes x "
+                      f"MPIReplicatedData slice, {r['targets_per_rep']} targets x {n} sources per repetition, "
+                      f"extrapolated to {n} targets", "pairs_per_s": pps}
+
+
 def time_oracle_port(reps: int, threads: int, n_targets: int = 64) -> dict:
     """The oracle's C restatement of the same FP64 direct sum on a slice of n_targets targets."""
     import oracle
@@ -346,15 +382,66 @@ def run_gpu_poisson(args) -> None:
                 "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 8},
         "gpu_launches": launches, "clocks": clk,
     }
+    if roof is not None:
+        roof["traffic"] = profile_summary_traffic(f"poisson_{name}")
+    if env_int("RANK", 0) == 0 and world == 1 and not args.no_cpu_baseline:
+        out_line["cpu_baseline"] = poisson_cpu_baseline(n)
     print(json.dumps(out_line))
 
 
 ENSEMBLE_METRIC = "ensemble RK4 steps/s: 64 instances (icos L5/L6/L7/L8 x 16, 27.85M sources), learned treecode"
+ENSEMBLE_TUNE_GRID = ((128, 256, 512), (0.5, 0.6), (2e-7, 5e-7))  # leaf sizes, theta, learned budgets
+
+
+def ensemble_tune(ctx, kern, inst, tol: float = 1e-6) -> dict:
+    """Per size class (icos level): the autotuner on the class's first instance (learned selector, order bias
+    2, leaf x theta x budget x batch level), judged on 4096 sampled targets against the FP64 direct sum."""
+    import torch
+
+    from lpmcxx_b200.autotune import autotune
+
+    tuned = {}
+    for level in sorted({lvl for lvl, _, _ in inst}):
+        _, p, n_src = next(x for x in inst if x[0] == level)
+        d = torch.tensor(p, device="cuda")
+        res = autotune(ctx, kern, d[:n_src], d, tol=tol, learned=True, grid=ENSEMBLE_TUNE_GRID,
+                       batch_levels=(0, -1), order_biases=(2,), sample=4096, reps=2)
+        if res.best is None:
+            raise RuntimeError(f"ensemble tuning: no candidate meets {tol} at icos L{level}")
+        tuned[level] = res.as_dict()
+        tuned[level]["candidates"] = len(res.tried)
+    return tuned
+
+
+def ensemble_accuracy(ctx, kern, ens, inst, sample: int = 4096, seed: int = 11) -> list:
+    """Relative L2 velocity error of every instance's treecode against the FP64 direct sum, on `sample`
+    seeded targets of its current state."""
+    import torch
+
+    import lpmcxx_b200 as L
+
+    errs = []
+    rng = np.random.default_rng(seed)
+    for i, (_, p, n_src) in enumerate(inst):
+        rk = ens.instance(i)
+        state = torch.empty((p.shape[0], 4), dtype=torch.float64, device="cuda")
+        rk.get_state(state)
+        u = torch.empty((3, p.shape[0]), dtype=torch.float64, device="cuda")
+        rk.velocity(u)
+        torch.cuda.synchronize()
+        idx = torch.as_tensor(np.sort(rng.choice(p.shape[0], size=min(sample, p.shape[0]), replace=False)),
+                              device="cuda")
+        ref = torch.empty((3, idx.numel()), dtype=torch.float64, device="cuda")
+        ctx.direct_sum_dev(kern, L.LPM_PREC_F64, state[:n_src], state[idx].contiguous(), ref)
+        torch.cuda.synchronize()
+        errs.append(float(torch.linalg.norm(u[:, idx] - ref) / torch.linalg.norm(ref)))
+    return errs
 
 
 def run_gpu_ensemble(args) -> None:
-    """The ensemble configuration: 64 Biot-Savart RK4 instances of uneven sizes; a step advances every
-    instance by one RK4 step (one replay of the ensemble's graph)."""
+    """The ensemble configuration: 64 Biot-Savart RK4 instances of uneven sizes (icos L5..L8), each with the
+    solver settings the autotuner picked for its size class; a step advances every instance by one RK4 step
+    (one replay of the ensemble's graph)."""
     import torch
 
     import lpmcxx_b200 as L
@@ -363,17 +450,23 @@ def run_gpu_ensemble(args) -> None:
 
     local = env_int("LOCAL_RANK", 0)
     world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
     torch.cuda.set_device(local)
     inst = W.ensemble_instances()
     ctx = L.Context(local)
-    p_, theta, leaf = TREE_SETTINGS["tree_learned"]
-    solver = L.tree_solver(L.LPM_PREC_F32, p_, leaf, theta, learned=True, tolerance=LEARNED_EPS)
-    ens = L.Ensemble(ctx, L.biot_savart_kernel(), solver, [n for _, _, n in inst], [p.shape[0] for _, p, _ in inst],
-                     lanes=args.lanes)
+    kern = L.biot_savart_kernel()
+    ctx.use_torch_stream()
+    tuned = ensemble_tune(ctx, kern, inst)
+    solvers = [L.tree_solver(L.LPM_PREC_F32, 10, tuned[lvl]["max_per_leaf"], tuned[lvl]["theta"], learned=True,
+                             tolerance=tuned[lvl]["eps"]) for lvl, _, _ in inst]
+    ens = L.Ensemble(ctx, kern, solvers, [n for _, _, n in inst], [p.shape[0] for _, p, _ in inst], lanes=args.lanes)
     ens.set_mlp(learned.load()[0])
-    for i, (_, p, _) in enumerate(inst):
-        ens.instance(i).set_param("order_bias", LEARNED_ORDER_BIAS)
-        ens.instance(i).set_state(p)
+    for i, (lvl, p, _) in enumerate(inst):
+        rk = ens.instance(i)
+        rk.set_param("order_bias", tuned[lvl]["order_bias"])
+        rk.set_param("batch_level", tuned[lvl]["batch_level"])
+        rk.set_state(p)
+    err_t0 = ensemble_accuracy(ctx, kern, ens, inst)
     dt = 0.01
     ens.step(dt, args.warmup, use_graph=True)
     torch.cuda.synchronize()
@@ -394,18 +487,58 @@ def run_gpu_ensemble(args) -> None:
     clk = clocks.stop()
     launches = ctx.launch_count - launches0
     value = world * args.steps / (sum(ms) * 1e-3)
+    err_final = ensemble_accuracy(ctx, kern, ens, inst)
+    # work of one step: four evaluations per instance, each as its last one (tree statistics)
+    work = 0.0
+    for i in range(len(inst)):
+        st = ens.instance(i).tree_stats()
+        work += 4.0 * (FLOPS_PER_BS_PAIR * st["near_pairs"] + 8.0 * st["far_terms"] + 40.0 * st["far_evals"])
+    fp32_peak = ctx.fma_peak_tflops(L.LPM_PREC_F32)
+    achieved = work / (float(np.mean(ms)) * 1e-3) * 1e-12
+    # end to end: every instance's state from pinned host memory, one step, every state back
+    host = [torch.tensor(p).pin_memory() for _, p, _ in inst]
+    back = [torch.empty_like(h).pin_memory() for h in host]
+    e2e_s = []
+    for _ in range(max(1, min(args.steps, 5))):
+        t0 = time.perf_counter()
+        for i, h in enumerate(host):
+            ens.instance(i).set_state(h)
+        ens.step(dt, 1, use_graph=True)
+        for i, b in enumerate(back):
+            ens.instance(i).get_state(b)
+        e2e_s.append(time.perf_counter() - t0)
+    state_bytes = int(sum(p.shape[0] for _, p, _ in inst)) * 32
     n_total = int(sum(p.shape[0] for _, p, _ in inst))
+    pairs_step = float(sum(4.0 * p.shape[0] * n for _, p, n in inst))
     out = {
         "metric": ENSEMBLE_METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": float(np.mean(ms)), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": f"64 instances: icos L5/L6/L7/L8 x 16, RH m=4 + seeded Gaussian, {n_total:,} particles",
-                   "solver": f"learned treecode theta={theta}, {leaf} per leaf, budget {LEARNED_EPS}, "
-                             f"order bias {LEARNED_ORDER_BIAS}",
-                   "lanes": args.lanes, "dt": dt, "graph": "one CUDA graph replay per ensemble step"},
-        "particle_steps_per_s": value * n_total, "gpu_launches": launches, "clocks": clk,
+                   "solver": "learned treecode, per size class the autotuned leaf / theta / budget / batch level "
+                             "(order bias 2)", "tuned": {f"L{k}": v for k, v in tuned.items()},
+                   "lanes": args.lanes, "dt": dt, "graph": "one CUDA graph replay per ensemble step",
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "rel_l2_vs_fp64_direct": {"sample": "4096 seeded targets per instance, FP64 GPU direct sum",
+                                  "t0_max": max(err_t0), "t0_median": float(np.median(err_t0)),
+                                  "final_max": max(err_final), "final_median": float(np.median(err_final)),
+                                  "final_step": args.warmup + args.steps},
+        "particle_steps_per_s": value * n_total,
+        "roofline": {"bound": "fp32", "kernel": "whole step (near + far field, all instances)",
+                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "traffic": None, "peak_source": "measured FMA microbenchmark (lpm_fma_peak) on this GPU",
+                     "work": "17 flops per near pair + 8 per far coefficient + 40 per far evaluation, 4 "
+                             "evaluations per step, from each instance's tree statistics"},
+        "e2e": {"value": world / float(np.mean(e2e_s)), "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes},
+        "gpu_launches": launches, "clocks": clk,
     }
     ens.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(reps=2)
+        out["cpu_baseline"] = {"value": base["pairs_per_s"] / pairs_step, "unit": "steps/s", "cores": base["cores"],
+                               "kind": base["kind"],
+                               "sample": base["sample"] + f"; the ensemble step's {pairs_step:.3e} pairs at that rate"}
     print(json.dumps(out))
 
 
@@ -432,7 +565,7 @@ def pairwise_direct_f32(ctx, kern, state0, n_src: int, fp32_peak: float, u64, st
             "timing": "one evaluation after one warm-up, CUDA events around the launch"}
 
 
-def poisson_summary(ctx, device: int, n: int = 1_048_576, reps: int = 5) -> dict:
+def poisson_summary(ctx, device: int, n: int = 1_048_576, reps: int = 5, cpu: bool = True) -> dict:
     """The 3D Poisson treecode configuration inside the headline run: evaluations/s at n points (median
     of `reps` evaluations after 3 warm-up ones), its error against the FP64 direct sum, the dominant
     kernel's roofline and the near / far split."""
@@ -441,6 +574,7 @@ def poisson_summary(ctx, device: int, n: int = 1_048_576, reps: int = 5) -> dict
     import lpmcxx_b200 as L
     import lpmcxx_b200.workloads as W
 
+    ctx.use_torch_stream()  # the library enqueues on the stream the CUDA events below are recorded on
     pts = torch.tensor(W.poisson_cube(n), device="cuda")
     kern = L.poisson_kernel()
     order, theta, leaf = POISSON_SETTINGS
@@ -485,7 +619,8 @@ def poisson_summary(ctx, device: int, n: int = 1_048_576, reps: int = 5) -> dict
             "near_kernel": {"ms": near_ms, "tflops": near_tf, "frac": near_tf / fp32_peak},
             "far_kernel": {"ms": far_ms, "tflops": far_tf, "frac": far_tf / fp32_peak,
                            "launches": prof.get("far_kernel", {}).get("launches")},
-            "peak_tflops_fp32": fp32_peak, "tree_stats": st}
+            "peak_tflops_fp32": fp32_peak, "tree_stats": st,
+            "cpu_baseline": poisson_cpu_baseline(n) if cpu else None}
 
 
 def run_gpu(args) -> None:
@@ -618,7 +753,7 @@ def run_gpu(args) -> None:
         fp64_peak = ctx.fma_peak_tflops(L.LPM_PREC_F64)
         pairwise = None if args.no_extras else pairwise_direct_f32(ctx, kern, state0, n_src, fp32_peak, u64, stream)
     torch.cuda.synchronize()
-    poisson = None if (args.no_extras or world > 1) else poisson_summary(ctx, local)
+    poisson = None if (args.no_extras or world > 1) else poisson_summary(ctx, local, cpu=not args.no_cpu_baseline)
 
     # dominant kernel of the headline step
     dom = max(prof.items(), key=lambda kv: kv[1]["ms"]) if prof else (None, None)

@@ -356,6 +356,10 @@ int lpm_rk4_set_mlp(lpm_rk4* rk, const float* params);
 typedef struct lpm_ensemble lpm_ensemble;
 int lpm_ensemble_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver, int n_inst,
                         const int64_t* n_src, const int64_t* n_pts, int lanes, lpm_ensemble** out);
+/* lpm_ensemble_create with one solver per instance (solvers: n_inst descriptors), e.g. leaf sizes and
+ * acceptance parameters tuned per instance size. */
+int lpm_ensemble_create_each(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solvers, int n_inst,
+                             const int64_t* n_src, const int64_t* n_pts, int lanes, lpm_ensemble** out);
 int lpm_ensemble_destroy(lpm_ensemble* ens);
 int lpm_ensemble_instance(lpm_ensemble* ens, int i, lpm_rk4** rk);
 int lpm_ensemble_lane_of(const lpm_ensemble* ens, int i, int* lane);

@@ -288,12 +288,18 @@ class Ensemble:
     """lpm_ensemble: independent RK4 problems of uneven sizes, advanced together by one CUDA graph per
     step spread over `lanes` streams.  `instance(i)` gives an RK4 handle for states."""
 
-    def __init__(self, ctx: Context, kernel: KernelDesc, solver: _capi.SolverDesc, n_src, n_pts, lanes: int = 8):
+    def __init__(self, ctx: Context, kernel: KernelDesc, solver, n_src, n_pts, lanes: int = 8):
+        """solver: one SolverDesc for every instance, or a sequence of them (one per instance)."""
         n_src = np.ascontiguousarray(n_src, dtype=np.int64)
         n_pts = np.ascontiguousarray(n_pts, dtype=np.int64)
         h = C.c_void_p()
-        check(lib().lpm_ensemble_create(ctx.h, C.byref(kernel), C.byref(solver), len(n_src), ptr(n_src), ptr(n_pts),
-                                        lanes, C.byref(h)), "lpm_ensemble_create")
+        if isinstance(solver, _capi.SolverDesc):
+            check(lib().lpm_ensemble_create(ctx.h, C.byref(kernel), C.byref(solver), len(n_src), ptr(n_src),
+                                            ptr(n_pts), lanes, C.byref(h)), "lpm_ensemble_create")
+        else:
+            arr = (_capi.SolverDesc * len(solver))(*solver)
+            check(lib().lpm_ensemble_create_each(ctx.h, C.byref(kernel), arr, len(n_src), ptr(n_src), ptr(n_pts),
+                                                 lanes, C.byref(h)), "lpm_ensemble_create_each")
         self.h, self.ctx = h, ctx
         self.n_src, self.n_pts = n_src, n_pts
 

@@ -125,6 +125,7 @@ SIGNATURES = {
     "lpm_rk4_source_tree": (C.c_int, [P, C.POINTER(P)]),
     "lpm_rk4_set_mlp": (C.c_int, [P, P]),
     "lpm_ensemble_create": (C.c_int, [P, P, P, C.c_int, P, P, C.c_int, P]),
+    "lpm_ensemble_create_each": (C.c_int, [P, P, P, C.c_int, P, P, C.c_int, P]),
     "lpm_ensemble_destroy": (C.c_int, [P]),
     "lpm_ensemble_instance": (C.c_int, [P, C.c_int, P]),
     "lpm_ensemble_lane_of": (C.c_int, [P, C.c_int, P]),

@@ -1,6 +1,6 @@
-"""Autotuner for the treecode: picks the fastest (leaf size, acceptance theta, batch cell level, and the
-fixed order or the learned selector's per-pair budget and order bias) that meets a relative L2 tolerance on
-a workload.
+"""Autotuner for the treecode: picks the fastest (leaf size, acceptance theta, batch cell level, the fixed
+order or the learned selector's per-pair budget and order bias, and the near-field tile shape) that meets a
+relative L2 tolerance on a workload.
 
 Accuracy is judged on a random sample of targets against the FP64 direct sum (the library's own
 `lpm_direct_sum_dev`, which is parity-tested against the reference); time is the median of CUDA-event
@@ -9,7 +9,11 @@ parameters (`TreeSum.set_param`), so a sweep costs one octree allocation per lea
 
     best = autotune(ctx, L.biot_savart_kernel(), src, tgt, tol=1e-6, order_biases=(0, 2))
     solver = tuned_solver(best)            # an lpm_solver_desc for TreeSum / RK4
-    # then set_param("batch_level", best.best.batch_level) and set_param("order_bias", best.best.bias)
+    # then set_param("batch_level", best.best.batch_level) and set_param("order_bias", best.best.bias),
+    # set_param("near_targets", best.best.near_targets) and set_param("near_tile", best.best.near_tile)
+
+The tile shape (targets per thread of the near-field kernel and sources staged per shared-memory tile)
+changes no result, only the time, so it is searched last, on the fastest qualifying setting.
 """
 from __future__ import annotations
 
@@ -30,6 +34,8 @@ class Candidate:
     bias: int = 0           # learned: orders added to every selector choice
     ms: float | None = None
     rel_err: float | None = None
+    near_targets: int = 2   # near-field tile shape (run-time parameters "near_targets", "near_tile")
+    near_tile: int = 512
 
 
 @dataclass
@@ -43,7 +49,8 @@ class TuneResult:
         b = self.best
         return {"learned": self.learned, "max_per_leaf": b.max_per_leaf, "theta": b.theta,
                 ("eps" if self.learned else "order"): b.knob, "batch_level": b.batch_level,
-                "order_bias": b.bias, "ms": b.ms, "rel_err": b.rel_err}
+                "order_bias": b.bias, "ms": b.ms, "rel_err": b.rel_err, "near_targets": b.near_targets,
+                "near_tile": b.near_tile}
 
 
 def default_grid(learned: bool, kernel_kind: int):
@@ -76,13 +83,15 @@ def _timed_eval(ctx, ts, src, tgt, out, reps):
 
 def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bool = True, params=None,
              grid=None, batch_levels=(0, -1), sample: int = 4096, reps: int = 3, seed: int = 0,
-             safety: float = 0.8, order_biases=(0,)) -> TuneResult:
+             safety: float = 0.8, order_biases=(0,), tiles=((2, 256), (2, 512), (2, 1024), (4, 256), (4, 512),
+                                                            (4, 1024))) -> TuneResult:
     """Sweep the grid on device-resident src (n_src, 4) / tgt (n_tgt, 4) float64 tensors.
 
     tol: relative L2 tolerance over the sampled targets (a candidate must reach safety * tol).
     learned: tune the learned selector's budget (Biot-Savart only) instead of the fixed order.
     batch_levels: offsets from each solver's default batch cell level to try (0 = default).
     order_biases: learned only, the selector order biases to try (set_param "order_bias").
+    tiles: (near_targets, near_tile) shapes of the near-field kernel, tried on the best setting.
     """
     import torch
 
@@ -131,20 +140,42 @@ def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bo
                         ts.set_param("batch_level", lvl)
                         ms = _timed_eval(ctx, ts, src, tgt, out, reps)
                         err = float(torch.linalg.norm(out[:, idx_t] - ref)) / ref_norm
-                        c = Candidate(leaf, theta, knob, lvl, bias, ms, err)
+                        c = Candidate(leaf, theta, knob, lvl, bias, ms, err, int(ts.get_param("near_targets")),
+                                      int(ts.get_param("near_tile")))
                         res.tried.append(c)
                         if err <= safety * tol and (res.best is None or ms < res.best.ms):
                             res.best = c
                     ts.set_param("batch_level", level0)
         finally:
             ts.close()
+    if res.best is not None and tiles:
+        b = res.best
+        ts = TreeSum(ctx, kernel, tree_solver(LPM_PREC_F32, 10 if learned else int(b.knob), b.max_per_leaf, b.theta,
+                                              learned=learned, tolerance=b.knob if learned else 0.0), n_src, n_tgt)
+        try:
+            if learned:
+                ts.set_mlp(params)
+                ts.set_param("order_bias", b.bias)
+            ts.set_param("batch_level", b.batch_level)
+            for nt, tile in tiles:
+                ts.set_param("near_targets", nt)
+                ts.set_param("near_tile", tile)
+                ms = _timed_eval(ctx, ts, src, tgt, out, reps)
+                err = float(torch.linalg.norm(out[:, idx_t] - ref)) / ref_norm
+                c = Candidate(b.max_per_leaf, b.theta, b.knob, b.batch_level, b.bias, ms, err, nt, tile)
+                res.tried.append(c)
+                if err <= safety * tol and ms < res.best.ms:
+                    res.best = c
+        finally:
+            ts.close()
     return res
 
 
 def tuned_solver(result: TuneResult, precision: int = LPM_PREC_F32):
-    """lpm_solver_desc of the tuned setting (the batch level and the order bias are run-time parameters:
-    apply them with set_param("batch_level", result.best.batch_level) and set_param("order_bias",
-    result.best.bias) on the TreeSum / RK4 made from this descriptor)."""
+    """lpm_solver_desc of the tuned setting (the batch level, the order bias and the near-field tile shape
+    are run-time parameters: apply them with set_param("batch_level", ...), set_param("order_bias", ...),
+    set_param("near_targets", ...) and set_param("near_tile", ...) on the TreeSum / RK4 made from this
+    descriptor; apply_tuned does all four)."""
     b = result.best
     if b is None:
         raise ValueError("no candidate met the tolerance")
@@ -153,4 +184,14 @@ def tuned_solver(result: TuneResult, precision: int = LPM_PREC_F32):
     return tree_solver(precision, int(b.knob), b.max_per_leaf, b.theta)
 
 
-__all__ = ["autotune", "tuned_solver", "TuneResult", "Candidate", "default_grid", "LPM_PREC_F64"]
+def apply_tuned(result: TuneResult, solver) -> None:
+    """Set the tuned run-time parameters on a TreeSum or RK4 made from tuned_solver(result)."""
+    b = result.best
+    solver.set_param("batch_level", b.batch_level)
+    if result.learned:
+        solver.set_param("order_bias", b.bias)
+    solver.set_param("near_targets", b.near_targets)
+    solver.set_param("near_tile", b.near_tile)
+
+
+__all__ = ["autotune", "tuned_solver", "apply_tuned", "TuneResult", "Candidate", "default_grid", "LPM_PREC_F64"]

@@ -296,7 +296,8 @@ __global__ void __launch_bounds__(kThreads) bs_f32_kernel(const float4* __restri
                                                           const float4* __restrict__ tgt,
                                                           const double4* __restrict__ tgt64, int64_t n_tgt,
                                                           float d2x2, double mult, double* __restrict__ out,
-                                                          int64_t stride, int64_t coinc_n, int64_t coinc_off) {
+                                                          int64_t stride, int64_t coinc_n, int64_t coinc_off,
+                                                          int64_t src_part) {
     __shared__ float4 tile[kTile];
     const int64_t blk0 = (int64_t)blockIdx.x * (kThreads * kTpt32);
     const int64_t base = blk0 + threadIdx.x;
@@ -312,12 +313,14 @@ __global__ void __launch_bounds__(kThreads) bs_f32_kernel(const float4* __restri
     // source indices that may coincide with this block's targets
     const int64_t c_lo = blk0 < coinc_n ? blk0 + coinc_off : INT64_MAX;
     const int64_t c_hi = blk0 < coinc_n ? min(blk0 + kThreads * kTpt32, coinc_n) + coinc_off : INT64_MIN;
-    for (int64_t j0 = 0; j0 < n_src; j0 += kTile) {
+    // gridDim.y source parts of src_part sources each (a multiple of kTile): blockIdx.y sums its part
+    const int64_t j_begin = (int64_t)blockIdx.y * src_part, j_end = min(n_src, j_begin + src_part);
+    for (int64_t j0 = j_begin; j0 < j_end; j0 += kTile) {
         __syncthreads();
         const int64_t j = j0 + threadIdx.x;
-        tile[threadIdx.x] = j < n_src ? src[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        tile[threadIdx.x] = j < j_end ? src[j] : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();
-        const int m = (int)min((int64_t)kTile, n_src - j0);
+        const int m = (int)min((int64_t)kTile, j_end - j0);
 #pragma unroll
         for (int t = 0; t < kTpt32; ++t) { ax[t] = 0.f; ay[t] = 0.f; az[t] = 0.f; }
         if (j0 < c_hi && j0 + m > c_lo)
@@ -333,9 +336,17 @@ __global__ void __launch_bounds__(kThreads) bs_f32_kernel(const float4* __restri
         if (i < n_tgt) {
             const double4 p = tgt64[i];
             const double nm = -mult;
-            out[i] = nm * (p.y * Dz[t] - p.z * Dy[t]);
-            out[stride + i] = nm * (p.z * Dx[t] - p.x * Dz[t]);
-            out[2 * stride + i] = nm * (p.x * Dy[t] - p.y * Dx[t]);
+            const double u0 = nm * (p.y * Dz[t] - p.z * Dy[t]), u1 = nm * (p.z * Dx[t] - p.x * Dz[t]),
+                         u2 = nm * (p.x * Dy[t] - p.y * Dx[t]);
+            if (gridDim.y == 1) {
+                out[i] = u0;
+                out[stride + i] = u1;
+                out[2 * stride + i] = u2;
+            } else {  // two parts added onto a zeroed output: 0 + a + b == 0 + b + a, so the result is exact
+                atomicAdd(out + i, u0);
+                atomicAdd(out + stride + i, u1);
+                atomicAdd(out + 2 * stride + i, u2);
+            }
         }
     }
 }
@@ -370,7 +381,7 @@ __device__ __forceinline__ void poisson_f32_tile(const float4* tile, int m, cons
 __global__ void __launch_bounds__(kThreads) poisson_f32_kernel(const float4* __restrict__ src, int64_t n_src,
                                                                const float4* __restrict__ tgt, int64_t n_tgt,
                                                                double mult, double* __restrict__ out, int64_t coinc_n,
-                                                               int64_t coinc_off) {
+                                                               int64_t coinc_off, int64_t src_part) {
     __shared__ float4 tile[kTile];
     const int64_t blk0 = (int64_t)blockIdx.x * (kThreads * kTpt32);
     const int64_t base = blk0 + threadIdx.x;
@@ -385,12 +396,13 @@ __global__ void __launch_bounds__(kThreads) poisson_f32_kernel(const float4* __r
     }
     const int64_t c_lo = blk0 < coinc_n ? blk0 + coinc_off : INT64_MAX;
     const int64_t c_hi = blk0 < coinc_n ? min(blk0 + kThreads * kTpt32, coinc_n) + coinc_off : INT64_MIN;
-    for (int64_t j0 = 0; j0 < n_src; j0 += kTile) {
+    const int64_t j_begin = (int64_t)blockIdx.y * src_part, j_end = min(n_src, j_begin + src_part);
+    for (int64_t j0 = j_begin; j0 < j_end; j0 += kTile) {
         __syncthreads();
         const int64_t j = j0 + threadIdx.x;
-        tile[threadIdx.x] = j < n_src ? src[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        tile[threadIdx.x] = j < j_end ? src[j] : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();
-        const int m = (int)min((int64_t)kTile, n_src - j0);
+        const int m = (int)min((int64_t)kTile, j_end - j0);
 #pragma unroll
         for (int t = 0; t < kTpt32; ++t) acc[t] = 0.f;
         if (j0 < c_hi && j0 + m > c_lo)
@@ -403,7 +415,10 @@ __global__ void __launch_bounds__(kThreads) poisson_f32_kernel(const float4* __r
 #pragma unroll
     for (int t = 0; t < kTpt32; ++t) {
         const int64_t i = base + t * kThreads;
-        if (i < n_tgt) out[i] = mult * phi[t];
+        if (i < n_tgt) {
+            if (gridDim.y == 1) out[i] = mult * phi[t];
+            else atomicAdd(out + i, mult * phi[t]);  // two parts onto zero: exact in either order
+        }
     }
 }
 
@@ -462,23 +477,61 @@ int direct_sum_f64(lpm_ctx* ctx, const lpm_kernel_desc& k, const double4* src, i
 // FP32 sums take FP32 copies of sources (w pre-scaled by 2 for Biot-Savart) and targets, plus the
 // FP64 targets for the Biot-Savart epilogue.  Targets 0..coinc_n-1 may coincide with sources
 // coinc_off..coinc_off+coinc_n-1 (face-centroid targets and their own sources).
+namespace {
+// Source parts of an FP32 direct sum: the target blocks alone may fill their last wave of resident blocks
+// poorly (at 3 resident 256-thread blocks per SM, 1,920 blocks are 4.3 waves on 148 SMs, the fifth a third
+// full).  Splitting the sources in two halves doubles the blocks at half the work each; the split is taken
+// when it shortens the estimate ceil(blocks parts / resident) / parts.  Two parts only: two addends onto
+// a zeroed output are exact in either order, so the result does not depend on which part finishes first.
+template <typename Kern>
+int source_parts(lpm_ctx* ctx, Kern kern, int64_t blocks, int64_t n_src) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0) != cudaSuccess || per_sm < 1)
+        return 1;
+    const double resident = (double)per_sm * ctx->num_sms;
+    if (n_src < 2 * kTile) return 1;
+    const double t1 = std::ceil(blocks / resident), t2 = std::ceil(2.0 * blocks / resident) / 2.0;
+    return t2 < t1 ? 2 : 1;
+}
+}  // namespace
+
 int direct_sum_f32_impl(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* src, int64_t n_src, const float4* tgt,
                         const double4* tgt64, int64_t n_tgt, double* out, int64_t out_stride, int64_t coinc_n,
                         int64_t coinc_off) {
     if (n_tgt <= 0) return LPM_OK;
     const unsigned grid = grid_for(n_tgt, kThreads * kTpt32);
+    auto zero_rows = [&](int rows) -> int {
+        for (int c = 0; c < rows; ++c)
+            LPM_CUDA_TRY(cudaMemsetAsync(out + (size_t)c * out_stride, 0, sizeof(double) * (size_t)n_tgt, ctx->stream));
+        return LPM_OK;
+    };
     if (k.kind == LPM_KERNEL_BIOT_SAVART_SPHERE) {
         const double mult = -1.0 / (4.0 * kPi * k.radius);
-        if (k.delta != 0.0)
-            LPM_LAUNCH(ctx, "bs_f32_kernel", bs_f32_kernel<true>, grid, kThreads, 0, src, n_src, tgt, tgt64, n_tgt,
-                                                                    (float)(2.0 * k.delta * k.delta), mult, out,
-                                                                    out_stride, coinc_n, coinc_off);
+        const bool delta = k.delta != 0.0;
+        const int parts = delta ? source_parts(ctx, bs_f32_kernel<true>, grid, n_src)
+                                : source_parts(ctx, bs_f32_kernel<false>, grid, n_src);
+        const int64_t part = parts == 1 ? n_src : ((n_src + 2 * kTile - 1) / (2 * kTile)) * kTile;
+        if (parts > 1) {
+            int rc = zero_rows(3);
+            if (rc) return rc;
+        }
+        const dim3 g(grid, parts);
+        if (delta)
+            LPM_LAUNCH(ctx, "bs_f32_kernel", bs_f32_kernel<true>, g, kThreads, 0, src, n_src, tgt, tgt64, n_tgt,
+                       (float)(2.0 * k.delta * k.delta), mult, out, out_stride, coinc_n, coinc_off, part);
         else
-            LPM_LAUNCH(ctx, "bs_f32_kernel", bs_f32_kernel<false>, grid, kThreads, 0, src, n_src, tgt, tgt64, n_tgt, 0.0f, mult, out,
-                                                                     out_stride, coinc_n, coinc_off);
+            LPM_LAUNCH(ctx, "bs_f32_kernel", bs_f32_kernel<false>, g, kThreads, 0, src, n_src, tgt, tgt64, n_tgt, 0.0f,
+                       mult, out, out_stride, coinc_n, coinc_off, part);
     } else if (k.kind == LPM_KERNEL_POISSON_3D) {
-        LPM_LAUNCH(ctx, "poisson_f32_kernel", poisson_f32_kernel, grid, kThreads, 0, src, n_src, tgt, n_tgt, 1.0 / (4.0 * kPi), out,
-                                                               coinc_n, coinc_off);
+        const int parts = source_parts(ctx, poisson_f32_kernel, grid, n_src);
+        const int64_t part = parts == 1 ? n_src : ((n_src + 2 * kTile - 1) / (2 * kTile)) * kTile;
+        if (parts > 1) {
+            int rc = zero_rows(1);
+            if (rc) return rc;
+        }
+        const dim3 g(grid, parts);
+        LPM_LAUNCH(ctx, "poisson_f32_kernel", poisson_f32_kernel, g, kThreads, 0, src, n_src, tgt, n_tgt,
+                   1.0 / (4.0 * kPi), out, coinc_n, coinc_off, part);
     } else {
         set_error("invalid kernel");
         return LPM_ERR_KERNEL;

@@ -75,9 +75,25 @@ extern "C" int lpm_ensemble_destroy(lpm_ensemble* e) {
     return LPM_OK;
 }
 
+static int ensemble_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solvers,
+                           int solver_stride, int n_inst, const int64_t* n_src, const int64_t* n_pts, int lanes,
+                           lpm_ensemble** out);
+
 extern "C" int lpm_ensemble_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver,
                                    int n_inst, const int64_t* n_src, const int64_t* n_pts, int lanes,
                                    lpm_ensemble** out) {
+    return ensemble_create(ctx, kernel, solver, 0, n_inst, n_src, n_pts, lanes, out);
+}
+
+extern "C" int lpm_ensemble_create_each(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solvers,
+                                        int n_inst, const int64_t* n_src, const int64_t* n_pts, int lanes,
+                                        lpm_ensemble** out) {
+    return ensemble_create(ctx, kernel, solvers, 1, n_inst, n_src, n_pts, lanes, out);
+}
+
+static int ensemble_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver,
+                           int solver_stride, int n_inst, const int64_t* n_src, const int64_t* n_pts, int lanes,
+                           lpm_ensemble** out) {
     if (!ctx || !kernel || !solver || !n_src || !n_pts || !out || n_inst < 1 || lanes < 1 || lanes > 64) {
         set_error("lpm_ensemble_create: bad argument (1 <= lanes <= 64, n_inst >= 1)");
         return LPM_ERR_ARG;
@@ -121,7 +137,8 @@ extern "C" int lpm_ensemble_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, 
     }
     e->inst.assign(n_inst, nullptr);
     for (int i = 0; i < n_inst; ++i) {
-        int rc = lpm_rk4_create(e->lanes[e->lane_of[i]], kernel, solver, n_src[i], n_pts[i], &e->inst[i]);
+        int rc = lpm_rk4_create(e->lanes[e->lane_of[i]], kernel, solver + (size_t)i * solver_stride, n_src[i],
+                                n_pts[i], &e->inst[i]);
         if (rc) {
             lpm_ensemble_destroy(e);
             return rc;

@@ -298,27 +298,50 @@ __global__ void tree_init_kernel(Octree t) {
 
 // For each node of level l holding more than max_per_leaf points: the 9 boundaries of its
 // level-(l+1) digit ranges, and the number of non-empty children.
-__global__ void split_level_kernel(Octree t, int l) {
+__global__ void __launch_bounds__(256) split_level_kernel(Octree t, int l) {
+    // One block per node (grid-stride over the level): warp d (1..7) finds the first position of the node's
+    // sorted key range whose level-(l+1) digit is >= d by a 32-ary search (32 probes per round, ~4 rounds
+    // for a million keys instead of ~20 dependent probes of a binary search).
+    __shared__ int cs_sh[9];
     const int lb = t.level_range[2 * l], le = t.level_range[2 * l + 1];
-    for (int i = lb + blockIdx.x * blockDim.x + threadIdx.x; i < le; i += gridDim.x * blockDim.x) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    for (int i = lb + blockIdx.x; i < le; i += gridDim.x) {
         const int s = t.node_start[i], e = t.node_end[i];
-        int32_t* cs = t.child_start + (int64_t)(i - lb) * 9;
-        int nchild = 0;
-        if (e - s > t.max_per_leaf) {
-            cs[0] = s;
-            cs[8] = e;
-            for (int d = 1; d < 8; ++d) {  // first position whose digit >= d
-                int lo = s, hi = e;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (level_digit(t.keys[mid], l + 1) < d) lo = mid + 1;
-                    else hi = mid;
+        const bool split = e - s > t.max_per_leaf;  // uniform per block
+        if (split) {
+            if (w >= 1 && w <= 7) {
+                const int d = w;
+                int lo = s, hi = e;  // the boundary b satisfies lo <= b <= hi; positions lo..hi-1 are keys
+                while (hi - lo > 32) {
+                    const int64_t L = hi - lo;
+                    const int p = lo + (int)(((int64_t)lane * L) >> 5);
+                    const unsigned below = __ballot_sync(full, level_digit(t.keys[p], l + 1) < d);
+                    const int c = __popc(below);  // probes 0..c-1 lie below the boundary (digits are sorted)
+                    const int nlo = c == 0 ? lo : lo + (int)(((int64_t)(c - 1) * L) >> 5) + 1;
+                    const int nhi = c == 32 ? hi : lo + (int)(((int64_t)c * L) >> 5);
+                    lo = nlo;
+                    hi = nhi;
                 }
-                cs[d] = lo;
+                const bool lt = lane < hi - lo && level_digit(t.keys[lo + lane], l + 1) < d;
+                const int c = __popc(__ballot_sync(full, lt));
+                if (lane == 0) cs_sh[d] = lo + c;
+            } else if (w == 0 && lane == 0) {
+                cs_sh[0] = s;
+                cs_sh[8] = e;
             }
-            for (int d = 0; d < 8; ++d) nchild += cs[d + 1] > cs[d];
         }
-        t.node_split[i - lb] = nchild;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int nchild = 0;
+            if (split) {
+                int32_t* cs = t.child_start + (int64_t)(i - lb) * 9;
+                for (int d = 0; d <= 8; ++d) cs[d] = cs_sh[d];
+                for (int d = 0; d < 8; ++d) nchild += cs_sh[d + 1] > cs_sh[d];
+            }
+            t.node_split[i - lb] = nchild;
+        }
+        __syncthreads();  // cs_sh is reused by the next node
     }
 }
 
@@ -516,8 +539,9 @@ int octree_build(lpm_ctx* ctx, Octree& t, const double4* pts, int64_t n, const R
     LPM_LAUNCH(ctx, "tree_init_kernel", tree_init_kernel, 1, 1, 0, t);
     const unsigned sgrid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(t.node_cap, 256),
                                                                              4 * ctx->num_sms));
+    const unsigned split_grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(t.node_cap, 8 * ctx->num_sms));
     for (int l = 0; l < t.max_depth; ++l) {
-        LPM_LAUNCH(ctx, "split_level_kernel", split_level_kernel, sgrid, 256, 0, t, l);
+        LPM_LAUNCH(ctx, "split_level_kernel", split_level_kernel, split_grid, 256, 0, t, l);
         LPM_LAUNCH(ctx, "emit_level_kernel", emit_level_kernel, 1, 1024, 0, t, l);
     }
     LPM_LAUNCH(ctx, "fill_i32_kernel", fill_i32_kernel, grid_for(n + 1, 256), 256, 0, t.leaf_flag, n + 1, 0);

@@ -442,6 +442,8 @@ struct TraverseArgs {
     const float* mlp_norm;
     uint8_t* decisions;  // n_batches x kDecisionCap selector classes (count pass writes, fill pass reads)
     int heavy_cap;       // nodes with moments / coefficients: only these can be far clusters
+    uint32_t* near_work;  // count pass: each batch's near-field (target, source) pairs, saturated at 2^32 - 1
+    uint32_t* far_work;   // count pass: each batch's far coefficient evaluations, saturated at 2^32 - 1
 };
 
 constexpr int kWarpStack = 1024;
@@ -533,7 +535,11 @@ __global__ void __launch_bounds__(128, LPM_TRAVERSE_MIN_BLOCKS) traverse_kernel(
     if (t.counters[1] == 0 || t.counters[0] == 0 || b >= *A.nbat) {
         if (!A.fill) {
             if (lane <= kPMax) A.far_cnt[lane * A.nb1 + b] = 0;
-            if (lane == 0) A.near_cnt[b] = 0;
+            if (lane == 0) {
+                A.near_cnt[b] = 0;
+                A.near_work[b] = 0;
+                A.far_work[b] = 0;
+            }
         }
         return;
     }
@@ -658,10 +664,66 @@ __global__ void __launch_bounds__(128, LPM_TRAVERSE_MIN_BLOCKS) traverse_kernel(
     if (!A.fill && lane <= kPMax) A.far_cnt[lane * A.nb1 + b] = pcnt[w][lane];
     if (!A.fill && lane == 0) {
         A.near_cnt[b] = nnear;
+        A.near_work[b] = (uint32_t)min(near_pairs, 0xffffffffull);
+        A.far_work[b] = (uint32_t)min(far_terms, 0xffffffffull);
         atomicAdd(&A.pair_counts[0], far_pairs);
         atomicAdd(&A.pair_counts[1], near_pairs);
         atomicAdd(&A.pair_counts[2], far_terms);
     }
+}
+
+// ---------------------------------------------------------------------------------- batch schedule
+// Batches in decreasing order of work, bucketed by log2(work) in half-octave steps: a persistent kernel
+// that takes batches in this order from an atomic ticket ends on its smallest batches, so few SMs idle at
+// its tail.  Each batch is still computed by one block, so the results do not depend on the order.
+constexpr int kSchedBuckets = 64;
+// the solver's schedule scratch (int32): near buckets and cursors, far buckets and cursors, then one ticket
+// for the near launch and one per far order
+constexpr int kAuxNearHist = 0, kAuxNearCur = 64, kAuxFarHist = 128, kAuxFarCur = 192, kAuxNearTicket = 256,
+              kAuxFarTicket = 257, kAuxInts = 257 + 16;
+
+__device__ __forceinline__ int sched_bucket(uint32_t work) {
+    const int l2 = (int)(2.0f * __log2f((float)work + 1.0f));
+    return kSchedBuckets - 1 - min(max(l2, 0), kSchedBuckets - 1);
+}
+
+// hist[0:64] and cursor[0:64] zeroed by the caller.
+__global__ void sched_hist_kernel(const uint32_t* __restrict__ work, const int32_t* __restrict__ nbat,
+                                  int32_t* __restrict__ hist) {
+    const int n = *nbat;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x)
+        atomicAdd(&hist[sched_bucket(work[b])], 1);
+}
+
+__global__ void sched_scatter_kernel(const uint32_t* __restrict__ work, const int32_t* __restrict__ nbat,
+                                     const int32_t* __restrict__ hist, int32_t* __restrict__ cursor,
+                                     int32_t* __restrict__ order) {
+    __shared__ int base[kSchedBuckets];
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int k = 0; k < kSchedBuckets; ++k) {
+            base[k] = acc;
+            acc += hist[k];
+        }
+    }
+    __syncthreads();
+    const int n = *nbat;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) {
+        const int k = sched_bucket(work[b]);
+        order[base[k] + atomicAdd(&cursor[k], 1)] = b;
+    }
+}
+
+// The next batch of a persistent kernel's block: order[ticket++] while tickets last, else -1.  ticket is
+// zeroed before the launch.
+__device__ __forceinline__ int next_batch(int32_t* ticket, const int32_t* __restrict__ order, int nbat, int* slot) {
+    __syncthreads();  // every thread is done with the previous batch's shared memory
+    if (threadIdx.x == 0) {
+        const int k = atomicAdd(ticket, 1);
+        *slot = k < nbat ? order[k] : -1;
+    }
+    __syncthreads();
+    return *slot;
 }
 
 // ---------------------------------------------------------------------------------- far field
@@ -858,6 +920,8 @@ struct FarArgs {
     int n_ent;
     const int32_t* gtab;  // order-P gather table: canonical index of each Horner-sequence entry
     double* V;
+    const int32_t* order;  // batches by decreasing far work (the persistent grid's visiting order)
+    int32_t* ticket;       // this launch's ticket, zeroed before it
 };
 
 #ifndef LPM_FAR_STAGE_UNITS
@@ -902,10 +966,11 @@ __global__ void __launch_bounds__(kBatch, kFarMinBlocks) far_order_kernel(FarArg
     using S = FarShape<P, F4>;
     extern __shared__ float4 fbuf[];  // 2 stages of S::kStage units, then 2 x kK centres
     double4* ctr = (double4*)(fbuf + 2 * S::kStage);
-    const int64_t b = blockIdx.x;
-    if (b >= *A.nbat) return;  // uniform per block
+    __shared__ int slot;
+    const int nbat = *A.nbat;
+    for (int64_t b = next_batch(A.ticket, A.order, nbat, &slot); b >= 0; b = next_batch(A.ticket, A.order, nbat, &slot)) {
     const int64_t f0 = A.far_off[b], f1 = min(f0 + (int64_t)A.far_cnt[b], A.far_cap);
-    if (f0 >= f1) return;  // uniform per block
+    if (f0 >= f1) continue;  // uniform per block
     const int64_t q0 = A.batch_first[b], qe = A.batch_first[b + 1];
     const int64_t q = q0 + threadIdx.x;
     const bool live = q0 + (int64_t)(threadIdx.x & ~31) < qe;  // warp-uniform
@@ -937,6 +1002,7 @@ __global__ void __launch_bounds__(kBatch, kFarMinBlocks) far_order_kernel(FarArg
         A.V[q] += acc[0];
         A.V[A.n_tgt + q] += acc[1];
         A.V[2 * A.n_tgt + q] += acc[2];
+    }
     }
 }
 
@@ -1078,13 +1144,16 @@ __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kerne
     using S = FarShape<P, float4, kFar2StageUnits>;
     extern __shared__ float4 fbuf[];  // 2 stages of S::kStage units, then 2 x kK centres (FP32 offsets)
     float4* ctr = fbuf + 2 * S::kStage;
-    const int64_t b = blockIdx.x;
-    if (b >= *A.nbat) return;  // uniform per block
+    __shared__ int slot;
+    const int nbat = *A.nbat;
+    for (int64_t b = next_batch(A.ticket, A.order, nbat, &slot); b >= 0; b = next_batch(A.ticket, A.order, nbat, &slot)) {
     const int64_t f0 = A.far_off[b], f1 = min(f0 + (int64_t)A.far_cnt[b], A.far_cap);
-    if (f0 >= f1) return;  // uniform per block
+    if (f0 >= f1) continue;  // uniform per block
     const int64_t q0 = A.batch_first[b], qe = A.batch_first[b + 1];
-    const int64_t qa = q0 + threadIdx.x, qb = qa + kFar2Threads;
-    const bool live = q0 + (int64_t)(threadIdx.x & ~31) < qe;  // warp-uniform (second targets lie further on)
+    // warp w holds targets 64 w .. 64 w + 63 of the batch (lane l: 64 w + l and 64 w + l + 32), so a warp past
+    // the batch's last target idles as a whole (batches average ~109 of 128 targets)
+    const int64_t qa = q0 + 64 * (threadIdx.x >> 5) + (threadIdx.x & 31), qb = qa + 32;
+    const bool live = q0 + 64 * (int64_t)(threadIdx.x >> 5) < qe;  // warp-uniform
     const double4 o = A.tgt_sorted[q0];  // the block's origin for FP32 offsets
     float x[2][3], xo[2][3];
 #pragma unroll
@@ -1130,6 +1199,7 @@ __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kerne
         A.V[qb] += acc[1][0];
         A.V[A.n_tgt + qb] += acc[1][1];
         A.V[2 * A.n_tgt + qb] += acc[1][2];
+    }
     }
 }
 
@@ -1232,16 +1302,19 @@ __global__ void __launch_bounds__(kBatch / T) far_scalar_kernel(FarArgs A, int s
     static_assert(T == 1 || (T == 2 && sizeof(F) == 4), "two targets per thread in FP32 only");
     extern __shared__ float4 fbuf[];  // 2 stages of kK x kUnits units, then 2 x kK centres
     double4* ctr = (double4*)(fbuf + 2 * kK * kUnits);
-    const int64_t b = blockIdx.x;
-    if (b >= *A.nbat) return;  // uniform per block
+    __shared__ int slot;
+    const int nbat = *A.nbat;
+    for (int64_t b = next_batch(A.ticket, A.order, nbat, &slot); b >= 0; b = next_batch(A.ticket, A.order, nbat, &slot)) {
     const int64_t f0 = A.far_off[b], f1 = min(f0 + (int64_t)A.far_cnt[b], A.far_cap);
-    if (f0 >= f1) return;  // uniform per block
+    if (f0 >= f1) continue;  // uniform per block
     const int64_t q0 = A.batch_first[b], qe = A.batch_first[b + 1];
-    const int64_t q = q0 + threadIdx.x;
-    const bool live = q0 + (int64_t)(threadIdx.x & ~31) < qe;  // warp-uniform (later targets lie further on)
+    // warp w holds targets 32 T w .. 32 T (w + 1) - 1 of the batch (lane l: 32 T w + l + 32 t), so a warp past
+    // the batch's last target idles as a whole
+    const int64_t q = q0 + 32 * T * (threadIdx.x >> 5) + (threadIdx.x & 31);
+    const bool live = q0 + 32 * T * (int64_t)(threadIdx.x >> 5) < qe;  // warp-uniform
     double4 x[T];
 #pragma unroll
-    for (int t = 0; t < T; ++t) x[t] = q + t * kNT < qe ? A.tgt_sorted[q + t * kNT] : make_double4(2, 2, 2, 0);
+    for (int t = 0; t < T; ++t) x[t] = q + 32 * t < qe ? A.tgt_sorted[q + 32 * t] : make_double4(2, 2, 2, 0);
     const F* base = (const F*)(sizeof(F) == 8 ? (const void*)A.B64 : (const void*)A.B32);
     auto gather = [&](int64_t s0, int n, float4* buf, double4* cs) {
         for (int i = threadIdx.x; i < n * kUnits; i += kNT) {
@@ -1292,7 +1365,8 @@ __global__ void __launch_bounds__(kBatch / T) far_scalar_kernel(FarArgs A, int s
     }
 #pragma unroll
     for (int t = 0; t < T; ++t)
-        if (q + t * kNT < qe) A.V[q + t * kNT] += acc[t];
+        if (q + 32 * t < qe) A.V[q + 32 * t] += acc[t];
+    }
 }
 
 typedef void (*FarScalarFn)(FarArgs, int);
@@ -1468,10 +1542,9 @@ __global__ void __launch_bounds__(kBatch) label_kernel(Octree t, const int2* __r
 #ifndef LPM_NEAR_TARGETS
 #define LPM_NEAR_TARGETS 2
 #endif
-constexpr int kNearTargets = LPM_NEAR_TARGETS;       // targets per thread (even; 4 measured slower than 2)
-constexpr int kNearThreads = kBatch / kNearTargets;  // kBatch targets per block
+constexpr int kNearTargets = LPM_NEAR_TARGETS;  // default targets per thread (2 or 4; run-time "near_targets")
 
-constexpr int kNearStreamTile = 512;  // sources staged per tile
+constexpr int kNearStreamTile = 512;  // default sources staged per tile (256, 512 or 1024; run-time "near_tile")
 constexpr int kNearRuns = 128;        // source ranges resolved per chunk
 
 // One tile of the stream: m tree-ordered sources (FP32 absolute coordinates, w pre-scaled by 2)
@@ -1566,31 +1639,57 @@ __device__ __forceinline__ void finish_target_scalar(int64_t q, int64_t qe, cons
     U[tperm[q]] = mult * (V[q] + D[0]);
 }
 
-template <bool kScalar>
-__global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const double4* __restrict__ tgt_sorted,
-                                                            int64_t n_tgt, const int32_t* __restrict__ tperm,
-                                                            const int32_t* __restrict__ batch_first,
-                                                            const int32_t* __restrict__ nbat,
-                                                            const int32_t* __restrict__ near_off,
-                                                            const int32_t* __restrict__ near_cnt,
-                                                            const int2* __restrict__ near_list, int64_t near_cap,
-                                                            const float4* __restrict__ src32,
-                                                            const double* __restrict__ V, double mult,
-                                                            double* __restrict__ U) {
-    constexpr int kT = kNearTargets, kNW = kNearThreads / 32, kRPT = kNearRuns / kNearThreads;
-    static_assert(kT % 2 == 0 && kNearThreads % 32 == 0 && kNearRuns % kNearThreads == 0, "near kernel shape");
-    __shared__ float4 tile[kNearStreamTile];
+struct NearArgs {
+    Octree t;
+    const double4* tgt_sorted;
+    int64_t n_tgt;
+    const int32_t* tperm;
+    const int32_t* batch_first;
+    const int32_t* nbat;
+    const int32_t* near_off;
+    const int32_t* near_cnt;
+    const int2* near_list;
+    int64_t near_cap;
+    const float4* src32;
+    const double* V;
+    double mult;
+    double* U;
+    const int32_t* order;  // batches in decreasing order of near work
+    int32_t* ticket;       // zeroed before the launch
+};
+
+// Persistent: every block takes batches from the ticket in `order` until none is left; one batch at a time
+// through the body below.
+// Tile shape: KT targets per thread (kBatch / KT threads) and KTILE sources staged in shared memory per
+// tile; instances for KT in {2, 4} and KTILE in {256, 512, 1024} are chosen at run time.
+template <bool kScalar, int KT, int KTILE>
+__global__ void __launch_bounds__(kBatch / KT) near_kernel(NearArgs A) {
+    constexpr int kT = KT, kThreads = kBatch / KT, kNW = kThreads / 32, kRPT = kNearRuns / kThreads;
+    static_assert(kT % 2 == 0 && kThreads % 32 == 0 && kNearRuns % kThreads == 0, "near kernel shape");
+    __shared__ __align__(16) float4 tile[2][KTILE];  // double-buffered: tile p + 1 arrives while p is summed
     __shared__ int r_start[kNearRuns], r_pre[kNearRuns + 1];
     __shared__ int warp_tot[kNW];
-    const int64_t b = blockIdx.x;
-    if (b >= *nbat) return;  // uniform per block
+    __shared__ int slot;
+    const Octree& t = A.t;
+    const double4* __restrict__ tgt_sorted = A.tgt_sorted;
+    const int32_t* __restrict__ batch_first = A.batch_first;
+    const int32_t* __restrict__ near_off = A.near_off;
+    const int32_t* __restrict__ near_cnt = A.near_cnt;
+    const int2* __restrict__ near_list = A.near_list;
+    const float4* __restrict__ src32 = A.src32;
+    const int64_t near_cap = A.near_cap;
+    const int nbat = *A.nbat;
+    for (int64_t b = next_batch(A.ticket, A.order, nbat, &slot); b >= 0; b = next_batch(A.ticket, A.order, nbat, &slot)) {
     const int64_t qe = batch_first[b + 1];
-    // targets i, i + kNearThreads, ... of the batch
+    // warp w holds targets 32 kT w .. 32 kT (w + 1) - 1 of the batch (lane l: 32 kT w + l + 32 u), so a warp
+    // past the batch's last target skips the arithmetic as a whole
+    const int64_t qw = batch_first[b] + 32 * kT * (threadIdx.x >> 5) + (threadIdx.x & 31);
+    const bool live = batch_first[b] + 32 * kT * (int64_t)(threadIdx.x >> 5) < qe;  // warp-uniform
     float tx[kT], ty[kT], tz[kT];
     double D[kT][3];
 #pragma unroll
     for (int u = 0; u < kT; ++u) {
-        const int64_t q = batch_first[b] + threadIdx.x + u * kNearThreads;
+        const int64_t q = qw + 32 * u;
         const double4 x = q < qe ? tgt_sorted[q] : make_double4(2, 2, 2, 0);
         tx[u] = (float)x.x;
         ty[u] = (float)x.y;
@@ -1639,34 +1738,67 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(Octree t, const doub
         }
         if (threadIdx.x == 0) r_pre[kNearRuns] = total;
         __syncthreads();
-        for (int p0 = 0; p0 < total; p0 += kNearStreamTile) {
-            const int m = min(kNearStreamTile, total - p0);
-            if (p0 > 0) __syncthreads();
-            for (int j = threadIdx.x; j < m; j += kNearThreads) {
+        // the sources of positions p0 .. p0 + KTILE - 1 of the chunk's stream go to tile[buf] by asynchronous
+        // copies (the run holding position p found by binary search of the prefix offsets)
+        auto stage = [&](int p0, int buf) {
+            const int m = min(KTILE, total - p0);
+            int lo = 0;
+            for (int j = threadIdx.x; j < m; j += kThreads) {
                 const int p = p0 + j;
-                int lo = 0, hi = kNearRuns;  // last run r with r_pre[r] <= p
+                int hi = kNearRuns;  // last run r with r_pre[r] <= p (positions grow: search from the last one)
                 while (hi - lo > 1) {
                     const int mid = (lo + hi) >> 1;
                     if (r_pre[mid] <= p) lo = mid;
                     else hi = mid;
                 }
-                tile[j] = src32[r_start[lo] + (p - r_pre[lo])];
+                cp_async16(&tile[buf][j], src32 + r_start[lo] + (p - r_pre[lo]));
             }
-            __syncthreads();
-            if constexpr (kScalar)
-                near_tile_scalar<kT / 2>(tile, m, tx, ty, tz, D);
-            else
-                near_tile<kT / 2>(tile, m, tx, ty, tz, D);
+        };
+        int buf = 0;
+        if (total > 0) stage(0, 0);
+        cp_async_commit();
+        for (int p0 = 0; p0 < total; p0 += KTILE, buf ^= 1) {
+            const int m = min(KTILE, total - p0);
+            if (p0 + KTILE < total) stage(p0 + KTILE, buf ^ 1);
+            cp_async_commit();
+            cp_async_wait_prev();  // this thread's copies into tile[buf] have landed
+            __syncthreads();       // ... and every other thread's
+            if (live) {
+                if constexpr (kScalar)
+                    near_tile_scalar<kT / 2>(tile[buf], m, tx, ty, tz, D);
+                else
+                    near_tile<kT / 2>(tile[buf], m, tx, ty, tz, D);
+            }
+            __syncthreads();  // tile[buf] is read before the next stage refills it
         }
     }
 #pragma unroll
     for (int u = 0; u < kT; ++u) {
-        const int64_t q = batch_first[b] + threadIdx.x + u * kNearThreads;
+        const int64_t q = qw + 32 * u;
         if constexpr (kScalar)
-            finish_target_scalar(q, qe, D[u], tperm, V, mult, U);
+            finish_target_scalar(q, qe, D[u], A.tperm, A.V, A.mult, A.U);
         else if (q < qe)
-            finish_target(q, qe, n_tgt, tgt_sorted[q], D[u], tperm, V, mult, U);  // FP64 position re-read
+            finish_target(q, qe, A.n_tgt, tgt_sorted[q], D[u], A.tperm, A.V, A.mult, A.U);  // FP64 position re-read
     }
+    }
+}
+
+typedef void (*NearFn)(NearArgs);
+
+// The near kernel of a tile shape (targets per thread 2 or 4; staged sources 256, 512 or 1024) and its
+// block size; nullptr for another shape.
+NearFn near_select(bool scalar, int targets, int tile, int* threads) {
+    *threads = kBatch / targets;
+#define LPM_NEAR_CASE(T, TILE)                                                              \
+    if (targets == T && tile == TILE) return scalar ? near_kernel<true, T, TILE> : near_kernel<false, T, TILE>;
+    LPM_NEAR_CASE(2, 256)
+    LPM_NEAR_CASE(2, 512)
+    LPM_NEAR_CASE(2, 1024)
+    LPM_NEAR_CASE(4, 256)
+    LPM_NEAR_CASE(4, 512)
+    LPM_NEAR_CASE(4, 1024)
+#undef LPM_NEAR_CASE
+    return nullptr;
 }
 
 // host-side tables --------------------------------------------------------------------------------
@@ -1755,6 +1887,16 @@ struct TreeSolver {
     __nv_bfloat16* mlp_w = nullptr;
     float* mlp_norm = nullptr;
     uint8_t* decisions = nullptr;  // selector decisions of the count pass, reused by the fill pass
+    // batch schedules of the persistent near and far kernels
+    uint32_t* near_work = nullptr;    // per batch: near-field pairs (count pass)
+    uint32_t* far_work = nullptr;     // per batch: far coefficient evaluations (count pass)
+    int32_t* sched_order = nullptr;   // batches by decreasing near work
+    int32_t* far_order = nullptr;     // batches by decreasing far work
+    int32_t* sched_aux = nullptr;     // kAux* layout below
+    int near_blocks = 1;              // persistent grids: resident blocks on the whole device
+    int near_targets = kNearTargets;  // near kernel tile shape (run-time "near_targets", "near_tile")
+    int near_tile = kNearStreamTile;
+    int far_blocks[kPMax + 1][2] = {};  // per order, FP32 / FP64 far kernel
     std::vector<void*> allocs;
 };
 
@@ -1844,6 +1986,23 @@ int upload_constants() {
 }
 
 }  // namespace
+
+// Select the near kernel's tile shape and size its persistent grid (resident blocks on the device).
+static int near_shape(TreeSolver* t, int targets, int tile) {
+    int threads = 0;
+    NearFn fn = near_select(t->scalar, targets, tile, &threads);
+    if (!fn) {
+        set_error("tree solver: near_targets must be 2 or 4 and near_tile 256, 512 or 1024");
+        return LPM_ERR_ARG;
+    }
+    int per_sm = 0;
+    LPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0));
+    t->near_targets = targets;
+    t->near_tile = tile;
+    t->near_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(t->n_batches,
+                                                                  (int64_t)std::max(per_sm, 1) * t->ctx->num_sms));
+    return LPM_OK;
+}
 
 int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_solver_desc& solver, int64_t n_src,
                        int64_t n_tgt, TreeSolver** out) {
@@ -1976,6 +2135,11 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->near_off, (size_t)t->n_batches + 1));
     A(talloc(t, &t->flags, 8));
     A(talloc(t, &t->root_r, 1));
+    A(talloc(t, &t->near_work, (size_t)t->n_batches + 1));
+    A(talloc(t, &t->far_work, (size_t)t->n_batches + 1));
+    A(talloc(t, &t->sched_order, (size_t)t->n_batches + 1));
+    A(talloc(t, &t->far_order, (size_t)t->n_batches + 1));
+    A(talloc(t, &t->sched_aux, kAuxInts));
     A(talloc(t, &t->pair_counts, 3));
     A(talloc(t, &t->V, 3 * ntg));
     if (t->learned) {
@@ -2006,6 +2170,31 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
         if (ea != cudaSuccess) {
             tree_solver_destroy(t);
             return cuda_status(ea, "cudaFuncSetAttribute (far_kernel)");
+        }
+        rc = near_shape(t, t->near_targets, t->near_tile);
+        if (rc) {
+            tree_solver_destroy(t);
+            return rc;
+        }
+        int per_sm = 0;
+        for (int P = 1; P <= kPMax && ea == cudaSuccess; ++P)
+            for (int f64 = 0; f64 < 2 && ea == cudaSuccess; ++f64) {
+                size_t smem = 0;
+                int threads = 0;
+                per_sm = 0;
+                if (scalar) {
+                    FarScalarFn fs = far_scalar_select(P, f64 != 0, &smem, &threads);
+                    ea = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs, threads, smem);
+                } else {
+                    FarKernelFn fn = far_kernel_select(P, f64 != 0, &smem, &threads);
+                    ea = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+                }
+                t->far_blocks[P][f64] = (int)std::max<int64_t>(
+                    1, std::min<int64_t>(t->n_batches, (int64_t)std::max(per_sm, 1) * ctx->num_sms));
+            }
+        if (ea != cudaSuccess) {
+            tree_solver_destroy(t);
+            return cuda_status(ea, "cudaOccupancyMaxActiveBlocksPerMultiprocessor (far kernels)");
         }
     }
     rc = alloc_lists(t, std::max<int64_t>(t->n_batches * 256, 1024), std::max<int64_t>(t->n_batches * 64, 1024));
@@ -2055,6 +2244,8 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     A.mlp_norm = t->mlp_norm;
     A.decisions = t->decisions;
     A.heavy_cap = t->heavy_cap;
+    A.near_work = t->near_work;
+    A.far_work = t->far_work;
     LPM_CUDA_TRY(cudaMemsetAsync(t->pair_counts, 0, 3 * sizeof(unsigned long long), ctx->stream));
     const unsigned g = grid_for(t->n_batches, 4);
     LPM_LAUNCH(ctx, "traverse_kernel", traverse_kernel, g, 128, 0, A);
@@ -2163,6 +2354,19 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     // far field: one launch per order present (only the fixed order, or the selector's orders 1..11),
     // each adding its bucket's contributions to V
     LPM_CUDA_TRY(cudaMemsetAsync(t->V, 0, 3 * (size_t)n_tgt * sizeof(double), ctx->stream));
+    // batch schedules: far and near work of every batch (from the traversal's count pass), bucketed in
+    // decreasing order; zeroed buckets, cursors and tickets first
+    LPM_CUDA_TRY(cudaMemsetAsync(t->sched_aux, 0, kAuxInts * sizeof(int32_t), ctx->stream));
+    const unsigned gsch = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(t->n_batches, 256),
+                                                                            2 * ctx->num_sms));
+    LPM_LAUNCH(ctx, "sched_hist_kernel", sched_hist_kernel, gsch, 256, 0, t->far_work, t->tcount + 1,
+               t->sched_aux + kAuxFarHist);
+    LPM_LAUNCH(ctx, "sched_scatter_kernel", sched_scatter_kernel, gsch, 256, 0, t->far_work, t->tcount + 1,
+               t->sched_aux + kAuxFarHist, t->sched_aux + kAuxFarCur, t->far_order);
+    LPM_LAUNCH(ctx, "sched_hist_kernel", sched_hist_kernel, gsch, 256, 0, t->near_work, t->tcount + 1,
+               t->sched_aux + kAuxNearHist);
+    LPM_LAUNCH(ctx, "sched_scatter_kernel", sched_scatter_kernel, gsch, 256, 0, t->near_work, t->tcount + 1,
+               t->sched_aux + kAuxNearHist, t->sched_aux + kAuxNearCur, t->sched_order);
     {
         const int64_t nb1 = t->n_batches + 1;
         const bool sel = t->learned && t->mlp_loaded;
@@ -2183,28 +2387,47 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
             F.n_ent = t->n_ent;
             F.gtab = t->gtab + t->ct.table_off[P];
             F.V = t->V;
+            F.order = t->far_order;
+            F.ticket = t->sched_aux + kAuxFarTicket + P;
             size_t smem = 0;
+            const bool f64 = P >= t->f64_from;
+            const unsigned grid = (unsigned)t->far_blocks[P][f64 ? 1 : 0];
             if (t->scalar) {
                 F.B64 = (const double4*)t->A64;
                 F.B32 = (const float4*)t->A32;
                 int threads = 0;
-                FarScalarFn fs = far_scalar_select(P, P >= t->f64_from, &smem, &threads);
-                LPM_LAUNCH(ctx, "far_kernel", fs, (unsigned)t->n_batches, threads, smem, F, t->a_stride);
+                FarScalarFn fs = far_scalar_select(P, f64, &smem, &threads);
+                LPM_LAUNCH(ctx, "far_kernel", fs, grid, threads, smem, F, t->a_stride);
             } else {
                 int threads = 0;
-                FarKernelFn fn = far_kernel_select(P, P >= t->f64_from, &smem, &threads);
-                LPM_LAUNCH(ctx, "far_kernel", fn, (unsigned)t->n_batches, threads, smem, F);
+                FarKernelFn fn = far_kernel_select(P, f64, &smem, &threads);
+                LPM_LAUNCH(ctx, "far_kernel", fn, grid, threads, smem, F);
             }
         }
     }
-    if (t->scalar)
-        LPM_LAUNCH(ctx, "near_kernel", near_kernel<true>, (unsigned)t->n_batches, kNearThreads, 0, t->st, t->tgt_sorted,
-                   n_tgt, t->tperm, t->batch_first, t->tcount + 1, t->near_off, t->near_cnt, t->near_list, t->near_cap,
-                   t->src32, t->V, 1.0 / (4.0 * kPi), U);
-    else
-        LPM_LAUNCH(ctx, "near_kernel", near_kernel<false>, (unsigned)t->n_batches, kNearThreads, 0, t->st,
-                   t->tgt_sorted, n_tgt, t->tperm, t->batch_first, t->tcount + 1, t->near_off, t->near_cnt,
-                   t->near_list, t->near_cap, t->src32, t->V, -1.0 / (4.0 * kPi * t->kernel.radius), U);
+    // near field: batches by decreasing near work, taken by a persistent grid
+    {
+        NearArgs N{};
+        N.t = t->st;
+        N.tgt_sorted = t->tgt_sorted;
+        N.n_tgt = n_tgt;
+        N.tperm = t->tperm;
+        N.batch_first = t->batch_first;
+        N.nbat = t->tcount + 1;
+        N.near_off = t->near_off;
+        N.near_cnt = t->near_cnt;
+        N.near_list = t->near_list;
+        N.near_cap = t->near_cap;
+        N.src32 = t->src32;
+        N.V = t->V;
+        N.U = U;
+        N.order = t->sched_order;
+        N.ticket = t->sched_aux + kAuxNearTicket;
+        N.mult = t->scalar ? 1.0 / (4.0 * kPi) : -1.0 / (4.0 * kPi * t->kernel.radius);
+        int threads = 0;
+        NearFn fn = near_select(t->scalar, t->near_targets, t->near_tile, &threads);
+        LPM_LAUNCH(ctx, "near_kernel", fn, (unsigned)t->near_blocks, threads, 0, N);
+    }
     if (can_sync) return tree_check(t);
     return LPM_OK;
 }
@@ -2281,6 +2504,8 @@ int tree_get_param(const TreeSolver* t, const char* name, double* value) {
     else if (n == "order_bias") *value = t->order_bias;
     else if (n == "batch_level") *value = t->batch_level;
     else if (n == "batch_level_max") *value = t->batch_level_max;
+    else if (n == "near_targets") *value = t->near_targets;
+    else if (n == "near_tile") *value = t->near_tile;
     else if (n == "root_maxr") *value = t->root_maxr;
     else if (n == "root_first") *value = (double)t->root_first;
     else if (n == "order") *value = t->order;
@@ -2307,6 +2532,10 @@ int tree_set_param(TreeSolver* t, const char* name, double value) {
             return LPM_ERR_ARG;
         }
         t->order_bias = (int)value;
+    } else if (n == "near_targets" && (value == 2.0 || value == 4.0)) {
+        return near_shape(t, (int)value, t->near_tile);
+    } else if (n == "near_tile" && (value == 256.0 || value == 512.0 || value == 1024.0)) {
+        return near_shape(t, t->near_targets, (int)value);
     } else if (n == "root_maxr" && value >= 0.0 && std::isfinite(value)) {
         t->root_maxr = value;
     } else if (n == "root_first" && value >= 0.0 && value <= (double)t->n_tgt && value == std::floor(value)) {

@@ -8,6 +8,8 @@
  *   direct KIND LEVEL DELTA ZETA.bin OUTDIR          DirectSum(pmesh, BiotSavartSphere(DELTA)).meshSolve
  *   tree   KIND LEVEL ORDER LEAF THETA ZETA.bin OUTDIR TreeSum(ORDER, LEAF, pmesh, kernel).meshSolve(THETA)
  *   poisson N XYZQ.bin OUTDIR                          DirectSum(particles, PoissonGreensFn3d).meshfreeSolve
+ *   ptree N XYZ.bin LEAF                               TreeSum(coords, 8, LEAF, 0): the meshfree constructor's
+ *                                                      tree (prints its node count and depth)
  *   scalar KIND LEVEL KERNEL PARAM ZETA.bin OUTDIR     DirectSum(pmesh, ScalarKernel).meshSolve with the reference's
  *                                                      SphereGreensFn(PARAM) | PlanarGreensFnFreeBoundaries |
  *                                                      SecondOrderDelta3d(PARAM) | SphereDelta(PARAM)
@@ -156,6 +158,14 @@ int main(int argc, char** argv) {
             for (long i = 0; i < n; ++i) out[i] = phi->getScalar(i);
             write_f64(std::string(argv[4]) + "/potential.bin", out);
             std::printf("{\"cmd\": \"poisson\", \"n\": %ld}\n", n);
+        } else if (cmd == "ptree" && argc == 5) {
+            const long n = std::atol(argv[2]);
+            const std::vector<double> p = read_f64(argv[3]);
+            if ((long)p.size() != 3 * n) throw std::runtime_error("XYZ.bin must hold N x 3 values");
+            auto crds = std::make_shared<EuclideanCoords>(n, CARTESIAN_3D_GEOMETRY);
+            for (long i = 0; i < n; ++i) crds->insert(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
+            TreeSum ts(crds, 8, std::atoi(argv[4]), 0.0);
+            std::printf("{\"cmd\": \"ptree\", \"n_nodes\": %ld, \"depth\": %d}\n", (long)ts.nNodes(), ts.depth());
         } else {
             std::fprintf(stderr, "usage: see the header of dropin_driver.cpp\n");
             MPI_Finalize();

@@ -22,6 +22,7 @@
  *   vtktime  KIND LEVEL OUTDIR                     times writeToVtkFile of the mesh with vorticity (rh) and a zero
  *                                                  velocity field (no solve) -> OUTDIR/mesh.vtk
  *   poisson  NPTS SEED OUTDIR                      DirectSum::meshfreeSolve (src/LpmDirectSum.cpp:240-252)
+ *   time_poisson NPTS SEED [REPS]                  the same on this rank's slice, timed (CPU baseline)
  *                                                  with a 1/(4 pi r) ScalarKernel subclass
  *   pointtree NPTS SEED MAXLEAF OUTDIR             TreeSum(coords,...) meshfree ctor (src/LpmTreeSum.cpp:208-219)
  * KIND is icos|cube.  ZETA is rh (2z - sphereHarmonic54, the Rossby-Haurwitz m=4 wave with
@@ -258,7 +259,7 @@ static uint64_t splitmix64(uint64_t& s) {
 static double uniform_pm1(uint64_t& s) { return 2.0 * ((splitmix64(s) >> 11) * (1.0 / 9007199254740992.0)) - 1.0; }
 
 static int usage() {
-    fprintf(stderr, "usage: ref_harness mesh|direct|scalar|vtk|tree|treesum|poisson|pointtree ...\n");
+    fprintf(stderr, "usage: ref_harness mesh|direct|scalar|vtk|tree|treesum|poisson|time_poisson|pointtree ...\n");
     return 2;
 }
 
@@ -454,6 +455,37 @@ int main(int argc, char** argv) {
             npy_f64(out, "charge", qv);
             npy_f64(out, "potential", pv);
             printf("{\"cmd\": \"poisson\", \"seconds\": %.6f}\n", secs);
+        } else if (cmd == "time_poisson" && (argc == 4 || argc == 5)) {
+            // times DirectSum::meshfreeSolve (1/(4 pi r) kernel) on this rank's MPIReplicatedData slice of
+            // the NPTS-point splitmix64 cube, REPS times (no output files): the 3D Poisson CPU baseline
+            const index_type n = atol(argv[2]);
+            uint64_t s = strtoull(argv[3], nullptr, 0);
+            const int reps = argc == 5 ? atoi(argv[4]) : 1;
+            auto crds = std::make_shared<EuclideanCoords>(n, CARTESIAN_3D_GEOMETRY);
+            auto q = std::make_shared<Field>(n, 1, "charge", "n/a");
+            auto phi = std::make_shared<Field>(n, 1, "potential", "n/a");
+            for (index_type i = 0; i < n; ++i) {
+                const double x = uniform_pm1(s), y = uniform_pm1(s), z = uniform_pm1(s);
+                crds->insert(x, y, z);
+                const double c = uniform_pm1(s);
+                q->insert(c);
+                phi->insert(0.0);
+            }
+            auto parts = std::make_shared<Particles>(crds, nullptr,
+                                                     std::vector<std::shared_ptr<Field>>{q, phi}, rank);
+            std::shared_ptr<ScalarKernel> kernel(new Poisson3dKernel());
+            DirectSum solver(parts, kernel, "potential", "charge");
+            MPIReplicatedData mp(n, rank, size);
+            std::string secs = "[";
+            for (int r = 0; r < reps; ++r) {
+                const auto t0 = std::chrono::steady_clock::now();
+                solver.meshfreeSolve(mp);
+                const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                secs += (r ? ", " : "") + std::to_string(t);
+            }
+            secs += "]";
+            printf("{\"cmd\": \"time_poisson\", \"rank\": %d, \"size\": %d, \"seconds\": %s, \"targets\": %ld, "
+                   "\"sources\": %ld}\n", rank, size, secs.c_str(), (long)mp.msgSize(rank), (long)n);
         } else if (cmd == "pointtree" && argc == 6) {
             const index_type n = atol(argv[2]);
             uint64_t s = strtoull(argv[3], nullptr, 0);

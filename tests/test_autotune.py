@@ -5,7 +5,7 @@ import pytest
 
 import lpmcxx_b200 as L
 import lpmcxx_b200.workloads as W
-from lpmcxx_b200.autotune import autotune, default_grid, tuned_solver
+from lpmcxx_b200.autotune import apply_tuned, autotune, default_grid, tuned_solver
 
 
 def test_default_grids():
@@ -31,11 +31,15 @@ def test_autotune_learned_sphere(ctx):
                    grid=((128, 256), (0.5, 0.6), (1e-8, 3e-8, 3e-7)), sample=2048, order_biases=(0, 2))
     check(res, tol)
     assert {c.bias for c in res.tried} == {0, 2}
+    # the near-field tile shape is searched too: every shape was timed on the best setting, and the pick is
+    # the fastest qualifying one among them
+    shapes = {(c.near_targets, c.near_tile) for c in res.tried}
+    assert shapes == {(2, 256), (2, 512), (2, 1024), (4, 256), (4, 512), (4, 1024)}
     # the tuned descriptor reproduces the accuracy on all targets
     ts = L.TreeSum(ctx, L.biot_savart_kernel(), tuned_solver(res), n_src, p.shape[0])
     ts.set_mlp(L.learned.load()[0])
-    ts.set_param("batch_level", res.best.batch_level)
-    ts.set_param("order_bias", res.best.bias)
+    apply_tuned(res, ts)
+    assert (ts.get_param("near_targets"), ts.get_param("near_tile")) == (res.best.near_targets, res.best.near_tile)
     out = torch.empty((3, p.shape[0]), dtype=torch.float64, device="cuda")
     ts.eval(d[:n_src], d, out)
     ts.close()

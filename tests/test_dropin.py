@@ -114,3 +114,43 @@ def test_dropin_treesum_node_count_matches_reference_tree():
         out = json.loads(run("tree", "icos", 4, 6, 64, 0.5, f"{d}/zeta.bin", d).strip().splitlines()[-1])
     assert out["n_nodes"] == ref["node_level"].shape[0]
     assert out["depth"] == 0
+
+
+@pytest.mark.gpu
+@needs_driver
+def test_dropin_meshfree_treesum_node_count_matches_reference_tree():
+    """TreeSum(coords, ...) builds the reference's meshfree tree (Tree(coords) root, split while a node holds
+    more than the leaf capacity): its nNodes() is the reference tree's node count."""
+    ref = golden("pointtree_8000_m10.npz")
+    xyz = ref["xyz"]
+    with tempfile.TemporaryDirectory() as d:
+        xyz.astype("<f8").tofile(f"{d}/xyz.bin")
+        out = json.loads(run("ptree", xyz.shape[0], f"{d}/xyz.bin", 10).strip().splitlines()[-1])
+    assert out["n_nodes"] == ref["node_level"].shape[0]
+    assert out["depth"] == 0
+
+
+@pytest.mark.gpu
+@needs_driver
+def test_dropin_treesum_fp64_far_field_switch(ctx):
+    """LPM_B200_PRECISION=f64 evaluates the drop-in TreeSum's far expansions in FP64: its output is the host
+    API's FP64-far-field treecode (lpm_tree_sum_mesh with LPM_PREC_F64) on the same mesh and field, and
+    differs from the FP32 far field's."""
+    import lpmcxx_b200 as L
+
+    g = golden("direct_icos4_rh.npz")
+    out = {}
+    for prec in ("f32", "f64"):
+        with tempfile.TemporaryDirectory() as d:
+            g["face_zeta"].astype("<f8").tofile(f"{d}/zeta.bin")
+            env = dict(os.environ, LPM_B200_PRECISION=prec, LPM_MESH_SEED_DIR=str(DRIVER.parent / "meshSeeds"))
+            r = subprocess.run([str(DRIVER), "tree", "icos", "4", "8", "32", "0.5", f"{d}/zeta.bin", d],
+                               capture_output=True, text=True, env=env, timeout=600)
+            assert r.returncode == 0, r.stderr
+            out[prec] = np.fromfile(f"{d}/vert_vel.bin").reshape(-1, 3)
+    mesh = L.build_mesh("icos", 4)
+    vo, _, _ = L.tree_sum_mesh(ctx, L.biot_savart_kernel(), L.tree_solver(L.LPM_PREC_F64, 8, 32, 0.5), mesh,
+                               g["face_zeta"])
+    assert rel_linf(out["f64"], vo.T) < 1e-13
+    assert np.abs(out["f64"] - out["f32"]).max() > 0.0
+    assert rel_l2(out["f64"], g["vert_vel"]) < 1e-3

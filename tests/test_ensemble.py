@@ -44,3 +44,74 @@ def test_ensemble_matches_single_instances(ctx, learned):
         want = rk.get_state()
         rk.close()
         assert np.array_equal(got[i], want), i
+
+
+@pytest.mark.gpu
+def test_ensemble_instances_track_fp64_direct_rk4(ctx):
+    """Every instance of a learned-treecode ensemble (the ensemble workload's RH wave + seeded Gaussian, icos
+    L3..L5, headline selector setting) stays within the treecode's error budget of the FP64 direct-sum RK4
+    run of the same instance: after 3 graph-replayed steps of dt 0.01 the displacement X_3 - X_0 differs from
+    the FP64 direct sum's by at most 5e-6 relative (L2 over the instance), and the velocity at the final
+    state by at most 2e-6 relative."""
+    import torch
+
+    inst = W.ensemble_instances(levels=(3, 4, 5), per_level=2, seed=77)
+    solver = L.tree_solver(L.LPM_PREC_F32, 10, 128, 0.5, learned=True, tolerance=5e-7)
+    ens = L.Ensemble(ctx, L.biot_savart_kernel(), solver, [n for _, _, n in inst], [p.shape[0] for _, p, _ in inst],
+                     lanes=3)
+    ens.set_mlp(L.learned.load()[0])
+    ens.set_param("order_bias", 2)
+    for i, (_, p, _) in enumerate(inst):
+        ens.instance(i).set_state(p)
+    ens.step(0.01, 3, use_graph=True)
+    torch.cuda.synchronize()
+    for i, (_, p, n_src) in enumerate(inst):
+        rki = ens.instance(i)
+        got = rki.get_state()
+        u_tree = torch.empty((3, p.shape[0]), dtype=torch.float64, device="cuda")
+        rki.velocity(u_tree)
+        torch.cuda.synchronize()
+        rk = L.RK4(ctx, L.biot_savart_kernel(), L.direct_solver(L.LPM_PREC_F64), n_src, p.shape[0])
+        rk.set_state(p)
+        rk.step(0.01, 3, use_graph=False)
+        want = rk.get_state()
+        rk.set_state(got)
+        u64 = torch.empty_like(u_tree)
+        rk.velocity(u64)
+        torch.cuda.synchronize()
+        rk.close()
+        disp_err = np.linalg.norm(got[:, :3] - want[:, :3]) / np.linalg.norm(want[:, :3] - p[:, :3])
+        vel_err = float(torch.linalg.norm(u_tree - u64) / torch.linalg.norm(u64))
+        assert disp_err < 5e-6, (i, disp_err)
+        assert vel_err < 2e-6, (i, vel_err)
+        assert np.array_equal(got[:, 3], p[:, 3])  # strengths are carried unchanged
+
+
+@pytest.mark.gpu
+def test_ensemble_set_param_between_graph_steps_takes_effect(ctx):
+    """Changing an instance's parameter after the ensemble's step graph exists drops that graph: the next
+    steps use the new value, as an uncaptured run of the same instances does."""
+    inst = W.ensemble_instances(levels=(3, 4), per_level=1, seed=5)
+    solver = L.tree_solver(L.LPM_PREC_F32, 10, 128, 0.5, learned=True, tolerance=5e-7)
+    params = L.learned.load()[0]
+    ens = L.Ensemble(ctx, L.biot_savart_kernel(), solver, [n for _, _, n in inst], [p.shape[0] for _, p, _ in inst],
+                     lanes=2)
+    ens.set_mlp(params)
+    for i, (_, p, _) in enumerate(inst):
+        ens.instance(i).set_state(p)
+    ens.step(0.01, 2, use_graph=True)   # warm-up step + one graph replay
+    ens.instance(1).set_param("order_bias", 3)
+    ens.instance(0).set_param("theta", 0.4)
+    ens.step(0.01, 2, use_graph=True)
+    got = [ens.instance(i).get_state() for i in range(len(inst))]
+    ens.close()
+    for i, (_, p, n_src) in enumerate(inst):
+        rk = L.RK4(ctx, L.biot_savart_kernel(), solver, n_src, p.shape[0])
+        rk.set_mlp(params)
+        rk.set_state(p)
+        rk.step(0.01, 2, use_graph=False)
+        rk.set_param("order_bias" if i == 1 else "theta", 3 if i == 1 else 0.4)
+        rk.step(0.01, 2, use_graph=False)
+        want = rk.get_state()
+        rk.close()
+        assert np.array_equal(got[i], want), i
