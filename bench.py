@@ -118,11 +118,13 @@ def reference_harness() -> Path | None:
     return p if p.exists() else None
 
 
-def time_reference_direct(reps: int, procs: int, targets_per_proc: int = 3) -> dict:
-    """The reference's DirectSum::meshSolve on icos L8 (Gaussian vortex), `procs` processes each timing a
-    MPIReplicatedData slice of ~targets_per_proc vertex targets, `reps` times.  Returns per-rep pair rates."""
+def time_reference_direct(reps: int, procs: int, targets_per_proc: int = 3, kind: str = "icos",
+                          level: int = LEVEL) -> dict:
+    """The reference's DirectSum::meshSolve on a `kind` level-`level` mesh (Gaussian vortex), `procs` processes
+    each timing a MPIReplicatedData slice of ~targets_per_proc vertex targets, `reps` times.  Returns per-rep
+    pair rates."""
     exe = reference_harness()
-    n_verts = 2 + 10 * 4 ** LEVEL
+    n_verts = 2 + (10 if kind == "icos" else 6) * 4 ** level
     size = max(procs, n_verts // targets_per_proc)
     env = dict(os.environ)
     env["LPM_MESH_SEED_DIR"] = str(ROOT / "oracle" / "_ref" / "meshSeeds")
@@ -131,7 +133,7 @@ def time_reference_direct(reps: int, procs: int, targets_per_proc: int = 3) -> d
     for r in range(procs):
         e = dict(env)
         e["LPM_STUB_RANK"] = str(r)
-        jobs.append(subprocess.Popen([str(exe), "time_direct", "icos", str(LEVEL), "gauss", str(reps)],
+        jobs.append(subprocess.Popen([str(exe), "time_direct", kind, str(level), "gauss", str(reps)],
                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, env=e))
     results = []
     for j in jobs:
@@ -387,6 +389,111 @@ def run_gpu_poisson(args) -> None:
     if env_int("RANK", 0) == 0 and world == 1 and not args.no_cpu_baseline:
         out_line["cpu_baseline"] = poisson_cpu_baseline(n)
     print(json.dumps(out_line))
+
+
+CUBE_METRIC = "direct-sum RK4 steps/s, cubed sphere L8 (393,216 sources), FP32 (FP64-accumulated) and FP64"
+
+
+def run_gpu_direct_cube(args) -> None:
+    """The at-scale direct-sum configuration: cubed sphere refined 8 levels (393,216 face sources + 393,218
+    vertices), Gaussian vortex, RK4 steps of dt = 0.005 by the FP32 direct sum (the line's value) and the FP64
+    one; K timed steps each after the warm-up, then the two trajectories compared."""
+    import torch
+
+    import lpmcxx_b200 as L
+    import lpmcxx_b200.workloads as W
+
+    local = env_int("LOCAL_RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    torch.cuda.set_device(local)
+    _, p, n_src = W.gaussian_vortex_mesh("cube", 8)
+    n = p.shape[0]
+    ctx = L.Context(local)
+    stream = torch.cuda.Stream()
+    kern = L.biot_savart_kernel()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    res = {}
+    with torch.cuda.stream(stream):
+        ctx.use_torch_stream()
+        state0 = torch.tensor(p, device="cuda")
+        for prec in (L.LPM_PREC_F32, L.LPM_PREC_F64):
+            rk = L.RK4(ctx, kern, L.direct_solver(prec), n_src, n)
+            rk.set_state(state0)
+            rk.step(0.005, args.warmup, use_graph=True)
+            rk.set_state(state0)
+            rk.step(0.005, 1, use_graph=True)
+            rk.set_state(state0)
+            torch.cuda.synchronize()
+            launches0 = ctx.launch_count
+            ms = []
+            clocks = ClockSampler(local).start() if prec == L.LPM_PREC_F32 else None
+            for _ in range(args.steps):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                rk.step(0.005, 1, use_graph=True)
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            clk = clocks.stop() if clocks else None
+            final = rk.get_state()
+            ctx.set_profiling(True)
+            u = torch.empty((3, n), dtype=torch.float64, device="cuda")
+            rk.velocity(u)
+            prof = ctx.profile_report()
+            ctx.set_profiling(False)
+            res[prec] = {"ms": ms, "final": final, "prof": prof, "clk": clk, "launches": ctx.launch_count - launches0}
+            if prec == L.LPM_PREC_F32:  # end to end through the host API: pinned state in, one step, state out
+                host_in = torch.tensor(p).pin_memory()
+                host_out = torch.empty_like(host_in).pin_memory()
+                e2e_s = []
+                for _ in range(min(args.steps, 3)):
+                    t0 = time.perf_counter()
+                    rk.set_state(host_in)
+                    rk.step(0.005, 1, use_graph=True)
+                    rk.get_state(host_out)
+                    e2e_s.append(time.perf_counter() - t0)
+            rk.close()
+        fp32_peak = ctx.fma_peak_tflops(L.LPM_PREC_F32)
+        fp64_peak = ctx.fma_peak_tflops(L.LPM_PREC_F64)
+    r32, r64 = res[L.LPM_PREC_F32], res[L.LPM_PREC_F64]
+    d32 = r32["final"][:, :3] - p[:, :3]
+    d64 = r64["final"][:, :3] - p[:, :3]
+    pairs = float(n_src) * float(n)
+    k32 = r32["prof"]["bs_f32_kernel"]["ms"]
+    k64 = r64["prof"]["bs_f64_kernel"]["ms"]
+    value = world * args.steps / (sum(r32["ms"]) * 1e-3)
+    tf32 = FLOPS_PER_BS_PAIR * pairs / (k32 * 1e-3) * 1e-12
+    out = {
+        "metric": CUBE_METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": float(np.mean(r32["ms"])), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"cube L8 Gaussian vortex: {n_src:,} face-centroid sources + {n - n_src:,} vertices, "
+                               "RK4 dt=0.005", "solver": "FP32 direct sum, FP64 accumulation across tiles",
+                   "l2": "flushed (256 MiB write) before every timed step", "graph": "one CUDA graph replay per step"},
+        "fp64_direct_steps_per_s": world * args.steps / (sum(r64["ms"]) * 1e-3),
+        "rel_displacement_fp32_vs_fp64": float(np.linalg.norm(d32 - d64) / np.linalg.norm(d64)),
+        "displacement_steps": args.warmup + 1 + args.steps,
+        "roofline": {"bound": "fp32", "kernel": "bs_f32_kernel", "achieved": tf32, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": tf32 / fp32_peak, "traffic": profile_summary_traffic("bs_f32_kernel"),
+                     "peak_source": "measured FMA microbenchmark (lpm_fma_peak) on this GPU"},
+        "fp64_kernel": {"kernel": "bs_f64_kernel", "tflops": FLOPS_PER_BS_PAIR * pairs / (k64 * 1e-3) * 1e-12,
+                        "peak_tflops": fp64_peak},
+        "e2e": {"value": world / float(np.mean(e2e_s)), "unit": "steps/s", "h2d_bytes_per_step": n * 32,
+                "d2h_bytes_per_step": n * 32},
+        "gpu_launches": r32["launches"], "clocks": r32["clk"],
+    }
+    if env_int("RANK", 0) == 0 and world == 1 and not args.no_cpu_baseline and reference_harness() is not None:
+        procs = max(1, min(os.cpu_count() or 1, 32))
+        r = time_reference_direct(2, procs, kind="cube", level=8)
+        pps = float(np.median([r["pairs_per_rep"] / t for t in r["rep_seconds"]]))
+        out["cpu_baseline"] = {"value": pps / (4.0 * pairs), "unit": "steps/s", "cores": procs, "kind": "reference",
+                               "sample": f"reference DirectSum::meshSolve (FP64), {procs} processes x "
+                                         f"MPIReplicatedData slice, {r['targets_per_rep']} targets x {r['n_src']} "
+                                         "sources per repetition, extrapolated to 4 evaluations of all targets",
+                               "pairs_per_s": pps}
+    print(json.dumps(out))
 
 
 ENSEMBLE_METRIC = "ensemble RK4 steps/s: 64 instances (icos L5/L6/L7/L8 x 16, 27.85M sources), learned treecode"
@@ -853,9 +960,10 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the extra keys of the headline line (FP32 direct-sum kernel, Poisson treecode)")
-    ap.add_argument("--workload", default="sphere_rk4", choices=["sphere_rk4", "poisson_cube", "ensemble"],
+    ap.add_argument("--workload", default="sphere_rk4",
+                    choices=["sphere_rk4", "poisson_cube", "ensemble", "direct_cube"],
                     help="sphere_rk4: the Biot-Savart RK4 headline; poisson_cube: the 3D Poisson treecode; "
-                         "ensemble: 64 uneven RK4 instances")
+                         "ensemble: 64 uneven RK4 instances; direct_cube: FP32 / FP64 direct-sum RK4 at cube L8")
     ap.add_argument("--lanes", type=int, default=8, help="ensemble: streams the instances are spread over")
     ap.add_argument("--points", type=int, default=1_048_576, help="poisson_cube: number of points")
     args = ap.parse_args()
@@ -867,6 +975,8 @@ def main() -> None:
         run_gpu_poisson(args)
     elif args.workload == "ensemble":
         run_gpu_ensemble(args)
+    elif args.workload == "direct_cube":
+        run_gpu_direct_cube(args)
     else:
         run_gpu(args)
 

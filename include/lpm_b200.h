@@ -37,7 +37,8 @@ extern "C" {
 #define LPM_ERR_KERNEL 2     /* unsupported kernel: the reference's "invalid kernel" logic_error */
 #define LPM_ERR_OOM 3        /* device or host allocation failed (std::bad_alloc) */
 #define LPM_ERR_CUDA 4       /* a CUDA runtime call failed */
-#define LPM_ERR_TIMEOUT 5    /* a bounded device-side wait gave up */
+/* 5 is not used: no entry point waits on the device (persistent kernels take work from atomic counters and
+ * never spin on a flag) */
 #define LPM_ERR_CAPACITY 6   /* a fixed capacity was exceeded (tree depth / node pool / scratch) */
 #define LPM_ERR_INTERNAL 7   /* an internal consistency check failed */
 #define LPM_ERR_NO_DEVICE 8  /* no CUDA device / unsupported device */
@@ -109,6 +110,19 @@ int lpm_mesh_build(int kind, int level, double radius, double* vert_xyz, double*
 /* Vertex indices of every face (n_faces x 3 for LPM_MESH_ICOS_TRI, x 4 for LPM_MESH_CUBED_SPHERE), in
  * the order of Faces::vertexIndices (src/LpmFaces.cpp:63-69): the connectivity lpm_write_vtk writes. */
 int lpm_mesh_face_vertices(int kind, int level, int64_t* face_verts);
+/* lpm_mesh_build on the GPU (PolyMesh2d(seed, level), src/LpmPolyMesh2d.cpp:20-93, refined level by level
+ * by kernels): DEVICE arrays vert_xyz (n_verts x 3), face_xyz (n_faces x 3, may be NULL), face_area (n_faces,
+ * may be NULL), face_divided (n_faces), face_verts (n_faces x 3|4, may be NULL).  Same index order as the
+ * host generator and the reference; vertex coordinates and centroids bit-identical to them, areas within 1e-13
+ * relative (the CUDA math library's atan2 / tan in L'Huilier's formula).  Allocates its
+ * edge tables on the device for the call; returns after the arrays are written (level <= 12). */
+int lpm_mesh_build_dev(lpm_ctx* ctx, int kind, int level, double radius, double* vert_xyz, double* face_xyz,
+                       double* face_area, uint8_t* face_divided, int64_t* face_verts);
+/* The RK4 particle state of a device mesh (n_leaves + n_verts) x 4: the leaf faces' centroids carrying
+ * face_src x area (the leaves are the last n_leaves faces), then the vertices with strength 0 (device arrays,
+ * enqueued on the context's stream). */
+int lpm_mesh_particles_dev(lpm_ctx* ctx, int kind, int level, const double* vert_xyz, const double* face_xyz,
+                           const double* face_area, const double* face_src, double* state);
 
 /* ---- field output in the reference's file formats (host; fields may be device-resident) */
 typedef struct lpm_field_desc {
@@ -230,7 +244,11 @@ typedef struct lpm_solver_desc {
     int32_t max_per_leaf; /* octree leaf capacity (maxParticlesPerBox) */
     double theta;         /* multipole acceptance parameter */
     int32_t order_policy; /* LPM_ORDER_* */
-    int32_t reserved;
+    int32_t sakajo_depth; /* 0: the source tree is TreeSum's octree (split while a node holds more than
+                             max_per_leaf sources); L > 0 (Biot-Savart): the tree of Sakajo (2009) as SakajoTree
+                             builds it (src/LpmSakajo2009.cpp:25-63): the box Box3d(radius) bisected 3L times
+                             along z, x, y in turn, every non-empty child that meets the sphere kept, leaves at
+                             that fixed depth summed directly; max_per_leaf is then ignored */
     double tolerance;     /* LPM_ORDER_LEARNED: per-pair error budget relative to |mult| * sum|w| (0 = 2e-8) */
 } lpm_solver_desc;
 
@@ -367,6 +385,11 @@ int lpm_ensemble_set_mlp(lpm_ensemble* ens, const float* params);
 /* lpm_rk4_set_param on every instance; drops the captured step (the next graph step first runs uncaptured). */
 int lpm_ensemble_set_param(lpm_ensemble* ens, const char* name, double value);
 int lpm_ensemble_step(lpm_ensemble* ens, double dt, int nsteps, int use_graph);
+
+/* ---- testing (no reference counterpart): failure injection on the host side.  The device allocation made
+ * after `after` further successful ones reports failure (LPM_ERR_OOM from the entry point that made it), once;
+ * a negative value turns the injection off.  Process-wide. */
+int lpm_debug_fail_allocations(int64_t after);
 
 #ifdef __cplusplus
 }

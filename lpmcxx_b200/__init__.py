@@ -92,6 +92,39 @@ def build_mesh(kind: str, level: int, radius: float = 1.0) -> SphereMesh:
     return SphereMesh(kind, level, v, f, a, d)
 
 
+def build_mesh_dev(ctx, kind: str, level: int, radius: float = 1.0, face_verts: bool = False) -> dict:
+    """The mesh of build_mesh refined on the GPU (lpm_mesh_build_dev): CUDA tensors vert_xyz, face_xyz,
+    face_area, face_divided (and face_verts)."""
+    import torch
+
+    k = _capi.LPM_MESH_ICOS_TRI if kind == "icos" else _capi.LPM_MESH_CUBED_SPHERE
+    nv, nf, _ = mesh_counts(kind, level)
+    ns = 3 if kind == "icos" else 4
+    out = {"vert_xyz": torch.empty((nv, 3), dtype=torch.float64, device="cuda"),
+           "face_xyz": torch.empty((nf, 3), dtype=torch.float64, device="cuda"),
+           "face_area": torch.empty(nf, dtype=torch.float64, device="cuda"),
+           "face_divided": torch.empty(nf, dtype=torch.uint8, device="cuda")}
+    if face_verts:
+        out["face_verts"] = torch.empty((nf, ns), dtype=torch.int64, device="cuda")
+    check(lib().lpm_mesh_build_dev(ctx.h, k, level, radius, ptr(out["vert_xyz"]), ptr(out["face_xyz"]),
+                                   ptr(out["face_area"]), ptr(out["face_divided"]), ptr(out.get("face_verts"))),
+          "lpm_mesh_build_dev")
+    return out
+
+
+def mesh_particles_dev(ctx, kind: str, level: int, mesh: dict, face_src):
+    """RK4 particles of a device mesh: (n_leaves + n_verts, 4) CUDA tensor, leaf centroids with face_src x
+    area, then the vertices with strength 0."""
+    import torch
+
+    k = _capi.LPM_MESH_ICOS_TRI if kind == "icos" else _capi.LPM_MESH_CUBED_SPHERE
+    nv, nf, nl = mesh_counts(kind, level)
+    state = torch.empty((nl + nv, 4), dtype=torch.float64, device="cuda")
+    check(lib().lpm_mesh_particles_dev(ctx.h, k, level, ptr(mesh["vert_xyz"]), ptr(mesh["face_xyz"]),
+                                       ptr(mesh["face_area"]), ptr(face_src), ptr(state)), "lpm_mesh_particles_dev")
+    return state
+
+
 class Context:
     """One device + stream + scratch buffers (lpm_ctx)."""
 
@@ -200,9 +233,11 @@ def direct_solver(precision: int = LPM_PREC_F64) -> _capi.SolverDesc:
 
 
 def tree_solver(precision: int = LPM_PREC_F32, order: int = 8, max_per_leaf: int = 512, theta: float = 0.7,
-                learned: bool = False, tolerance: float = 0.0) -> _capi.SolverDesc:
+                learned: bool = False, tolerance: float = 0.0, sakajo_depth: int = 0) -> _capi.SolverDesc:
+    """Treecode descriptor.  sakajo_depth = L > 0 selects the Sakajo (2009) fixed-depth tree (3L bisections
+    along z, x, y in turn) instead of the octree split at max_per_leaf."""
     return _capi.SolverDesc(_capi.LPM_METHOD_TREE, precision, order, max_per_leaf, theta,
-                            _capi.LPM_ORDER_LEARNED if learned else _capi.LPM_ORDER_FIXED, 0, tolerance)
+                            _capi.LPM_ORDER_LEARNED if learned else _capi.LPM_ORDER_FIXED, sakajo_depth, tolerance)
 
 
 class RK4:

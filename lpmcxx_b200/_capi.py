@@ -17,7 +17,6 @@ LPM_ERR_ARG = 1
 LPM_ERR_KERNEL = 2
 LPM_ERR_OOM = 3
 LPM_ERR_CUDA = 4
-LPM_ERR_TIMEOUT = 5
 LPM_ERR_CAPACITY = 6
 LPM_ERR_INTERNAL = 7
 LPM_ERR_NO_DEVICE = 8
@@ -53,7 +52,7 @@ class FieldDesc(C.Structure):
 
 class SolverDesc(C.Structure):
     _fields_ = [("method", C.c_int32), ("precision", C.c_int32), ("order", C.c_int32), ("max_per_leaf", C.c_int32),
-                ("theta", C.c_double), ("order_policy", C.c_int32), ("reserved", C.c_int32),
+                ("theta", C.c_double), ("order_policy", C.c_int32), ("sakajo_depth", C.c_int32),
                 ("tolerance", C.c_double)]
 
 
@@ -83,6 +82,8 @@ SIGNATURES = {
     "lpm_mesh_counts": (C.c_int, [C.c_int, C.c_int, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
     "lpm_mesh_build": (C.c_int, [C.c_int, C.c_int, D, P, P, P, P]),
     "lpm_mesh_face_vertices": (C.c_int, [C.c_int, C.c_int, P]),
+    "lpm_mesh_build_dev": (C.c_int, [P, C.c_int, C.c_int, D, P, P, P, P, P]),
+    "lpm_mesh_particles_dev": (C.c_int, [P, C.c_int, C.c_int, P, P, P, P, P]),
     "lpm_write_vtk": (C.c_int, [C.c_char_p, C.c_char_p, I64, P, C.c_int32, C.c_int32, P, I64, C.c_int32, P, P,
                                 C.c_int32, C.POINTER(FieldDesc), C.c_int32, C.POINTER(FieldDesc)]),
     "lpm_write_csv": (C.c_int, [C.c_char_p, I64, P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(FieldDesc)]),
@@ -132,6 +133,7 @@ SIGNATURES = {
     "lpm_ensemble_set_mlp": (C.c_int, [P, P]),
     "lpm_ensemble_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
     "lpm_ensemble_step": (C.c_int, [P, C.c_double, C.c_int, C.c_int]),
+    "lpm_debug_fail_allocations": (C.c_int, [C.c_int64]),
 }
 
 _lib = None

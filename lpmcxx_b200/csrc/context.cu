@@ -3,6 +3,8 @@
 // device buffers the solvers reuse between calls.
 #include "lpm_internal.h"
 
+#include <atomic>
+
 #include <cstdarg>
 #include <cstring>
 #include <new>
@@ -18,6 +20,24 @@ void set_error(const char* fmt, ...) {
     va_start(ap, fmt);
     vsnprintf(g_err, sizeof(g_err), fmt, ap);
     va_end(ap);
+}
+
+// Allocation-failure injection for tests: after `g_fail_after` more successful device allocations, the next
+// one reports cudaErrorMemoryAllocation without allocating (once; negative = off).
+static std::atomic<int64_t> g_fail_after{-1};
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+    int64_t v = g_fail_after.load();
+    while (v >= 0) {
+        if (g_fail_after.compare_exchange_weak(v, v - 1)) {
+            if (v == 0) {
+                *p = nullptr;
+                return cudaErrorMemoryAllocation;
+            }
+            break;
+        }
+    }
+    return cudaMalloc(p, bytes);
 }
 
 int cuda_status(cudaError_t e, const char* what) {
@@ -41,9 +61,10 @@ void* scratch(lpm_ctx* ctx, int slot, size_t bytes) {
         b.ptr = nullptr;
         b.bytes = 0;
     }
+    ++ctx->generation;  // graphs captured with the old address must be captured again
     size_t want = bytes + bytes / 8;  // grow with headroom
     want = (want + 255) & ~size_t(255);
-    if (cudaMalloc(&b.ptr, want) != cudaSuccess) {
+    if (dev_alloc(&b.ptr, want) != cudaSuccess) {
         cudaGetLastError();
         b.ptr = nullptr;
         set_error("device allocation of %zu bytes failed (scratch slot %d)", want, slot);
@@ -229,3 +250,8 @@ int lpm_ctx_synchronize(lpm_ctx* ctx) {
 int64_t lpm_ctx_launch_count(const lpm_ctx* ctx) { return ctx ? ctx->launches : -1; }
 
 }  // extern "C"
+
+extern "C" int lpm_debug_fail_allocations(int64_t after) {
+    lpm::g_fail_after.store(after < 0 ? -1 : after);
+    return LPM_OK;
+}

@@ -21,6 +21,7 @@ lpm_ctx* rk4_context(lpm_rk4* rk);
 int rk4_tree_check(lpm_rk4* rk);
 int rk4_set_mlp_internal(lpm_rk4* rk, const float* params);
 int rk4_set_param_internal(lpm_rk4* rk, const char* name, double value);
+uint64_t rk4_buffer_generation(const lpm_rk4* rk);
 void rk4_set_owner(lpm_rk4* rk, lpm_ensemble* e);
 int ensemble_invalidate(lpm_ensemble* e);
 }  // namespace lpm
@@ -39,7 +40,16 @@ struct lpm_ensemble {
     double graph_dt = 0.0;
     int64_t graph_nodes = 0;
     bool warmed = false;
+    std::vector<uint64_t> graph_gen;   // per instance: buffer generation at capture
 };
+
+// Whether any instance reallocated a buffer since the ensemble's graph was captured.
+static bool ens_graph_stale(const lpm_ensemble* e) {
+    if (e->graph_gen.size() != e->inst.size()) return true;
+    for (size_t i = 0; i < e->inst.size(); ++i)
+        if (e->graph_gen[i] != rk4_buffer_generation(e->inst[i])) return true;
+    return false;
+}
 
 static void ens_drop_graph(lpm_ensemble* e) {
     if (e->exec) cudaGraphExecDestroy(e->exec);
@@ -251,6 +261,8 @@ static int ens_capture(lpm_ensemble* e, double dt) {
     e->graph_nodes = (int64_t)nodes;
     LPM_CUDA_TRY(cudaGraphInstantiate(&e->exec, g, 0));
     e->graph_dt = dt;
+    e->graph_gen.resize(e->inst.size());
+    for (size_t i = 0; i < e->inst.size(); ++i) e->graph_gen[i] = rk4_buffer_generation(e->inst[i]);
     return LPM_OK;
 }
 
@@ -272,7 +284,8 @@ extern "C" int lpm_ensemble_step(lpm_ensemble* e, double dt, int nsteps, int use
         if (n_plain > 0) e->warmed = true;
     }
     if (s < nsteps) {
-        if (!e->exec || e->graph_dt != dt) {
+        // a graph holds the buffer addresses of its capture: captured again after any reallocation
+        if (!e->exec || e->graph_dt != dt || ens_graph_stale(e)) {
             int rc = ens_capture(e, dt);
             if (rc) return rc;
         }

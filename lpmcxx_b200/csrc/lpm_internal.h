@@ -48,6 +48,8 @@ struct lpm_ctx {
     // pinned host staging (host-facing entry points)
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // incremented whenever a scratch slot is reallocated: a CUDA graph captured before holds the old address
+    uint64_t generation = 0;
 };
 
 namespace lpm {
@@ -92,6 +94,8 @@ void* scratch(lpm_ctx* ctx, int slot, size_t bytes);
 void* pinned(lpm_ctx* ctx, size_t bytes);
 
 int cuda_status(cudaError_t e, const char* what);
+// cudaMalloc through the library's allocation-failure injection point (lpm_debug_fail_allocations).
+cudaError_t dev_alloc(void** p, size_t bytes);
 
 #define LPM_CUDA_TRY(call)                                              \
     do {                                                                \

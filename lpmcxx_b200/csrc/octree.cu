@@ -214,7 +214,7 @@ int radix_sort_impl(lpm_ctx* ctx, K* keys, int32_t* vals, K* tk, int32_t* tv, in
 // ---------------------------------------------------------------------------------- keys
 __global__ void morton_keys_kernel(const double4* __restrict__ pts, int64_t n, RootBox root,
                                    uint64_t* __restrict__ keys, int32_t* __restrict__ vals,
-                                   int32_t* __restrict__ counters) {
+                                   int32_t* __restrict__ counters, int bits, int max_depth) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     root = resolve_root(root);
     bool in = false;
@@ -224,7 +224,21 @@ __global__ void morton_keys_kernel(const double4* __restrict__ pts, int64_t n, R
         in = root.lo[0] <= c[0] && c[0] < root.hi[0] && root.lo[1] <= c[1] && c[1] < root.hi[1] &&
              root.lo[2] <= c[2] && c[2] < root.hi[2];
         uint64_t key = kKeyOutside;
-        if (in) {
+        if (in && bits == 1) {  // binary: level l bisects axis (l + 1) mod 3 (the Sakajo tree's (j + 2) mod 3, j = l - 1)
+            double lo[3] = {root.lo[0], root.lo[1], root.lo[2]};
+            double hi[3] = {root.hi[0], root.hi[1], root.hi[2]};
+            key = 0;
+            for (int l = 1; l <= max_depth; ++l) {
+                const int a = (l + 1) % 3;
+                const double mid = 0.5 * (lo[a] + hi[a]);  // Box3d::bisectAlongDims midpoint
+                if (c[a] < mid) {
+                    hi[a] = mid;
+                } else {
+                    lo[a] = mid;
+                    key |= 1ull << (kMaxLevels - l);
+                }
+            }
+        } else if (in) {
             double lo[3] = {root.lo[0], root.lo[1], root.lo[2]};
             double hi[3] = {root.hi[0], root.hi[1], root.hi[2]};
             key = 0;
@@ -269,8 +283,40 @@ __global__ void root_extent_kernel(const double4* __restrict__ pts, int64_t firs
     if ((threadIdx.x & 31) == 0 && m) atomicMax(r_dev, m);
 }
 
-__device__ __forceinline__ int level_digit(uint64_t key, int level) {
-    return (int)((key >> (3 * (kKeyLevels - level))) & 7ull);
+__device__ __forceinline__ int level_digit(uint64_t key, int level, int bits) {
+    return bits == 1 ? (int)((key >> (kMaxLevels - level)) & 1ull) : (int)((key >> (3 * (kKeyLevels - level))) & 7ull);
+}
+
+// Box of child digit d of a level-l node (box pb): all three axes for octrees (ix + 2 iy + 4 iz), axis
+// (l + 2) mod 3 for binary trees.
+__device__ __forceinline__ void child_box(const double* pb, int l, int d, int bits, double* cb) {
+    for (int a = 0; a < 3; ++a) {
+        const double mid = 0.5 * (pb[2 * a] + pb[2 * a + 1]);
+        const bool split = bits == 3 || a == (l + 2) % 3;
+        const bool upper = bits == 3 ? ((d >> a) & 1) : (d & 1);
+        cb[2 * a] = split && upper ? mid : pb[2 * a];
+        cb[2 * a + 1] = split && !upper ? mid : pb[2 * a + 1];
+    }
+}
+
+// Box3d::intersectsSphere about the origin (src/LpmBox3d.cpp:79-129): the box's closest point lies inside
+// the sphere and its farthest corner outside (distances sqrt((x x + y y) + z z), rounded step by step).
+__device__ __forceinline__ double mag3(double x, double y, double z) {
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+}
+__device__ bool box_meets_sphere(const double* b, double r) {
+    double c[3];
+    const bool inside = b[0] <= 0.0 && 0.0 < b[1] && b[2] <= 0.0 && 0.0 < b[3] && b[4] <= 0.0 && 0.0 < b[5];
+    for (int a = 0; a < 3; ++a) {
+        const double lo = b[2 * a], hi = b[2 * a + 1];
+        c[a] = inside ? 0.0 : (lo == hi ? lo : (lo >= 0.0 ? lo : (hi <= 0.0 ? hi : 0.0)));
+    }
+    double far = 0.0;
+    for (int k = 0; k < 8; ++k) {
+        const double d = mag3(b[(k & 1) ? 1 : 0], b[(k & 2) ? 3 : 2], b[(k & 4) ? 5 : 4]);
+        far = d > far ? d : far;
+    }
+    return mag3(c[0], c[1], c[2]) <= r && far >= r;
 }
 
 __global__ void tree_init_kernel(Octree t) {
@@ -287,7 +333,7 @@ __global__ void tree_init_kernel(Octree t) {
     }
     t.level_range[0] = 0;
     t.level_range[1] = 1;
-    for (int l = 1; l < kKeyLevels + 2; ++l) {
+    for (int l = 1; l < kMaxLevels + 2; ++l) {
         t.level_range[2 * l] = 1;
         t.level_range[2 * l + 1] = 1;
     }
@@ -306,29 +352,30 @@ __global__ void __launch_bounds__(256) split_level_kernel(Octree t, int l) {
     const int lb = t.level_range[2 * l], le = t.level_range[2 * l + 1];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
+    const int nd = 1 << t.bits;  // digits per level
     for (int i = lb + blockIdx.x; i < le; i += gridDim.x) {
         const int s = t.node_start[i], e = t.node_end[i];
         const bool split = e - s > t.max_per_leaf;  // uniform per block
         if (split) {
-            if (w >= 1 && w <= 7) {
+            if (w >= 1 && w < nd) {
                 const int d = w;
                 int lo = s, hi = e;  // the boundary b satisfies lo <= b <= hi; positions lo..hi-1 are keys
                 while (hi - lo > 32) {
                     const int64_t L = hi - lo;
                     const int p = lo + (int)(((int64_t)lane * L) >> 5);
-                    const unsigned below = __ballot_sync(full, level_digit(t.keys[p], l + 1) < d);
+                    const unsigned below = __ballot_sync(full, level_digit(t.keys[p], l + 1, t.bits) < d);
                     const int c = __popc(below);  // probes 0..c-1 lie below the boundary (digits are sorted)
                     const int nlo = c == 0 ? lo : lo + (int)(((int64_t)(c - 1) * L) >> 5) + 1;
                     const int nhi = c == 32 ? hi : lo + (int)(((int64_t)c * L) >> 5);
                     lo = nlo;
                     hi = nhi;
                 }
-                const bool lt = lane < hi - lo && level_digit(t.keys[lo + lane], l + 1) < d;
+                const bool lt = lane < hi - lo && level_digit(t.keys[lo + lane], l + 1, t.bits) < d;
                 const int c = __popc(__ballot_sync(full, lt));
                 if (lane == 0) cs_sh[d] = lo + c;
             } else if (w == 0 && lane == 0) {
                 cs_sh[0] = s;
-                cs_sh[8] = e;
+                cs_sh[nd] = e;
             }
         }
         __syncthreads();
@@ -336,8 +383,16 @@ __global__ void __launch_bounds__(256) split_level_kernel(Octree t, int l) {
             int nchild = 0;
             if (split) {
                 int32_t* cs = t.child_start + (int64_t)(i - lb) * 9;
-                for (int d = 0; d <= 8; ++d) cs[d] = cs_sh[d];
-                for (int d = 0; d < 8; ++d) nchild += cs_sh[d + 1] > cs_sh[d];
+                for (int d = 0; d <= nd; ++d) cs[d] = cs_sh[d];
+                for (int d = 0; d < nd; ++d) {
+                    bool keep = cs_sh[d + 1] > cs_sh[d];
+                    if (keep && t.sphere_r > 0.0) {
+                        double cb[6];
+                        child_box(t.node_box + 6 * (int64_t)i, l, d, t.bits, cb);
+                        keep = box_meets_sphere(cb, t.sphere_r);
+                    }
+                    nchild += keep;
+                }
             }
             t.node_split[i - lb] = nchild;
         }
@@ -370,23 +425,19 @@ __global__ void emit_level_kernel(Octree t, int l) {
         t.node_nchild[node] = (int8_t)nc;
         const int32_t* cs = t.child_start + (int64_t)i * 9;
         const double* pb = t.node_box + 6 * (int64_t)node;
-        double mid[3];
-        for (int a = 0; a < 3; ++a) mid[a] = 0.5 * (pb[2 * a] + pb[2 * a + 1]);
         int k = run;
-        for (int d = 0; d < 8; ++d) {
+        for (int d = 0; d < (1 << t.bits); ++d) {
             if (cs[d + 1] <= cs[d]) continue;
+            double cb[6];
+            child_box(pb, l, d, t.bits, cb);
+            if (t.sphere_r > 0.0 && !box_meets_sphere(cb, t.sphere_r)) continue;  // as counted by split_level
             t.node_start[k] = cs[d];
             t.node_end[k] = cs[d + 1];
             t.node_parent[k] = node;
             t.node_first_child[k] = -1;
             t.node_nchild[k] = 0;
             t.node_level[k] = (int8_t)(l + 1);
-            double* cb = t.node_box + 6 * (int64_t)k;
-            for (int a = 0; a < 3; ++a) {
-                const bool upper = (d >> a) & 1;
-                cb[2 * a] = upper ? mid[a] : pb[2 * a];
-                cb[2 * a + 1] = upper ? pb[2 * a + 1] : mid[a];
-            }
+            for (int a = 0; a < 6; ++a) t.node_box[6 * (int64_t)k + a] = cb[a];
             ++k;
         }
         run += nc;
@@ -406,7 +457,8 @@ __global__ void leaf_flags_kernel(Octree t, int64_t n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
         if (t.node_nchild[i] == 0) {
             t.leaf_flag[t.node_start[i]] = 1;
-            if (t.node_end[i] - t.node_start[i] > t.max_per_leaf) atomicOr(&t.counters[2], 1);  // depth limit
+            if (t.max_per_leaf > 0 && t.node_end[i] - t.node_start[i] > t.max_per_leaf)
+                atomicOr(&t.counters[2], 1);  // depth limit
         }
     }
     (void)n;
@@ -449,7 +501,7 @@ int morton_keys(lpm_ctx* ctx, const double4* pts, int64_t n, const RootBox& root
                 int32_t* counter) {
     if (n <= 0) return LPM_OK;
     LPM_LAUNCH(ctx, "morton_keys_kernel", morton_keys_kernel, grid_for(n, 256), 256, 0, pts, n, root, keys, vals,
-               counter);
+               counter, 3, kKeyLevels);
     return LPM_OK;
 }
 
@@ -469,19 +521,29 @@ int radix_sort_u32(lpm_ctx* ctx, uint32_t* keys, int32_t* vals, uint32_t* tk, in
     return radix_sort_impl<uint32_t>(ctx, keys, vals, tk, tv, n, 0, bits);
 }
 
-int octree_alloc(Octree& t, int64_t n, int max_per_leaf, int max_depth) {
+int octree_alloc(Octree& t, int64_t n, int max_per_leaf, int max_depth, int bits, double sphere_r) {
     octree_free(t);
     t.n = n;
     t.max_per_leaf = max_per_leaf;
-    t.max_depth = std::min(std::max(max_depth, 1), kKeyLevels);
-    // every internal node has >= 2 points in distinct children or splits a range of > max points:
-    // n_nodes <= 8 * (internal nodes) + 1 and internal nodes <= depth * n / (max_per_leaf + 1) + 1
-    const int64_t internal = (int64_t)t.max_depth * (n / (max_per_leaf + 1) + 1) + 1;
-    t.node_cap = std::min<int64_t>(8 * internal + 1, std::max<int64_t>(2 * n + 16, 64));
+    t.bits = bits == 1 ? 1 : 3;
+    t.levels = t.bits == 1 ? kMaxLevels : kKeyLevels;
+    t.max_depth = std::min(std::max(max_depth, 1), t.levels);
+    t.sphere_r = t.bits == 1 ? sphere_r : 0.0;
+    if (t.bits == 1) {
+        // every non-empty node splits to max_depth: level l holds at most min(n, 2^l) nodes
+        int64_t cap = 0;
+        for (int l = 0; l <= t.max_depth; ++l) cap += l < 62 ? std::min<int64_t>(n, 1ll << l) : n;
+        t.node_cap = cap + 16;
+    } else {
+        // every internal node has >= 2 points in distinct children or splits a range of > max points:
+        // n_nodes <= 8 * (internal nodes) + 1 and internal nodes <= depth * n / (max_per_leaf + 1) + 1
+        const int64_t internal = (int64_t)t.max_depth * (n / (max_per_leaf + 1) + 1) + 1;
+        t.node_cap = std::min<int64_t>(8 * internal + 1, std::max<int64_t>(2 * n + 16, 64));
+    }
     const size_t nn = (size_t)std::max<int64_t>(n, 1), nc = (size_t)t.node_cap;
     cudaError_t e = cudaSuccess;
     auto A = [&](void** p, size_t bytes) {
-        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) e = dev_alloc((void**)p, bytes);
     };
     A((void**)&t.keys, nn * 8);
     A((void**)&t.perm, nn * 4);
@@ -497,7 +559,7 @@ int octree_alloc(Octree& t, int64_t n, int max_per_leaf, int max_depth) {
     A((void**)&t.node_box, nc * 6 * 8);
     A((void**)&t.node_split, nc * 4);
     A((void**)&t.child_start, nc * 9 * 4);
-    A((void**)&t.level_range, 2 * (kKeyLevels + 2) * 4);
+    A((void**)&t.level_range, 2 * (kMaxLevels + 2) * 4);
     A((void**)&t.counters, 16 * 4);
     A((void**)&t.leaf_node, nc * 4);
     A((void**)&t.node_leaf, nc * 4);
@@ -514,12 +576,14 @@ void octree_free(Octree& t) {
                   t.level_range, t.counters, t.leaf_node, t.node_leaf};
     for (void* p : ps)
         if (p) cudaFree(p);
-    const int64_t n = t.n;
-    const int mpl = t.max_per_leaf, md = t.max_depth;
+    const Octree keep = t;
     t = Octree();
-    t.n = n;
-    t.max_per_leaf = mpl;
-    t.max_depth = md;
+    t.n = keep.n;
+    t.max_per_leaf = keep.max_per_leaf;
+    t.max_depth = keep.max_depth;
+    t.bits = keep.bits;
+    t.levels = keep.levels;
+    t.sphere_r = keep.sphere_r;
 }
 
 int octree_build(lpm_ctx* ctx, Octree& t, const double4* pts, int64_t n, const RootBox& root) {
@@ -531,9 +595,9 @@ int octree_build(lpm_ctx* ctx, Octree& t, const double4* pts, int64_t n, const R
     LPM_CUDA_TRY(cudaMemsetAsync(t.counters, 0, 16 * 4, ctx->stream));
     if (n > 0)
         LPM_LAUNCH(ctx, "morton_keys_kernel", morton_keys_kernel, grid_for(n, 256), 256, 0, pts, n, root, t.keys,
-                   t.perm, t.counters);
+                   t.perm, t.counters, t.bits, t.max_depth);
     // the key bits that decide levels 1..max_depth (and the outside flag in bit 63)
-    const int bit_lo = std::max(0, 3 * (kKeyLevels - t.max_depth)) & ~7;
+    const int bit_lo = std::max(0, t.bits * (t.levels - t.max_depth)) & ~7;
     int rc = radix_sort_u64(ctx, t.keys, t.perm, t.tmp_keys, t.tmp_vals, n, bit_lo);
     if (rc) return rc;
     LPM_LAUNCH(ctx, "tree_init_kernel", tree_init_kernel, 1, 1, 0, t);

@@ -7,6 +7,7 @@
 namespace lpm {
 
 constexpr int kKeyLevels = 21;        // 3 bits per level in a 63-bit key; bit 63 marks "outside the root box"
+constexpr int kMaxLevels = 63;        // binary (1 bit per level) trees: up to 63 levels
 constexpr uint64_t kKeyOutside = ~0ull;
 
 // Exclusive prefix sum of n int32 values (in may equal out).  Uses ctx scratch slot kSlotMisc2.
@@ -51,10 +52,18 @@ __device__ __forceinline__ RootBox resolve_root(const RootBox& r) {
 int root_extent(lpm_ctx* ctx, const double4* pts, int64_t first, int64_t n, int mode, unsigned long long* r_dev);
 
 // Octree over points (double4, xyz used).  All arrays device-resident; sizes are capacities.
+// bits = 3: every level bisects all three axes (8 children, child order ix + 2 iy + 4 iz); nodes holding more
+// than max_per_leaf points split.  bits = 1: the Sakajo (2009) tree (src/LpmSakajo2009.cpp:25-63): level l
+// bisects axis (l + 2) mod 3 (z, x, y, z, ...), every non-empty node splits down to max_depth
+// (max_per_leaf = 0), and with sphere_r > 0 a child is kept only if its box meets the sphere of that radius
+// about the origin (Box3d::intersectsSphere, src/LpmBox3d.cpp:125-129).
 struct Octree {
     int64_t n = 0;          // points given
     int max_per_leaf = 0;
-    int max_depth = 0;      // levels the keys are split to (<= kKeyLevels)
+    int max_depth = 0;      // levels the keys are split to (<= levels)
+    int bits = 3;           // key bits per level: 3 (octree) or 1 (binary, axis-cycling)
+    int levels = kKeyLevels;  // levels a key holds: 63 / bits
+    double sphere_r = 0.0;  // binary trees: keep children that meet this sphere (0: keep every non-empty one)
     int64_t node_cap = 0;
     RootBox root{};
     // per point (sorted order)
@@ -84,7 +93,7 @@ struct Octree {
 int morton_keys(lpm_ctx* ctx, const double4* pts, int64_t n, const RootBox& root, uint64_t* keys, int32_t* vals,
                 int32_t* counter);
 
-int octree_alloc(Octree& t, int64_t n, int max_per_leaf, int max_depth);
+int octree_alloc(Octree& t, int64_t n, int max_per_leaf, int max_depth, int bits = 3, double sphere_r = 0.0);
 void octree_free(Octree& t);
 // Build over pts[0:n] with the given root box.  Fully asynchronous (capturable): no host reads.
 int octree_build(lpm_ctx* ctx, Octree& t, const double4* pts, int64_t n, const RootBox& root);

@@ -37,6 +37,7 @@ struct lpm_rk4 {
     int64_t graph_nodes = 0;
     bool warmed = false;
     lpm_ensemble* owner = nullptr;  // the ensemble whose captured step replays this instance, if any
+    uint64_t graph_ctx_gen = 0, graph_tree_gen = 0;  // buffer generations the graph was captured with
 };
 
 namespace lpm {
@@ -113,6 +114,10 @@ static int rk4_one_step(lpm_rk4* rk, double dt) {
 
 // One uncaptured-or-captured RK4 step of rk on its context's current stream (for the ensemble).
 int rk4_step_enqueue(lpm_rk4* rk, double dt) { return rk4_one_step(rk, dt); }
+// Generations of the buffers a step of rk uses (its context's scratch, its treecode's arrays).
+uint64_t rk4_buffer_generation(const lpm_rk4* rk) {
+    return rk->ctx->generation * 1000003ull + (rk->tree ? tree_generation(rk->tree) : 0);
+}
 lpm_ctx* rk4_context(lpm_rk4* rk) { return rk->ctx; }
 int rk4_tree_check(lpm_rk4* rk) { return rk->tree ? tree_check(rk->tree) : LPM_OK; }
 void rk4_set_owner(lpm_rk4* rk, lpm_ensemble* e) { rk->owner = e; }
@@ -172,6 +177,8 @@ static int capture_step(lpm_rk4* rk, double dt) {
     rk->graph_nodes = (int64_t)nodes;
     LPM_CUDA_TRY(cudaGraphInstantiate(&rk->graph_exec, g, 0));
     rk->graph_dt = dt;
+    rk->graph_ctx_gen = ctx->generation;
+    rk->graph_tree_gen = rk->tree ? tree_generation(rk->tree) : 0;
     return LPM_OK;
 }
 
@@ -214,11 +221,11 @@ extern "C" int lpm_rk4_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const
     rk->n = n_pts;
     const size_t n = (size_t)n_pts;
     cudaError_t e = cudaSuccess;
-    e = cudaMalloc(&rk->X, n * sizeof(double4));
-    if (e == cudaSuccess) e = cudaMalloc(&rk->Xs, n * sizeof(double4));
-    if (e == cudaSuccess) e = cudaMalloc(&rk->Xs32, n * sizeof(float4));
-    if (e == cudaSuccess) e = cudaMalloc(&rk->U, 3 * n * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&rk->K, 3 * n * sizeof(double));
+    e = dev_alloc((void**)&rk->X, n * sizeof(double4));
+    if (e == cudaSuccess) e = dev_alloc((void**)&rk->Xs, n * sizeof(double4));
+    if (e == cudaSuccess) e = dev_alloc((void**)&rk->Xs32, n * sizeof(float4));
+    if (e == cudaSuccess) e = dev_alloc((void**)&rk->U, 3 * n * sizeof(double));
+    if (e == cudaSuccess) e = dev_alloc((void**)&rk->K, 3 * n * sizeof(double));
     if (e != cudaSuccess) {
         lpm_rk4_destroy(rk);
         return cuda_status(e, "cudaMalloc (RK4 state)");
@@ -330,7 +337,11 @@ extern "C" int lpm_rk4_step(lpm_rk4* rk, double dt, int nsteps, int use_graph) {
         rk->warmed = true;
         return LPM_OK;
     }
-    if (s < nsteps && (!rk->graph_exec || rk->graph_dt != dt)) {
+    // a graph holds the buffer addresses of its capture: after any reallocation (an uncaptured evaluation
+    // regrew the interaction lists, the per-node arrays or a scratch slot) it is captured again
+    const bool stale = rk->graph_exec && (rk->graph_ctx_gen != ctx->generation ||
+                                          (rk->tree && rk->graph_tree_gen != tree_generation(rk->tree)));
+    if (s < nsteps && (!rk->graph_exec || rk->graph_dt != dt || stale)) {
         int rc = capture_step(rk, dt);
         if (rc) return rc;
     }

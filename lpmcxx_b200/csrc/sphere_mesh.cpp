@@ -211,6 +211,33 @@ int64_t ipow4(int l) {
 
 }  // namespace
 
+namespace lpm {
+// The level-0 mesh of a seed (vertices scaled by radius, n x 3; edges as orig, dest, left, right; faces as
+// their edge lists, 3 or 4 per face): the start of the device refinement (mesh_refine.cu).
+int mesh_seed(int kind, double radius, std::vector<double>& vxyz, std::vector<int32_t>& edges,
+              std::vector<int32_t>& faces) {
+    if (kind != LPM_MESH_ICOS_TRI && kind != LPM_MESH_CUBED_SPHERE) return LPM_ERR_ARG;
+    const bool icos = kind == LPM_MESH_ICOS_TRI;
+    const int nsv = icos ? 12 : 8, nse = icos ? 30 : 12, nsf = icos ? 20 : 6, ns = icos ? 3 : 4;
+    vxyz.clear();
+    edges.clear();
+    faces.clear();
+    for (int i = 0; i < nsv; ++i) {
+        const char* const* s = icos ? kIcosVerts[i] : kCubeVerts[i];
+        V3 v{std::strtod(s[0], nullptr), std::strtod(s[1], nullptr), std::strtod(s[2], nullptr)};
+        v.x *= radius; v.y *= radius; v.z *= radius;
+        vxyz.push_back(v.x);
+        vxyz.push_back(v.y);
+        vxyz.push_back(v.z);
+    }
+    for (int i = 0; i < nse; ++i)
+        for (int k = 0; k < 4; ++k) edges.push_back(icos ? kIcosEdges[i][k] : kCubeEdges[i][k]);
+    for (int i = 0; i < nsf; ++i)
+        for (int j = 0; j < ns; ++j) faces.push_back(icos ? kIcosFaces[i][j] : kCubeFaces[i][j]);
+    return LPM_OK;
+}
+}  // namespace lpm
+
 extern "C" int lpm_mesh_counts(int kind, int level, int64_t* n_verts, int64_t* n_faces, int64_t* n_leaves) {
     if ((kind != LPM_MESH_ICOS_TRI && kind != LPM_MESH_CUBED_SPHERE) || level < 0 || level > 12 || !n_verts ||
         !n_faces || !n_leaves)

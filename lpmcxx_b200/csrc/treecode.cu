@@ -1897,6 +1897,7 @@ struct TreeSolver {
     int near_targets = kNearTargets;  // near kernel tile shape (run-time "near_targets", "near_tile")
     int near_tile = kNearStreamTile;
     int far_blocks[kPMax + 1][2] = {};  // per order, FP32 / FP64 far kernel
+    uint64_t generation = 0;          // reallocations of the lists and per-node arrays (tree_generation)
     std::vector<void*> allocs;
 };
 
@@ -1919,7 +1920,7 @@ namespace {
 
 template <typename Tp>
 cudaError_t talloc(TreeSolver* t, Tp** p, size_t count) {
-    cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(Tp));
+    cudaError_t e = dev_alloc((void**)p, std::max<size_t>(count, 1) * sizeof(Tp));
     if (e == cudaSuccess) t->allocs.push_back(*p);
     return e;
 }
@@ -1932,6 +1933,7 @@ int alloc_lists(TreeSolver* t, int64_t far_cap, int64_t near_cap) {
             *p = nullptr;
         }
     }
+    ++t->generation;
     cudaError_t e = talloc(t, &t->far_list, (size_t)far_cap);
     if (e == cudaSuccess) e = talloc(t, &t->near_list, (size_t)near_cap);
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc (interaction lists)");
@@ -1952,6 +1954,7 @@ int heavy_alloc(TreeSolver* t, int64_t need) {
         }
         return talloc(t, p, (size_t)cap * per_node);
     };
+    ++t->generation;
     cudaError_t e = regrow(&t->node_mom, (size_t)cd * cd * cd);
     if (e == cudaSuccess && t->scalar) e = regrow(&t->A64, (size_t)t->a_stride);
     if (e == cudaSuccess && t->scalar) e = regrow(&t->A32, (size_t)t->a_stride);
@@ -2015,10 +2018,15 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     // Biot-Savart: order p = multi-indices |k| < p (the reference's SumNode); Poisson: |k| <= p (the
     // reference's TaylorSeries3d convention), i.e. internal order p + 1
     const int order = scalar ? solver.order + 1 : solver.order;
-    if (order < 1 || order > kPMax || solver.max_per_leaf < 1 || !(solver.theta > 0.0) || solver.theta >= 1.0 ||
-        n_src >= INT32_MAX || n_tgt >= INT32_MAX) {
-        set_error("tree solver: need 1 <= order <= %d (Poisson: 0 <= order <= %d), max_per_leaf >= 1, 0 < theta < 1",
-                  kPMax, kPMax - 1);
+    const int sakajo = solver.sakajo_depth;
+    if (order < 1 || order > kPMax || (sakajo == 0 && solver.max_per_leaf < 1) || !(solver.theta > 0.0) ||
+        solver.theta >= 1.0 || n_src >= INT32_MAX || n_tgt >= INT32_MAX || sakajo < 0 || 3 * sakajo > kMaxLevels) {
+        set_error("tree solver: need 1 <= order <= %d (Poisson: 0 <= order <= %d), max_per_leaf >= 1 (octree) or "
+                  "1 <= sakajo_depth <= 21, 0 < theta < 1", kPMax, kPMax - 1);
+        return LPM_ERR_ARG;
+    }
+    if (sakajo > 0 && scalar) {
+        set_error("tree solver: the Sakajo tree is built for the sphere (Biot-Savart kernel)");
         return LPM_ERR_ARG;
     }
     if (scalar && solver.order_policy == LPM_ORDER_LEARNED) {
@@ -2058,7 +2066,13 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
         const int64_t cells = std::min<int64_t>(std::max<int64_t>(n_tgt, 1), (int64_t)cells_at_l + 64);
         t->n_batches = (n_tgt + kBatch - 1) / kBatch + cells;
     }
-    rc = octree_alloc(t->st, std::max<int64_t>(n_src, 1), solver.max_per_leaf, kTreeDepth);
+    if (sakajo > 0) {
+        // SakajoTree: root Box3d(radius) padded by 1e-5 (src/LpmSakajo2009.cpp:25-39), 3L axis-cycling bisections
+        rc = octree_alloc(t->st, std::max<int64_t>(n_src, 1), 0, 3 * sakajo, 1, kernel.radius);
+        t->root_maxr = kernel.radius;
+    } else {
+        rc = octree_alloc(t->st, std::max<int64_t>(n_src, 1), solver.max_per_leaf, kTreeDepth);
+    }
     if (rc) {
         delete t;
         return rc;
@@ -2114,7 +2128,9 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     A(talloc(t, &t->node_wabs, nn));
     // moments, coefficients and features (~40 KB per node at order 11) are sized for a realistic node
     // count, not the octree's worst case, and grown by uncaptured evaluations (heavy_alloc)
-    t->heavy_cap = (int)std::min<int64_t>((int64_t)nn, 6 * (std::max<int64_t>(n_src, 1) / solver.max_per_leaf) + 1024);
+    t->heavy_cap = (int)std::min<int64_t>((int64_t)nn, sakajo > 0 ? 2 * std::max<int64_t>(n_src, 1) + 1024
+                                                                   : 6 * (std::max<int64_t>(n_src, 1) /
+                                                                          solver.max_per_leaf) + 1024);
     const size_t nh = (size_t)t->heavy_cap;
     A(talloc(t, &t->node_mom, nh * cd * cd * cd));
     if (scalar) {
@@ -2321,7 +2337,7 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     const unsigned gl = (unsigned)std::max<int64_t>(1, std::min<int64_t>(t->st.node_cap, 16 * ctx->num_sms));
     LPM_LAUNCH(ctx, "leaf_p2m_kernel", leaf_p2m_kernel, gl, 128, 0, t->st, t->src_sorted, t->pm, t->mono, t->n_mono,
                t->node_ctr, t->node_wabs, t->node_mom, t->src32, t->scalar ? 1.0 : 2.0, t->heavy_cap);
-    for (int l = kTreeDepth - 1; l >= 0; --l)
+    for (int l = t->st.max_depth - 1; l >= 0; --l)
         LPM_LAUNCH(ctx, "m2m_level_kernel", m2m_level_kernel, gl, 128, (size_t)16 * t->n_mono * sizeof(double), t->st,
                    l, t->pm, t->mono, t->n_mono, t->node_ctr, t->node_wabs, t->node_mom, t->heavy_cap);
     if (t->scalar)
@@ -2460,6 +2476,8 @@ int tree_check(TreeSolver* t) {
     return LPM_OK;
 }
 
+uint64_t tree_generation(const TreeSolver* t) { return t->generation; }
+
 const Octree& tree_source_octree(const TreeSolver* t, int64_t* n_points) {
     *n_points = t->n_src;
     return t->st;
@@ -2504,6 +2522,7 @@ int tree_get_param(const TreeSolver* t, const char* name, double* value) {
     else if (n == "order_bias") *value = t->order_bias;
     else if (n == "batch_level") *value = t->batch_level;
     else if (n == "batch_level_max") *value = t->batch_level_max;
+    else if (n == "sakajo_depth") *value = t->solver.sakajo_depth;
     else if (n == "near_targets") *value = t->near_targets;
     else if (n == "near_tile") *value = t->near_tile;
     else if (n == "root_maxr") *value = t->root_maxr;

@@ -13,6 +13,10 @@ const Octree& tree_source_octree(const TreeSolver* t, int64_t* n_points);
 // A read-only lpm_tree over an octree owned elsewhere (lpm_tree_destroy frees the view only).
 int tree_view_create(lpm_ctx* ctx, const Octree& t, int64_t n, lpm_tree** out);
 
+// Incremented whenever the solver reallocates a device array (interaction lists, per-node arrays): a CUDA
+// graph captured before holds the old addresses and must be captured again.
+uint64_t tree_generation(const TreeSolver* t);
+
 int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_solver_desc& solver, int64_t n_src,
                        int64_t n_tgt, TreeSolver** out);
 void tree_solver_destroy(TreeSolver* t);

@@ -129,6 +129,59 @@ def leaf_hashes(members: np.ndarray, leaf_offsets: np.ndarray) -> np.ndarray:
         return np.add.reduceat(z, off[:-1]) if m.size else np.zeros(0, np.uint64)
 
 
+def sakajo_tree(xyz: np.ndarray, depth: int, radius: float = 1.0) -> dict:
+    """The tree of SakajoTree(order, depth, radius) over points xyz (src/LpmSakajo2009.cpp:25-63) with the
+    points dropped into it as computeMoments does (:74-79, 201-213): root Box3d(radius) padded by 1e-5; a node
+    of binary level j < 3 depth is bisected along axis (j + 2) mod 3 at its midpoint and keeps a child whose
+    box meets the sphere (Box3d::intersectsSphere, src/LpmBox3d.cpp:79-129); a point follows the children whose
+    half-open box holds it, down to level 3 depth.  Returns the non-empty nodes in depth-first order (level,
+    parent, point count, box) and the leaves' members (increasing index), as the harness dumps them."""
+    pts = np.asarray(xyz, dtype=np.float64)
+
+    def mag(x, y, z):
+        return float(np.sqrt(x * x + y * y + z * z))
+
+    def meets(b):
+        if b[0] <= 0.0 < b[1] and b[2] <= 0.0 < b[3] and b[4] <= 0.0 < b[5]:
+            c = (0.0, 0.0, 0.0)
+        else:
+            c = tuple(lo if lo == hi else (lo if lo >= 0.0 else (hi if hi <= 0.0 else 0.0))
+                      for lo, hi in ((b[0], b[1]), (b[2], b[3]), (b[4], b[5])))
+        far = max(mag(b[i], b[2 + j], b[4 + k]) for i in (0, 1) for j in (0, 1) for k in (0, 1))
+        return mag(*c) <= radius and far >= radius
+
+    r = -radius
+    lo, hi = r - 1e-5, radius + 1e-5
+    out = {"node_level": [], "node_parent": [], "node_count": [], "node_box": [], "leaf_offsets": [0], "members": []}
+
+    def walk(box, idx, level, parent):
+        if idx.size == 0:
+            return
+        me = len(out["node_level"])
+        out["node_level"].append(level)
+        out["node_parent"].append(parent)
+        out["node_count"].append(idx.size)
+        out["node_box"].append(list(box))
+        if level == 3 * depth:
+            out["members"].extend(idx.tolist())
+            out["leaf_offsets"].append(len(out["members"]))
+            return
+        a = (level + 2) % 3
+        mid = 0.5 * (box[2 * a] + box[2 * a + 1])
+        below = pts[idx, a] < mid
+        for upper in (False, True):
+            cb = list(box)
+            cb[2 * a + (0 if upper else 1)] = mid
+            if meets(cb):
+                walk(cb, idx[below != upper], level + 1, me)
+
+    inside = np.all((pts >= [lo, lo, lo]) & (pts < [hi, hi, hi]), axis=1)
+    walk([lo, hi, lo, hi, lo, hi], np.nonzero(inside)[0], 0, -1)
+    return {"node_level": np.array(out["node_level"]), "node_parent": np.array(out["node_parent"]),
+            "node_count": np.array(out["node_count"]), "node_box": np.array(out["node_box"]),
+            "leaf_offsets": np.array(out["leaf_offsets"]), "members": np.array(out["members"], dtype=np.int64)}
+
+
 def mesh_root_box(vert_xyz: np.ndarray) -> np.ndarray:
     """Box3d(maxR) with its 1e-5 padding (src/LpmBox3d.h:21-33), maxR over the vertices
     (Coords::maxR, src/LpmCoords.cpp:136-143) -- the root of TreeSum's mesh constructor."""

@@ -23,6 +23,8 @@
  *                                                  velocity field (no solve) -> OUTDIR/mesh.vtk
  *   poisson  NPTS SEED OUTDIR                      DirectSum::meshfreeSolve (src/LpmDirectSum.cpp:240-252)
  *   time_poisson NPTS SEED [REPS]                  the same on this rank's slice, timed (CPU baseline)
+ *   sakajo   KIND LEVEL DEPTH OUTDIR              SakajoTree(4, DEPTH) over the leaf-face centroids
+ *                                                 (src/LpmSakajo2009.cpp:25-63,74-79,201-213): its non-empty nodes
  *                                                  with a 1/(4 pi r) ScalarKernel subclass
  *   pointtree NPTS SEED MAXLEAF OUTDIR             TreeSum(coords,...) meshfree ctor (src/LpmTreeSum.cpp:208-219)
  * KIND is icos|cube.  ZETA is rh (2z - sphereHarmonic54, the Rossby-Haurwitz m=4 wave with
@@ -39,6 +41,8 @@
 #include "LpmMPIReplicatedData.h"
 #include "LpmDirectSum.h"
 #include "LpmTreeSum.h"
+#include "LpmSakajo2009.h"
+#include "LpmSphericalCoords.h"
 #include "LpmVtkFileIO.h"
 #include <fstream>
 #include "LpmEuclideanCoords.h"
@@ -230,6 +234,48 @@ struct TreeProbe : public TreeSum {
     }
 };
 
+// SakajoTree's nodes after computeMoments: the non-empty ones (holding at least one point below them) in
+// depth-first order with their level, parent, point count and box, and the leaf membership at full depth.
+struct SakajoProbe : public SakajoTree {
+    using SakajoTree::SakajoTree;
+    int64_t count(const Node* node) const {
+        int64_t c = (int64_t)node->coordsContained.size();
+        for (const auto& k : node->kids) c += count(k.get());
+        return c;
+    }
+    void walk(const Node* node, int64_t parent, std::vector<int64_t>& level, std::vector<int64_t>& par,
+              std::vector<int64_t>& ncoords, std::vector<double>& box, std::vector<int64_t>& leaf_begin,
+              std::vector<int64_t>& members) const {
+        const int64_t c = count(node);
+        if (c == 0) return;
+        const int64_t me = (int64_t)level.size();
+        level.push_back(node->level);
+        par.push_back(parent);
+        ncoords.push_back(c);
+        const Box3d& b = node->box;
+        const double bb[6] = {b.xmin, b.xmax, b.ymin, b.ymax, b.zmin, b.zmax};
+        box.insert(box.end(), bb, bb + 6);
+        if (!node->coordsContained.empty()) {
+            leaf_begin.push_back((int64_t)members.size());
+            for (index_type j : node->coordsContained) members.push_back((int64_t)j);
+        }
+        for (const auto& k : node->kids) walk(k.get(), me, level, par, ncoords, box, leaf_begin, members);
+    }
+    void dump(const std::string& out) const {
+        std::vector<int64_t> level, par, ncoords, leaf_begin, members;
+        std::vector<double> box;
+        walk(_root.get(), -1, level, par, ncoords, box, leaf_begin, members);
+        leaf_begin.push_back((int64_t)members.size());
+        npy_i64(out, "node_level", level);
+        npy_i64(out, "node_parent", par);
+        npy_i64(out, "node_ncoords", ncoords);
+        npy_f64(out, "node_box", box, 6);
+        npy_i64(out, "leaf_offsets", leaf_begin);
+        npy_i64(out, "leaf_members", members);
+        npy_i64(out, "n_nodes_all", {(int64_t)_nnodes});
+    }
+};
+
 template <typename... Args>
 static TreeProbe* new_zeroed_probe(Args&&... args) {
     void* mem = ::operator new(sizeof(TreeProbe));
@@ -259,7 +305,7 @@ static uint64_t splitmix64(uint64_t& s) {
 static double uniform_pm1(uint64_t& s) { return 2.0 * ((splitmix64(s) >> 11) * (1.0 / 9007199254740992.0)) - 1.0; }
 
 static int usage() {
-    fprintf(stderr, "usage: ref_harness mesh|direct|scalar|vtk|tree|treesum|poisson|time_poisson|pointtree ...\n");
+    fprintf(stderr, "usage: ref_harness mesh|direct|scalar|vtk|tree|treesum|poisson|time_poisson|sakajo|pointtree ...\n");
     return 2;
 }
 
@@ -486,6 +532,26 @@ int main(int argc, char** argv) {
             secs += "]";
             printf("{\"cmd\": \"time_poisson\", \"rank\": %d, \"size\": %d, \"seconds\": %s, \"targets\": %ld, "
                    "\"sources\": %ld}\n", rank, size, secs.c_str(), (long)mp.msgSize(rank), (long)n);
+        } else if (cmd == "sakajo" && argc == 6) {
+            // SakajoTree(order 4, DEPTH, radius 1) over the leaf-face centroids of a mesh, computeMoments with
+            // the RH circulation, then the non-empty nodes and the full-depth leaf membership
+            auto seed = make_seed(argv[2]);
+            auto pm = std::make_shared<MeshedParticles>(*seed, atoi(argv[3]), false, 1.0, rank);
+            init_vorticity(*pm, "rh");
+            auto sc = std::make_shared<SphericalCoords>(pm->nLeafFaces());
+            auto circ = std::make_shared<Field>(pm->nLeafFaces(), 1, "circulation", "n/a");
+            std::vector<double> xyz;
+            for (index_type i = 0; i < pm->nFaces(); ++i) {
+                if (pm->faceIsDivided(i)) continue;
+                const XyzVector c = pm->getFaceCentroid(i);
+                sc->insert(c.x, c.y, c.z);
+                circ->insert(pm->getFaceFieldPtr("vorticity")->getScalar(i) * pm->getFaceArea(i));
+                xyz.push_back(c.x); xyz.push_back(c.y); xyz.push_back(c.z);
+            }
+            SakajoProbe tree(4, atoi(argv[4]), 1.0, 0.0, rank);
+            tree.computeMoments(sc, circ);
+            tree.dump(argv[5]);
+            npy_f64(argv[5], "xyz", xyz, 3);
         } else if (cmd == "pointtree" && argc == 6) {
             const index_type n = atol(argv[2]);
             uint64_t s = strtoull(argv[3], nullptr, 0);

@@ -20,11 +20,13 @@ Fixtures
   tree_icos8_m512.npz        TreeSum's mesh constructor at the treecode's full size (icos level 8, 512 per
                              leaf): node levels, parents, counts, boxes, leaf offsets and a digest of each
                              leaf's members (oracle.leaf_hashes) instead of the 1.3M member indices
+  sakajo_icos4_d3.npz,       SakajoTree(4, depth) over the leaf-face centroids (icos level 4 depth 3, cube level 4
+  sakajo_cube4_d2.npz        depth 2): its non-empty nodes and full-depth leaf membership, and the points
   vtk_icos2_rh.npz,          MeshedParticles::writeToVtkFile (non-Lagrangian icos level 2 / Lagrangian cube
   vtk_cube2_gauss_lag.npz    level 2) with vorticity and DirectSum velocity fields, and
                              VtkWriter::writePointsAndFieldsToCSV of the vertices: the files' bytes and the
                              field values written
-`python make_golden.py scalar vtk tree8` remakes only the named groups.
+`python make_golden.py scalar vtk tree8 sakajo` remakes only the named groups.
 """
 from __future__ import annotations
 
@@ -86,8 +88,16 @@ def tree8_fixture() -> None:
                         leaf_hash=oracle.leaf_hashes(z["leaf_members"], z["leaf_offsets"]))
 
 
+def sakajo_fixture() -> None:
+    for kind, level, depth in (("icos", 4, 3), ("cube", 4, 2)):
+        d = harness("sakajo", kind, level, depth)
+        z = load(d, "node_level", "node_parent", "node_ncoords", "node_box", "leaf_offsets", "leaf_members",
+                 "n_nodes_all", "xyz")
+        np.savez_compressed(HERE / f"sakajo_{kind}{level}_d{depth}.npz", **z)
+
+
 def main() -> None:
-    groups = {"scalar": scalar_fixture, "vtk": vtk_fixtures, "tree8": tree8_fixture}
+    groups = {"scalar": scalar_fixture, "vtk": vtk_fixtures, "tree8": tree8_fixture, "sakajo": sakajo_fixture}
     if sys.argv[1:]:
         for g in sys.argv[1:]:
             groups[g]()
@@ -95,6 +105,7 @@ def main() -> None:
     scalar_fixture()
     vtk_fixtures()
     tree8_fixture()
+    sakajo_fixture()
     for kind in ("icos", "cube"):
         d = harness("mesh", kind, 3)
         np.savez_compressed(HERE / f"mesh_{kind}3.npz",

@@ -168,3 +168,45 @@ def test_gpu_treesum_source_tree_matches_reference(ctx, kind, level, max_leaf):
     check_against_reference(g, members, offsets, tree.nodes(), lambda idx: leaf_faces[idx])
     tree.close()
     ts.close()
+
+
+SAKAJO = [("icos", 4, 3), ("cube", 4, 2)]
+
+
+@pytest.mark.parametrize("kind,level,depth", SAKAJO)
+def test_oracle_sakajo_tree_matches_reference(kind, level, depth):
+    g = golden(f"sakajo_{kind}{level}_d{depth}.npz")
+    t = oracle.sakajo_tree(g["xyz"], depth)
+    assert np.array_equal(t["node_level"], g["node_level"])
+    assert np.array_equal(t["node_parent"], g["node_parent"])
+    assert np.array_equal(t["node_count"], g["node_ncoords"])
+    assert np.array_equal(t["node_box"], g["node_box"])
+    assert np.array_equal(t["leaf_offsets"], g["leaf_offsets"])
+    assert np.array_equal(t["members"], g["leaf_members"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,level,depth", SAKAJO)
+def test_gpu_sakajo_tree_matches_reference(ctx, kind, level, depth):
+    """The treecode's source tree in Sakajo mode (sakajo_depth = L) is the reference SakajoTree's: every
+    non-empty node (depth-first: level, parent, point count, box) and the full-depth leaves' members."""
+    torch = ctx.use_torch_stream()
+    g = golden(f"sakajo_{kind}{level}_d{depth}.npz")
+    pts = oracle.pack4(g["xyz"], np.ones(g["xyz"].shape[0]))
+    d = torch.tensor(pts, device="cuda")
+    ts = L.TreeSum(ctx, L.biot_savart_kernel(), L.tree_solver(L.LPM_PREC_F32, 6, 1, 0.5, sakajo_depth=depth),
+                   pts.shape[0], pts.shape[0])
+    assert ts.get_param("sakajo_depth") == depth
+    out = torch.empty((3, pts.shape[0]), dtype=torch.float64, device="cuda")
+    ts.eval(d, d, out)
+    tree = ts.source_tree()
+    nodes = tree.nodes()
+    assert np.array_equal(nodes["node_level"], g["node_level"])
+    assert np.array_equal(nodes["node_parent"], g["node_parent"])
+    assert np.array_equal(nodes["node_count"], g["node_ncoords"])
+    assert np.array_equal(nodes["node_box"], g["node_box"])
+    members, offsets = tree.leaf_membership()
+    assert np.array_equal(offsets, g["leaf_offsets"])
+    assert np.array_equal(members, g["leaf_members"])
+    tree.close()
+    ts.close()

@@ -196,3 +196,27 @@ def test_poisson_treecode_1m_against_oracle(ctx):
     gpu64 = torch.empty((1, idx.size), dtype=torch.float64, device="cuda")
     ctx.direct_sum_dev(L.poisson_kernel(), L.LPM_PREC_F64, d, torch.tensor(p[idx], device="cuda"), gpu64)
     assert rel_l2(gpu64[0].cpu().numpy(), ref) < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("depth,order,tol", [(3, 8, 1e-4), (4, 10, 1e-5)])
+def test_sakajo_treecode_against_fp64_direct(ctx, depth, order, tol):
+    """The Sakajo (2009) tree with the library's far field (Chebyshev-form expansion of 1/|x - y|^2, batch
+    acceptance, FP32 near field): the velocity of the RH + Gaussian field on icos L6 against the FP64 direct
+    sum (the reference's SakajoTree shares TreeSum's moment-sign and series defects, so it is no accuracy
+    oracle)."""
+    torch = ctx.use_torch_stream()
+    inst = W.ensemble_instances(levels=(6,), per_level=1, seed=3)
+    _, p, n_src = inst[0]
+    d = torch.tensor(p, device="cuda")
+    ts = L.TreeSum(ctx, L.biot_savart_kernel(), L.tree_solver(L.LPM_PREC_F32, order, 1, 0.5, sakajo_depth=depth),
+                   n_src, p.shape[0])
+    out = torch.empty((3, p.shape[0]), dtype=torch.float64, device="cuda")
+    ts.eval(d[:n_src], d, out)
+    st = ts.stats()
+    ts.close()
+    ref = torch.empty_like(out)
+    ctx.direct_sum_dev(L.biot_savart_kernel(), L.LPM_PREC_F64, d[:n_src], d, ref, n_coincident=n_src)
+    err = float(torch.linalg.norm(out - ref) / torch.linalg.norm(ref))
+    assert st["far_evals"] > 0 and st["near_pairs"] > 0
+    assert err < tol, err
