@@ -92,6 +92,11 @@ const char* lpm_last_error(void);
 int64_t lpm_ctx_launch_count(const lpm_ctx* ctx);
 /* Per-kernel CUDA-event timing of uncaptured launches (on = 1).  lpm_ctx_profile_report synchronises,
  * writes {"kernel": {"ms": total, "launches": n}, ...} as JSON into buf and clears the records. */
+/* Run-time parameters of a context (no reference counterpart): "direct_targets" = targets per thread of the
+ * FP32 direct-sum tile kernels, 2, 4 (default) or 8 (results agree to FP32 rounding; the fastest depends on the
+ * sizes: lpmcxx_b200/autotune.py autotune_direct picks it). */
+int lpm_ctx_set_param(lpm_ctx* ctx, const char* name, double value);
+int lpm_ctx_get_param(const lpm_ctx* ctx, const char* name, double* value);
 int lpm_ctx_set_profiling(lpm_ctx* ctx, int on);
 int lpm_ctx_profile_report(lpm_ctx* ctx, char* buf, size_t len);
 

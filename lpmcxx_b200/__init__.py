@@ -172,6 +172,15 @@ class Context:
     def launch_count(self) -> int:
         return lib().lpm_ctx_launch_count(self.h)
 
+    def set_param(self, name: str, value: float) -> None:
+        """Context parameter (lpm_ctx_set_param): "direct_targets" (2, 4 or 8)."""
+        check(lib().lpm_ctx_set_param(self.h, name.encode(), float(value)), "lpm_ctx_set_param")
+
+    def get_param(self, name: str) -> float:
+        v = C.c_double()
+        check(lib().lpm_ctx_get_param(self.h, name.encode(), C.byref(v)), "lpm_ctx_get_param")
+        return v.value
+
     def set_profiling(self, on: bool) -> None:
         check(lib().lpm_ctx_set_profiling(self.h, 1 if on else 0), "lpm_ctx_set_profiling")
 

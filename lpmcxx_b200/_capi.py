@@ -78,6 +78,8 @@ SIGNATURES = {
     "lpm_ctx_launch_count": (C.c_int64, [P]),
     "lpm_fma_peak": (C.c_int, [P, C.c_int, C.POINTER(D)]),
     "lpm_ctx_set_profiling": (C.c_int, [P, C.c_int]),
+    "lpm_ctx_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
+    "lpm_ctx_get_param": (C.c_int, [P, C.c_char_p, P]),
     "lpm_ctx_profile_report": (C.c_int, [P, C.c_char_p, C.c_size_t]),
     "lpm_mesh_counts": (C.c_int, [C.c_int, C.c_int, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
     "lpm_mesh_build": (C.c_int, [C.c_int, C.c_int, D, P, P, P, P]),

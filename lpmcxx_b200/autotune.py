@@ -184,6 +184,37 @@ def tuned_solver(result: TuneResult, precision: int = LPM_PREC_F32):
     return tree_solver(precision, int(b.knob), b.max_per_leaf, b.theta)
 
 
+def autotune_direct(ctx: Context, kernel: KernelDesc, src, tgt, shapes=(2, 4, 8), reps: int = 3,
+                    n_coincident: int = 0) -> dict:
+    """Tile shape of the FP32 direct sum (targets per thread, the context's "direct_targets"): every shape timed
+    on device-resident src / tgt (median of `reps` CUDA-event timed sums after one warm-up); the fastest is set on
+    the context and returned with the timings and the largest relative deviation between the shapes' sums."""
+    import torch
+
+    comps = 1 if int(kernel.kind) == LPM_KERNEL_POISSON_3D else 3
+    out = torch.empty((comps, tgt.shape[0]), dtype=torch.float64, device=tgt.device)
+    ms, sums = {}, {}
+    for t in shapes:
+        ctx.set_param("direct_targets", t)
+        ctx.direct_sum_dev(kernel, LPM_PREC_F32, src, tgt, out, n_coincident=n_coincident)
+        times = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ctx.direct_sum_dev(kernel, LPM_PREC_F32, src, tgt, out, n_coincident=n_coincident)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms[t] = float(np.median(times))
+        sums[t] = out.clone()
+    best = min(ms, key=ms.get)
+    ctx.set_param("direct_targets", best)
+    ref = sums[best]
+    dev = max(float(torch.linalg.norm(v - ref) / torch.linalg.norm(ref)) for v in sums.values())
+    return {"direct_targets": best, "ms": ms, "max_rel_deviation": dev}
+
+
 def apply_tuned(result: TuneResult, solver) -> None:
     """Set the tuned run-time parameters on a TreeSum or RK4 made from tuned_solver(result)."""
     b = result.best
@@ -194,4 +225,4 @@ def apply_tuned(result: TuneResult, solver) -> None:
     solver.set_param("near_tile", b.near_tile)
 
 
-__all__ = ["autotune", "tuned_solver", "apply_tuned", "TuneResult", "Candidate", "default_grid", "LPM_PREC_F64"]
+__all__ = ["autotune", "autotune_direct", "tuned_solver", "apply_tuned", "TuneResult", "Candidate", "default_grid", "LPM_PREC_F64"]

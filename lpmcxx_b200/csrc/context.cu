@@ -4,6 +4,7 @@
 #include "lpm_internal.h"
 
 #include <atomic>
+#include <string>
 
 #include <cstdarg>
 #include <cstring>
@@ -254,4 +255,31 @@ int64_t lpm_ctx_launch_count(const lpm_ctx* ctx) { return ctx ? ctx->launches : 
 extern "C" int lpm_debug_fail_allocations(int64_t after) {
     lpm::g_fail_after.store(after < 0 ? -1 : after);
     return LPM_OK;
+}
+
+extern "C" int lpm_ctx_set_param(lpm_ctx* ctx, const char* name, double value) {
+    if (!ctx || !name) {
+        lpm::set_error("lpm_ctx_set_param: null argument");
+        return LPM_ERR_ARG;
+    }
+    const std::string n(name);
+    if (n == "direct_targets" && (value == 2.0 || value == 4.0 || value == 8.0)) {
+        ctx->direct_tpt = (int)value;
+        return LPM_OK;
+    }
+    lpm::set_error("lpm_ctx_set_param: unknown parameter or value out of range: %s = %g", name, value);
+    return LPM_ERR_ARG;
+}
+
+extern "C" int lpm_ctx_get_param(const lpm_ctx* ctx, const char* name, double* value) {
+    if (!ctx || !name || !value) {
+        lpm::set_error("lpm_ctx_get_param: null argument");
+        return LPM_ERR_ARG;
+    }
+    if (std::string(name) == "direct_targets") {
+        *value = ctx->direct_tpt;
+        return LPM_OK;
+    }
+    lpm::set_error("lpm_ctx_get_param: unknown parameter %s", name);
+    return LPM_ERR_ARG;
 }

@@ -65,7 +65,6 @@ __device__ __forceinline__ float rsqrt32(float x) {
 constexpr int kThreads = 256;
 constexpr int kTile = 256;
 constexpr int kTpt64 = 2;
-constexpr int kTpt32 = 4;
 
 // ------------------------------------------------------------------ FP64 Biot-Savart
 template <bool kDelta>
@@ -258,18 +257,18 @@ int launch_scalar_f64(lpm_ctx* ctx, const char* name, K kern, bool skip_self, co
 // src.w holds 2*strength.  Coincident (target, source) pairs -- a face-centroid target and its
 // own source -- can only sit at equal indices (see coinc_* arguments); tiles that may contain one
 // run the guarded loop, all others the unguarded one.
-template <bool kGuard, bool kDelta>
+template <bool kGuard, bool kDelta, int TPT>
 __device__ __forceinline__ void bs_f32_tile(const float4* tile, int m, const float* tx, const float* ty,
                                             const float* tz, float* ax, float* ay, float* az, float d2x2) {
     // Targets go in pairs through packed FMAs (fma.rn.f32x2); each lane rounds as the scalar form
     // d = t - s, rr = fma(dz, dz, fma(dy, dy, dx dx)), f = w / rr, a += f d:  t - s is fma(s, -1, t) and
     // a product is fma(a, b, -0), both exact restatements of the single-rounded operation.
-    static_assert(kTpt32 % 2 == 0, "targets are processed in pairs");
+    static_assert(TPT % 2 == 0, "targets are processed in pairs");
 #pragma unroll 4
     for (int k = 0; k < m; ++k) {
         const float4 s = tile[k];
 #pragma unroll
-        for (int t = 0; t < kTpt32; t += 2) {
+        for (int t = 0; t < TPT; t += 2) {
             float dx0, dx1, dy0, dy1, dz0, dz1, r0, r1, f0, f1;
             fma2p(dx0, dx1, s.x, s.x, -1.0f, tx[t], tx[t + 1]);
             fma2p(dy0, dy1, s.y, s.y, -1.0f, ty[t], ty[t + 1]);
@@ -291,7 +290,8 @@ __device__ __forceinline__ void bs_f32_tile(const float4* tile, int m, const flo
     }
 }
 
-template <bool kDelta>
+// TPT targets per thread (2, 4 or 8; the context's "direct_targets"), kThreads x TPT targets per block.
+template <bool kDelta, int TPT>
 __global__ void __launch_bounds__(kThreads) bs_f32_kernel(const float4* __restrict__ src, int64_t n_src,
                                                           const float4* __restrict__ tgt,
                                                           const double4* __restrict__ tgt64, int64_t n_tgt,
@@ -299,12 +299,12 @@ __global__ void __launch_bounds__(kThreads) bs_f32_kernel(const float4* __restri
                                                           int64_t stride, int64_t coinc_n, int64_t coinc_off,
                                                           int64_t src_part) {
     __shared__ float4 tile[kTile];
-    const int64_t blk0 = (int64_t)blockIdx.x * (kThreads * kTpt32);
+    const int64_t blk0 = (int64_t)blockIdx.x * (kThreads * TPT);
     const int64_t base = blk0 + threadIdx.x;
-    float tx[kTpt32], ty[kTpt32], tz[kTpt32], ax[kTpt32], ay[kTpt32], az[kTpt32];
-    double Dx[kTpt32], Dy[kTpt32], Dz[kTpt32];
+    float tx[TPT], ty[TPT], tz[TPT], ax[TPT], ay[TPT], az[TPT];
+    double Dx[TPT], Dy[TPT], Dz[TPT];
 #pragma unroll
-    for (int t = 0; t < kTpt32; ++t) {
+    for (int t = 0; t < TPT; ++t) {
         const int64_t i = base + t * kThreads;
         const float4 p = i < n_tgt ? tgt[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         tx[t] = p.x; ty[t] = p.y; tz[t] = p.z;
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(kThreads) bs_f32_kernel(const float4* __restri
     }
     // source indices that may coincide with this block's targets
     const int64_t c_lo = blk0 < coinc_n ? blk0 + coinc_off : INT64_MAX;
-    const int64_t c_hi = blk0 < coinc_n ? min(blk0 + kThreads * kTpt32, coinc_n) + coinc_off : INT64_MIN;
+    const int64_t c_hi = blk0 < coinc_n ? min(blk0 + kThreads * TPT, coinc_n) + coinc_off : INT64_MIN;
     // gridDim.y source parts of src_part sources each (a multiple of kTile): blockIdx.y sums its part
     const int64_t j_begin = (int64_t)blockIdx.y * src_part, j_end = min(n_src, j_begin + src_part);
     for (int64_t j0 = j_begin; j0 < j_end; j0 += kTile) {
@@ -322,16 +322,16 @@ __global__ void __launch_bounds__(kThreads) bs_f32_kernel(const float4* __restri
         __syncthreads();
         const int m = (int)min((int64_t)kTile, j_end - j0);
 #pragma unroll
-        for (int t = 0; t < kTpt32; ++t) { ax[t] = 0.f; ay[t] = 0.f; az[t] = 0.f; }
+        for (int t = 0; t < TPT; ++t) { ax[t] = 0.f; ay[t] = 0.f; az[t] = 0.f; }
         if (j0 < c_hi && j0 + m > c_lo)
-            bs_f32_tile<true, kDelta>(tile, m, tx, ty, tz, ax, ay, az, d2x2);
+            bs_f32_tile<true, kDelta, TPT>(tile, m, tx, ty, tz, ax, ay, az, d2x2);
         else
-            bs_f32_tile<false, kDelta>(tile, m, tx, ty, tz, ax, ay, az, d2x2);
+            bs_f32_tile<false, kDelta, TPT>(tile, m, tx, ty, tz, ax, ay, az, d2x2);
 #pragma unroll
-        for (int t = 0; t < kTpt32; ++t) { Dx[t] += ax[t]; Dy[t] += ay[t]; Dz[t] += az[t]; }
+        for (int t = 0; t < TPT; ++t) { Dx[t] += ax[t]; Dy[t] += ay[t]; Dz[t] += az[t]; }
     }
 #pragma unroll
-    for (int t = 0; t < kTpt32; ++t) {
+    for (int t = 0; t < TPT; ++t) {
         const int64_t i = base + t * kThreads;
         if (i < n_tgt) {
             const double4 p = tgt64[i];
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(kThreads) bs_f32_kernel(const float4* __restri
 }
 
 // ------------------------------------------------------------------ FP32 Poisson
-template <bool kGuard>
+template <bool kGuard, int TPT>
 __device__ __forceinline__ void poisson_f32_tile(const float4* tile, int m, const float* tx, const float* ty,
                                                  const float* tz, float* acc) {
     // targets in pairs through packed FMAs, rounded as the scalar form (see bs_f32_tile)
@@ -360,7 +360,7 @@ __device__ __forceinline__ void poisson_f32_tile(const float4* tile, int m, cons
     for (int k = 0; k < m; ++k) {
         const float4 s = tile[k];
 #pragma unroll
-        for (int t = 0; t < kTpt32; t += 2) {
+        for (int t = 0; t < TPT; t += 2) {
             float dx0, dx1, dy0, dy1, dz0, dz1, r0, r1;
             fma2p(dx0, dx1, s.x, s.x, -1.0f, tx[t], tx[t + 1]);
             fma2p(dy0, dy1, s.y, s.y, -1.0f, ty[t], ty[t + 1]);
@@ -378,24 +378,25 @@ __device__ __forceinline__ void poisson_f32_tile(const float4* tile, int m, cons
     }
 }
 
+template <int TPT>
 __global__ void __launch_bounds__(kThreads) poisson_f32_kernel(const float4* __restrict__ src, int64_t n_src,
                                                                const float4* __restrict__ tgt, int64_t n_tgt,
                                                                double mult, double* __restrict__ out, int64_t coinc_n,
                                                                int64_t coinc_off, int64_t src_part) {
     __shared__ float4 tile[kTile];
-    const int64_t blk0 = (int64_t)blockIdx.x * (kThreads * kTpt32);
+    const int64_t blk0 = (int64_t)blockIdx.x * (kThreads * TPT);
     const int64_t base = blk0 + threadIdx.x;
-    float tx[kTpt32], ty[kTpt32], tz[kTpt32], acc[kTpt32];
-    double phi[kTpt32];
+    float tx[TPT], ty[TPT], tz[TPT], acc[TPT];
+    double phi[TPT];
 #pragma unroll
-    for (int t = 0; t < kTpt32; ++t) {
+    for (int t = 0; t < TPT; ++t) {
         const int64_t i = base + t * kThreads;
         const float4 p = i < n_tgt ? tgt[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         tx[t] = p.x; ty[t] = p.y; tz[t] = p.z;
         phi[t] = 0.0;
     }
     const int64_t c_lo = blk0 < coinc_n ? blk0 + coinc_off : INT64_MAX;
-    const int64_t c_hi = blk0 < coinc_n ? min(blk0 + kThreads * kTpt32, coinc_n) + coinc_off : INT64_MIN;
+    const int64_t c_hi = blk0 < coinc_n ? min(blk0 + kThreads * TPT, coinc_n) + coinc_off : INT64_MIN;
     const int64_t j_begin = (int64_t)blockIdx.y * src_part, j_end = min(n_src, j_begin + src_part);
     for (int64_t j0 = j_begin; j0 < j_end; j0 += kTile) {
         __syncthreads();
@@ -404,16 +405,16 @@ __global__ void __launch_bounds__(kThreads) poisson_f32_kernel(const float4* __r
         __syncthreads();
         const int m = (int)min((int64_t)kTile, j_end - j0);
 #pragma unroll
-        for (int t = 0; t < kTpt32; ++t) acc[t] = 0.f;
+        for (int t = 0; t < TPT; ++t) acc[t] = 0.f;
         if (j0 < c_hi && j0 + m > c_lo)
-            poisson_f32_tile<true>(tile, m, tx, ty, tz, acc);
+            poisson_f32_tile<true, TPT>(tile, m, tx, ty, tz, acc);
         else
-            poisson_f32_tile<false>(tile, m, tx, ty, tz, acc);
+            poisson_f32_tile<false, TPT>(tile, m, tx, ty, tz, acc);
 #pragma unroll
-        for (int t = 0; t < kTpt32; ++t) phi[t] += acc[t];
+        for (int t = 0; t < TPT; ++t) phi[t] += acc[t];
     }
 #pragma unroll
-    for (int t = 0; t < kTpt32; ++t) {
+    for (int t = 0; t < TPT; ++t) {
         const int64_t i = base + t * kThreads;
         if (i < n_tgt) {
             if (gridDim.y == 1) out[i] = mult * phi[t];
@@ -495,11 +496,28 @@ int source_parts(lpm_ctx* ctx, Kern kern, int64_t blocks, int64_t n_src) {
 }
 }  // namespace
 
+template <int TPT>
+static int direct_sum_f32_tpt(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* src, int64_t n_src,
+                              const float4* tgt, const double4* tgt64, int64_t n_tgt, double* out, int64_t out_stride,
+                              int64_t coinc_n, int64_t coinc_off);
+
 int direct_sum_f32_impl(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* src, int64_t n_src, const float4* tgt,
                         const double4* tgt64, int64_t n_tgt, double* out, int64_t out_stride, int64_t coinc_n,
                         int64_t coinc_off) {
+    switch (ctx->direct_tpt) {
+        case 2: return direct_sum_f32_tpt<2>(ctx, k, src, n_src, tgt, tgt64, n_tgt, out, out_stride, coinc_n, coinc_off);
+        case 8: return direct_sum_f32_tpt<8>(ctx, k, src, n_src, tgt, tgt64, n_tgt, out, out_stride, coinc_n, coinc_off);
+        default:
+            return direct_sum_f32_tpt<4>(ctx, k, src, n_src, tgt, tgt64, n_tgt, out, out_stride, coinc_n, coinc_off);
+    }
+}
+
+template <int TPT>
+static int direct_sum_f32_tpt(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* src, int64_t n_src,
+                              const float4* tgt, const double4* tgt64, int64_t n_tgt, double* out, int64_t out_stride,
+                              int64_t coinc_n, int64_t coinc_off) {
     if (n_tgt <= 0) return LPM_OK;
-    const unsigned grid = grid_for(n_tgt, kThreads * kTpt32);
+    const unsigned grid = grid_for(n_tgt, kThreads * TPT);
     auto zero_rows = [&](int rows) -> int {
         for (int c = 0; c < rows; ++c)
             LPM_CUDA_TRY(cudaMemsetAsync(out + (size_t)c * out_stride, 0, sizeof(double) * (size_t)n_tgt, ctx->stream));
@@ -508,8 +526,8 @@ int direct_sum_f32_impl(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* sr
     if (k.kind == LPM_KERNEL_BIOT_SAVART_SPHERE) {
         const double mult = -1.0 / (4.0 * kPi * k.radius);
         const bool delta = k.delta != 0.0;
-        const int parts = delta ? source_parts(ctx, bs_f32_kernel<true>, grid, n_src)
-                                : source_parts(ctx, bs_f32_kernel<false>, grid, n_src);
+        const int parts = delta ? source_parts(ctx, bs_f32_kernel<true, TPT>, grid, n_src)
+                                : source_parts(ctx, bs_f32_kernel<false, TPT>, grid, n_src);
         const int64_t part = parts == 1 ? n_src : ((n_src + 2 * kTile - 1) / (2 * kTile)) * kTile;
         if (parts > 1) {
             int rc = zero_rows(3);
@@ -517,20 +535,20 @@ int direct_sum_f32_impl(lpm_ctx* ctx, const lpm_kernel_desc& k, const float4* sr
         }
         const dim3 g(grid, parts);
         if (delta)
-            LPM_LAUNCH(ctx, "bs_f32_kernel", bs_f32_kernel<true>, g, kThreads, 0, src, n_src, tgt, tgt64, n_tgt,
+            LPM_LAUNCH(ctx, "bs_f32_kernel", (bs_f32_kernel<true, TPT>), g, kThreads, 0, src, n_src, tgt, tgt64, n_tgt,
                        (float)(2.0 * k.delta * k.delta), mult, out, out_stride, coinc_n, coinc_off, part);
         else
-            LPM_LAUNCH(ctx, "bs_f32_kernel", bs_f32_kernel<false>, g, kThreads, 0, src, n_src, tgt, tgt64, n_tgt, 0.0f,
+            LPM_LAUNCH(ctx, "bs_f32_kernel", (bs_f32_kernel<false, TPT>), g, kThreads, 0, src, n_src, tgt, tgt64, n_tgt, 0.0f,
                        mult, out, out_stride, coinc_n, coinc_off, part);
     } else if (k.kind == LPM_KERNEL_POISSON_3D) {
-        const int parts = source_parts(ctx, poisson_f32_kernel, grid, n_src);
+        const int parts = source_parts(ctx, poisson_f32_kernel<TPT>, grid, n_src);
         const int64_t part = parts == 1 ? n_src : ((n_src + 2 * kTile - 1) / (2 * kTile)) * kTile;
         if (parts > 1) {
             int rc = zero_rows(1);
             if (rc) return rc;
         }
         const dim3 g(grid, parts);
-        LPM_LAUNCH(ctx, "poisson_f32_kernel", poisson_f32_kernel, g, kThreads, 0, src, n_src, tgt, n_tgt,
+        LPM_LAUNCH(ctx, "poisson_f32_kernel", poisson_f32_kernel<TPT>, g, kThreads, 0, src, n_src, tgt, n_tgt,
                    1.0 / (4.0 * kPi), out, coinc_n, coinc_off, part);
     } else {
         set_error("invalid kernel");

@@ -50,6 +50,8 @@ struct lpm_ctx {
     size_t pinned_bytes = 0;
     // incremented whenever a scratch slot is reallocated: a CUDA graph captured before holds the old address
     uint64_t generation = 0;
+    // FP32 direct sums: targets per thread of the tile kernels (2, 4 or 8; lpm_ctx_set_param "direct_targets")
+    int direct_tpt = 4;
 };
 
 namespace lpm {

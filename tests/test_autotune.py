@@ -57,3 +57,28 @@ def test_autotune_fixed_poisson(ctx):
     res = autotune(ctx, L.poisson_kernel(), d, d, tol, learned=False, grid=((128, 256), (0.5, 0.7), (4, 6)),
                    batch_levels=(0,), sample=2048)
     check(res, tol)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["biot_savart", "poisson"])
+def test_autotune_direct_tile_shape(ctx, kernel):
+    """The FP32 direct sum's tile shape (2, 4 or 8 targets per thread) is tuned at run time: every shape is timed,
+    the fastest is kept on the context, and the shapes' sums agree to FP32 rounding."""
+    from lpmcxx_b200.autotune import autotune_direct
+
+    torch = ctx.use_torch_stream()
+    if kernel == "biot_savart":
+        _, p, n_src = W.gaussian_vortex_mesh("icos", 6)
+        kern, nc = L.biot_savart_kernel(), n_src
+    else:
+        p = W.poisson_cube(100_000)
+        n_src, kern, nc = p.shape[0], L.poisson_kernel(), p.shape[0]
+    d = torch.tensor(p, device="cuda")
+    res = autotune_direct(ctx, kern, d[:n_src], d, n_coincident=nc)
+    assert set(res["ms"]) == {2, 4, 8}
+    assert res["direct_targets"] == min(res["ms"], key=res["ms"].get)
+    assert ctx.get_param("direct_targets") == res["direct_targets"]
+    assert res["max_rel_deviation"] < 1e-6
+    ctx.set_param("direct_targets", 4)
+    with pytest.raises(L.LpmError):
+        ctx.set_param("direct_targets", 3)
