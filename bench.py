@@ -501,24 +501,26 @@ def run_gpu_direct_cube(args) -> None:
 
 
 ENSEMBLE_METRIC = "ensemble RK4 steps/s: 64 instances (icos L5/L6/L7/L8 x 16, 27.85M sources), learned treecode"
-ENSEMBLE_TUNE_GRID = ((128, 256, 512), (0.5, 0.6), (2e-7, 5e-7))  # leaf sizes, theta, learned budgets
+ENSEMBLE_TUNE_GRID = ((128, 256, 512), (0.4, 0.5, 0.6), (2e-7, 5e-7))  # leaf sizes, theta, learned budgets
 
 
-def ensemble_tune(ctx, kern, inst, tol: float = 5e-7) -> dict:
-    """Per size class (icos level): the autotuner on the class's first instance (learned selector, order bias
-    2, leaf x theta x budget x batch level, then the near tile shape), judged on 4096 sampled targets against
-    the FP64 direct sum.  The class's other instances carry other vortices, so the tolerance is half the 1e-6
-    the configuration asks of every instance (with the tuner's own 0.8 safety factor on top)."""
+def ensemble_tune(ctx, kern, inst, tol: float = 1e-6) -> dict:
+    """Per size class (icos level): the autotuner (learned selector, order bias 2, leaf x theta x budget x batch
+    level, then the near tile shape) timed on the class's first instance; the chosen setting meets the tolerance
+    (with the tuner's 0.8 safety factor) on 4096 sampled targets of every instance of the class against the FP64
+    direct sum, since the instances carry different vortices."""
     import torch
 
     from lpmcxx_b200.autotune import autotune
 
     tuned = {}
     for level in sorted({lvl for lvl, _, _ in inst}):
-        _, p, n_src = next(x for x in inst if x[0] == level)
-        d = torch.tensor(p, device="cuda")
+        members = [torch.tensor(p, device="cuda") for lvl, p, _ in inst if lvl == level]
+        n_src = next(n for lvl, _, n in inst if lvl == level)
+        d = members[0]
         res = autotune(ctx, kern, d[:n_src], d, tol=tol, learned=True, grid=ENSEMBLE_TUNE_GRID,
-                       batch_levels=(0, -1), order_biases=(2,), sample=4096, reps=2)
+                       batch_levels=(0, -1), order_biases=(2,), sample=4096, reps=2,
+                       also=[(m[:n_src], m) for m in members[1:]])
         if res.best is None:
             raise RuntimeError(f"ensemble tuning: no candidate meets {tol} at icos L{level}")
         tuned[level] = res.as_dict()

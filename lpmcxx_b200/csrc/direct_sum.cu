@@ -577,6 +577,16 @@ int check_kernel_desc(const lpm_kernel_desc* k) {
     return LPM_OK;
 }
 
+// The FP32 direct sums exist for the Biot-Savart and 3D Poisson kernels only; every FP32 entry point checks
+// this before it launches anything.
+int check_f32_kind(const lpm_kernel_desc& k) {
+    if (k.kind != LPM_KERNEL_BIOT_SAVART_SPHERE && k.kind != LPM_KERNEL_POISSON_3D) {
+        set_error("invalid kernel: the FP32 direct sum takes the Biot-Savart and 3D Poisson kernels (use LPM_PREC_F64)");
+        return LPM_ERR_KERNEL;
+    }
+    return LPM_OK;
+}
+
 // Device entry shared by the C ABI: FP64 or FP32 (FP32 copies go to scratch slots).
 int direct_sum_any(lpm_ctx* ctx, const lpm_kernel_desc& k, int precision, const double4* src, int64_t n_src,
                    const double4* tgt, int64_t n_tgt, double* out, int64_t coinc_n, int64_t coinc_off) {
@@ -585,14 +595,12 @@ int direct_sum_any(lpm_ctx* ctx, const lpm_kernel_desc& k, int precision, const 
         set_error("unknown precision %d", precision);
         return LPM_ERR_ARG;
     }
-    if (k.kind != LPM_KERNEL_BIOT_SAVART_SPHERE && k.kind != LPM_KERNEL_POISSON_3D) {
-        set_error("invalid kernel: the FP32 direct sum takes the Biot-Savart and 3D Poisson kernels (use LPM_PREC_F64)");
-        return LPM_ERR_KERNEL;
-    }
+    int rc = check_f32_kind(k);
+    if (rc) return rc;
     float4* s32 = (float4*)scratch(ctx, kSlotSrc32, sizeof(float4) * (size_t)std::max<int64_t>(n_src, 1));
     float4* t32 = (float4*)scratch(ctx, kSlotTgt32, sizeof(float4) * (size_t)std::max<int64_t>(n_tgt, 1));
     if (!s32 || !t32) return LPM_ERR_OOM;
-    int rc = pack_f32(ctx, src, n_src, s32, k.kind == LPM_KERNEL_BIOT_SAVART_SPHERE);
+    rc = pack_f32(ctx, src, n_src, s32, k.kind == LPM_KERNEL_BIOT_SAVART_SPHERE);
     if (rc) return rc;
     rc = pack_f32(ctx, tgt, n_tgt, t32, false);
     if (rc) return rc;

@@ -140,6 +140,7 @@ int direct_sum_any(lpm_ctx* ctx, const lpm_kernel_desc& k, int precision, const 
                    const double4* tgt, int64_t n_tgt, double* out, int64_t coinc_n, int64_t coinc_off);
 int pack_f32(lpm_ctx* ctx, const double4* in, int64_t n, float4* out, bool scale_w2);
 int check_kernel_desc(const lpm_kernel_desc* k);
+int check_f32_kind(const lpm_kernel_desc& k);  // LPM_ERR_KERNEL unless Biot-Savart or 3D Poisson
 
 // Packed FP32 (fma.rn.f32x2, sm_100): two FP32 FMAs in one instruction, each lane rounded like fmaf.
 // (d0, d1) = (a0 b + c0, a1 b + c1).

@@ -57,6 +57,8 @@ extern "C" int lpm_direct_sum_f32_noalloc(const lpm_kernel_desc* kernel, const d
                                           void* cuda_stream) {
     int rc = check_kernel_desc(kernel);
     if (rc) return rc;
+    rc = check_f32_kind(*kernel);
+    if (rc) return rc;
     if (n_src < 0 || n_tgt < 0 || (n_src > 0 && !src) || (n_tgt > 0 && (!tgt || !out)) || n_coincident < 0 ||
         n_coincident > std::min(n_src, n_tgt)) {
         set_error("lpm_direct_sum_f32_noalloc: bad sizes or null pointers");

@@ -49,6 +49,43 @@ def test_autotune_learned_sphere(ctx):
 
 
 @pytest.mark.gpu
+def test_autotune_meets_tolerance_on_every_workload(ctx):
+    """With `also`, the pick is timed on the first workload but meets the tolerance on every one: checked here
+    against the FP64 direct sum on all targets of each of four ensemble members (icos L5, different vortices),
+    and the reported error is the largest over the members."""
+    torch = ctx.use_torch_stream()
+    inst = W.ensemble_instances(levels=(5,), per_level=4)
+    ds = [torch.tensor(p, device="cuda") for _, p, _ in inst]
+    n_src = inst[0][2]
+    tol = 1e-6
+    res = autotune(ctx, L.biot_savart_kernel(), ds[0][:n_src], ds[0], tol, learned=True,
+                   grid=((128, 256), (0.5, 0.6, 0.7), (3e-7, 1e-6)), sample=2048, order_biases=(2,),
+                   also=[(d[:n_src], d) for d in ds[1:]])
+    check(res, tol)
+    ts = L.TreeSum(ctx, L.biot_savart_kernel(), tuned_solver(res), n_src, ds[0].shape[0])
+    ts.set_mlp(L.learned.load()[0])
+    apply_tuned(res, ts)
+    errs = []
+    for d in ds:
+        out = torch.empty((3, d.shape[0]), dtype=torch.float64, device="cuda")
+        ts.eval(d[:n_src], d, out)
+        ref = torch.empty_like(out)
+        ctx.direct_sum_dev(L.biot_savart_kernel(), L.LPM_PREC_F64, d[:n_src], d, ref)
+        errs.append(float(torch.linalg.norm(out - ref) / torch.linalg.norm(ref)))
+    ts.close()
+    assert max(errs) < tol
+    assert res.best.rel_err >= 0.5 * max(errs)  # the largest over the members, on 2048 sampled targets each
+
+
+def test_autotune_rejects_larger_extra_workload():
+    torch = pytest.importorskip("torch")
+    small = torch.zeros((10, 4), dtype=torch.float64)
+    big = torch.zeros((20, 4), dtype=torch.float64)
+    with pytest.raises(ValueError, match="larger than the first"):
+        autotune(None, L.biot_savart_kernel(), small, small, 1e-6, learned=False, also=[(big, big)])
+
+
+@pytest.mark.gpu
 def test_autotune_fixed_poisson(ctx):
     torch = ctx.use_torch_stream()
     p = W.poisson_cube(60_000)

@@ -50,3 +50,21 @@ def test_no_alloc_rejects_oversized_calls(ctx):
                                                 None)
     assert rc == _capi.LPM_ERR_CAPACITY
     assert b"static scratch" in _capi.lib().lpm_last_error()
+
+
+@pytest.mark.parametrize("kernel", [L.sphere_greens_kernel(), L.planar_log_kernel(), L.delta3d_kernel(0.1),
+                                    L.sphere_delta_kernel(0.1)], ids=["sphere_greens", "planar_log", "delta3d",
+                                                                      "sphere_delta"])
+def test_no_alloc_rejects_scalar_kernels_before_any_launch(ctx, kernel):
+    """The scalar kernels have no FP32 direct sum: the call fails with the regular entry point's message before
+    the capacity check and before it writes the shared array or the output (which keeps its NaNs)."""
+    torch = ctx.use_torch_stream()
+    n = 300_000  # also over capacity: the kind check comes first
+    d = torch.zeros((n, 4), dtype=torch.float64, device="cuda")
+    out = torch.full((1, n), float("nan"), dtype=torch.float64, device="cuda")
+    rc = _capi.lib().lpm_direct_sum_f32_noalloc(C.byref(kernel), d.data_ptr(), n, d.data_ptr(), n, 0,
+                                                out.data_ptr(), None)
+    assert rc == _capi.LPM_ERR_KERNEL
+    assert b"FP32 direct sum takes the Biot-Savart and 3D Poisson kernels" in _capi.lib().lpm_last_error()
+    torch.cuda.synchronize()
+    assert torch.isnan(out).all()
