@@ -270,15 +270,20 @@ def far_entries(p: int) -> int:
 
 def kernel_work(kernel: str, n_src: int, n_tgt: int, stats: dict | None, order: int) -> tuple[float, str] | None:
     """Algorithmic flops of one launch of `kernel`: 17 per Biot-Savart pair (direct and near field), 8 per
-    far-field expansion coefficient plus 40 per (target, cluster) evaluation."""
+    far-field expansion coefficient plus FLOPS_PER_FAR_EVAL per (target, cluster) evaluation."""
     if kernel in ("bs_f32_kernel", "bs_f64_kernel"):
         return FLOPS_PER_BS_PAIR * float(n_src) * float(n_tgt), "TFLOP/s"
     if kernel == "near_kernel" and stats:
         return FLOPS_PER_BS_PAIR * float(stats["near_pairs"]), "TFLOP/s"
     if kernel == "far_kernel" and stats:
-        # 4 coefficient FMAs (8 flops) per expansion coefficient + ~40 flops of setup per evaluation
-        return 8.0 * float(stats["far_terms"]) + 40.0 * float(stats["far_evals"]), "TFLOP/s"
+        # 4 coefficient FMAs (8 flops) per expansion coefficient + the per-evaluation setup and fold
+        return 8.0 * float(stats["far_terms"]) + FLOPS_PER_FAR_EVAL * float(stats["far_evals"]), "TFLOP/s"
     return None
+
+
+# Per (target, cluster) evaluation outside the Horner scheme: d = c - x (3), |d|^2 (5), 1/|d|^2 (1), the
+# scaled offsets e = d/|d|^2 (3) and the folded sum h += (d g0 + g)/|d|^2 (12).
+FLOPS_PER_FAR_EVAL = 24.0
 
 
 POISSON_METRIC = "3D Poisson 1/(4 pi r) treecode evaluations/s @1,048,576 pts (p=6, theta=0.6) vs FP64 direct"
@@ -582,6 +587,7 @@ def run_gpu_ensemble(args) -> None:
         rk.set_param("batch_level", tuned[lvl]["batch_level"])
         rk.set_param("near_targets", tuned[lvl]["near_targets"])
         rk.set_param("near_tile", tuned[lvl]["near_tile"])
+        rk.set_param("near_split", tuned[lvl]["near_split"])
         rk.set_state(p)
     err_t0 = ensemble_accuracy(ctx, kern, ens, inst)
     dt = 0.01
@@ -609,7 +615,7 @@ def run_gpu_ensemble(args) -> None:
     work = 0.0
     for i in range(len(inst)):
         st = ens.instance(i).tree_stats()
-        work += 4.0 * (FLOPS_PER_BS_PAIR * st["near_pairs"] + 8.0 * st["far_terms"] + 40.0 * st["far_evals"])
+        work += 4.0 * (FLOPS_PER_BS_PAIR * st["near_pairs"] + 8.0 * st["far_terms"] + FLOPS_PER_FAR_EVAL * st["far_evals"])
     fp32_peak = ctx.fma_peak_tflops(L.LPM_PREC_F32)
     achieved = work / (float(np.mean(ms)) * 1e-3) * 1e-12
     # end to end: every instance's state from pinned host memory, one step, every state back
@@ -644,7 +650,7 @@ def run_gpu_ensemble(args) -> None:
         "roofline": {"bound": "fp32", "kernel": "whole step (near + far field, all instances)",
                      "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                      "traffic": None, "peak_source": "measured FMA microbenchmark (lpm_fma_peak) on this GPU",
-                     "work": "17 flops per near pair + 8 per far coefficient + 40 per far evaluation, 4 "
+                     "work": "17 flops per near pair + 8 per far coefficient + 24 per far evaluation, 4 "
                              "evaluations per step, from each instance's tree statistics"},
         "e2e": {"value": world / float(np.mean(e2e_s)), "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes},

@@ -283,7 +283,11 @@ int lpm_treesum_stats(lpm_treesum* ts, int64_t* out10);
  * LPM_PREC_F64); "batch_level": octree level whose cells a target batch may not straddle (1 .. the
  * level chosen at creation; coarser levels give fuller batches); "order_bias" (LPM_ORDER_LEARNED solvers
  * only, LPM_ERR_ARG otherwise; acts while selector weights are loaded): 0..3 orders added to every order the
- * selector picks, capped at 11.
+ * selector picks, capped at 11.  "eps": the learned selector's per-pair error budget.  The near-field tile
+ * shape changes the time only (and the FP32 rounding, since it moves the points where FP32 partial sums fold
+ * into FP64): "near_targets" 2 or 4 targets per thread, "near_tile" 256, 512 or 1024 sources staged in shared
+ * memory per tile, "near_split" 1 or 2 thread groups that each hold a whole target batch and sum their share
+ * of every tile.
  * The source octree's root box is the reference's Box3d(R) with its 1e-5 padding (src/LpmBox3d.h:21-33), so
  * that its leaves are the reference TreeSum's (src/LpmTreeSum.cpp:221-238).  Biot-Savart: R = "root_maxr"
  * when positive (default 0), else maxR (Coords::maxR, src/LpmCoords.cpp:136-143) of the targets from index

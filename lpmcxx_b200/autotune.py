@@ -10,7 +10,8 @@ parameters (`TreeSum.set_param`), so a sweep costs one octree allocation per lea
     best = autotune(ctx, L.biot_savart_kernel(), src, tgt, tol=1e-6, order_biases=(0, 2))
     solver = tuned_solver(best)            # an lpm_solver_desc for TreeSum / RK4
     # then set_param("batch_level", best.best.batch_level) and set_param("order_bias", best.best.bias),
-    # set_param("near_targets", best.best.near_targets) and set_param("near_tile", best.best.near_tile)
+    # set_param("near_targets", ...), set_param("near_tile", ...) and set_param("near_split", ...) from
+    # best.best (apply_tuned does all of these)
 
 The tile shape (targets per thread of the near-field kernel and sources staged per shared-memory tile)
 changes no result, only the time, so it is searched last, on the fastest qualifying setting.
@@ -34,8 +35,9 @@ class Candidate:
     bias: int = 0           # learned: orders added to every selector choice
     ms: float | None = None
     rel_err: float | None = None
-    near_targets: int = 2   # near-field tile shape (run-time parameters "near_targets", "near_tile")
+    near_targets: int = 2   # near-field tile shape (run-time "near_targets", "near_tile", "near_split")
     near_tile: int = 512
+    near_split: int = 1
 
 
 @dataclass
@@ -50,7 +52,7 @@ class TuneResult:
         return {"learned": self.learned, "max_per_leaf": b.max_per_leaf, "theta": b.theta,
                 ("eps" if self.learned else "order"): b.knob, "batch_level": b.batch_level,
                 "order_bias": b.bias, "ms": b.ms, "rel_err": b.rel_err, "near_targets": b.near_targets,
-                "near_tile": b.near_tile}
+                "near_tile": b.near_tile, "near_split": b.near_split}
 
 
 def default_grid(learned: bool, kernel_kind: int):
@@ -83,15 +85,16 @@ def _timed_eval(ctx, ts, src, tgt, out, reps):
 
 def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bool = True, params=None,
              grid=None, batch_levels=(0, -1), sample: int = 4096, reps: int = 3, seed: int = 0,
-             safety: float = 0.8, order_biases=(0,), tiles=((2, 256), (2, 512), (2, 1024), (4, 256), (4, 512),
-                                                            (4, 1024)), also=()) -> TuneResult:
+             safety: float = 0.8, order_biases=(0,),
+             tiles=tuple((t, s, g) for g in (1, 2) for t in (2, 4) for s in (256, 512, 1024)),
+             also=()) -> TuneResult:
     """Sweep the grid on device-resident src (n_src, 4) / tgt (n_tgt, 4) float64 tensors.
 
     tol: relative L2 tolerance over the sampled targets (a candidate must reach safety * tol).
     learned: tune the learned selector's budget (Biot-Savart only) instead of the fixed order.
     batch_levels: offsets from each solver's default batch cell level to try (0 = default).
     order_biases: learned only, the selector order biases to try (set_param "order_bias").
-    tiles: (near_targets, near_tile) shapes of the near-field kernel, tried on the best setting.
+    tiles: (near_targets, near_tile, near_split) shapes of the near-field kernel, tried on the best setting.
     also: further (src, tgt) workloads, no larger than the first, that the chosen setting must meet the tolerance
       on too (other states of the same problem: an ensemble's members, later time steps).  Time is judged on the
       first workload only; a candidate faster than the best so far is checked on every workload in `also`, and its
@@ -168,7 +171,7 @@ def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bo
                         if checks and err <= safety * tol and (res.best is None or ms < res.best.ms):
                             err = worst_error(ts, err)
                         c = Candidate(leaf, theta, knob, lvl, bias, ms, err, int(ts.get_param("near_targets")),
-                                      int(ts.get_param("near_tile")))
+                                      int(ts.get_param("near_tile")), int(ts.get_param("near_split")))
                         res.tried.append(c)
                         if err <= safety * tol and (res.best is None or ms < res.best.ms):
                             res.best = c
@@ -184,14 +187,15 @@ def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bo
                 ts.set_mlp(params)
                 ts.set_param("order_bias", b.bias)
             ts.set_param("batch_level", b.batch_level)
-            for nt, tile in tiles:
+            for nt, tile, split in tiles:
                 ts.set_param("near_targets", nt)
                 ts.set_param("near_tile", tile)
+                ts.set_param("near_split", split)
                 ms = _timed_eval(ctx, ts, src, tgt, out, reps)
                 err = float(torch.linalg.norm(out[:, idx_t] - ref)) / ref_norm
                 if checks and err <= safety * tol and ms < res.best.ms:
                     err = worst_error(ts, err)
-                c = Candidate(b.max_per_leaf, b.theta, b.knob, b.batch_level, b.bias, ms, err, nt, tile)
+                c = Candidate(b.max_per_leaf, b.theta, b.knob, b.batch_level, b.bias, ms, err, nt, tile, split)
                 res.tried.append(c)
                 if err <= safety * tol and ms < res.best.ms:
                     res.best = c
@@ -203,8 +207,8 @@ def autotune(ctx: Context, kernel: KernelDesc, src, tgt, tol: float, learned: bo
 def tuned_solver(result: TuneResult, precision: int = LPM_PREC_F32):
     """lpm_solver_desc of the tuned setting (the batch level, the order bias and the near-field tile shape
     are run-time parameters: apply them with set_param("batch_level", ...), set_param("order_bias", ...),
-    set_param("near_targets", ...) and set_param("near_tile", ...) on the TreeSum / RK4 made from this
-    descriptor; apply_tuned does all four)."""
+    set_param("near_targets", ...), set_param("near_tile", ...) and set_param("near_split", ...) on the
+    TreeSum / RK4 made from this descriptor; apply_tuned does all of them)."""
     b = result.best
     if b is None:
         raise ValueError("no candidate met the tolerance")
@@ -252,6 +256,7 @@ def apply_tuned(result: TuneResult, solver) -> None:
         solver.set_param("order_bias", b.bias)
     solver.set_param("near_targets", b.near_targets)
     solver.set_param("near_tile", b.near_tile)
+    solver.set_param("near_split", b.near_split)
 
 
 __all__ = ["autotune", "autotune_direct", "tuned_solver", "apply_tuned", "TuneResult", "Candidate", "default_grid", "LPM_PREC_F64"]

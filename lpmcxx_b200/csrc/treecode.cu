@@ -1091,29 +1091,31 @@ constexpr int kFar2MinBlocks = LPM_FAR2_MIN_BLOCKS;
 
 // The far2 kernel's per-entry work in FP32 throughout: centres and targets are offsets from a point of the
 // batch (its first target), so d = c - x is one FP32 subtraction; 1/|d|^2 by the approximate reciprocal
-// (1 ulp); contributions summed in FP32 over a stage (acc32) and folded into FP64 once per stage.  x holds
-// the targets' absolute FP32 coordinates (for x cross d), xo their offsets, c the centre's offset.
+// (1 ulp).  A cluster adds x cross (2/|d|^2) (d g0 + g) to the target's sum, linear in the target position x,
+// so the kernel sums only h = (1/|d|^2) (d g0 + g) over the clusters and applies 2 x cross (.) once per
+// target at the end in FP64: acc32 += h in FP32 over a stage, folded into FP64 once per stage.  Every step
+// runs on the two targets together (fma.rn.f32x2, each lane rounding as the scalar operation); xo holds the
+// targets' offsets and c the centre's.
 template <int P>
-__device__ __forceinline__ void far_one_acc2_f32(const float4* __restrict__ Bc, const float (&x)[2][3],
-                                                 const float (&xo)[2][3], const float4 c, float (&acc32)[2][3]) {
-    float d[2][3], e[2][4], g[2][4];
+__device__ __forceinline__ void far_one_acc2_f32(const float4* __restrict__ Bc, const float (&xo)[2][3],
+                                                 const float4 c, float (&acc32)[2][3]) {
+    float d[2][3], e[2][4], g[2][4], r0, r1;
+    fma2p(d[0][0], d[1][0], xo[0][0], xo[1][0], -1.0f, c.x, c.x);  // c - xo, one rounding
+    fma2p(d[0][1], d[1][1], xo[0][1], xo[1][1], -1.0f, c.y, c.y);
+    fma2p(d[0][2], d[1][2], xo[0][2], xo[1][2], -1.0f, c.z, c.z);
+    fma2v(r0, r1, d[0][0], d[1][0], d[0][0], d[1][0], -0.0f, -0.0f);
+    fma2v(r0, r1, d[0][1], d[1][1], d[0][1], d[1][1], r0, r1);
+    fma2v(r0, r1, d[0][2], d[1][2], d[0][2], d[1][2], r0, r1);
+    e[0][3] = rcp32(r0);
+    e[1][3] = rcp32(r1);
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-        const float dx = c.x - xo[t][0], dy = c.y - xo[t][1], dz = c.z - xo[t][2];
-        const float inv = rcp32(dx * dx + dy * dy + dz * dz);
-        d[t][0] = dx; d[t][1] = dy; d[t][2] = dz;
-        e[t][0] = dx * inv; e[t][1] = dy * inv; e[t][2] = dz * inv; e[t][3] = inv;
-    }
+    for (int k = 0; k < 3; ++k) fma2v(e[0][k], e[1][k], d[0][k], d[1][k], e[0][3], e[1][3], -0.0f, -0.0f);
     horner2_f32x2<P>(Bc, e, g);
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-        const float dx = d[t][0], dy = d[t][1], dz = d[t][2];
-        const float s = 2.0f * e[t][3];
-        const float G0 = s * g[t][0], Gx = s * g[t][1], Gy = s * g[t][2], Gz = s * g[t][3];
-        const float xx = x[t][0], xy = x[t][1], xz = x[t][2];
-        acc32[t][0] += (xy * dz - xz * dy) * G0 + (xy * Gz - xz * Gy);
-        acc32[t][1] += (xz * dx - xx * dz) * G0 + (xz * Gx - xx * Gz);
-        acc32[t][2] += (xx * dy - xy * dx) * G0 + (xx * Gy - xy * Gx);
+    for (int k = 0; k < 3; ++k) {
+        float h0, h1;
+        fma2v(h0, h1, d[0][k], d[1][k], g[0][0], g[1][0], g[0][k + 1], g[1][k + 1]);
+        fma2v(acc32[0][k], acc32[1][k], h0, h1, e[0][3], e[1][3], acc32[0][k], acc32[1][k]);
     }
 }
 
@@ -1155,12 +1157,11 @@ __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kerne
     const int64_t qa = q0 + 64 * (threadIdx.x >> 5) + (threadIdx.x & 31), qb = qa + 32;
     const bool live = q0 + 64 * (int64_t)(threadIdx.x >> 5) < qe;  // warp-uniform
     const double4 o = A.tgt_sorted[q0];  // the block's origin for FP32 offsets
-    float x[2][3], xo[2][3];
+    float xo[2][3];
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
         const int64_t q = t ? qb : qa;
         const double4 p = q < qe ? A.tgt_sorted[q] : make_double4(0, 0, 1, 0);
-        x[t][0] = (float)p.x; x[t][1] = (float)p.y; x[t][2] = (float)p.z;
         xo[t][0] = (float)(p.x - o.x); xo[t][1] = (float)(p.y - o.y); xo[t][2] = (float)(p.z - o.z);
     }
     double acc[2][3] = {{0, 0, 0}, {0, 0, 0}};
@@ -1180,7 +1181,7 @@ __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kerne
             const float4* Bc = fbuf + (size_t)s * S::kStage;
             const float4* cs = ctr + s * S::kK;
             float acc32[2][3] = {{0, 0, 0}, {0, 0, 0}};
-            for (int k = 0; k < n; ++k) far_one_acc2_f32<P>(Bc + (size_t)k * entries_for(P), x, xo, cs[k], acc32);
+            for (int k = 0; k < n; ++k) far_one_acc2_f32<P>(Bc + (size_t)k * entries_for(P), xo, cs[k], acc32);
 #pragma unroll
             for (int t = 0; t < 2; ++t)
 #pragma unroll
@@ -1190,15 +1191,15 @@ __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kerne
         __syncthreads();  // stage s consumed before it is refilled
         s0 = s1;
     }
-    if (qa < qe) {
-        A.V[qa] += acc[0][0];
-        A.V[A.n_tgt + qa] += acc[0][1];
-        A.V[2 * A.n_tgt + qa] += acc[0][2];
-    }
-    if (qb < qe) {
-        A.V[qb] += acc[1][0];
-        A.V[A.n_tgt + qb] += acc[1][1];
-        A.V[2 * A.n_tgt + qb] += acc[1][2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {  // V += 2 x cross (sum of h), x the FP64 target
+        const int64_t q = t ? qb : qa;
+        if (q >= qe) continue;
+        const double4 p = A.tgt_sorted[q];
+        const double hx = 2.0 * acc[t][0], hy = 2.0 * acc[t][1], hz = 2.0 * acc[t][2];
+        A.V[q] += p.y * hz - p.z * hy;
+        A.V[A.n_tgt + q] += p.z * hx - p.x * hz;
+        A.V[2 * A.n_tgt + q] += p.x * hy - p.y * hx;
     }
     }
 }
@@ -1544,7 +1545,10 @@ __global__ void __launch_bounds__(kBatch) label_kernel(Octree t, const int2* __r
 #endif
 constexpr int kNearTargets = LPM_NEAR_TARGETS;  // default targets per thread (2 or 4; run-time "near_targets")
 
-constexpr int kNearStreamTile = 512;  // default sources staged per tile (256, 512 or 1024; run-time "near_tile")
+constexpr int kNearStreamTile = 1024;  // default sources staged per tile (256, 512 or 1024; run-time "near_tile")
+constexpr int kNearSplit = 2;          // default source groups per batch (1 or 2; run-time "near_split")
+// The defaults (2 targets per thread, 1024 staged sources, 2 groups) were the fastest near-field shape measured
+// at icos L7 and L8 (learned treecode, 512 per leaf) and within 0.4% of the fastest on 1M uniform Poisson points.
 constexpr int kNearRuns = 128;        // source ranges resolved per chunk
 
 // One tile of the stream: m tree-ordered sources (FP32 absolute coordinates, w pre-scaled by 2)
@@ -1660,12 +1664,16 @@ struct NearArgs {
 
 // Persistent: every block takes batches from the ticket in `order` until none is left; one batch at a time
 // through the body below.
-// Tile shape: KT targets per thread (kBatch / KT threads) and KTILE sources staged in shared memory per
-// tile; instances for KT in {2, 4} and KTILE in {256, 512, 1024} are chosen at run time.
-template <bool kScalar, int KT, int KTILE>
-__global__ void __launch_bounds__(kBatch / KT) near_kernel(NearArgs A) {
-    constexpr int kT = KT, kThreads = kBatch / KT, kNW = kThreads / 32, kRPT = kNearRuns / kThreads;
-    static_assert(kT % 2 == 0 && kThreads % 32 == 0 && kNearRuns % kThreads == 0, "near kernel shape");
+// Tile shape: KT targets per thread and KTILE sources staged in shared memory per tile; KS groups of
+// kBatch / KT threads each hold the whole batch and sum their own contiguous share of every tile (KS = 2
+// gives each source read from shared memory to KT targets while keeping two warps on a batch), and the
+// groups' sums are added in shared memory at the end of the batch.  Instances for KT in {2, 4}, KTILE in
+// {256, 512, 1024} and KS in {1, 2} are chosen at run time.
+template <bool kScalar, int KT, int KTILE, int KS>
+__global__ void __launch_bounds__(kBatch / KT * KS) near_kernel(NearArgs A) {
+    constexpr int kT = KT, kTT = kBatch / KT, kThreads = kTT * KS, kNW = kThreads / 32, kRPT = kNearRuns / kThreads;
+    static_assert(kT % 2 == 0 && kTT % 32 == 0 && kNearRuns % kThreads == 0, "near kernel shape");
+    static_assert((KS - 1) * 3 * kBatch * sizeof(double) <= sizeof(float4) * KTILE, "group sums fit one tile");
     __shared__ __align__(16) float4 tile[2][KTILE];  // double-buffered: tile p + 1 arrives while p is summed
     __shared__ int r_start[kNearRuns], r_pre[kNearRuns + 1];
     __shared__ int warp_tot[kNW];
@@ -1681,10 +1689,11 @@ __global__ void __launch_bounds__(kBatch / KT) near_kernel(NearArgs A) {
     const int nbat = *A.nbat;
     for (int64_t b = next_batch(A.ticket, A.order, nbat, &slot); b >= 0; b = next_batch(A.ticket, A.order, nbat, &slot)) {
     const int64_t qe = batch_first[b + 1];
-    // warp w holds targets 32 kT w .. 32 kT (w + 1) - 1 of the batch (lane l: 32 kT w + l + 32 u), so a warp
-    // past the batch's last target skips the arithmetic as a whole
-    const int64_t qw = batch_first[b] + 32 * kT * (threadIdx.x >> 5) + (threadIdx.x & 31);
-    const bool live = batch_first[b] + 32 * kT * (int64_t)(threadIdx.x >> 5) < qe;  // warp-uniform
+    // within each group, warp w holds targets 32 kT w .. 32 kT (w + 1) - 1 of the batch (lane l: 32 kT w + l +
+    // 32 u), so a warp past the batch's last target skips the arithmetic as a whole
+    const int tid = (int)threadIdx.x % kTT, part = (int)threadIdx.x / kTT;
+    const int64_t qw = batch_first[b] + 32 * kT * (tid >> 5) + (tid & 31);
+    const bool live = batch_first[b] + 32 * kT * (int64_t)(tid >> 5) < qe;  // warp-uniform
     float tx[kT], ty[kT], tz[kT];
     double D[kT][3];
 #pragma unroll
@@ -1764,13 +1773,31 @@ __global__ void __launch_bounds__(kBatch / KT) near_kernel(NearArgs A) {
             cp_async_wait_prev();  // this thread's copies into tile[buf] have landed
             __syncthreads();       // ... and every other thread's
             if (live) {
+                const int h = (m + KS - 1) / KS, lo = min(m, part * h), cnt = min(m - lo, h);  // this group's share
                 if constexpr (kScalar)
-                    near_tile_scalar<kT / 2>(tile[buf], m, tx, ty, tz, D);
+                    near_tile_scalar<kT / 2>(tile[buf] + lo, cnt, tx, ty, tz, D);
                 else
-                    near_tile<kT / 2>(tile[buf], m, tx, ty, tz, D);
+                    near_tile<kT / 2>(tile[buf] + lo, cnt, tx, ty, tz, D);
             }
             __syncthreads();  // tile[buf] is read before the next stage refills it
         }
+    }
+    if constexpr (KS > 1) {  // add the other groups' sums to group 0's through the (consumed) tile buffer
+        double* red = reinterpret_cast<double*>(&tile[0][0]);
+        __syncthreads();
+        if (part > 0)
+#pragma unroll
+            for (int u = 0; u < kT; ++u)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) red[(((part - 1) * kT + u) * 3 + c) * kTT + tid] = D[u][c];
+        __syncthreads();
+        if (part > 0) continue;  // block-uniform barriers follow only in next_batch
+#pragma unroll
+        for (int g = 1; g < KS; ++g)
+#pragma unroll
+            for (int u = 0; u < kT; ++u)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) D[u][c] += red[(((g - 1) * kT + u) * 3 + c) * kTT + tid];
     }
 #pragma unroll
     for (int u = 0; u < kT; ++u) {
@@ -1785,18 +1812,25 @@ __global__ void __launch_bounds__(kBatch / KT) near_kernel(NearArgs A) {
 
 typedef void (*NearFn)(NearArgs);
 
-// The near kernel of a tile shape (targets per thread 2 or 4; staged sources 256, 512 or 1024) and its
-// block size; nullptr for another shape.
-NearFn near_select(bool scalar, int targets, int tile, int* threads) {
-    *threads = kBatch / targets;
-#define LPM_NEAR_CASE(T, TILE)                                                              \
-    if (targets == T && tile == TILE) return scalar ? near_kernel<true, T, TILE> : near_kernel<false, T, TILE>;
-    LPM_NEAR_CASE(2, 256)
-    LPM_NEAR_CASE(2, 512)
-    LPM_NEAR_CASE(2, 1024)
-    LPM_NEAR_CASE(4, 256)
-    LPM_NEAR_CASE(4, 512)
-    LPM_NEAR_CASE(4, 1024)
+// The near kernel of a tile shape (targets per thread 2 or 4; staged sources 256, 512 or 1024; 1 or 2
+// source groups) and its block size; nullptr for another shape.
+NearFn near_select(bool scalar, int targets, int tile, int split, int* threads) {
+    *threads = kBatch / targets * split;
+#define LPM_NEAR_CASE(T, TILE, S)                                     \
+    if (targets == T && tile == TILE && split == S)                    \
+        return scalar ? near_kernel<true, T, TILE, S> : near_kernel<false, T, TILE, S>;
+    LPM_NEAR_CASE(2, 256, 1)
+    LPM_NEAR_CASE(2, 512, 1)
+    LPM_NEAR_CASE(2, 1024, 1)
+    LPM_NEAR_CASE(4, 256, 1)
+    LPM_NEAR_CASE(4, 512, 1)
+    LPM_NEAR_CASE(4, 1024, 1)
+    LPM_NEAR_CASE(2, 256, 2)
+    LPM_NEAR_CASE(2, 512, 2)
+    LPM_NEAR_CASE(2, 1024, 2)
+    LPM_NEAR_CASE(4, 256, 2)
+    LPM_NEAR_CASE(4, 512, 2)
+    LPM_NEAR_CASE(4, 1024, 2)
 #undef LPM_NEAR_CASE
     return nullptr;
 }
@@ -1896,6 +1930,7 @@ struct TreeSolver {
     int near_blocks = 1;              // persistent grids: resident blocks on the whole device
     int near_targets = kNearTargets;  // near kernel tile shape (run-time "near_targets", "near_tile")
     int near_tile = kNearStreamTile;
+    int near_split = kNearSplit;      // source groups per batch (run-time "near_split")
     int far_blocks[kPMax + 1][2] = {};  // per order, FP32 / FP64 far kernel
     uint64_t generation = 0;          // reallocations of the lists and per-node arrays (tree_generation)
     std::vector<void*> allocs;
@@ -1991,17 +2026,18 @@ int upload_constants() {
 }  // namespace
 
 // Select the near kernel's tile shape and size its persistent grid (resident blocks on the device).
-static int near_shape(TreeSolver* t, int targets, int tile) {
+static int near_shape(TreeSolver* t, int targets, int tile, int split) {
     int threads = 0;
-    NearFn fn = near_select(t->scalar, targets, tile, &threads);
+    NearFn fn = near_select(t->scalar, targets, tile, split, &threads);
     if (!fn) {
-        set_error("tree solver: near_targets must be 2 or 4 and near_tile 256, 512 or 1024");
+        set_error("tree solver: near_targets must be 2 or 4, near_tile 256, 512 or 1024 and near_split 1 or 2");
         return LPM_ERR_ARG;
     }
     int per_sm = 0;
     LPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0));
     t->near_targets = targets;
     t->near_tile = tile;
+    t->near_split = split;
     t->near_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(t->n_batches,
                                                                   (int64_t)std::max(per_sm, 1) * t->ctx->num_sms));
     return LPM_OK;
@@ -2187,7 +2223,7 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
             tree_solver_destroy(t);
             return cuda_status(ea, "cudaFuncSetAttribute (far_kernel)");
         }
-        rc = near_shape(t, t->near_targets, t->near_tile);
+        rc = near_shape(t, t->near_targets, t->near_tile, t->near_split);
         if (rc) {
             tree_solver_destroy(t);
             return rc;
@@ -2441,7 +2477,7 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
         N.ticket = t->sched_aux + kAuxNearTicket;
         N.mult = t->scalar ? 1.0 / (4.0 * kPi) : -1.0 / (4.0 * kPi * t->kernel.radius);
         int threads = 0;
-        NearFn fn = near_select(t->scalar, t->near_targets, t->near_tile, &threads);
+        NearFn fn = near_select(t->scalar, t->near_targets, t->near_tile, t->near_split, &threads);
         LPM_LAUNCH(ctx, "near_kernel", fn, (unsigned)t->near_blocks, threads, 0, N);
     }
     if (can_sync) return tree_check(t);
@@ -2525,6 +2561,7 @@ int tree_get_param(const TreeSolver* t, const char* name, double* value) {
     else if (n == "sakajo_depth") *value = t->solver.sakajo_depth;
     else if (n == "near_targets") *value = t->near_targets;
     else if (n == "near_tile") *value = t->near_tile;
+    else if (n == "near_split") *value = t->near_split;
     else if (n == "root_maxr") *value = t->root_maxr;
     else if (n == "root_first") *value = (double)t->root_first;
     else if (n == "order") *value = t->order;
@@ -2552,9 +2589,11 @@ int tree_set_param(TreeSolver* t, const char* name, double value) {
         }
         t->order_bias = (int)value;
     } else if (n == "near_targets" && (value == 2.0 || value == 4.0)) {
-        return near_shape(t, (int)value, t->near_tile);
+        return near_shape(t, (int)value, t->near_tile, t->near_split);
     } else if (n == "near_tile" && (value == 256.0 || value == 512.0 || value == 1024.0)) {
-        return near_shape(t, t->near_targets, (int)value);
+        return near_shape(t, t->near_targets, (int)value, t->near_split);
+    } else if (n == "near_split" && (value == 1.0 || value == 2.0)) {
+        return near_shape(t, t->near_targets, t->near_tile, (int)value);
     } else if (n == "root_maxr" && value >= 0.0 && std::isfinite(value)) {
         t->root_maxr = value;
     } else if (n == "root_first" && value >= 0.0 && value <= (double)t->n_tgt && value == std::floor(value)) {

@@ -33,13 +33,14 @@ def test_autotune_learned_sphere(ctx):
     assert {c.bias for c in res.tried} == {0, 2}
     # the near-field tile shape is searched too: every shape was timed on the best setting, and the pick is
     # the fastest qualifying one among them
-    shapes = {(c.near_targets, c.near_tile) for c in res.tried}
-    assert shapes == {(2, 256), (2, 512), (2, 1024), (4, 256), (4, 512), (4, 1024)}
+    shapes = {(c.near_targets, c.near_tile, c.near_split) for c in res.tried}
+    assert shapes == {(t, s, g) for t in (2, 4) for s in (256, 512, 1024) for g in (1, 2)}
     # the tuned descriptor reproduces the accuracy on all targets
     ts = L.TreeSum(ctx, L.biot_savart_kernel(), tuned_solver(res), n_src, p.shape[0])
     ts.set_mlp(L.learned.load()[0])
     apply_tuned(res, ts)
-    assert (ts.get_param("near_targets"), ts.get_param("near_tile")) == (res.best.near_targets, res.best.near_tile)
+    assert (ts.get_param("near_targets"), ts.get_param("near_tile"), ts.get_param("near_split")) == \
+        (res.best.near_targets, res.best.near_tile, res.best.near_split)
     out = torch.empty((3, p.shape[0]), dtype=torch.float64, device="cuda")
     ts.eval(d[:n_src], d, out)
     ts.close()

@@ -146,8 +146,9 @@ def test_poisson_treecode_fp64_far_field_matches_fp32(ctx):
 @pytest.mark.gpu
 @pytest.mark.parametrize("kernel", ["biot_savart", "poisson"])
 def test_near_tile_shapes_agree(ctx, kernel):
-    """Every near-field tile shape (2 or 4 targets per thread, 256 / 512 / 1024 staged sources) gives the same
-    sums up to FP32 rounding (the shape moves the FP32-to-FP64 fold points only); invalid shapes are refused."""
+    """Every near-field tile shape (2 or 4 targets per thread, 256 / 512 / 1024 staged sources, 1 or 2 source
+    groups) gives the same sums up to FP32 rounding (the shape moves the FP32-to-FP64 fold points only); invalid
+    shapes are refused."""
     torch = ctx.use_torch_stream()
     if kernel == "biot_savart":
         _, p, n_src = W.gaussian_vortex_mesh("icos", 5)
@@ -161,16 +162,19 @@ def test_near_tile_shapes_agree(ctx, kernel):
     outs = {}
     for nt in (2, 4):
         for tile in (256, 512, 1024):
-            ts.set_param("near_targets", nt)
-            ts.set_param("near_tile", tile)
-            out = torch.empty((comps, p.shape[0]), dtype=torch.float64, device="cuda")
-            ts.eval(d[:n_src], d, out)
-            outs[(nt, tile)] = out
-    for bad in (("near_targets", 3), ("near_tile", 384)):
+            for split in (1, 2):
+                ts.set_param("near_targets", nt)
+                ts.set_param("near_tile", tile)
+                ts.set_param("near_split", split)
+                assert ts.get_param("near_split") == split
+                out = torch.empty((comps, p.shape[0]), dtype=torch.float64, device="cuda")
+                ts.eval(d[:n_src], d, out)
+                outs[(nt, tile, split)] = out
+    for bad in (("near_targets", 3), ("near_tile", 384), ("near_split", 3)):
         with pytest.raises(L.LpmError):
             ts.set_param(*bad)
     ts.close()
-    ref = outs[(2, 512)]
+    ref = outs[(2, 512, 1)]
     for k, o in outs.items():
         assert float(torch.linalg.norm(o - ref) / torch.linalg.norm(ref)) < 1e-6, k
 
