@@ -56,7 +56,13 @@ __host__ __device__ constexpr int entries_for(int P) {                          
     for (int m = 0; 2 * m < P; ++m) e += tet(P - 2 * m);
     return e;
 }
-__host__ __device__ constexpr int cube_dim(int pm) { return pm + 1; }
+// Node moments are stored packed: the monomials (a, b, c) with a + b + c <= pm in a-major, then b, then c
+// order, mono_count(pm) doubles per node.
+__host__ __device__ constexpr int tet_count(int n) { return (n + 1) * (n + 2) * (n + 3) / 6; }
+__host__ __device__ constexpr int mono_count(int pm) { return tet_count(pm); }
+__host__ __device__ constexpr int mono_index(int a, int b, int c, int pm) {
+    return tet_count(pm) - tet_count(pm - a) + b * (pm - a + 1) - b * (b - 1) / 2 + c;
+}
 
 struct CutoffTable {
     int32_t direct_below[kPMax + 1];  // a cluster with fewer sources than this is summed directly
@@ -109,17 +115,33 @@ __global__ void gather_sources_kernel(const double4* __restrict__ X, const int32
 
 // Leaves: centre (mean position), radius, FP32 source copies (w scaled by wscale: 2 folds the factor of
 // 1/(1 - x.y) = 2/|x - y|^2 of the sphere kernel into the strength) and ordinary moments
-// mom[a][b][c] = sum_j w_j h^(a,b,c) for a+b+c <= pm.
-__global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* __restrict__ src, int pm,
-                                                       const int4* __restrict__ mono, int n_mono,
-                                                       double4* __restrict__ node_ctr, double* __restrict__ node_wabs,
-                                                       double* __restrict__ node_mom, float4* __restrict__ src32,
-                                                       double wscale, int heavy_cap) {
+// mom[a][b][c] = sum_j w_j h^(a,b,c) for a+b+c <= pm.  A moment unit (a, b, c0) is a run of
+// kP2mRun monomials (a, b, c0 .. c0 + kP2mRun - 1) (those past a + b + c = pm are computed and dropped): per
+// particle its thread reads w, h_x^a, h_y^b, h_z^c0 and h_z from the power tables and walks the run by
+// multiplying with h_z, five shared-memory reads for four moments.
+constexpr int kP2mRun = 4;
+constexpr int kP2mThreads = 128;
+constexpr int kP2mUnitsPerThread = 2;
+constexpr int p2m_units_for(int pm) {
+    int n = 0;
+    for (int a = 0; a <= pm; ++a)
+        for (int b = 0; a + b <= pm; ++b) n += (pm - a - b + kP2mRun) / kP2mRun;
+    return n;
+}
+static_assert(p2m_units_for(kPMax) <= kP2mThreads * kP2mUnitsPerThread, "leaf moment units per block");
+
+__global__ void __launch_bounds__(kP2mThreads) leaf_p2m_kernel(Octree t, const double4* __restrict__ src, int pm,
+                                                               const int4* __restrict__ units, int n_units,
+                                                               double4* __restrict__ node_ctr,
+                                                               double* __restrict__ node_wabs,
+                                                               double* __restrict__ node_mom,
+                                                               float4* __restrict__ src32, double wscale,
+                                                               int heavy_cap) {
     __shared__ double sh[32];
     __shared__ double pw[32][3][kPMax + 1];
     __shared__ double ww[32];
     const int nleaves = t.counters[3];
-    const int cd = cube_dim(pm);
+    const int nm = mono_count(pm);
     for (int leaf = blockIdx.x; leaf < nleaves; leaf += gridDim.x) {
         const int node = t.leaf_node[leaf];
         const int s = t.node_start[node], e = t.node_end[node];
@@ -146,7 +168,7 @@ __global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* 
         // moments, 32 particles at a time with their power tables in shared memory (nodes past the
         // moment capacity get none: the traversal never accepts them as far clusters)
         if (node >= heavy_cap) continue;  // uniform per block
-        double acc[4] = {0, 0, 0, 0};
+        double acc[kP2mUnitsPerThread][kP2mRun] = {};
         for (int q0 = s; q0 < e; q0 += 32) {
             __syncthreads();
             if (threadIdx.x < 32) {
@@ -168,45 +190,75 @@ __global__ void __launch_bounds__(128) leaf_p2m_kernel(Octree t, const double4* 
             __syncthreads();
             const int np = min(32, e - q0);
 #pragma unroll
-            for (int r4 = 0; r4 < 4; ++r4) {
-                const int term = threadIdx.x + r4 * blockDim.x;
-                if (term < n_mono) {
-                    const int4 k = mono[term];
-                    double a2 = acc[r4];
-                    for (int j = 0; j < np; ++j) a2 = fma(ww[j] * pw[j][0][k.x], pw[j][1][k.y] * pw[j][2][k.z], a2);
-                    acc[r4] = a2;
+            for (int r2 = 0; r2 < kP2mUnitsPerThread; ++r2) {
+                const int u = threadIdx.x + r2 * kP2mThreads;
+                if (u < n_units) {
+                    const int4 k = units[u];
+                    for (int j = 0; j < np; ++j) {
+                        double v = ww[j] * pw[j][0][k.x] * pw[j][1][k.y] * pw[j][2][k.z];
+                        const double hz = pw[j][2][1];
+#pragma unroll
+                        for (int c = 0; c < kP2mRun; ++c) {
+                            acc[r2][c] += v;
+                            v *= hz;
+                        }
+                    }
                 }
             }
         }
-        double* mout = node_mom + (size_t)node * cd * cd * cd;
+        double* mout = node_mom + (size_t)node * nm;
 #pragma unroll
-        for (int r4 = 0; r4 < 4; ++r4) {
-            const int term = threadIdx.x + r4 * blockDim.x;
-            if (term < n_mono) {
-                const int4 k = mono[term];
-                mout[(k.x * cd + k.y) * cd + k.z] = acc[r4];
+        for (int r2 = 0; r2 < kP2mUnitsPerThread; ++r2) {
+            const int u = threadIdx.x + r2 * kP2mThreads;
+            if (u < n_units) {
+                const int4 k = units[u];  // the run's monomials are consecutive in the packed order
+                const int base = mono_index(k.x, k.y, k.z, pm);
+#pragma unroll
+                for (int c = 0; c < kP2mRun; ++c)
+                    if (k.x + k.y + k.z + c <= pm) mout[base + c] = acc[r2][c];
             }
         }
         __syncthreads();
     }
 }
 
-// Internal nodes of level l: centre = count-weighted mean of the children's centres, radius bound
+// Internal nodes: centre = count-weighted mean of the children's centres, radius bound
 // max(|c_child - c| + r_child), moments shifted from the children:
 // m_k(c) = sum_child sum_{j <= k} C(k, j) (c_child - c)^(k-j) m_j(c_child).
 // The children's moments (packed in monomial order), their shift powers and the binomial table are
 // staged in shared memory, so the inner loops read no global or constant memory.
+//
+// One launch does the whole upward pass: pending[node] counts the internal children not yet done; a block
+// starts at each internal node whose children are all leaves (their moments come from leaf_p2m_kernel), and
+// the block that completes a node's last internal child goes on to the node itself (no level barriers, no
+// waits).  Writers fence before the counter's decrement and the next block reads the children through L2.
 
-__global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm, const int4* __restrict__ mono,
-                                                        int n_mono, double4* __restrict__ node_ctr,
-                                                        double* __restrict__ node_wabs,
-                                                        double* __restrict__ node_mom, int heavy_cap) {
+// A double4 written by another block of the running launch: two 16-byte loads that skip L1.
+__device__ __forceinline__ double4 ldcg4(const double4* p) {
+    const double2 a = __ldcg((const double2*)p), b = __ldcg((const double2*)p + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__global__ void m2m_pending_kernel(Octree t, int32_t* __restrict__ pending) {
+    const int nn = t.counters[1];
+    for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < nn; node += gridDim.x * blockDim.x) {
+        const int nc = t.node_nchild[node];
+        int p = 0;
+        for (int k = 0; k < nc; ++k) p += t.node_nchild[t.node_first_child[node] + k] > 0;
+        pending[node] = p;
+    }
+}
+
+__global__ void __launch_bounds__(128) m2m_upward_kernel(Octree t, int pm, const int4* __restrict__ mono,
+                                                         int n_mono, double4* __restrict__ node_ctr,
+                                                         double* __restrict__ node_wabs,
+                                                         double* __restrict__ node_mom, int heavy_cap,
+                                                         int32_t* __restrict__ pending) {
     extern __shared__ double m2m_sh[];  // 2 x 8 x n_mono: child moments and their partial shifts
     __shared__ double dp[8][3][kPMax + 1];
     __shared__ double bin[kPMax + 1][kPMax + 1];
     __shared__ int mono_idx[kPMax + 1][kPMax + 1][kPMax + 1];  // (a, b, c) -> position in the monomial list
-    const int lb = t.level_range[2 * l], le = t.level_range[2 * l + 1];
-    const int cd = cube_dim(pm);
+    __shared__ int climb;
     for (int i = threadIdx.x; i < (kPMax + 1) * (kPMax + 1); i += blockDim.x)
         bin[i / (kPMax + 1)][i % (kPMax + 1)] = c_binom[i / (kPMax + 1)][i % (kPMax + 1)];
     for (int i = threadIdx.x; i < n_mono; i += blockDim.x) {
@@ -214,33 +266,47 @@ __global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm,
         mono_idx[k.x][k.y][k.z] = i;
     }
     __syncthreads();
-    for (int node = lb + blockIdx.x; node < le; node += gridDim.x) {
+    // one internal node (block-wide); the children's centres, weights and moments were written by other
+    // blocks of this launch (or by leaf_p2m_kernel) and are read past L1
+    auto m2m_node = [&](int node) {
         const int nc = t.node_nchild[node];
-        if (nc == 0) continue;  // a leaf: done by leaf_p2m_kernel
         const int fc = t.node_first_child[node];
+        double4 ch[8];  // the children's centres, loaded together
+        double m[8], wc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k < nc) {
+                ch[k] = ldcg4(node_ctr + fc + k);
+                m[k] = (double)(t.node_end[fc + k] - t.node_start[fc + k]);
+                wc[k] = __ldcg(node_wabs + fc + k);
+            }
+        }
         double cx = 0, cy = 0, cz = 0, cnt = 0, wabs = 0;
-        for (int k = 0; k < nc; ++k) {
-            const double4 cc = node_ctr[fc + k];
-            const double m = (double)(t.node_end[fc + k] - t.node_start[fc + k]);
-            cx += m * cc.x; cy += m * cc.y; cz += m * cc.z; cnt += m;
-            wabs += node_wabs[fc + k];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k < nc) {
+                cx += m[k] * ch[k].x; cy += m[k] * ch[k].y; cz += m[k] * ch[k].z; cnt += m[k];
+                wabs += wc[k];
+            }
         }
         cx /= cnt; cy /= cnt; cz /= cnt;
         double r = 0;
-        for (int k = 0; k < nc; ++k) {
-            const double4 cc = node_ctr[fc + k];
-            const double dx = cc.x - cx, dy = cc.y - cy, dz = cc.z - cz;
-            r = fmax(r, sqrt(dx * dx + dy * dy + dz * dz) + cc.w);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k < nc) {
+                const double dx = ch[k].x - cx, dy = ch[k].y - cy, dz = ch[k].z - cz;
+                r = fmax(r, sqrt(dx * dx + dy * dy + dz * dz) + ch[k].w);
+            }
         }
         if (threadIdx.x == 0) {
             node_ctr[node] = make_double4(cx, cy, cz, r);
             node_wabs[node] = wabs;
         }
-        if (fc + nc > heavy_cap) continue;  // uniform per block: a child (numbered after node) has no moments
+        if (fc + nc > heavy_cap) return;  // uniform per block: a child (numbered after node) has no moments
         __syncthreads();  // the previous node's readers of dp / m2m_sh are done
         if (threadIdx.x < nc * 3) {
             const int k = threadIdx.x / 3, a = threadIdx.x % 3;
-            const double4 cc = node_ctr[fc + k];
+            const double4 cc = ldcg4(node_ctr + fc + k);  // (dynamic k: not from the register copies)
             const double d = a == 0 ? cc.x - cx : (a == 1 ? cc.y - cy : cc.z - cz);
             double v = 1.0;
             for (int q = 0; q <= pm; ++q) {
@@ -250,11 +316,9 @@ __global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm,
         }
         double* S0 = m2m_sh;                  // nc x n_mono
         double* S1 = m2m_sh + 8 * n_mono;     // nc x n_mono
-        for (int i = threadIdx.x; i < nc * n_mono; i += blockDim.x) {
-            const int k = i / n_mono, term = i - k * n_mono;
-            const int4 j = mono[term];
-            S0[i] = node_mom[(size_t)(fc + k) * cd * cd * cd + (j.x * cd + j.y) * cd + j.z];
-        }
+        const double* cm = node_mom + (size_t)fc * n_mono;  // the children are consecutive nodes
+#pragma unroll 4
+        for (int i = threadIdx.x; i < nc * n_mono; i += blockDim.x) S0[i] = __ldcg(cm + i);
         __syncthreads();
         // the shift factorises by axis: three 1D binomial shifts (x, then y, then z with the sum over
         // children), (k_x + 1) + (k_y + 1) + (k_z + 1) terms per monomial instead of their product
@@ -276,14 +340,35 @@ __global__ void __launch_bounds__(128) m2m_level_kernel(Octree t, int l, int pm,
             S0[i] = acc;
         }
         __syncthreads();
-        double* mout = node_mom + (size_t)node * cd * cd * cd;
+        double* mout = node_mom + (size_t)node * n_mono;
         for (int term = threadIdx.x; term < n_mono; term += blockDim.x) {
             const int4 kk = mono[term];
             double acc = 0;
             for (int k = 0; k < nc; ++k)
                 for (int j2 = 0; j2 <= kk.z; ++j2)
                     acc = fma(bin[kk.z][j2] * dp[k][2][kk.z - j2], S0[k * n_mono + mono_idx[kk.x][kk.y][j2]], acc);
-            mout[(kk.x * cd + kk.y) * cd + kk.z] = acc;
+            mout[term] = acc;
+        }
+    };
+    const int nn = t.counters[1];
+    for (int start = blockIdx.x; start < nn; start += gridDim.x) {
+        const int nc = t.node_nchild[start];
+        bool first = nc > 0;  // an internal node whose children are all leaves (uniform per block)
+        for (int k = 0; k < nc; ++k) first = first && t.node_nchild[t.node_first_child[start] + k] == 0;
+        if (!first) continue;
+        for (int node = start;;) {
+            m2m_node(node);
+            __threadfence();  // this thread's writes of node's data before the counter moves
+            __syncthreads();
+            const int parent = t.node_parent[node];
+            if (parent < 0) break;  // uniform: the root
+            if (threadIdx.x == 0) {
+                climb = atomicSub(pending + parent, 1) == 1;  // the parent's last internal child
+                __threadfence();
+            }
+            __syncthreads();
+            if (!climb) break;
+            node = parent;
         }
     }
 }
@@ -293,9 +378,9 @@ __global__ void coeff_kernel(Octree t, int pm, const int4* __restrict__ ent, int
                              const double* __restrict__ node_mom, double4* __restrict__ B64,
                              float4* __restrict__ B32, int heavy_cap) {
     const int nn = min(t.counters[1], heavy_cap);
-    const int cd = cube_dim(pm);
+    const int nm = mono_count(pm);
     for (int node = blockIdx.x; node < nn; node += gridDim.x) {
-        const double* mom = node_mom + (size_t)node * cd * cd * cd;
+        const double* mom = node_mom + (size_t)node * nm;
         for (int i = threadIdx.x; i < n_ent; i += blockDim.x) {
             const int4 mk = ent[i];  // (m, a, b, c)
             const int m = mk.x, a = mk.y, b = mk.z, c = mk.w, q = a + b + c;
@@ -305,10 +390,10 @@ __global__ void coeff_kernel(Octree t, int pm, const int4* __restrict__ ent, int
                     const int j2 = m - j0 - j1;
                     const double mult = c_fact[m] / (c_fact[j0] * c_fact[j1] * c_fact[j2]);
                     const int A = a + 2 * j0, Bb = b + 2 * j1, Cc = c + 2 * j2;
-                    n0 += mult * mom[(A * cd + Bb) * cd + Cc];
-                    n1 += mult * mom[((A + 1) * cd + Bb) * cd + Cc];
-                    n2 += mult * mom[(A * cd + Bb + 1) * cd + Cc];
-                    n3 += mult * mom[(A * cd + Bb) * cd + Cc + 1];
+                    n0 += mult * mom[mono_index(A, Bb, Cc, pm)];
+                    n1 += mult * mom[mono_index(A + 1, Bb, Cc, pm)];
+                    n2 += mult * mom[mono_index(A, Bb + 1, Cc, pm)];
+                    n3 += mult * mom[mono_index(A, Bb, Cc + 1, pm)];
                 }
             }
             const double pre = ((m & 1) ? -1.0 : 1.0) * c_binom[q + m][m] * ((q & 1) ? -1.0 : 1.0) *
@@ -329,9 +414,9 @@ __global__ void coeff_scalar_kernel(Octree t, int pm, const int4* __restrict__ e
                                     const double* __restrict__ node_mom, double* __restrict__ A64,
                                     float* __restrict__ A32, int heavy_cap) {
     const int nn = min(t.counters[1], heavy_cap);
-    const int cd = cube_dim(pm);
+    const int nm = mono_count(pm);
     for (int node = blockIdx.x; node < nn; node += gridDim.x) {
-        const double* mom = node_mom + (size_t)node * cd * cd * cd;
+        const double* mom = node_mom + (size_t)node * nm;
         for (int i = threadIdx.x; i < stride; i += blockDim.x) {
             double v = 0.0;
             if (i < n_ent) {
@@ -341,7 +426,7 @@ __global__ void coeff_scalar_kernel(Octree t, int pm, const int4* __restrict__ e
                 for (int j0 = 0; j0 <= m; ++j0)
                     for (int j1 = 0; j1 <= m - j0; ++j1) {
                         const int j2 = m - j0 - j1;
-                        n0 += mom[((a + 2 * j0) * cd + b + 2 * j1) * cd + c + 2 * j2] /
+                        n0 += mom[mono_index(a + 2 * j0, b + 2 * j1, c + 2 * j2, pm)] /
                               (c_fact[j0] * c_fact[j1] * c_fact[j2]);
                     }
                 double g = 1.0;  // Gamma(q+m+1/2) / Gamma(1/2)
@@ -456,16 +541,16 @@ __global__ void node_feature_kernel(Octree t, int pm, const double4* __restrict_
                                     const double* __restrict__ node_wabs, const double* __restrict__ node_mom,
                                     float* __restrict__ node_feat, int heavy_cap) {
     const int nn = min(t.counters[1], heavy_cap);
-    const int cd = cube_dim(pm);
+    const int nm = mono_count(pm);
     for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < nn; node += gridDim.x * blockDim.x) {
-        const double* mom = node_mom + (size_t)node * cd * cd * cd;
+        const double* mom = node_mom + (size_t)node * nm;
         double norm[3] = {0, 0, 0};
         for (int d = 0; d < 3; ++d) {
             const int n = 2 * (d + 1);
             if (n > pm) continue;
             for (int a = 0; a <= n; ++a)
                 for (int b = 0; a + b <= n; ++b) {
-                    const double v = mom[(a * cd + b) * cd + (n - a - b)];
+                    const double v = mom[mono_index(a, b, n - a - b, pm)];
                     norm[d] += v * v;
                 }
         }
@@ -885,8 +970,9 @@ __device__ __forceinline__ void fma4(F (&r)[4], F e, const F (&v)[4]) {
     r[3] = fma(r[3], e, v[3]);
 }
 
-// One far entry at one target in F arithmetic: acc += 2 [(x cross d) G0 + x cross G], d = c - x,
-// G = g / |d|^2, g from the order-P Horner scheme (fully unrolled for P).
+// One far entry at one target in F arithmetic.  The cluster's contribution 2 x cross (d g0 + g) / |d|^2
+// (d = c - x, g from the order-P Horner scheme, fully unrolled for P) is linear in the target position x, so
+// acc sums h = (d g0 + g) / |d|^2 and the caller applies 2 x cross acc once per target.
 template <int P, typename F, typename F4>
 __device__ __forceinline__ void far_one_acc(const F4* __restrict__ Bc, const double4& x, double cx, double cy,
                                             double cz, double (&acc)[3]) {
@@ -897,12 +983,9 @@ __device__ __forceinline__ void far_one_acc(const F4* __restrict__ Bc, const dou
         horner_f32x2<P>((const float4*)Bc, dx * inv, dy * inv, dz * inv, inv, g0, g1, g2, g3);
     else
         horner<P, F, F4>(Bc, dx * inv, dy * inv, dz * inv, inv, g0, g1, g2, g3);
-    const F s = F(2) * inv;
-    const F G0 = s * g0, Gx = s * g1, Gy = s * g2, Gz = s * g3;
-    const F xx = (F)x.x, xy = (F)x.y, xz = (F)x.z;
-    acc[0] += (double)((xy * dz - xz * dy) * G0 + (xy * Gz - xz * Gy));
-    acc[1] += (double)((xz * dx - xx * dz) * G0 + (xz * Gx - xx * Gz));
-    acc[2] += (double)((xx * dy - xy * dx) * G0 + (xx * Gy - xy * Gx));
+    acc[0] += (double)(inv * fma(dx, g0, g1));
+    acc[1] += (double)(inv * fma(dy, g0, g2));
+    acc[2] += (double)(inv * fma(dz, g0, g3));
 }
 
 struct FarArgs {
@@ -998,10 +1081,11 @@ __global__ void __launch_bounds__(kBatch, kFarMinBlocks) far_order_kernel(FarArg
         __syncthreads();  // stage s consumed before it is refilled
         s0 = s1;
     }
-    if (q < qe) {
-        A.V[q] += acc[0];
-        A.V[A.n_tgt + q] += acc[1];
-        A.V[2 * A.n_tgt + q] += acc[2];
+    if (q < qe) {  // V += 2 x cross acc
+        const double hx = 2.0 * acc[0], hy = 2.0 * acc[1], hz = 2.0 * acc[2];
+        A.V[q] += x.y * hz - x.z * hy;
+        A.V[A.n_tgt + q] += x.z * hx - x.x * hz;
+        A.V[2 * A.n_tgt + q] += x.x * hy - x.y * hx;
     }
     }
 }
@@ -1903,6 +1987,9 @@ struct TreeSolver {
     int n_ent = 0;
     int4* ent = nullptr;
     int4* mono = nullptr;
+    int4* p2m_units = nullptr;  // leaf moment units (a, b, c0)
+    int32_t* m2m_pending = nullptr;  // per node: internal children whose moments are not yet shifted
+    int n_units = 0;
     int n_mono = 0;
     int32_t* gtab = nullptr;
     CutoffTable ct{};
@@ -1980,7 +2067,6 @@ int alloc_lists(TreeSolver* t, int64_t far_cap, int64_t near_cap) {
 // Regrow the per-node moment / coefficient / feature arrays to hold `need` nodes (with headroom).
 int heavy_alloc(TreeSolver* t, int64_t need) {
     const int64_t cap = std::min<int64_t>(t->st.node_cap, need + need / 2 + 256);
-    const int cd = cube_dim(t->pm);
     auto regrow = [&](auto** p, size_t per_node) -> cudaError_t {
         if (*p) {
             cudaFree(*p);
@@ -1990,7 +2076,7 @@ int heavy_alloc(TreeSolver* t, int64_t need) {
         return talloc(t, p, (size_t)cap * per_node);
     };
     ++t->generation;
-    cudaError_t e = regrow(&t->node_mom, (size_t)cd * cd * cd);
+    cudaError_t e = regrow(&t->node_mom, (size_t)mono_count(t->pm));
     if (e == cudaSuccess && t->scalar) e = regrow(&t->A64, (size_t)t->a_stride);
     if (e == cudaSuccess && t->scalar) e = regrow(&t->A32, (size_t)t->a_stride);
     if (e == cudaSuccess && !t->scalar) e = regrow(&t->B64, (size_t)t->n_ent);
@@ -2114,14 +2200,18 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
         return rc;
     }
     const size_t nn = (size_t)t->st.node_cap;
-    const int cd = cube_dim(t->pm);
-    std::vector<int4> ent, mono;
+    std::vector<int4> ent, mono;  // mono in the packed moment order (mono_index)
     canonical_entries(t->pm, ent);
     for (int a = 0; a <= t->pm; ++a)
         for (int b = 0; a + b <= t->pm; ++b)
             for (int c = 0; a + b + c <= t->pm; ++c) mono.push_back(make_int4(a, b, c, 0));
+    std::vector<int4> units;  // leaf moment units: runs of kP2mRun monomials along c
+    for (int a = 0; a <= t->pm; ++a)
+        for (int b = 0; a + b <= t->pm; ++b)
+            for (int c = 0; a + b + c <= t->pm; c += kP2mRun) units.push_back(make_int4(a, b, c, 0));
     t->n_ent = (int)ent.size();
     t->n_mono = (int)mono.size();
+    t->n_units = (int)units.size();
     // gather tables: for order P, the canonical index of each entry of the order-P Horner sequence
     std::vector<int32_t> gtab;
     for (int P = 1; P <= kPMax; ++P) {
@@ -2168,7 +2258,7 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
                                                                    : 6 * (std::max<int64_t>(n_src, 1) /
                                                                           solver.max_per_leaf) + 1024);
     const size_t nh = (size_t)t->heavy_cap;
-    A(talloc(t, &t->node_mom, nh * cd * cd * cd));
+    A(talloc(t, &t->node_mom, nh * mono_count(t->pm)));
     if (scalar) {
         t->a_stride = (t->n_ent + 3) & ~3;  // 16-byte aligned rows in FP32 and FP64
         A(talloc(t, &t->A64, nh * t->a_stride));
@@ -2179,6 +2269,8 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     }
     A(talloc(t, &t->ent, ent.size()));
     A(talloc(t, &t->mono, mono.size()));
+    A(talloc(t, &t->p2m_units, units.size()));
+    A(talloc(t, &t->m2m_pending, nn));
     A(talloc(t, &t->gtab, gtab.size()));
     const size_t far_rows = (size_t)(kPMax + 1) * ((size_t)t->n_batches + 1);  // order-bucketed rows
     A(talloc(t, &t->far_cnt, far_rows));
@@ -2202,9 +2294,11 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     }
     if (e == cudaSuccess) e = cudaMemcpy(t->ent, ent.data(), ent.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(t->mono, mono.data(), mono.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(t->p2m_units, units.data(), units.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !gtab.empty())
         e = cudaMemcpy(t->gtab, gtab.data(), gtab.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(t->node_mom, 0, nh * cd * cd * cd * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(t->node_mom, 0, nh * mono_count(t->pm) * sizeof(double));
     // the count arrays carry one extra zero entry so that their exclusive scans also yield the totals
     if (e == cudaSuccess) e = cudaMemset(t->far_cnt, 0, far_rows * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMemset(t->near_cnt, 0, ((size_t)t->n_batches + 1) * sizeof(int32_t));
@@ -2217,7 +2311,7 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
         // M2M stages two 8-child copies of the moments: opt in for the largest order any solver may use
         const int mono_max = (kPMax + 1) * (kPMax + 2) * (kPMax + 3) / 6;
         if (ea == cudaSuccess)
-            ea = cudaFuncSetAttribute(m2m_level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            ea = cudaFuncSetAttribute(m2m_upward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(16 * mono_max * sizeof(double)));
         if (ea != cudaSuccess) {
             tree_solver_destroy(t);
@@ -2371,11 +2465,12 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     LPM_LAUNCH(ctx, "gather_sources_kernel", gather_sources_kernel, gs, 256, 0, src, t->st.perm, t->st.counters,
                t->src_sorted);
     const unsigned gl = (unsigned)std::max<int64_t>(1, std::min<int64_t>(t->st.node_cap, 16 * ctx->num_sms));
-    LPM_LAUNCH(ctx, "leaf_p2m_kernel", leaf_p2m_kernel, gl, 128, 0, t->st, t->src_sorted, t->pm, t->mono, t->n_mono,
+    LPM_LAUNCH(ctx, "leaf_p2m_kernel", leaf_p2m_kernel, gl, kP2mThreads, 0, t->st, t->src_sorted, t->pm, t->p2m_units,
+               t->n_units,
                t->node_ctr, t->node_wabs, t->node_mom, t->src32, t->scalar ? 1.0 : 2.0, t->heavy_cap);
-    for (int l = t->st.max_depth - 1; l >= 0; --l)
-        LPM_LAUNCH(ctx, "m2m_level_kernel", m2m_level_kernel, gl, 128, (size_t)16 * t->n_mono * sizeof(double), t->st,
-                   l, t->pm, t->mono, t->n_mono, t->node_ctr, t->node_wabs, t->node_mom, t->heavy_cap);
+    LPM_LAUNCH(ctx, "m2m_pending_kernel", m2m_pending_kernel, gl, 128, 0, t->st, t->m2m_pending);
+    LPM_LAUNCH(ctx, "m2m_upward_kernel", m2m_upward_kernel, gl, 128, (size_t)16 * t->n_mono * sizeof(double), t->st,
+               t->pm, t->mono, t->n_mono, t->node_ctr, t->node_wabs, t->node_mom, t->heavy_cap, t->m2m_pending);
     if (t->scalar)
         LPM_LAUNCH(ctx, "coeff_kernel", coeff_scalar_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->a_stride,
                    t->node_mom, t->A64, t->A32, t->heavy_cap);
