@@ -4,6 +4,7 @@ import numpy as np
 import pytest
 
 import lpmcxx_b200 as L
+import lpmcxx_b200.learned  # noqa: F401  (L.learned: the shipped selector weights)
 import lpmcxx_b200.workloads as W
 
 
