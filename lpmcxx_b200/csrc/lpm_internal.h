@@ -79,8 +79,8 @@ enum ScratchSlot {
     kSlotTree10,
     kSlotTree11,
     kSlotTree12,
-    kSlotTree13,
-    kSlotTree14,
+    kSlotSideCounts,    // radix digit counts of the target sort (runs on a second stream beside the tree build)
+    kSlotSideSums,      // scan block sums of the same
     kSlotRk0,
     kSlotRk1,
     kSlotRk2,

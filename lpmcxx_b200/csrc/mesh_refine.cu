@@ -27,7 +27,8 @@
 namespace lpm {
 int mesh_seed(int kind, double radius, std::vector<double>& vxyz, std::vector<int32_t>& edges,
               std::vector<int32_t>& faces);
-int scan_exclusive_i32(lpm_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, int32_t* total_dev);
+int scan_exclusive_i32(lpm_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, int32_t* total_dev,
+                       int sums_slot);
 
 namespace {
 
@@ -297,7 +298,7 @@ extern "C" int lpm_mesh_build_dev(lpm_ctx* ctx, int kind, int level, double radi
     for (int k = 0; k < level; ++k) {
         const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(nk + 1, 256), 8 * ctx->num_sms));
         LPM_LAUNCH(ctx, "mesh_count_kernel", mesh_count_kernel, g, 256, 0, m, (int)f0, (int)nk, cnt);
-        rc = scan_exclusive_i32(ctx, cnt, cnt, nk + 1, nullptr);
+        rc = scan_exclusive_i32(ctx, cnt, cnt, nk + 1, nullptr, kSlotMisc2);
         if (rc) return rc;
         LPM_LAUNCH(ctx, "mesh_divide_kernel", mesh_divide_kernel, g, 256, 0, m, (int)f0, (int)nk, (int)v0, (int)e0,
                    (int)(f0 + nk), cnt, face_divided);

@@ -178,10 +178,11 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const K* __
 }
 
 template <typename K>
-int radix_sort_impl(lpm_ctx* ctx, K* keys, int32_t* vals, K* tk, int32_t* tv, int64_t n, int bit_lo, int bit_hi) {
+int radix_sort_impl(lpm_ctx* ctx, K* keys, int32_t* vals, K* tk, int32_t* tv, int64_t n, int bit_lo, int bit_hi,
+                    int counts_slot, int sums_slot) {
     if (n <= 1) return LPM_OK;
     const int nblocks = (int)((n + kSortTile - 1) / kSortTile);
-    int32_t* counts = (int32_t*)scratch(ctx, kSlotMisc1, sizeof(int32_t) * 256 * (size_t)nblocks);
+    int32_t* counts = (int32_t*)scratch(ctx, counts_slot, sizeof(int32_t) * 256 * (size_t)nblocks);
     if (!counts) return LPM_ERR_OOM;
     K* src_k = keys;
     int32_t* src_v = vals;
@@ -196,7 +197,7 @@ int radix_sort_impl(lpm_ctx* ctx, K* keys, int32_t* vals, K* tk, int32_t* tv, in
             LPM_LAUNCH(ctx, "scan_single_block_kernel", scan_single_block_kernel, 1, 1024, 0, counts,
                        (int64_t)256 * nblocks, (int32_t*)nullptr);
         } else {
-            const int rc = scan_exclusive_i32(ctx, counts, counts, (int64_t)256 * nblocks, nullptr);
+            const int rc = scan_exclusive_i32(ctx, counts, counts, (int64_t)256 * nblocks, nullptr, sums_slot);
             if (rc) return rc;
         }
         LPM_LAUNCH(ctx, "radix_scatter_kernel", radix_scatter_kernel<K>, nblocks, kSortThreads, 0, src_k, src_v, dst_k,
@@ -485,10 +486,10 @@ __global__ void fill_i32_kernel(int32_t* p, int64_t n, int32_t v) {
 
 }  // namespace
 
-int scan_exclusive_i32(lpm_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, int32_t* total_dev) {
+int scan_exclusive_i32(lpm_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, int32_t* total_dev, int sums_slot) {
     if (n <= 0) return LPM_OK;
     const int nblocks = (int)((n + kScanTile - 1) / kScanTile);
-    int32_t* sums = (int32_t*)scratch(ctx, kSlotMisc2, sizeof(int32_t) * (size_t)(nblocks + 1));
+    int32_t* sums = (int32_t*)scratch(ctx, sums_slot, sizeof(int32_t) * (size_t)(nblocks + 1));
     if (!sums) return LPM_ERR_OOM;
     LPM_LAUNCH(ctx, "scan_block_sums_kernel", scan_block_sums_kernel, nblocks, kScanThreads, 0, in, n, sums);
     LPM_LAUNCH(ctx, "scan_single_block_kernel", scan_single_block_kernel, 1, 1024, 0, sums, (int64_t)nblocks,
@@ -513,12 +514,13 @@ int root_extent(lpm_ctx* ctx, const double4* pts, int64_t first, int64_t n, int 
     return LPM_OK;
 }
 
-int radix_sort_u64(lpm_ctx* ctx, uint64_t* keys, int32_t* vals, uint64_t* tk, int32_t* tv, int64_t n, int bit_lo) {
-    return radix_sort_impl<uint64_t>(ctx, keys, vals, tk, tv, n, bit_lo, 64);
+int radix_sort_u64(lpm_ctx* ctx, uint64_t* keys, int32_t* vals, uint64_t* tk, int32_t* tv, int64_t n, int bit_lo,
+                   int counts_slot, int sums_slot) {
+    return radix_sort_impl<uint64_t>(ctx, keys, vals, tk, tv, n, bit_lo, 64, counts_slot, sums_slot);
 }
 
 int radix_sort_u32(lpm_ctx* ctx, uint32_t* keys, int32_t* vals, uint32_t* tk, int32_t* tv, int64_t n, int bits) {
-    return radix_sort_impl<uint32_t>(ctx, keys, vals, tk, tv, n, 0, bits);
+    return radix_sort_impl<uint32_t>(ctx, keys, vals, tk, tv, n, 0, bits, kSlotMisc1, kSlotMisc2);
 }
 
 int octree_alloc(Octree& t, int64_t n, int max_per_leaf, int max_depth, int bits, double sphere_r) {

@@ -10,13 +10,15 @@ constexpr int kKeyLevels = 21;        // 3 bits per level in a 63-bit key; bit 6
 constexpr int kMaxLevels = 63;        // binary (1 bit per level) trees: up to 63 levels
 constexpr uint64_t kKeyOutside = ~0ull;
 
-// Exclusive prefix sum of n int32 values (in may equal out).  Uses ctx scratch slot kSlotMisc2.
-int scan_exclusive_i32(lpm_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, int32_t* total_dev);
+// Exclusive prefix sum of n int32 values (in may equal out).  Uses ctx scratch slot `sums_slot`.
+int scan_exclusive_i32(lpm_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, int32_t* total_dev,
+                       int sums_slot = kSlotMisc2);
 
 // Stable LSD radix sort of (key, value) pairs over key bits [bit_lo, 64), 8 bits per pass.
-// keys/vals are sorted in place (ping-pong through tmp_keys/tmp_vals, which must hold n items).
+// keys/vals are sorted in place (ping-pong through tmp_keys/tmp_vals, which must hold n items).  Digit counts
+// go to ctx scratch slot `counts_slot`, scan sums to `sums_slot` (sorts on concurrent streams use distinct slots).
 int radix_sort_u64(lpm_ctx* ctx, uint64_t* keys, int32_t* vals, uint64_t* tmp_keys, int32_t* tmp_vals, int64_t n,
-                   int bit_lo);
+                   int bit_lo, int counts_slot = kSlotMisc1, int sums_slot = kSlotMisc2);
 int radix_sort_u32(lpm_ctx* ctx, uint32_t* keys, int32_t* vals, uint32_t* tmp_keys, int32_t* tmp_vals, int64_t n,
                    int bits);
 

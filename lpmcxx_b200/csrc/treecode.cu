@@ -2013,6 +2013,7 @@ struct TreeSolver {
     // the near field runs on `side` beside the far-field launches on the context's stream (fork / join events)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_tfork = nullptr, ev_tjoin = nullptr;  // target batches on `side` beside the tree build
     // learned order selection
     bool learned = false;     // order_policy == LPM_ORDER_LEARNED
     bool mlp_loaded = false;  // weights present; without them the fixed order is the fallback
@@ -2304,6 +2305,8 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&t->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_tfork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_tjoin, cudaEventDisableTiming);
     if (t->learned) {
         A(talloc(t, &t->node_feat, nh * kMlpIn));
         A(talloc(t, &t->mlp_w, kMlpParams));
@@ -2374,6 +2377,8 @@ void tree_solver_destroy(TreeSolver* t) {
     if (!t) return;
     if (t->ev_fork) cudaEventDestroy(t->ev_fork);
     if (t->ev_join) cudaEventDestroy(t->ev_join);
+    if (t->ev_tfork) cudaEventDestroy(t->ev_tfork);
+    if (t->ev_tjoin) cudaEventDestroy(t->ev_tjoin);
     if (t->side) cudaStreamDestroy(t->side);
     octree_free(t->st);
     for (void* p : t->allocs) cudaFree(p);
@@ -2470,6 +2475,39 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
             rc = root_extent(ctx, src, 0, n_src, rb.mode, t->root_r);
         if (rc) return rc;
     }
+    // targets in Morton order, cut into compact batches of at most kBatch.  Independent of the source tree until
+    // the traversal, so (profiling off) it runs on the solver's side stream while the source octree and its
+    // moments are built on the context's stream: both are chains of short latency-bound launches.  Its sort and
+    // scan use their own scratch slots.
+    const unsigned gt = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(n_tgt + 1, 256), 8 * ctx->num_sms));
+    auto target_batches = [&]() -> int {
+        LPM_CUDA_TRY(cudaMemsetAsync(t->tcount, 0, 4 * sizeof(int32_t), ctx->stream));
+        int r = morton_keys(ctx, X, n_tgt, rb, t->tkeys, t->tperm, t->tcount);
+        if (r) return r;
+        r = radix_sort_u64(ctx, t->tkeys, t->tperm, t->ttmpk, t->ttmpv, n_tgt, 32, kSlotSideCounts, kSlotSideSums);
+        if (r) return r;
+        LPM_CUDA_TRY(cudaMemsetAsync(t->bflag + n_tgt, 0, sizeof(int32_t), ctx->stream));
+        LPM_LAUNCH(ctx, "batch_flags_kernel", batch_flags_kernel, gt, 256, 0, t->tkeys, n_tgt,
+                   3 * (kKeyLevels - t->batch_level), t->bflag);
+        r = scan_exclusive_i32(ctx, t->bflag, t->bflag, n_tgt + 1, nullptr, kSlotSideSums);
+        if (r) return r;
+        LPM_LAUNCH(ctx, "batch_first_kernel", batch_first_kernel, gt, 256, 0, t->bflag, n_tgt, t->batch_first,
+                   t->tcount + 1, t->n_batches);
+        LPM_LAUNCH(ctx, "batch_kernel", batch_kernel, (unsigned)t->n_batches, kBatch, 0, X, t->tperm,
+                   t->batch_first, t->tcount + 1, t->tgt_sorted, t->batch_ctr);
+        return LPM_OK;
+    };
+    const bool tside = !ctx->profiling;
+    if (tside) {
+        LPM_CUDA_TRY(cudaEventRecord(t->ev_tfork, ctx->stream));
+        LPM_CUDA_TRY(cudaStreamWaitEvent(t->side, t->ev_tfork, 0));
+        cudaStream_t main_stream = ctx->stream;
+        ctx->stream = t->side;
+        rc = target_batches();
+        ctx->stream = main_stream;
+        if (rc) return rc;
+        LPM_CUDA_TRY(cudaEventRecord(t->ev_tjoin, t->side));
+    }
     rc = octree_build(ctx, t->st, src, n_src, rb);
     if (rc) return rc;
     if (can_sync) {  // grow the per-node arrays to this tree (a captured replay can only flag an overflow)
@@ -2501,22 +2539,12 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     if (t->learned)
         LPM_LAUNCH(ctx, "node_feature_kernel", node_feature_kernel, gl, 128, 0, t->st, t->pm, t->node_ctr,
                    t->node_wabs, t->node_mom, t->node_feat, t->heavy_cap);
-    // targets in Morton order, cut into compact batches of at most kBatch
-    LPM_CUDA_TRY(cudaMemsetAsync(t->tcount, 0, 4 * sizeof(int32_t), ctx->stream));
-    rc = morton_keys(ctx, X, n_tgt, rb, t->tkeys, t->tperm, t->tcount);
-    if (rc) return rc;
-    rc = radix_sort_u64(ctx, t->tkeys, t->tperm, t->ttmpk, t->ttmpv, n_tgt, 32);
-    if (rc) return rc;
-    const unsigned gt = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(n_tgt + 1, 256), 8 * ctx->num_sms));
-    LPM_CUDA_TRY(cudaMemsetAsync(t->bflag + n_tgt, 0, sizeof(int32_t), ctx->stream));
-    LPM_LAUNCH(ctx, "batch_flags_kernel", batch_flags_kernel, gt, 256, 0, t->tkeys, n_tgt,
-               3 * (kKeyLevels - t->batch_level), t->bflag);
-    rc = scan_exclusive_i32(ctx, t->bflag, t->bflag, n_tgt + 1, nullptr);
-    if (rc) return rc;
-    LPM_LAUNCH(ctx, "batch_first_kernel", batch_first_kernel, gt, 256, 0, t->bflag, n_tgt, t->batch_first,
-               t->tcount + 1, t->n_batches);
-    LPM_LAUNCH(ctx, "batch_kernel", batch_kernel, (unsigned)t->n_batches, kBatch, 0, X, t->tperm, t->batch_first,
-               t->tcount + 1, t->tgt_sorted, t->batch_ctr);
+    if (tside) {  // the target batches were formed on the side stream
+        LPM_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, t->ev_tjoin, 0));
+    } else {
+        rc = target_batches();
+        if (rc) return rc;
+    }
     rc = build_lists(t, can_sync);
     if (rc) return rc;
     // far field: one launch per order present (only the fixed order, or the selector's orders 1..11),
