@@ -2014,6 +2014,7 @@ struct TreeSolver {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_tfork = nullptr, ev_tjoin = nullptr;  // target batches on `side` beside the tree build
+    cudaEvent_t ev_cfork = nullptr, ev_cjoin = nullptr;  // far coefficients on `side` beside the traversal
     // learned order selection
     bool learned = false;     // order_policy == LPM_ORDER_LEARNED
     bool mlp_loaded = false;  // weights present; without them the fixed order is the fallback
@@ -2307,6 +2308,8 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_tfork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_tjoin, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_cfork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_cjoin, cudaEventDisableTiming);
     if (t->learned) {
         A(talloc(t, &t->node_feat, nh * kMlpIn));
         A(talloc(t, &t->mlp_w, kMlpParams));
@@ -2379,6 +2382,8 @@ void tree_solver_destroy(TreeSolver* t) {
     if (t->ev_join) cudaEventDestroy(t->ev_join);
     if (t->ev_tfork) cudaEventDestroy(t->ev_tfork);
     if (t->ev_tjoin) cudaEventDestroy(t->ev_tjoin);
+    if (t->ev_cfork) cudaEventDestroy(t->ev_cfork);
+    if (t->ev_cjoin) cudaEventDestroy(t->ev_cjoin);
     if (t->side) cudaStreamDestroy(t->side);
     octree_free(t->st);
     for (void* p : t->allocs) cudaFree(p);
@@ -2530,12 +2535,30 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     LPM_LAUNCH(ctx, "m2m_pending_kernel", m2m_pending_kernel, gl, 128, 0, t->st, t->m2m_pending);
     LPM_LAUNCH(ctx, "m2m_upward_kernel", m2m_upward_kernel, gl, 128, (size_t)16 * t->n_mono * sizeof(double), t->st,
                t->pm, t->mono, t->n_mono, t->node_ctr, t->node_wabs, t->node_mom, t->heavy_cap, t->m2m_pending);
-    if (t->scalar)
-        LPM_LAUNCH(ctx, "coeff_kernel", coeff_scalar_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->a_stride,
-                   t->node_mom, t->A64, t->A32, t->heavy_cap);
-    else
-        LPM_LAUNCH(ctx, "coeff_kernel", coeff_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->node_mom, t->B64,
-                   t->B32, t->heavy_cap);
+    // far-field coefficients: needed only by the far kernels, so (profiling off) on the side stream during the
+    // node features and the traversal
+    auto coefficients = [&]() -> int {
+        if (t->scalar)
+            LPM_LAUNCH(ctx, "coeff_kernel", coeff_scalar_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent,
+                       t->a_stride, t->node_mom, t->A64, t->A32, t->heavy_cap);
+        else
+            LPM_LAUNCH(ctx, "coeff_kernel", coeff_kernel, gl, 128, 0, t->st, t->pm, t->ent, t->n_ent, t->node_mom,
+                       t->B64, t->B32, t->heavy_cap);
+        return LPM_OK;
+    };
+    if (tside) {
+        LPM_CUDA_TRY(cudaEventRecord(t->ev_cfork, ctx->stream));
+        LPM_CUDA_TRY(cudaStreamWaitEvent(t->side, t->ev_cfork, 0));
+        cudaStream_t main_stream = ctx->stream;
+        ctx->stream = t->side;
+        rc = coefficients();
+        ctx->stream = main_stream;
+        if (rc) return rc;
+        LPM_CUDA_TRY(cudaEventRecord(t->ev_cjoin, t->side));
+    } else {
+        rc = coefficients();
+        if (rc) return rc;
+    }
     if (t->learned)
         LPM_LAUNCH(ctx, "node_feature_kernel", node_feature_kernel, gl, 128, 0, t->st, t->pm, t->node_ctr,
                    t->node_wabs, t->node_mom, t->node_feat, t->heavy_cap);
@@ -2547,6 +2570,7 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     }
     rc = build_lists(t, can_sync);
     if (rc) return rc;
+    if (tside) LPM_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, t->ev_cjoin, 0));  // the coefficients
     // far field: one launch per order present (only the fixed order, or the selector's orders 1..11),
     // each adding its bucket's contributions to V
     LPM_CUDA_TRY(cudaMemsetAsync(t->V, 0, 3 * (size_t)n_tgt * sizeof(double), ctx->stream));
