@@ -249,7 +249,8 @@ __global__ void m2m_pending_kernel(Octree t, int32_t* __restrict__ pending) {
     }
 }
 
-__global__ void __launch_bounds__(128) m2m_upward_kernel(Octree t, int pm, const int4* __restrict__ mono,
+constexpr int kM2mThreads = 256;
+__global__ void __launch_bounds__(kM2mThreads) m2m_upward_kernel(Octree t, int pm, const int4* __restrict__ mono,
                                                          int n_mono, double4* __restrict__ node_ctr,
                                                          double* __restrict__ node_wabs,
                                                          double* __restrict__ node_mom, int heavy_cap,
@@ -259,6 +260,8 @@ __global__ void __launch_bounds__(128) m2m_upward_kernel(Octree t, int pm, const
     __shared__ double bin[kPMax + 1][kPMax + 1];
     __shared__ int mono_idx[kPMax + 1][kPMax + 1][kPMax + 1];  // (a, b, c) -> position in the monomial list
     __shared__ int climb;
+    __shared__ double4 ch[8];  // the current node's children: centres (w = radius), counts, sum |w|
+    __shared__ double chm[8], chw[8];
     for (int i = threadIdx.x; i < (kPMax + 1) * (kPMax + 1); i += blockDim.x)
         bin[i / (kPMax + 1)][i % (kPMax + 1)] = c_binom[i / (kPMax + 1)][i % (kPMax + 1)];
     for (int i = threadIdx.x; i < n_mono; i += blockDim.x) {
@@ -271,42 +274,32 @@ __global__ void __launch_bounds__(128) m2m_upward_kernel(Octree t, int pm, const
     auto m2m_node = [&](int node) {
         const int nc = t.node_nchild[node];
         const int fc = t.node_first_child[node];
-        double4 ch[8];  // the children's centres, loaded together
-        double m[8], wc[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (k < nc) {
-                ch[k] = ldcg4(node_ctr + fc + k);
-                m[k] = (double)(t.node_end[fc + k] - t.node_start[fc + k]);
-                wc[k] = __ldcg(node_wabs + fc + k);
-            }
+        __syncthreads();  // the previous node's readers of ch / dp / m2m_sh are done
+        if ((int)threadIdx.x < nc) {  // the children's centres, counts and weights, one thread each
+            ch[threadIdx.x] = ldcg4(node_ctr + fc + threadIdx.x);
+            chm[threadIdx.x] = (double)(t.node_end[fc + threadIdx.x] - t.node_start[fc + threadIdx.x]);
+            chw[threadIdx.x] = __ldcg(node_wabs + fc + threadIdx.x);
         }
+        __syncthreads();
         double cx = 0, cy = 0, cz = 0, cnt = 0, wabs = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (k < nc) {
-                cx += m[k] * ch[k].x; cy += m[k] * ch[k].y; cz += m[k] * ch[k].z; cnt += m[k];
-                wabs += wc[k];
-            }
+        for (int k = 0; k < nc; ++k) {
+            cx += chm[k] * ch[k].x; cy += chm[k] * ch[k].y; cz += chm[k] * ch[k].z; cnt += chm[k];
+            wabs += chw[k];
         }
         cx /= cnt; cy /= cnt; cz /= cnt;
         double r = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (k < nc) {
-                const double dx = ch[k].x - cx, dy = ch[k].y - cy, dz = ch[k].z - cz;
-                r = fmax(r, sqrt(dx * dx + dy * dy + dz * dz) + ch[k].w);
-            }
+        for (int k = 0; k < nc; ++k) {
+            const double dx = ch[k].x - cx, dy = ch[k].y - cy, dz = ch[k].z - cz;
+            r = fmax(r, sqrt(dx * dx + dy * dy + dz * dz) + ch[k].w);
         }
         if (threadIdx.x == 0) {
             node_ctr[node] = make_double4(cx, cy, cz, r);
             node_wabs[node] = wabs;
         }
         if (fc + nc > heavy_cap) return;  // uniform per block: a child (numbered after node) has no moments
-        __syncthreads();  // the previous node's readers of dp / m2m_sh are done
         if (threadIdx.x < nc * 3) {
             const int k = threadIdx.x / 3, a = threadIdx.x % 3;
-            const double4 cc = ldcg4(node_ctr + fc + k);  // (dynamic k: not from the register copies)
+            const double4 cc = ch[k];
             const double d = a == 0 ? cc.x - cx : (a == 1 ? cc.y - cy : cc.z - cz);
             double v = 1.0;
             for (int q = 0; q <= pm; ++q) {
@@ -2533,7 +2526,7 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
                t->n_units,
                t->node_ctr, t->node_wabs, t->node_mom, t->src32, t->scalar ? 1.0 : 2.0, t->heavy_cap);
     LPM_LAUNCH(ctx, "m2m_pending_kernel", m2m_pending_kernel, gl, 128, 0, t->st, t->m2m_pending);
-    LPM_LAUNCH(ctx, "m2m_upward_kernel", m2m_upward_kernel, gl, 128, (size_t)16 * t->n_mono * sizeof(double), t->st,
+    LPM_LAUNCH(ctx, "m2m_upward_kernel", m2m_upward_kernel, gl, kM2mThreads, (size_t)16 * t->n_mono * sizeof(double), t->st,
                t->pm, t->mono, t->n_mono, t->node_ctr, t->node_wabs, t->node_mom, t->heavy_cap, t->m2m_pending);
     // far-field coefficients: needed only by the far kernels, so (profiling off) on the side stream during the
     // node features and the traversal
