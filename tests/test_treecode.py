@@ -180,6 +180,34 @@ def test_near_tile_shapes_agree(ctx, kernel):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["biot_savart", "poisson"])
+def test_stream_overlap_is_bitwise_neutral(ctx, kernel):
+    """An evaluation spreads over two streams (target batches and far coefficients beside the tree build and the
+    traversal; for the scalar kernel the near field beside the far field); with per-kernel profiling on every
+    kernel runs in order on one stream.  Both give bitwise the same sums, evaluation after evaluation."""
+    torch = ctx.use_torch_stream()
+    if kernel == "biot_savart":
+        _, p, n_src = W.gaussian_vortex_mesh("icos", 5)
+        kern, solver, comps = L.biot_savart_kernel(), L.tree_solver(L.LPM_PREC_F32, 8, 64, 0.5), 3
+    else:
+        p = W.poisson_cube(60_000)
+        n_src = p.shape[0]
+        kern, solver, comps = L.poisson_kernel(), L.tree_solver(L.LPM_PREC_F32, 6, 64, 0.6), 1
+    d = torch.tensor(p, device="cuda")
+    ts = L.TreeSum(ctx, kern, solver, n_src, p.shape[0])
+    outs = []
+    for prof in (False, True, False):
+        ctx.set_profiling(prof)
+        out = torch.empty((comps, p.shape[0]), dtype=torch.float64, device="cuda")
+        ts.eval(d[:n_src], d, out)
+        torch.cuda.synchronize()
+        outs.append(out)
+    ctx.set_profiling(False)
+    ts.close()
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
+
+
+@pytest.mark.gpu
 def test_poisson_treecode_1m_against_oracle(ctx):
     """The 3D Poisson configuration at its full size (1,048,576 points uniform in [-1, 1]^3, charges U(-1, 1),
     p = 6, theta = 0.6, 256 per leaf) against the oracle's FP64 direct sum (C restatement, self pair
