@@ -56,6 +56,13 @@ __host__ __device__ constexpr int entries_for(int P) {                          
     for (int m = 0; 2 * m < P; ++m) e += tet(P - 2 * m);
     return e;
 }
+// The FP32 far field of the highest order runs as two launches (its fully unrolled body overflows the
+// instruction cache): part 1 the Horner blocks m >= 1 times s, part 2 the block m = 0 (entries of the Horner
+// sequence: part 1 first, part 2 after); part 0 is the whole sequence.
+constexpr int kFarSplitOrder = 11;
+__host__ __device__ constexpr int part_entries(int P, int part) {
+    return part == 0 ? entries_for(P) : (part == 1 ? entries_for(P) - tet(P) : tet(P));
+}
 // Node moments are stored packed: the monomials (a, b, c) with a + b + c <= pm in a-major, then b, then c
 // order, mono_count(pm) doubles per node.
 __host__ __device__ constexpr int tet_count(int n) { return (n + 1) * (n + 2) * (n + 3) / 6; }
@@ -1009,9 +1016,9 @@ struct FarArgs {
 constexpr int kFarStageUnits = LPM_FAR_STAGE_UNITS;  // 16-byte units gathered per stage (at least one entry)
 constexpr int kFarMinBlocks = LPM_FAR_MIN_BLOCKS;    // resident blocks per SM the far kernels are built for
 
-template <int P, typename F4, int U = kFarStageUnits>
+template <int P, typename F4, int U = kFarStageUnits, int PART = 0>
 struct FarShape {
-    static constexpr int kUnits = entries_for(P) * (int)(sizeof(F4) / 16);  // per entry
+    static constexpr int kUnits = part_entries(P, PART) * (int)(sizeof(F4) / 16);  // per entry
     static constexpr int kK = kUnits >= U ? 1 : (U / kUnits > 32 ? 32 : U / kUnits);
     static constexpr int kStage = kK * kUnits;  // units per stage buffer
     static constexpr size_t kSmem = 2 * (size_t)kStage * 16 + 2 * (size_t)kK * sizeof(double4);
@@ -1088,13 +1095,13 @@ __global__ void __launch_bounds__(kBatch, kFarMinBlocks) far_order_kernel(FarArg
 // feeds both targets' chains (four packed FMAs per load instead of two) and each thread carries two
 // independent dependency chains.  e[t] = (e0, e1, e2, s) of target t; same arithmetic per target as
 // horner_f32x2.
-template <int P>
+template <int P, int PART = 0>
 __device__ __forceinline__ void horner2_f32x2(const float4* __restrict__ Bc, const float (&e)[2][4],
                                               float (&g)[2][4]) {
     int q = 0;
     float G[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
 #pragma unroll
-    for (int m = (P - 1) / 2; m >= 0; --m) {
+    for (int m = PART == 2 ? 0 : (P - 1) / 2; m >= (PART == 1 ? 1 : 0); --m) {
         const int Q = P - 2 * m;
         float Pa[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
 #pragma unroll
@@ -1138,13 +1145,17 @@ __device__ __forceinline__ void horner2_f32x2(const float4* __restrict__ Bc, con
         }
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
-            if (m == (P - 1) / 2) {
+            if (m == (PART == 2 ? 0 : (P - 1) / 2)) {
                 G[t][0] = Pa[t][0]; G[t][1] = Pa[t][1]; G[t][2] = Pa[t][2]; G[t][3] = Pa[t][3];
             } else {
                 fma2p(G[t][0], G[t][1], G[t][0], G[t][1], e[t][3], Pa[t][0], Pa[t][1]);
                 fma2p(G[t][2], G[t][3], G[t][2], G[t][3], e[t][3], Pa[t][2], Pa[t][3]);
             }
         }
+    }
+    if constexpr (PART == 1) {  // the blocks m >= 1 carry one more factor s
+#pragma unroll
+        for (int c = 0; c < 4; ++c) fma2v(G[0][c], G[1][c], G[0][c], G[1][c], e[0][3], e[1][3], -0.0f, -0.0f);
     }
 #pragma unroll
     for (int t = 0; t < 2; ++t)
@@ -1173,7 +1184,7 @@ constexpr int kFar2MinBlocks = LPM_FAR2_MIN_BLOCKS;
 // target at the end in FP64: acc32 += h in FP32 over a stage, folded into FP64 once per stage.  Every step
 // runs on the two targets together (fma.rn.f32x2, each lane rounding as the scalar operation); xo holds the
 // targets' offsets and c the centre's.
-template <int P>
+template <int P, int PART = 0>
 __device__ __forceinline__ void far_one_acc2_f32(const float4* __restrict__ Bc, const float (&xo)[2][3],
                                                  const float4 c, float (&acc32)[2][3]) {
     float d[2][3], e[2][4], g[2][4], r0, r1;
@@ -1187,7 +1198,7 @@ __device__ __forceinline__ void far_one_acc2_f32(const float4* __restrict__ Bc, 
     e[1][3] = rcp32(r1);
 #pragma unroll
     for (int k = 0; k < 3; ++k) fma2v(e[0][k], e[1][k], d[0][k], d[1][k], e[0][3], e[1][3], -0.0f, -0.0f);
-    horner2_f32x2<P>(Bc, e, g);
+    horner2_f32x2<P, PART>(Bc, e, g);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         float h0, h1;
@@ -1198,10 +1209,10 @@ __device__ __forceinline__ void far_one_acc2_f32(const float4* __restrict__ Bc, 
 
 // Stage gather of the far2 kernel: coefficients by cp.async as far_stage_gather, cluster centres as FP32
 // offsets from the block's origin o.
-template <int P>
+template <int P, int PART = 0>
 __device__ __forceinline__ void far2_stage_gather(const FarArgs& A, int64_t s0, int n, float4* buf, float4* ctr,
                                                   const double4& o) {
-    constexpr int kUnits = FarShape<P, float4>::kUnits;
+    constexpr int kUnits = FarShape<P, float4, kFarStageUnits, PART>::kUnits;
     for (int i = threadIdx.x; i < n * kUnits; i += kFar2Threads) {
         const int e = i / kUnits, j = i - e * kUnits;
         const int node = A.far_list[s0 + e].x;
@@ -1218,9 +1229,9 @@ __device__ __forceinline__ void far2_stage_gather(const FarArgs& A, int64_t s0, 
 // (128 registers; the odd orders spill up to 128 bytes to L1) with 768-unit stages: measured faster than
 // 6 blocks without spills, than more resident blocks with smaller stages (fewer block barriers per
 // coefficient) and than fewer blocks with larger ones.
-template <int P>
+template <int P, int PART = 0>
 __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kernel(FarArgs A) {
-    using S = FarShape<P, float4, kFar2StageUnits>;
+    using S = FarShape<P, float4, kFar2StageUnits, PART>;
     extern __shared__ float4 fbuf[];  // 2 stages of S::kStage units, then 2 x kK centres (FP32 offsets)
     float4* ctr = fbuf + 2 * S::kStage;
     __shared__ int slot;
@@ -1242,14 +1253,14 @@ __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kerne
         xo[t][0] = (float)(p.x - o.x); xo[t][1] = (float)(p.y - o.y); xo[t][2] = (float)(p.z - o.z);
     }
     double acc[2][3] = {{0, 0, 0}, {0, 0, 0}};
-    far2_stage_gather<P>(A, f0, (int)min((int64_t)S::kK, f1 - f0), fbuf, ctr, o);
+    far2_stage_gather<P, PART>(A, f0, (int)min((int64_t)S::kK, f1 - f0), fbuf, ctr, o);
     cp_async_commit();
     int s = 0;
     for (int64_t s0 = f0;; s ^= 1) {
         const int n = (int)min((int64_t)S::kK, f1 - s0);
         const int64_t s1 = s0 + n;
         if (s1 < f1)
-            far2_stage_gather<P>(A, s1, (int)min((int64_t)S::kK, f1 - s1), fbuf + (size_t)(s ^ 1) * S::kStage,
+            far2_stage_gather<P, PART>(A, s1, (int)min((int64_t)S::kK, f1 - s1), fbuf + (size_t)(s ^ 1) * S::kStage,
                                  ctr + (s ^ 1) * S::kK, o);
         cp_async_commit();
         cp_async_wait_prev();
@@ -1258,7 +1269,8 @@ __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kerne
             const float4* Bc = fbuf + (size_t)s * S::kStage;
             const float4* cs = ctr + s * S::kK;
             float acc32[2][3] = {{0, 0, 0}, {0, 0, 0}};
-            for (int k = 0; k < n; ++k) far_one_acc2_f32<P>(Bc + (size_t)k * entries_for(P), xo, cs[k], acc32);
+            for (int k = 0; k < n; ++k)
+                far_one_acc2_f32<P, PART>(Bc + (size_t)k * part_entries(P, PART), xo, cs[k], acc32);
 #pragma unroll
             for (int t = 0; t < 2; ++t)
 #pragma unroll
@@ -1504,6 +1516,17 @@ FarKernelFn far_kernel_for(bool f64, size_t* smem, int* threads) {
     }
     *smem = FarShape<P, float4>::kSmem;
     return far_order_kernel<P, float, float4>;
+}
+
+// The two launches of the FP32 far field at kFarSplitOrder (parts 1 and 2).
+FarKernelFn far_split_select(int part, size_t* smem, int* threads) {
+    *threads = kFar2Threads;
+    if (part == 1) {
+        *smem = FarShape<kFarSplitOrder, float4, kFar2StageUnits, 1>::kSmem;
+        return far_order2_kernel<kFarSplitOrder, 1>;
+    }
+    *smem = FarShape<kFarSplitOrder, float4, kFar2StageUnits, 2>::kSmem;
+    return far_order2_kernel<kFarSplitOrder, 2>;
 }
 
 // The order-P far kernel (FP64 or FP32 arithmetic) and its dynamic shared memory.
@@ -2028,6 +2051,7 @@ struct TreeSolver {
     int near_tile = kNearStreamTile;
     int near_split = kNearSplit;      // source groups per batch (run-time "near_split")
     int far_blocks[kPMax + 1][2] = {};  // per order, FP32 / FP64 far kernel
+    int far_split_blocks[2] = {};       // the two FP32 launches of order kFarSplitOrder
     uint64_t generation = 0;          // reallocations of the lists and per-node arrays (tree_generation)
     std::vector<void*> allocs;
 };
@@ -2355,6 +2379,15 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
                 t->far_blocks[P][f64] = (int)std::max<int64_t>(
                     1, std::min<int64_t>(t->n_batches, (int64_t)std::max(per_sm, 1) * ctx->num_sms));
             }
+        for (int part = 1; part <= 2 && ea == cudaSuccess && !scalar; ++part) {
+            size_t smem = 0;
+            int threads = 0;
+            per_sm = 0;
+            FarKernelFn fn = far_split_select(part, &smem, &threads);
+            ea = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+            t->far_split_blocks[part - 1] = (int)std::max<int64_t>(
+                1, std::min<int64_t>(t->n_batches, (int64_t)std::max(per_sm, 1) * ctx->num_sms));
+        }
         if (ea != cudaSuccess) {
             tree_solver_destroy(t);
             return cuda_status(ea, "cudaOccupancyMaxActiveBlocksPerMultiprocessor (far kernels)");
@@ -2643,6 +2676,14 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
                 int threads = 0;
                 FarScalarFn fs = far_scalar_select(P, f64, &smem, &threads);
                 LPM_LAUNCH(ctx, "far_kernel", fs, grid, threads, smem, F, t->a_stride);
+            } else if (P == kFarSplitOrder && !f64) {  // two launches, each on its own ticket
+                for (int part = 1; part <= 2; ++part) {
+                    int threads = 0;
+                    FarKernelFn fn = far_split_select(part, &smem, &threads);
+                    F.gtab = t->gtab + t->ct.table_off[P] + (part == 2 ? part_entries(P, 1) : 0);
+                    F.ticket = t->sched_aux + kAuxFarTicket + (part == 2 ? kPMax + 1 : P);
+                    LPM_LAUNCH(ctx, "far_kernel", fn, (unsigned)t->far_split_blocks[part - 1], threads, smem, F);
+                }
             } else {
                 int threads = 0;
                 FarKernelFn fn = far_kernel_select(P, f64, &smem, &threads);
