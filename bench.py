@@ -241,11 +241,15 @@ def profile_summary_traffic(kernel: str) -> float | None:
 # relative L2 <= 1e-6 against the FP64 direct sum on this workload; "tree_cfg2a" is the p=8, theta=0.7,
 # 512-per-leaf configuration (whose error is ~1e-4); "tree_learned" picks the order per pair with the
 # shipped selector (order 10 is its fallback) under the per-pair budget LEARNED_EPS, each chosen order raised
-# by LEARNED_ORDER_BIAS: a sweep at icos L8 (bias 0..3 x budget) gave the fastest setting within 0.8 x 1e-6
-# at bias 2, budget 5e-7 (rel L2 5.7e-7, 3% faster than bias 0 at budget 2e-8, rel L2 3.7e-7).
-TREE_SETTINGS = {"tree_f32": (10, 0.5, 256), "tree_cfg2a": (8, 0.7, 512), "tree_learned": (10, 0.5, 512)}
+# by LEARNED_ORDER_BIAS, target batches cut at one octree level coarser than the solver's default
+# (LEARNED_BATCH_LEVEL_OFFSET): the autotuner at icos L8 (leaf 384/512/768 x theta 0.45..0.55 x budget
+# 3e-7..8e-7 x bias 2, 3 x batch level default, default - 1; 8192 sampled targets against the FP64 direct sum)
+# gave the fastest 512-per-leaf setting within 0.8 x 1e-6 at theta 0.55, budget 5e-7, bias 2, batch level
+# default - 1 (13.5 ms per evaluation, rel L2 5.8e-7, against 14.2 ms for theta 0.5 at the default level).
+TREE_SETTINGS = {"tree_f32": (10, 0.5, 256), "tree_cfg2a": (8, 0.7, 512), "tree_learned": (10, 0.55, 512)}
 LEARNED_EPS = 5e-7
 LEARNED_ORDER_BIAS = 2
+LEARNED_BATCH_LEVEL_OFFSET = -1
 
 
 def solver_desc(name: str):
@@ -782,6 +786,7 @@ def run_gpu(args) -> None:
                 raise SystemExit("tree_learned: the shipped selector weights are missing")
             rk.set_mlp(params)
             rk.set_param("order_bias", LEARNED_ORDER_BIAS)
+            rk.set_param("batch_level", rk.get_param("batch_level") + LEARNED_BATCH_LEVEL_OFFSET)
         rk.set_state(state0)
         rk.step(args.dt, args.warmup, use_graph=True)
         stream.synchronize()
@@ -903,7 +908,9 @@ def run_gpu(args) -> None:
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32" if head != "direct_f64" else "f64", "data": "synthetic",
         "config": {"workload": workload_name(args.level, n_src, n, args.dt), "solver": head,
-                   **({"selector": f"budget {LEARNED_EPS}, order bias {LEARNED_ORDER_BIAS}, theta 0.5, 512 per leaf"}
+                   **({"selector": f"budget {LEARNED_EPS}, order bias {LEARNED_ORDER_BIAS}, "
+                                   f"theta {TREE_SETTINGS['tree_learned'][1]}, 512 per leaf, batch level "
+                                   f"default {LEARNED_BATCH_LEVEL_OFFSET:+d}"}
                       if head == "tree_learned" else {}),
                    "n_sources": n_src,
                    "n_targets": n, "dt": args.dt,
