@@ -378,8 +378,13 @@ int lpm_rk4_set_mlp(lpm_rk4* rk, const float* params);
 /* ---- ensembles (no reference counterpart): n_inst independent RK4 problems of uneven sizes advanced
  * together.  Instances are spread over `lanes` streams (each with its own internal context, assigned
  * longest-first by an n log n size estimate); after one uncaptured step, each step of every instance is
- * one replay of a single CUDA graph that forks onto the lanes and joins back.  Instance i is an lpm_rk4
- * (lpm_ensemble_instance) for setting and reading its state; lpm_ensemble_step is synchronous. */
+ * one replay of a single CUDA graph that forks onto the lanes and joins back.  In the fused mode (the
+ * default), each RK4 stage builds every instance's tree and interaction lists on the lanes and then runs the
+ * far field of ALL treecode instances as one persistent launch per Taylor order and their near field as one
+ * persistent launch per near tile shape, whose blocks take (instance, batch) items in decreasing order of
+ * work over the whole ensemble; results are bitwise those of the lane mode (set_param "fused" 0), where each
+ * instance's far and near launches run on its lane.  Instance i is an lpm_rk4 (lpm_ensemble_instance) for
+ * setting and reading its state; lpm_ensemble_step is synchronous. */
 typedef struct lpm_ensemble lpm_ensemble;
 int lpm_ensemble_create(lpm_ctx* ctx, const lpm_kernel_desc* kernel, const lpm_solver_desc* solver, int n_inst,
                         const int64_t* n_src, const int64_t* n_pts, int lanes, lpm_ensemble** out);
@@ -391,8 +396,11 @@ int lpm_ensemble_destroy(lpm_ensemble* ens);
 int lpm_ensemble_instance(lpm_ensemble* ens, int i, lpm_rk4** rk);
 int lpm_ensemble_lane_of(const lpm_ensemble* ens, int i, int* lane);
 int lpm_ensemble_set_mlp(lpm_ensemble* ens, const float* params);
-/* lpm_rk4_set_param on every instance; drops the captured step (the next graph step first runs uncaptured). */
+/* lpm_rk4_set_param on every instance; drops the captured step (the next graph step first runs uncaptured).
+ * "fused" (0 or 1) is the ensemble's own: the fused far / near launches described above. */
 int lpm_ensemble_set_param(lpm_ensemble* ens, const char* name, double value);
+/* The ensemble's own parameters ("fused"). */
+int lpm_ensemble_get_param(const lpm_ensemble* ens, const char* name, double* value);
 int lpm_ensemble_step(lpm_ensemble* ens, double dt, int nsteps, int use_graph);
 
 /* ---- testing (no reference counterpart): failure injection on the host side.  The device allocation made

@@ -330,7 +330,8 @@ class _RK4View(RK4):
 
 class Ensemble:
     """lpm_ensemble: independent RK4 problems of uneven sizes, advanced together by one CUDA graph per
-    step spread over `lanes` streams.  `instance(i)` gives an RK4 handle for states."""
+    step spread over `lanes` streams, the far and near fields of all instances in fused persistent launches
+    (set_param("fused", 0): per lane).  `instance(i)` gives an RK4 handle for states."""
 
     def __init__(self, ctx: Context, kernel: KernelDesc, solver, n_src, n_pts, lanes: int = 8):
         """solver: one SolverDesc for every instance, or a sequence of them (one per instance)."""
@@ -376,8 +377,15 @@ class Ensemble:
         check(lib().lpm_ensemble_set_mlp(self.h, ptr(p)), "lpm_ensemble_set_mlp")
 
     def set_param(self, name: str, value: float) -> None:
-        """lpm_ensemble_set_param: one run-time treecode parameter for every instance."""
+        """lpm_ensemble_set_param: one run-time treecode parameter for every instance, or the ensemble's own
+        "fused" (1: far and near fields of all instances in fused persistent launches; 0: per lane)."""
         check(lib().lpm_ensemble_set_param(self.h, name.encode(), float(value)), "lpm_ensemble_set_param")
+
+    def get_param(self, name: str) -> float:
+        """lpm_ensemble_get_param ("fused")."""
+        v = C.c_double()
+        check(lib().lpm_ensemble_get_param(self.h, name.encode(), C.byref(v)), "lpm_ensemble_get_param")
+        return v.value
 
     def step(self, dt: float, nsteps: int = 1, use_graph: bool = True) -> None:
         check(lib().lpm_ensemble_step(self.h, dt, nsteps, 1 if use_graph else 0), "lpm_ensemble_step")

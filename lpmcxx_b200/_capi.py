@@ -134,6 +134,7 @@ SIGNATURES = {
     "lpm_ensemble_lane_of": (C.c_int, [P, C.c_int, P]),
     "lpm_ensemble_set_mlp": (C.c_int, [P, P]),
     "lpm_ensemble_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
+    "lpm_ensemble_get_param": (C.c_int, [P, C.c_char_p, P]),
     "lpm_ensemble_step": (C.c_int, [P, C.c_double, C.c_int, C.c_int]),
     "lpm_debug_fail_allocations": (C.c_int, [C.c_int64]),
 }

@@ -7,12 +7,21 @@
 // captured into a single CUDA graph that forks onto the lanes and joins back, and the graph is replayed
 // once per step: small instances (20k particles) that cannot fill a B200 alone overlap with each other
 // and with the large ones.
+//
+// Fused mode (the default; set_param "fused"): each RK4 stage forks onto the lanes for every instance's
+// tree build, moments and interaction lists, joins, and then the far field of ALL instances runs as one
+// persistent launch per Taylor order and the near field as one persistent launch per near tile shape
+// (TreeFused, treecode.cu), whose blocks take (instance, batch) items in decreasing order of work over the
+// whole ensemble; the stage updates fork onto the lanes again.  The results are bitwise those of the lane
+// mode.  Without it, each instance's far and near launches run on its lane.
 #include "lpm_internal.h"
+#include "treecode.h"
 
 #include <algorithm>
 #include <cmath>
 #include <new>
 #include <numeric>
+#include <string>
 #include <vector>
 
 namespace lpm {
@@ -24,6 +33,10 @@ int rk4_set_param_internal(lpm_rk4* rk, const char* name, double value);
 uint64_t rk4_buffer_generation(const lpm_rk4* rk);
 void rk4_set_owner(lpm_rk4* rk, lpm_ensemble* e);
 int ensemble_invalidate(lpm_ensemble* e);
+int rk4_stage_begin(lpm_rk4* rk);
+int rk4_stage_update(lpm_rk4* rk, int stage, double dt);
+TreeSolver* rk4_tree(lpm_rk4* rk);
+double* rk4_stage_velocity(lpm_rk4* rk);
 }  // namespace lpm
 
 using namespace lpm;
@@ -41,6 +54,8 @@ struct lpm_ensemble {
     int64_t graph_nodes = 0;
     bool warmed = false;
     std::vector<uint64_t> graph_gen;   // per instance: buffer generation at capture
+    bool fused = true;                 // far and near fields of all instances in fused launches
+    TreeFused* fz = nullptr;           // their tables (on ctx's own stream)
 };
 
 // Whether any instance reallocated a buffer since the ensemble's graph was captured.
@@ -81,6 +96,7 @@ extern "C" int lpm_ensemble_destroy(lpm_ensemble* e) {
     for (cudaEvent_t ev : e->join) cudaEventDestroy(ev);
     if (e->fork) cudaEventDestroy(e->fork);
     for (lpm_ctx* c : e->lanes) lpm_ctx_destroy(c);
+    tree_fused_destroy(e->fz);
     delete e;
     return LPM_OK;
 }
@@ -199,6 +215,14 @@ extern "C" int lpm_ensemble_set_param(lpm_ensemble* e, const char* name, double 
     }
     int rc = ensemble_invalidate(e);
     if (rc) return rc;
+    if (std::string(name) == "fused") {
+        if (value != 0.0 && value != 1.0) {
+            set_error("lpm_ensemble_set_param: fused is 0 or 1");
+            return LPM_ERR_ARG;
+        }
+        e->fused = value != 0.0;
+        return LPM_OK;
+    }
     for (lpm_rk4* r : e->inst) {
         rc = rk4_set_param_internal(r, name, value);
         if (rc) return rc;
@@ -206,8 +230,104 @@ extern "C" int lpm_ensemble_set_param(lpm_ensemble* e, const char* name, double 
     return LPM_OK;
 }
 
+extern "C" int lpm_ensemble_get_param(const lpm_ensemble* e, const char* name, double* value) {
+    if (!e || !name || !value) {
+        set_error("lpm_ensemble_get_param: null argument");
+        return LPM_ERR_ARG;
+    }
+    if (std::string(name) == "fused") {
+        *value = e->fused ? 1.0 : 0.0;
+        return LPM_OK;
+    }
+    set_error("lpm_ensemble_get_param: unknown parameter '%s'", name);
+    return LPM_ERR_ARG;
+}
+
+// Binds every instance's treecode (current buffers and parameters) to the fused launches; the ensemble's
+// streams are idle.
+static int ens_bind(lpm_ensemble* e) {
+    if (!e->fz) {
+        int rc = tree_fused_create(e->ctx, &e->fz);
+        if (rc) return rc;
+    }
+    std::vector<TreeSolver*> ts(e->inst.size());
+    std::vector<double*> us(e->inst.size());
+    for (size_t i = 0; i < e->inst.size(); ++i) {
+        ts[i] = rk4_tree(e->inst[i]);
+        us[i] = rk4_stage_velocity(e->inst[i]);
+    }
+    // the fused launches run on the context's own stream (binding synchronises it)
+    cudaStream_t user = e->ctx->stream;
+    e->ctx->stream = e->ctx->own_stream;
+    const int rc = tree_fused_bind(e->fz, ts.data(), us.data(), (int)ts.size());
+    e->ctx->stream = user;
+    return rc;
+}
+
+// One fused step of every instance (four stages: per-instance work on the lanes, the far and near fields of
+// all instances on `origin`).  Uncaptured, the instances are bound again after each stage's lists are built
+// (they may have grown); captured, the caller has bound them.
+static int ens_enqueue_fused(lpm_ensemble* e, double dt, cudaStream_t origin, bool captured) {
+    const size_t L = e->lanes.size();
+    auto fork = [&]() -> cudaError_t {  // the lanes wait for origin's work so far
+        cudaError_t err = cudaEventRecord(e->fork, origin);
+        for (size_t l = 0; l < L && err == cudaSuccess; ++l) err = cudaStreamWaitEvent(e->lanes[l]->stream, e->fork, 0);
+        return err;
+    };
+    auto join = [&]() -> cudaError_t {  // origin waits for every lane's work so far
+        cudaError_t err = cudaSuccess;
+        for (size_t l = 0; l < L && err == cudaSuccess; ++l) {
+            err = cudaEventRecord(e->join[l], e->lanes[l]->stream);
+            if (err == cudaSuccess) err = cudaStreamWaitEvent(origin, e->join[l], 0);
+        }
+        return err;
+    };
+    for (int stage = 1; stage <= 4; ++stage) {
+        LPM_CUDA_TRY(fork());
+        for (lpm_rk4* r : e->inst) {
+            int rc = rk4_stage_begin(r);
+            if (rc) return rc;
+        }
+        LPM_CUDA_TRY(join());
+        if (!captured) {
+            LPM_CUDA_TRY(cudaStreamSynchronize(origin));
+            int rc = ens_bind(e);
+            if (rc) return rc;
+        }
+        cudaStream_t user = e->ctx->stream;
+        const bool prof = e->ctx->profiling;
+        e->ctx->stream = origin;
+        e->ctx->profiling = prof && !captured;  // per-kernel timing never inside a capture
+        int rc = tree_fused_run(e->fz);
+        e->ctx->stream = user;
+        e->ctx->profiling = prof;
+        if (rc) return rc;
+        LPM_CUDA_TRY(fork());
+        for (lpm_rk4* r : e->inst) {
+            rc = rk4_stage_update(r, stage, dt);
+            if (rc) return rc;
+        }
+        LPM_CUDA_TRY(join());
+    }
+    return LPM_OK;
+}
+
+// Whether the fused step applies: some instance uses the treecode.
+static bool ens_fusable(const lpm_ensemble* e) {
+    if (!e->fused) return false;
+    for (lpm_rk4* r : e->inst)
+        if (rk4_tree(r)) return true;
+    return false;
+}
+
 // One step of every instance, each on its lane's current stream.
 static int ens_enqueue(lpm_ensemble* e, double dt) {
+    if (ens_fusable(e)) {
+        int rc = ens_enqueue_fused(e, dt, e->ctx->own_stream, false);
+        if (rc) return rc;
+        LPM_CUDA_TRY(cudaStreamSynchronize(e->ctx->own_stream));
+        return LPM_OK;
+    }
     for (size_t i = 0; i < e->inst.size(); ++i) {
         int rc = rk4_step_enqueue(e->inst[i], dt);
         if (rc) return rc;
@@ -227,25 +347,39 @@ static int ens_capture(lpm_ensemble* e, double dt) {
         e->lanes[l]->stream = e->lanes[l]->own_stream;
         before[l] = e->lanes[l]->launches;
     }
+    const int64_t before_ctx = e->ctx->launches;  // the fused launches of the capture are counted per replay
     auto restore = [&]() {
         for (size_t l = 0; l < e->lanes.size(); ++l) {
             e->lanes[l]->stream = user[l];
             e->lanes[l]->launches = before[l];
         }
+        e->ctx->launches = before_ctx;
     };
+    const bool fused = ens_fusable(e);
+    if (fused) {  // the fused launches' tables hold the instances' buffers of this capture
+        int rc = ens_bind(e);
+        if (rc) {
+            restore();
+            return rc;
+        }
+    }
     cudaError_t err = cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal);
     if (err != cudaSuccess) {
         restore();
         return cuda_status(err, "cudaStreamBeginCapture");
     }
     int rc = LPM_OK;
-    err = cudaEventRecord(e->fork, origin);
-    for (size_t l = 0; l < e->lanes.size() && err == cudaSuccess; ++l)
-        err = cudaStreamWaitEvent(e->lanes[l]->stream, e->fork, 0);
-    if (err == cudaSuccess) rc = ens_enqueue(e, dt);
-    for (size_t l = 0; l < e->lanes.size() && err == cudaSuccess; ++l) {
-        err = cudaEventRecord(e->join[l], e->lanes[l]->stream);
-        if (err == cudaSuccess) err = cudaStreamWaitEvent(origin, e->join[l], 0);
+    if (fused) {
+        rc = ens_enqueue_fused(e, dt, origin, true);
+    } else {
+        err = cudaEventRecord(e->fork, origin);
+        for (size_t l = 0; l < e->lanes.size() && err == cudaSuccess; ++l)
+            err = cudaStreamWaitEvent(e->lanes[l]->stream, e->fork, 0);
+        if (err == cudaSuccess) rc = ens_enqueue(e, dt);
+        for (size_t l = 0; l < e->lanes.size() && err == cudaSuccess; ++l) {
+            err = cudaEventRecord(e->join[l], e->lanes[l]->stream);
+            if (err == cudaSuccess) err = cudaStreamWaitEvent(origin, e->join[l], 0);
+        }
     }
     cudaGraph_t g = nullptr;
     const cudaError_t end = cudaStreamEndCapture(origin, &g);

@@ -99,18 +99,33 @@ int rk4_velocity(lpm_rk4* rk, double* U) {
     return tree_velocity(rk->tree, rk->Xs, rk->n_src, rk->Xs, rk->n, U);
 }
 
-static int rk4_one_step(lpm_rk4* rk, double dt) {
+// The stage update from the stage velocity U: accumulates k, forms the next stage position (stage 4: the new
+// state).
+int rk4_stage_update(lpm_rk4* rk, int stage, double dt) {
     lpm_ctx* ctx = rk->ctx;
-    const unsigned grid = grid_for(rk->n, 256);
-    const float ws = wscale_for(rk->kernel);
+    LPM_LAUNCH(ctx, "rk4_update_kernel", rk4_update_kernel, grid_for(rk->n, 256), 256, 0, rk->X, rk->Xs, rk->Xs32,
+               rk->U, rk->K, rk->n, stage, dt, rk->kernel.radius, wscale_for(rk->kernel));
+    return LPM_OK;
+}
+
+static int rk4_one_step(lpm_rk4* rk, double dt) {
     for (int stage = 1; stage <= 4; ++stage) {
         int rc = rk4_velocity(rk, rk->U);
         if (rc) return rc;
-        LPM_LAUNCH(ctx, "rk4_update_kernel", rk4_update_kernel, grid, 256, 0, rk->X, rk->Xs, rk->Xs32, rk->U, rk->K,
-                   rk->n, stage, dt, rk->kernel.radius, ws);
+        rc = rk4_stage_update(rk, stage, dt);
+        if (rc) return rc;
     }
     return LPM_OK;
 }
+
+// The stage velocity of the fused ensemble step up to the far and near fields, which the ensemble's fused
+// launches add (treecode instances); a direct-sum instance computes its whole stage velocity here.
+int rk4_stage_begin(lpm_rk4* rk) {
+    if (rk->tree) return tree_fused_prepare(rk->tree, rk->Xs, rk->Xs, rk->U);
+    return rk4_velocity(rk, rk->U);
+}
+TreeSolver* rk4_tree(lpm_rk4* rk) { return rk->tree; }
+double* rk4_stage_velocity(lpm_rk4* rk) { return rk->U; }
 
 // One uncaptured-or-captured RK4 step of rk on its context's current stream (for the ensemble).
 int rk4_step_enqueue(lpm_rk4* rk, double dt) { return rk4_one_step(rk, dt); }

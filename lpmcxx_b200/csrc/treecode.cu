@@ -1224,21 +1224,14 @@ __device__ __forceinline__ void far2_stage_gather(const FarArgs& A, int64_t s0, 
     }
 }
 
-// far_order_kernel<P, float, float4> with two targets per thread (targets i and i + 64 of the batch):
-// 64 threads per block, stages of kFar2StageUnits, the same double buffering.  Built for 7 blocks per SM
-// (128 registers; the odd orders spill up to 128 bytes to L1) with 768-unit stages: measured faster than
-// 6 blocks without spills, than more resident blocks with smaller stages (fewer block barriers per
-// coefficient) and than fewer blocks with larger ones.
+// One batch b of the far2 kernel (the whole block); fbuf: 2 stages of S::kStage units, then 2 x kK centres
+// (FP32 offsets).
 template <int P, int PART = 0>
-__global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kernel(FarArgs A) {
+__device__ __forceinline__ void far2_batch(const FarArgs& A, int64_t b, float4* fbuf) {
     using S = FarShape<P, float4, kFar2StageUnits, PART>;
-    extern __shared__ float4 fbuf[];  // 2 stages of S::kStage units, then 2 x kK centres (FP32 offsets)
     float4* ctr = fbuf + 2 * S::kStage;
-    __shared__ int slot;
-    const int nbat = *A.nbat;
-    for (int64_t b = next_batch(A.ticket, A.order, nbat, &slot); b >= 0; b = next_batch(A.ticket, A.order, nbat, &slot)) {
     const int64_t f0 = A.far_off[b], f1 = min(f0 + (int64_t)A.far_cnt[b], A.far_cap);
-    if (f0 >= f1) continue;  // uniform per block
+    if (f0 >= f1) return;  // uniform per block
     const int64_t q0 = A.batch_first[b], qe = A.batch_first[b + 1];
     // warp w holds targets 64 w .. 64 w + 63 of the batch (lane l: 64 w + l and 64 w + l + 32), so a warp past
     // the batch's last target idles as a whole (batches average ~109 of 128 targets)
@@ -1290,7 +1283,20 @@ __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kerne
         A.V[A.n_tgt + q] += p.z * hx - p.x * hz;
         A.V[2 * A.n_tgt + q] += p.x * hy - p.y * hx;
     }
-    }
+}
+
+// far_order_kernel<P, float, float4> with two targets per thread (targets i and i + 64 of the batch):
+// 64 threads per block, stages of kFar2StageUnits, the same double buffering.  Built for 7 blocks per SM
+// (128 registers; the odd orders spill up to 128 bytes to L1) with 768-unit stages: measured faster than
+// 6 blocks without spills, than more resident blocks with smaller stages (fewer block barriers per
+// coefficient) and than fewer blocks with larger ones.
+template <int P, int PART = 0>
+__global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kernel(FarArgs A) {
+    extern __shared__ float4 fbuf[];
+    __shared__ int slot;
+    const int nbat = *A.nbat;
+    for (int64_t b = next_batch(A.ticket, A.order, nbat, &slot); b >= 0; b = next_batch(A.ticket, A.order, nbat, &slot))
+        far2_batch<P, PART>(A, b, fbuf);
 }
 
 // The Horner scheme of `horner` with scalar coefficients.
@@ -1772,22 +1778,20 @@ struct NearArgs {
     int32_t* ticket;       // zeroed before the launch
 };
 
-// Persistent: every block takes batches from the ticket in `order` until none is left; one batch at a time
-// through the body below.
+// One batch b of the near kernel (the whole block).
 // Tile shape: KT targets per thread and KTILE sources staged in shared memory per tile; KS groups of
 // kBatch / KT threads each hold the whole batch and sum their own contiguous share of every tile (KS = 2
 // gives each source read from shared memory to KT targets while keeping two warps on a batch), and the
 // groups' sums are added in shared memory at the end of the batch.  Instances for KT in {2, 4}, KTILE in
 // {256, 512, 1024} and KS in {1, 2} are chosen at run time.
 template <bool kScalar, int KT, int KTILE, int KS>
-__global__ void __launch_bounds__(kBatch / KT * KS) near_kernel(NearArgs A) {
+__device__ __forceinline__ void near_batch(const NearArgs& A, int64_t b) {
     constexpr int kT = KT, kTT = kBatch / KT, kThreads = kTT * KS, kNW = kThreads / 32, kRPT = kNearRuns / kThreads;
     static_assert(kT % 2 == 0 && kTT % 32 == 0 && kNearRuns % kThreads == 0, "near kernel shape");
     static_assert((KS - 1) * 3 * kBatch * sizeof(double) <= sizeof(float4) * KTILE, "group sums fit one tile");
     __shared__ __align__(16) float4 tile[2][KTILE];  // double-buffered: tile p + 1 arrives while p is summed
     __shared__ int r_start[kNearRuns], r_pre[kNearRuns + 1];
     __shared__ int warp_tot[kNW];
-    __shared__ int slot;
     const Octree& t = A.t;
     const double4* __restrict__ tgt_sorted = A.tgt_sorted;
     const int32_t* __restrict__ batch_first = A.batch_first;
@@ -1796,8 +1800,6 @@ __global__ void __launch_bounds__(kBatch / KT * KS) near_kernel(NearArgs A) {
     const int2* __restrict__ near_list = A.near_list;
     const float4* __restrict__ src32 = A.src32;
     const int64_t near_cap = A.near_cap;
-    const int nbat = *A.nbat;
-    for (int64_t b = next_batch(A.ticket, A.order, nbat, &slot); b >= 0; b = next_batch(A.ticket, A.order, nbat, &slot)) {
     const int64_t qe = batch_first[b + 1];
     // within each group, warp w holds targets 32 kT w .. 32 kT (w + 1) - 1 of the batch (lane l: 32 kT w + l +
     // 32 u), so a warp past the batch's last target skips the arithmetic as a whole
@@ -1901,7 +1903,7 @@ __global__ void __launch_bounds__(kBatch / KT * KS) near_kernel(NearArgs A) {
 #pragma unroll
                 for (int c = 0; c < 3; ++c) red[(((part - 1) * kT + u) * 3 + c) * kTT + tid] = D[u][c];
         __syncthreads();
-        if (part > 0) continue;  // block-uniform barriers follow only in next_batch
+        if (part > 0) return;  // block-uniform barriers follow only in next_batch
 #pragma unroll
         for (int g = 1; g < KS; ++g)
 #pragma unroll
@@ -1917,7 +1919,16 @@ __global__ void __launch_bounds__(kBatch / KT * KS) near_kernel(NearArgs A) {
         else if (q < qe)
             finish_target(q, qe, A.n_tgt, tgt_sorted[q], D[u], A.tperm, A.V, A.mult, A.U);  // FP64 x re-read
     }
-    }
+}
+
+// Persistent: every block takes batches from the ticket in `order` until none is left; one batch at a time
+// through near_batch.
+template <bool kScalar, int KT, int KTILE, int KS>
+__global__ void __launch_bounds__(kBatch / KT * KS) near_kernel(NearArgs A) {
+    __shared__ int slot;
+    const int nbat = *A.nbat;
+    for (int64_t b = next_batch(A.ticket, A.order, nbat, &slot); b >= 0; b = next_batch(A.ticket, A.order, nbat, &slot))
+        near_batch<kScalar, KT, KTILE, KS>(A, b);
 }
 
 typedef void (*NearFn)(NearArgs);
@@ -1942,6 +1953,179 @@ NearFn near_select(bool scalar, int targets, int tile, int split, int* threads) 
     LPM_NEAR_CASE(4, 512, 2)
     LPM_NEAR_CASE(4, 1024, 2)
 #undef LPM_NEAR_CASE
+    return nullptr;
+}
+
+// ---------------------------------------------------------------------------------- fused solvers
+// The far and near fields of many solvers' evaluations (an ensemble's instances at one RK4 stage) in one
+// persistent launch per far order and per near tile shape.  The work items are the (solver, batch) pairs of
+// every solver, bucketed by decreasing work over all of them, so that a launch ends on the smallest batches of
+// any solver; a block copies its item's solver arguments to shared memory and runs the per-batch body of the
+// solver's own launch, so every batch is summed exactly as there (bitwise the same results).
+struct FusedSched {
+    const int2* items;     // (solver, batch) by decreasing work over all solvers
+    const int32_t* total;  // number of items
+    int32_t* ticket;       // zeroed before the launch
+};
+struct FusedInst {
+    const uint32_t* far_work;
+    const uint32_t* near_work;
+    const int32_t* nbat;  // the solver's batch count; null: the solver takes no part
+};
+constexpr int kFusedFarSlots = kPMax + 2;  // slot P: order P; slot kPMax + 1: part 2 of kFarSplitOrder
+constexpr int kFusedNearGroups = 12;       // near tile shapes
+// fused schedule scratch (int32): far buckets and cursors, near buckets and cursors, the two item counts, one
+// ticket per far slot and one per near group
+constexpr int kFzFarHist = 0, kFzFarCur = 64, kFzNearHist = 128, kFzNearCur = 192, kFzTotals = 256,
+              kFzFarTicket = 258, kFzNearTicket = kFzFarTicket + kFusedFarSlots,
+              kFzInts = kFzNearTicket + kFusedNearGroups;
+
+// grid (x, solvers); the buckets are zeroed by the caller.
+__global__ void fused_hist_kernel(const FusedInst* __restrict__ inst, int32_t* __restrict__ aux) {
+    const FusedInst I = inst[blockIdx.y];
+    const int n = I.nbat ? *I.nbat : 0;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) {
+        atomicAdd(&aux[kFzFarHist + sched_bucket(I.far_work[b])], 1);
+        atomicAdd(&aux[kFzNearHist + sched_bucket(I.near_work[b])], 1);
+    }
+}
+
+__global__ void fused_scatter_kernel(const FusedInst* __restrict__ inst, int32_t* __restrict__ aux,
+                                     int2* __restrict__ far_items, int2* __restrict__ near_items) {
+    __shared__ int fbase[kSchedBuckets], nbase[kSchedBuckets];
+    if (threadIdx.x == 0) {
+        int fa = 0, na = 0;
+        for (int k = 0; k < kSchedBuckets; ++k) {
+            fbase[k] = fa;
+            fa += aux[kFzFarHist + k];
+            nbase[k] = na;
+            na += aux[kFzNearHist + k];
+        }
+        if (blockIdx.x == 0 && blockIdx.y == 0) {
+            aux[kFzTotals] = fa;
+            aux[kFzTotals + 1] = na;
+        }
+    }
+    __syncthreads();
+    const FusedInst I = inst[blockIdx.y];
+    const int n = I.nbat ? *I.nbat : 0;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) {
+        const int kf = sched_bucket(I.far_work[b]), kn = sched_bucket(I.near_work[b]);
+        far_items[fbase[kf] + atomicAdd(&aux[kFzFarCur + kf], 1)] = make_int2((int)blockIdx.y, b);
+        near_items[nbase[kn] + atomicAdd(&aux[kFzNearCur + kn], 1)] = make_int2((int)blockIdx.y, b);
+    }
+}
+
+// Whether a fused launch computes item (solver, b): the solver takes part in it and, for a far order, has
+// clusters of that order in batch b (a near item always writes its targets' result).
+__device__ __forceinline__ bool fused_has_work(const FarArgs& a, int b) {
+    return a.far_cnt != nullptr && a.far_cnt[b] > 0;
+}
+__device__ __forceinline__ bool fused_has_work(const NearArgs& a, int) { return a.near_cnt != nullptr; }
+
+// The block's next item of a fused launch, with its solver's arguments copied to araw; false when none is left.
+template <typename Args>
+__device__ __forceinline__ bool next_fused_item(const FusedSched& S, int n, const Args* __restrict__ tab,
+                                                uint32_t* araw, int2* item) {
+    __syncthreads();  // every thread is done with the previous item's shared memory
+    if (threadIdx.x == 0) {
+        int2 v = make_int2(-1, -1);
+        for (int k = atomicAdd(S.ticket, 1); k < n; k = atomicAdd(S.ticket, 1)) {
+            const int2 c = S.items[k];
+            if (fused_has_work(tab[c.x], c.y)) {
+                v = c;
+                break;
+            }
+        }
+        *item = v;
+    }
+    __syncthreads();
+    const int2 v = *item;
+    if (v.x < 0) return false;
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(tab + v.x);
+    for (int w = threadIdx.x; w < (int)(sizeof(Args) / 4); w += blockDim.x) araw[w] = src[w];
+    __syncthreads();
+    return true;
+}
+
+// far_order2_kernel over the items of many solvers: tab[s] holds solver s's arguments for this order (part).
+template <int P, int PART = 0>
+__global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_fused2_kernel(const FarArgs* __restrict__ tab,
+                                                                                  FusedSched S) {
+    static_assert(sizeof(FarArgs) % 4 == 0, "argument copy by words");
+    extern __shared__ float4 fbuf[];
+    __shared__ __align__(16) uint32_t araw[sizeof(FarArgs) / 4];
+    __shared__ int2 item;
+    const FarArgs& A = *reinterpret_cast<const FarArgs*>(araw);
+    const int n = *S.total;
+    while (next_fused_item(S, n, tab, araw, &item)) far2_batch<P, PART>(A, item.y, fbuf);
+}
+
+// near_kernel (Biot-Savart) over the items of many solvers sharing one tile shape.
+template <int KT, int KTILE, int KS>
+__global__ void __launch_bounds__(kBatch / KT * KS) near_fused_kernel(const NearArgs* __restrict__ tab, FusedSched S) {
+    static_assert(sizeof(NearArgs) % 4 == 0, "argument copy by words");
+    __shared__ __align__(16) uint32_t araw[sizeof(NearArgs) / 4];
+    __shared__ int2 item;
+    const NearArgs& A = *reinterpret_cast<const NearArgs*>(araw);
+    const int n = *S.total;
+    while (next_fused_item(S, n, tab, araw, &item)) near_batch<false, KT, KTILE, KS>(A, item.y);
+}
+
+typedef void (*FarFusedFn)(const FarArgs*, FusedSched);
+typedef void (*NearFusedFn)(const NearArgs*, FusedSched);
+
+// The fused far kernel of FP32 order P (1..kFar2MaxOrder; part 1 or 2 at kFarSplitOrder, else 0).
+template <int P>
+FarFusedFn far_fused_for(int part, size_t* smem) {
+    if constexpr (P == kFarSplitOrder) {
+        if (part == 2) {
+            *smem = FarShape<P, float4, kFar2StageUnits, 2>::kSmem;
+            return far_fused2_kernel<P, 2>;
+        }
+        *smem = FarShape<P, float4, kFar2StageUnits, 1>::kSmem;
+        return far_fused2_kernel<P, 1>;
+    } else {
+        *smem = FarShape<P, float4, kFar2StageUnits>::kSmem;
+        return far_fused2_kernel<P>;
+    }
+}
+FarFusedFn far_fused_select(int P, int part, size_t* smem, int* threads) {
+    static_assert(kFar2MaxOrder == 11 && kFarSplitOrder == 11, "fused far orders 1..11");
+    *threads = kFar2Threads;
+    switch (P) {
+        case 1: return far_fused_for<1>(part, smem);
+        case 2: return far_fused_for<2>(part, smem);
+        case 3: return far_fused_for<3>(part, smem);
+        case 4: return far_fused_for<4>(part, smem);
+        case 5: return far_fused_for<5>(part, smem);
+        case 6: return far_fused_for<6>(part, smem);
+        case 7: return far_fused_for<7>(part, smem);
+        case 8: return far_fused_for<8>(part, smem);
+        case 9: return far_fused_for<9>(part, smem);
+        case 10: return far_fused_for<10>(part, smem);
+        case 11: return far_fused_for<11>(part, smem);
+        default: return nullptr;
+    }
+}
+
+NearFusedFn near_fused_select(int targets, int tile, int split, int* threads) {
+    *threads = kBatch / targets * split;
+#define LPM_NEAR_FUSED_CASE(T, TILE, S) \
+    if (targets == T && tile == TILE && split == S) return near_fused_kernel<T, TILE, S>;
+    LPM_NEAR_FUSED_CASE(2, 256, 1)
+    LPM_NEAR_FUSED_CASE(2, 512, 1)
+    LPM_NEAR_FUSED_CASE(2, 1024, 1)
+    LPM_NEAR_FUSED_CASE(4, 256, 1)
+    LPM_NEAR_FUSED_CASE(4, 512, 1)
+    LPM_NEAR_FUSED_CASE(4, 1024, 1)
+    LPM_NEAR_FUSED_CASE(2, 256, 2)
+    LPM_NEAR_FUSED_CASE(2, 512, 2)
+    LPM_NEAR_FUSED_CASE(2, 1024, 2)
+    LPM_NEAR_FUSED_CASE(4, 256, 2)
+    LPM_NEAR_FUSED_CASE(4, 512, 2)
+    LPM_NEAR_FUSED_CASE(4, 1024, 2)
+#undef LPM_NEAR_FUSED_CASE
     return nullptr;
 }
 
@@ -2475,8 +2659,21 @@ static int build_lists(TreeSolver* t, bool can_sync) {
     return LPM_OK;
 }
 
-int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double4* X, int64_t n_tgt, double* U) {
+// The far-field orders of an evaluation: the fixed order, or the selector's orders 1..11.
+static void far_order_range(const TreeSolver* t, int* p_lo, int* p_hi) {
+    const bool sel = t->learned && t->mlp_loaded;
+    *p_lo = sel ? 1 : t->order;
+    *p_hi = sel ? std::min(t->pm, kMlpDirectClass) : t->order;
+}
+
+// Everything of an evaluation before its far and near fields: root box, target batches, source octree, moments,
+// coefficients, interaction lists, V cleared and, with `sched`, the batch schedules of the solver's own
+// persistent far and near launches.  *pending is false when the evaluation is complete already (no targets or
+// no sources).
+static int tree_prepare(TreeSolver* t, const double4* src, int64_t n_src, const double4* X, int64_t n_tgt,
+                        double* U, bool sched, bool* pending) {
     lpm_ctx* ctx = t->ctx;
+    *pending = false;
     if (n_src != t->n_src || n_tgt != t->n_tgt) {
         set_error("tree_velocity: sizes differ from the solver's");
         return LPM_ERR_ARG;
@@ -2600,6 +2797,8 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     // far field: one launch per order present (only the fixed order, or the selector's orders 1..11),
     // each adding its bucket's contributions to V
     LPM_CUDA_TRY(cudaMemsetAsync(t->V, 0, 3 * (size_t)n_tgt * sizeof(double), ctx->stream));
+    *pending = true;
+    if (!sched) return LPM_OK;
     // batch schedules: far and near work of every batch (from the traversal's count pass), bucketed in
     // decreasing order; zeroed buckets, cursors and tickets first
     LPM_CUDA_TRY(cudaMemsetAsync(t->sched_aux, 0, kAuxInts * sizeof(int32_t), ctx->stream));
@@ -2613,6 +2812,93 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
                t->sched_aux + kAuxNearHist);
     LPM_LAUNCH(ctx, "sched_scatter_kernel", sched_scatter_kernel, gsch, 256, 0, t->near_work, t->tcount + 1,
                t->sched_aux + kAuxNearHist, t->sched_aux + kAuxNearCur, t->sched_order);
+    return LPM_OK;
+}
+
+// The far kernels' arguments for order P of t's current evaluation (schedule: t's own).
+static FarArgs far_args(const TreeSolver* t, int P) {
+    const int64_t nb1 = t->n_batches + 1;
+    FarArgs F{};
+    F.tgt_sorted = t->tgt_sorted;
+    F.n_tgt = t->n_tgt;
+    F.batch_first = t->batch_first;
+    F.nbat = t->tcount + 1;
+    F.far_off = t->far_off + (size_t)P * nb1;
+    F.far_cnt = t->far_cnt + (size_t)P * nb1;
+    F.far_list = t->far_list;
+    F.far_cap = t->far_cap;
+    F.node_ctr = t->node_ctr;
+    F.B64 = t->B64;
+    F.B32 = t->B32;
+    F.n_ent = t->n_ent;
+    F.gtab = t->gtab + t->ct.table_off[P];
+    F.V = t->V;
+    F.order = t->far_order;
+    F.ticket = t->sched_aux + kAuxFarTicket + P;
+    return F;
+}
+
+// The near kernel's arguments for t's current evaluation, writing the result to U (schedule: t's own).
+static NearArgs near_args(const TreeSolver* t, double* U) {
+    NearArgs N{};
+    N.t = t->st;
+    N.tgt_sorted = t->tgt_sorted;
+    N.n_tgt = t->n_tgt;
+    N.batch_first = t->batch_first;
+    N.nbat = t->tcount + 1;
+    N.near_off = t->near_off;
+    N.near_cnt = t->near_cnt;
+    N.near_list = t->near_list;
+    N.near_cap = t->near_cap;
+    N.src32 = t->src32;
+    N.W = t->W;
+    N.tperm = t->tperm;
+    N.V = t->V;
+    N.mult = -1.0 / (4.0 * kPi * t->kernel.radius);
+    N.U = U;
+    N.order = t->sched_order;
+    N.ticket = t->sched_aux + kAuxNearTicket;
+    return N;
+}
+
+// Order P's far-field launch(es) of t on its context's stream, on the schedule tree_prepare made.
+static int tree_far_order(TreeSolver* t, int P) {
+    lpm_ctx* ctx = t->ctx;
+    FarArgs F = far_args(t, P);
+    size_t smem = 0;
+    const bool f64 = P >= t->f64_from;
+    const unsigned grid = (unsigned)t->far_blocks[P][f64 ? 1 : 0];
+    if (t->scalar) {
+        F.B64 = (const double4*)t->A64;
+        F.B32 = (const float4*)t->A32;
+        int threads = 0;
+        FarScalarFn fs = far_scalar_select(P, f64, &smem, &threads);
+        LPM_LAUNCH(ctx, "far_kernel", fs, grid, threads, smem, F, t->a_stride);
+    } else if (P == kFarSplitOrder && !f64) {  // two launches, each on its own ticket
+        for (int part = 1; part <= 2; ++part) {
+            int threads = 0;
+            FarKernelFn fn = far_split_select(part, &smem, &threads);
+            F.gtab = t->gtab + t->ct.table_off[P] + (part == 2 ? part_entries(P, 1) : 0);
+            F.ticket = t->sched_aux + kAuxFarTicket + (part == 2 ? kPMax + 1 : P);
+            LPM_LAUNCH(ctx, "far_kernel", fn, (unsigned)t->far_split_blocks[part - 1], threads, smem, F);
+        }
+    } else {
+        int threads = 0;
+        FarKernelFn fn = far_kernel_select(P, f64, &smem, &threads);
+        LPM_LAUNCH(ctx, "far_kernel", fn, grid, threads, smem, F);
+    }
+    return LPM_OK;
+}
+
+int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double4* X, int64_t n_tgt, double* U) {
+    lpm_ctx* ctx = t->ctx;
+    bool pending = false;
+    int rc = tree_prepare(t, src, n_src, X, n_tgt, U, true, &pending);
+    if (rc || !pending) return rc;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    LPM_CUDA_TRY(cudaStreamIsCapturing(ctx->stream, &cap));
+    const bool can_sync = cap == cudaStreamCaptureStatusNone;
+    const unsigned gt = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(n_tgt + 1, 256), 8 * ctx->num_sms));
     // near field: batches by decreasing near work, taken by a persistent grid.  Biot-Savart: after the far
     // field on the context's stream, writing u = mult (V - x cross D).  Scalar kernel: it writes W only and runs
     // on the solver's side stream beside the far-field launch, filling its tail (1M Poisson points: 7.37 ->
@@ -2620,24 +2906,7 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     // u; with per-kernel profiling on it runs after the far field on the context's stream, so that every kernel
     // is timed alone.
     auto launch_near = [&]() -> int {
-        NearArgs N{};
-        N.t = t->st;
-        N.tgt_sorted = t->tgt_sorted;
-        N.n_tgt = n_tgt;
-        N.batch_first = t->batch_first;
-        N.nbat = t->tcount + 1;
-        N.near_off = t->near_off;
-        N.near_cnt = t->near_cnt;
-        N.near_list = t->near_list;
-        N.near_cap = t->near_cap;
-        N.src32 = t->src32;
-        N.W = t->W;
-        N.tperm = t->tperm;
-        N.V = t->V;
-        N.mult = -1.0 / (4.0 * kPi * t->kernel.radius);
-        N.U = U;
-        N.order = t->sched_order;
-        N.ticket = t->sched_aux + kAuxNearTicket;
+        const NearArgs N = near_args(t, U);
         int threads = 0;
         NearFn fn = near_select(t->scalar, t->near_targets, t->near_tile, t->near_split, &threads);
         LPM_LAUNCH(ctx, "near_kernel", fn, (unsigned)t->near_blocks, threads, 0, N);
@@ -2645,51 +2914,11 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     };
     const bool overlap = t->scalar && !ctx->profiling;
     if (overlap) LPM_CUDA_TRY(cudaEventRecord(t->ev_fork, ctx->stream));
-    {
-        const int64_t nb1 = t->n_batches + 1;
-        const bool sel = t->learned && t->mlp_loaded;
-        const int p_lo = sel ? 1 : t->order, p_hi = sel ? std::min(t->pm, kMlpDirectClass) : t->order;
-        for (int P = p_lo; P <= p_hi; ++P) {
-            FarArgs F{};
-            F.tgt_sorted = t->tgt_sorted;
-            F.n_tgt = n_tgt;
-            F.batch_first = t->batch_first;
-            F.nbat = t->tcount + 1;
-            F.far_off = t->far_off + (size_t)P * nb1;
-            F.far_cnt = t->far_cnt + (size_t)P * nb1;
-            F.far_list = t->far_list;
-            F.far_cap = t->far_cap;
-            F.node_ctr = t->node_ctr;
-            F.B64 = t->B64;
-            F.B32 = t->B32;
-            F.n_ent = t->n_ent;
-            F.gtab = t->gtab + t->ct.table_off[P];
-            F.V = t->V;
-            F.order = t->far_order;
-            F.ticket = t->sched_aux + kAuxFarTicket + P;
-            size_t smem = 0;
-            const bool f64 = P >= t->f64_from;
-            const unsigned grid = (unsigned)t->far_blocks[P][f64 ? 1 : 0];
-            if (t->scalar) {
-                F.B64 = (const double4*)t->A64;
-                F.B32 = (const float4*)t->A32;
-                int threads = 0;
-                FarScalarFn fs = far_scalar_select(P, f64, &smem, &threads);
-                LPM_LAUNCH(ctx, "far_kernel", fs, grid, threads, smem, F, t->a_stride);
-            } else if (P == kFarSplitOrder && !f64) {  // two launches, each on its own ticket
-                for (int part = 1; part <= 2; ++part) {
-                    int threads = 0;
-                    FarKernelFn fn = far_split_select(part, &smem, &threads);
-                    F.gtab = t->gtab + t->ct.table_off[P] + (part == 2 ? part_entries(P, 1) : 0);
-                    F.ticket = t->sched_aux + kAuxFarTicket + (part == 2 ? kPMax + 1 : P);
-                    LPM_LAUNCH(ctx, "far_kernel", fn, (unsigned)t->far_split_blocks[part - 1], threads, smem, F);
-                }
-            } else {
-                int threads = 0;
-                FarKernelFn fn = far_kernel_select(P, f64, &smem, &threads);
-                LPM_LAUNCH(ctx, "far_kernel", fn, grid, threads, smem, F);
-            }
-        }
+    int p_lo = 0, p_hi = -1;
+    far_order_range(t, &p_lo, &p_hi);
+    for (int P = p_lo; P <= p_hi; ++P) {
+        rc = tree_far_order(t, P);
+        if (rc) return rc;
     }
     if (overlap) {  // enqueued after the far launches: the near blocks fill the SMs as far blocks retire
         LPM_CUDA_TRY(cudaStreamWaitEvent(t->side, t->ev_fork, 0));
@@ -2708,6 +2937,218 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
         LPM_LAUNCH(ctx, "combine_kernel", far_near_combine_kernel, gt, 256, 0, t->V, t->W, t->tperm, n_tgt,
                    1.0 / (4.0 * kPi), U);
     if (can_sync) return tree_check(t);
+    return LPM_OK;
+}
+
+// ---------------------------------------------------------------------------------- fused solvers (host)
+struct TreeFused {
+    lpm_ctx* ctx = nullptr;  // its stream carries the fused launches
+    int n = 0;               // solvers bound
+    int inst_cap = 0;
+    int64_t item_cap = 0;
+    std::vector<TreeSolver*> ts;
+    FusedInst* inst = nullptr;   // device, n
+    FarArgs* far_tab = nullptr;  // device, kFusedFarSlots x n (slot-major)
+    NearArgs* near_tab = nullptr;  // device, kFusedNearGroups x n (group-major)
+    int2* far_items = nullptr;
+    int2* near_items = nullptr;
+    int32_t* aux = nullptr;
+    bool far_on[kFusedFarSlots] = {};
+    std::vector<int4> groups;                 // near tile shapes present: (targets, tile, split, -)
+    std::vector<std::pair<int, int>> single;  // (solver, order) far launches outside the fused kernels
+    int64_t max_batches = 0;
+};
+
+// Whether every far order of t runs in the fused FP32 kernels (else t also keeps its own schedule for the
+// orders that do not).
+static bool fused_far_all(const TreeSolver* t) {
+    int p_lo = 0, p_hi = -1;
+    far_order_range(t, &p_lo, &p_hi);
+    return !t->scalar && p_hi <= kFar2MaxOrder && p_hi < t->f64_from;
+}
+
+// Whether t takes part in fused launches: a Biot-Savart evaluation with sources and targets.
+static bool fused_part(const TreeSolver* t) { return t && !t->scalar && t->n_src > 0 && t->n_tgt > 0; }
+
+int tree_fused_create(lpm_ctx* ctx, TreeFused** out) {
+    *out = nullptr;
+    TreeFused* f = new (std::nothrow) TreeFused();
+    if (!f) return LPM_ERR_OOM;
+    f->ctx = ctx;
+    *out = f;
+    return LPM_OK;
+}
+
+static void fused_free(TreeFused* f) {
+    cudaFree(f->inst);
+    cudaFree(f->far_tab);
+    cudaFree(f->near_tab);
+    cudaFree(f->far_items);
+    cudaFree(f->near_items);
+    cudaFree(f->aux);
+    f->inst = nullptr;
+    f->far_tab = nullptr;
+    f->near_tab = nullptr;
+    f->far_items = f->near_items = nullptr;
+    f->aux = nullptr;
+    f->inst_cap = 0;
+    f->item_cap = 0;
+}
+
+void tree_fused_destroy(TreeFused* f) {
+    if (!f) return;
+    fused_free(f);
+    delete f;
+}
+
+int tree_fused_prepare(TreeSolver* t, const double4* src, const double4* X, double* U) {
+    bool pending = false;
+    return tree_prepare(t, src, t->n_src, X, t->n_tgt, U, !fused_far_all(t), &pending);
+}
+
+int tree_fused_bind(TreeFused* f, TreeSolver* const* ts, double* const* Us, int n) {
+    if (n < 1 || n > 65535) {
+        set_error("fused solvers: 1 to 65535 solvers");
+        return LPM_ERR_ARG;
+    }
+    int64_t items = 0, max_nb = 0;
+    for (int i = 0; i < n; ++i)
+        if (fused_part(ts[i])) {
+            items += ts[i]->n_batches;
+            max_nb = std::max(max_nb, ts[i]->n_batches);
+        }
+    LPM_CUDA_TRY(cudaSetDevice(f->ctx->device));
+    if (n > f->inst_cap || items > f->item_cap) {
+        fused_free(f);
+        const int cap = std::max(n, 1);
+        const int64_t icap = std::max<int64_t>(items, 1);
+        cudaError_t e = cudaMalloc(&f->inst, sizeof(FusedInst) * (size_t)cap);
+        if (e == cudaSuccess) e = cudaMalloc(&f->far_tab, sizeof(FarArgs) * kFusedFarSlots * (size_t)cap);
+        if (e == cudaSuccess) e = cudaMalloc(&f->near_tab, sizeof(NearArgs) * kFusedNearGroups * (size_t)cap);
+        if (e == cudaSuccess) e = cudaMalloc(&f->far_items, sizeof(int2) * (size_t)icap);
+        if (e == cudaSuccess) e = cudaMalloc(&f->near_items, sizeof(int2) * (size_t)icap);
+        if (e == cudaSuccess) e = cudaMalloc(&f->aux, sizeof(int32_t) * kFzInts);
+        if (e != cudaSuccess) {
+            fused_free(f);
+            return cuda_status(e, "cudaMalloc (fused solvers)");
+        }
+        f->inst_cap = cap;
+        f->item_cap = icap;
+    }
+    std::vector<FusedInst> hinst((size_t)n, FusedInst{nullptr, nullptr, nullptr});
+    std::vector<FarArgs> hfar((size_t)kFusedFarSlots * n, FarArgs{});
+    std::vector<NearArgs> hnear((size_t)kFusedNearGroups * n, NearArgs{});
+    f->ts.assign(ts, ts + n);
+    f->n = n;
+    f->groups.clear();
+    f->single.clear();
+    for (bool& on : f->far_on) on = false;
+    for (int i = 0; i < n; ++i) {
+        TreeSolver* t = ts[i];
+        if (!fused_part(t)) continue;
+        hinst[i] = FusedInst{t->far_work, t->near_work, t->tcount + 1};
+        int p_lo = 0, p_hi = -1;
+        far_order_range(t, &p_lo, &p_hi);
+        for (int P = p_lo; P <= p_hi; ++P) {
+            if (P > kFar2MaxOrder || P >= t->f64_from) {
+                f->single.emplace_back(i, P);
+                continue;
+            }
+            hfar[(size_t)P * n + i] = far_args(t, P);
+            f->far_on[P] = true;
+            if (P == kFarSplitOrder) {
+                FarArgs F2 = far_args(t, P);
+                F2.gtab += part_entries(P, 1);
+                hfar[(size_t)(kPMax + 1) * n + i] = F2;
+                f->far_on[kPMax + 1] = true;
+            }
+        }
+        int g = 0;
+        while (g < (int)f->groups.size() && !(f->groups[g].x == t->near_targets && f->groups[g].y == t->near_tile &&
+                                                f->groups[g].z == t->near_split))
+            ++g;
+        if (g == (int)f->groups.size()) {
+            if (g == kFusedNearGroups) {
+                set_error("fused solvers: too many near tile shapes");
+                return LPM_ERR_ARG;
+            }
+            f->groups.push_back(make_int4(t->near_targets, t->near_tile, t->near_split, 0));
+        }
+        hnear[(size_t)g * n + i] = near_args(t, Us[i]);
+    }
+    f->max_batches = max_nb;
+    cudaStream_t s = f->ctx->stream;
+    LPM_CUDA_TRY(cudaMemcpyAsync(f->inst, hinst.data(), sizeof(FusedInst) * hinst.size(), cudaMemcpyHostToDevice, s));
+    LPM_CUDA_TRY(cudaMemcpyAsync(f->far_tab, hfar.data(), sizeof(FarArgs) * hfar.size(), cudaMemcpyHostToDevice, s));
+    LPM_CUDA_TRY(cudaMemcpyAsync(f->near_tab, hnear.data(), sizeof(NearArgs) * hnear.size(), cudaMemcpyHostToDevice,
+                                 s));
+    LPM_CUDA_TRY(cudaStreamSynchronize(s));  // the host tables go out of scope
+    return LPM_OK;
+}
+
+// Persistent grid of a fused kernel: its resident blocks on the whole device.
+template <typename Fn>
+static int fused_grid(lpm_ctx* ctx, Fn fn, int threads, size_t smem, unsigned* grid) {
+    int per_sm = 0;
+    LPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+    *grid = (unsigned)(std::max(per_sm, 1) * ctx->num_sms);
+    return LPM_OK;
+}
+
+int tree_fused_run(TreeFused* f) {
+    lpm_ctx* ctx = f->ctx;
+    const int n = f->n;
+    if (n < 1) {
+        set_error("fused solvers: nothing bound");
+        return LPM_ERR_ARG;
+    }
+    LPM_CUDA_TRY(cudaMemsetAsync(f->aux, 0, kFzInts * sizeof(int32_t), ctx->stream));
+    const dim3 gsch((unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(f->max_batches, 256), 64)),
+                    (unsigned)n);
+    LPM_LAUNCH(ctx, "fused_hist_kernel", fused_hist_kernel, gsch, 256, 0, f->inst, f->aux);
+    LPM_LAUNCH(ctx, "fused_scatter_kernel", fused_scatter_kernel, gsch, 256, 0, f->inst, f->aux, f->far_items,
+               f->near_items);
+    for (int P = 1; P <= kPMax; ++P) {
+        for (int part = 1; part <= 2; ++part) {  // part 2: the second launch of kFarSplitOrder
+            const int slot = part == 1 ? P : kPMax + 1;
+            if (part == 2 && P != kFarSplitOrder) break;
+            if (!f->far_on[slot]) continue;
+            size_t smem = 0;
+            int threads = 0;
+            FarFusedFn fn = far_fused_select(P, P == kFarSplitOrder ? part : 0, &smem, &threads);
+            if (!fn) {
+                set_error("fused solvers: no fused far kernel of order %d", P);
+                return LPM_ERR_ARG;
+            }
+            unsigned grid = 0;
+            int rc = fused_grid(ctx, fn, threads, smem, &grid);
+            if (rc) return rc;
+            const FusedSched S{f->far_items, f->aux + kFzTotals, f->aux + kFzFarTicket + slot};
+            LPM_LAUNCH(ctx, "far_kernel", fn, grid, threads, smem, f->far_tab + (size_t)slot * n, S);
+        }
+        for (const auto& sp : f->single) {  // orders outside the fused kernels: the solver's own launch
+            if (sp.second != P) continue;
+            TreeSolver* t = f->ts[sp.first];
+            cudaStream_t own = t->ctx->stream;
+            t->ctx->stream = ctx->stream;
+            const int rc = tree_far_order(t, P);
+            t->ctx->stream = own;
+            if (rc) return rc;
+        }
+    }
+    for (size_t g = 0; g < f->groups.size(); ++g) {
+        int threads = 0;
+        NearFusedFn fn = near_fused_select(f->groups[g].x, f->groups[g].y, f->groups[g].z, &threads);
+        if (!fn) {
+            set_error("fused solvers: no fused near kernel of this tile shape");
+            return LPM_ERR_ARG;
+        }
+        unsigned grid = 0;
+        int rc = fused_grid(ctx, fn, threads, 0, &grid);
+        if (rc) return rc;
+        const FusedSched S{f->near_items, f->aux + kFzTotals + 1, f->aux + kFzNearTicket + (int)g};
+        LPM_LAUNCH(ctx, "near_kernel", fn, grid, threads, 0, f->near_tab + g * (size_t)n, S);
+    }
     return LPM_OK;
 }
 

@@ -24,6 +24,20 @@ void tree_solver_destroy(TreeSolver* t);
 // targets tgt[0:n_tgt] from sources src[0:n_src] (x, y, z, w).  Targets may coincide with sources (their
 // self pair contributes nothing).
 int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double4* tgt, int64_t n_tgt, double* U);
+// Fused evaluations of many solvers (an ensemble's instances at one RK4 stage): each solver runs
+// tree_fused_prepare on its own context's stream (everything before the far and near fields), then, once that
+// work is joined into the fused context's stream, tree_fused_run enqueues there the far field of every bound
+// solver as one persistent launch per Taylor order and the near field as one per near tile shape (Biot-Savart
+// solvers; orders in FP64 or above the FP32 kernels' range keep the solver's own launch), bitwise the results
+// of tree_velocity.  tree_fused_bind records the solvers' current buffers and parameters (it synchronises the
+// fused context's stream): bind again after any reallocation (tree_generation) or parameter change, and never
+// while a fused launch may be running.
+struct TreeFused;
+int tree_fused_create(lpm_ctx* ctx, TreeFused** out);
+void tree_fused_destroy(TreeFused* f);
+int tree_fused_prepare(TreeSolver* t, const double4* src, const double4* tgt, double* U);
+int tree_fused_bind(TreeFused* f, TreeSolver* const* ts, double* const* Us, int n);
+int tree_fused_run(TreeFused* f);
 // Synchronises and reports capacity overflows of the last evaluation (LPM_ERR_CAPACITY).
 int tree_check(TreeSolver* t);
 // nodes, leaves, depth, far (batch, cluster) pairs, near runs, batches, overflow flags,

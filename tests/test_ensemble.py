@@ -116,3 +116,49 @@ def test_ensemble_set_param_between_graph_steps_takes_effect(ctx):
         want = rk.get_state()
         rk.close()
         assert np.array_equal(got[i], want), i
+
+
+@pytest.mark.gpu
+def test_fused_ensemble_equals_lane_mode(ctx):
+    """The fused step (far field of all instances as one persistent launch per Taylor order, near field as one
+    per near tile shape) gives bitwise the states of the lane mode, where every instance launches its own far
+    and near kernels, on a mixed ensemble: learned-order instances (one with FP64 orders >= 6, whose orders 6..11
+    keep their own launches; one with another near tile shape), fixed orders 8 and 12 (order 12 is above the
+    fused FP32 kernels) and an FP32 direct-sum instance."""
+    inst = W.ensemble_instances(levels=(3, 4, 5), per_level=2, seed=11)
+    learned = L.tree_solver(L.LPM_PREC_F32, 10, 128, 0.5, learned=True, tolerance=5e-7)
+    solvers = [learned, L.tree_solver(L.LPM_PREC_F32, 8, 64, 0.6), learned, L.direct_solver(L.LPM_PREC_F32),
+               learned, L.tree_solver(L.LPM_PREC_F32, 12, 128, 0.5)]
+    params = L.learned.load()[0]
+
+    def run(fused: bool, use_graph: bool, nsteps: int):
+        ens = L.Ensemble(ctx, L.biot_savart_kernel(), solvers, [n for _, _, n in inst],
+                         [p.shape[0] for _, p, _ in inst], lanes=3)
+        assert ens.get_param("fused") == 1.0  # the default
+        ens.set_param("fused", 1 if fused else 0)
+        assert ens.get_param("fused") == (1.0 if fused else 0.0)
+        for i in (0, 2, 4):
+            ens.instance(i).set_mlp(params)
+        ens.instance(2).set_param("f64_from", 6)
+        ens.instance(4).set_param("near_targets", 4)
+        ens.instance(4).set_param("near_tile", 512)
+        ens.instance(4).set_param("near_split", 1)
+        for i, (_, p, _) in enumerate(inst):
+            ens.instance(i).set_state(p)
+        ens.step(0.01, nsteps, use_graph=use_graph)
+        out = [ens.instance(i).get_state() for i in range(len(inst))]
+        ens.close()
+        return out
+
+    lanes = run(False, True, 3)
+    for use_graph, nsteps in ((True, 3), (False, 2)):
+        fused = run(True, use_graph, nsteps)
+        ref = lanes if nsteps == 3 else run(False, False, 2)
+        for i in range(len(inst)):
+            assert np.array_equal(fused[i], ref[i]), (use_graph, i)
+    with pytest.raises(L.LpmError):
+        e = L.Ensemble(ctx, L.biot_savart_kernel(), learned, [inst[0][2]], [inst[0][1].shape[0]], lanes=1)
+        try:
+            e.set_param("fused", 2)
+        finally:
+            e.close()
