@@ -619,23 +619,31 @@ def run_gpu_ensemble(args) -> None:
     launches = ctx.launch_count - launches0
     value = world * args.steps / (sum(ms) * 1e-3)
     err_final = ensemble_accuracy(ctx, kern, ens, inst)
-    # the same ensemble in lane mode (each instance's far and near launches on its lane) for comparison: a few
-    # steps after its own warm-up step and capture
+    # the same ensemble with the fused launches in one group, and in lane mode (each instance's far and near
+    # launches on its lane), for comparison: a few steps after their own warm-up step and capture
     states = [ens.instance(i).get_state() for i in range(len(inst))]
-    ens.set_param("fused", 0)
-    ens.step(dt, 1, use_graph=True)
-    torch.cuda.synchronize()
-    lane_ms = []
-    for _ in range(min(args.steps, 3)):
-        flush.zero_()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
+    groups = int(ens.get_param("fused_groups"))
+
+    def compare_ms(name, value):
+        ens.set_param(name, value)
         ens.step(dt, 1, use_graph=True)
-        e1.record()
-        e1.synchronize()
-        lane_ms.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        out_ms = []
+        for _ in range(min(args.steps, 3)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ens.step(dt, 1, use_graph=True)
+            e1.record()
+            e1.synchronize()
+            out_ms.append(e0.elapsed_time(e1))
+        return float(np.mean(out_ms))
+
+    one_group_ms = compare_ms("fused_groups", 1)
+    ens.set_param("fused_groups", groups)
+    lane_ms = compare_ms("fused", 0)
     ens.set_param("fused", 1)
     for i, st in enumerate(states):
         ens.instance(i).set_state(st)
@@ -670,16 +678,16 @@ def run_gpu_ensemble(args) -> None:
                    "solver": "learned treecode, per size class the autotuned leaf / theta / budget / batch level "
                              "(order bias 2)", "tuned": {f"L{k}": v for k, v in tuned.items()},
                    "lanes": args.lanes, "dt": dt,
-                   "graph": "one CUDA graph replay per ensemble step; per RK4 stage, the far field of all 64 "
-                            "instances is one persistent launch per Taylor order and their near field one per "
-                            "near tile shape (fused mode)",
+                   "graph": "one CUDA graph replay per ensemble step; per RK4 stage, the far field of each group "
+                            "of instances (the lanes in fused_groups groups stepping independently) is one "
+                            "persistent launch per Taylor order and their near field one per near tile shape",
                    "l2": "flushed (256 MiB write) before every timed step"},
         "rel_l2_vs_fp64_direct": {"sample": f"{ENSEMBLE_SAMPLE} seeded targets per instance, FP64 GPU direct sum",
                                   "t0_max": max(err_t0), "t0_median": float(np.median(err_t0)),
                                   "final_max": max(err_final), "final_median": float(np.median(err_final)),
                                   "final_step": args.warmup + args.steps},
         "particle_steps_per_s": value * n_total,
-        "lane_mode_ms_per_step": float(np.mean(lane_ms)),
+        "fused_groups": groups, "one_group_ms_per_step": one_group_ms, "lane_mode_ms_per_step": lane_ms,
         "roofline": {"bound": "fp32", "kernel": "whole step (near + far field, all instances)",
                      "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                      "traffic": None, "peak_source": "measured FMA microbenchmark (lpm_fma_peak) on this GPU",
@@ -954,6 +962,12 @@ def run_gpu(args) -> None:
                            f"steps (dt {args.dt:g}); FP64 GPU direct sum at each",
         "fp64_direct_steps_per_s": fp64_sps,
         "speedup_vs_fp64_direct": (value / world) / fp64_sps if fp64_sps else None,
+        # absolute rates: the direct sum's (target, source) interactions the step replaces, and the work the
+        # treecode computed (near pairs, far target-cluster evaluations) per second
+        "interactions_per_s": {
+            "direct_equivalent_pairs": value * 4.0 * n_src * n,
+            **({"near_pairs": value * 4.0 * tstats["near_pairs"], "far_evals": value * 4.0 * tstats["far_evals"]}
+               if tstats and "near_pairs" in tstats else {})},
         "roofline": roof,
         "kernel_profile_ms": {k: v for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])[:12]},
         "tree_stats": tstats,

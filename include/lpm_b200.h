@@ -397,9 +397,12 @@ int lpm_ensemble_instance(lpm_ensemble* ens, int i, lpm_rk4** rk);
 int lpm_ensemble_lane_of(const lpm_ensemble* ens, int i, int* lane);
 int lpm_ensemble_set_mlp(lpm_ensemble* ens, const float* params);
 /* lpm_rk4_set_param on every instance; drops the captured step (the next graph step first runs uncaptured).
- * "fused" (0 or 1) is the ensemble's own: the fused far / near launches described above. */
+ * The ensemble's own parameters: "fused" (0 or 1, default 1), the fused far / near launches described above;
+ * "fused_groups" (1 .. 64, default 2): the lanes form this many groups (lane l in group l mod G, at most one
+ * group per lane) that step independently on their own streams, each with its own fused launches, so that one
+ * group's tree builds and traversals overlap another's far and near fields. */
 int lpm_ensemble_set_param(lpm_ensemble* ens, const char* name, double value);
-/* The ensemble's own parameters ("fused"). */
+/* The ensemble's own parameters ("fused", "fused_groups"). */
 int lpm_ensemble_get_param(const lpm_ensemble* ens, const char* name, double* value);
 int lpm_ensemble_step(lpm_ensemble* ens, double dt, int nsteps, int use_graph);
 

@@ -13,7 +13,10 @@
 // persistent launch per Taylor order and the near field as one persistent launch per near tile shape
 // (TreeFused, treecode.cu), whose blocks take (instance, batch) items in decreasing order of work over the
 // whole ensemble; the stage updates fork onto the lanes again.  The results are bitwise those of the lane
-// mode.  Without it, each instance's far and near launches run on its lane.
+// mode.  Without it, each instance's far and near launches run on its lane.  With fused_groups = G > 1 the
+// lanes (and so the instances, balanced by the lane assignment) form G groups that step independently on
+// their own streams, each with its own fused launches: one group's tree builds and traversals (latency-bound
+// chains of small launches) overlap another group's far and near fields.
 #include "lpm_internal.h"
 #include "treecode.h"
 
@@ -55,7 +58,10 @@ struct lpm_ensemble {
     bool warmed = false;
     std::vector<uint64_t> graph_gen;   // per instance: buffer generation at capture
     bool fused = true;                 // far and near fields of all instances in fused launches
-    TreeFused* fz = nullptr;           // their tables (on ctx's own stream)
+    int groups = 2;                    // fused: groups of lanes stepping independently (set_param "fused_groups")
+    std::vector<TreeFused*> fz;        // per group: the fused launches' tables
+    std::vector<cudaStream_t> gstream; // per group g >= 1: its stream (group 0 uses the ensemble's stream)
+    std::vector<cudaEvent_t> gfork, gjoin;  // per group: fork from / join into the ensemble's stream
 };
 
 // Whether any instance reallocated a buffer since the ensemble's graph was captured.
@@ -96,7 +102,11 @@ extern "C" int lpm_ensemble_destroy(lpm_ensemble* e) {
     for (cudaEvent_t ev : e->join) cudaEventDestroy(ev);
     if (e->fork) cudaEventDestroy(e->fork);
     for (lpm_ctx* c : e->lanes) lpm_ctx_destroy(c);
-    tree_fused_destroy(e->fz);
+    for (TreeFused* f : e->fz) tree_fused_destroy(f);
+    for (cudaStream_t st : e->gstream)
+        if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : e->gfork) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : e->gjoin) cudaEventDestroy(ev);
     delete e;
     return LPM_OK;
 }
@@ -223,6 +233,14 @@ extern "C" int lpm_ensemble_set_param(lpm_ensemble* e, const char* name, double 
         e->fused = value != 0.0;
         return LPM_OK;
     }
+    if (std::string(name) == "fused_groups") {
+        if (!(value >= 1.0 && value <= 64.0) || value != std::floor(value)) {
+            set_error("lpm_ensemble_set_param: fused_groups is 1 .. 64");
+            return LPM_ERR_ARG;
+        }
+        e->groups = (int)value;
+        return LPM_OK;
+    }
     for (lpm_rk4* r : e->inst) {
         rc = rk4_set_param_internal(r, name, value);
         if (rc) return rc;
@@ -239,75 +257,131 @@ extern "C" int lpm_ensemble_get_param(const lpm_ensemble* e, const char* name, d
         *value = e->fused ? 1.0 : 0.0;
         return LPM_OK;
     }
+    if (std::string(name) == "fused_groups") {
+        *value = (double)e->groups;
+        return LPM_OK;
+    }
     set_error("lpm_ensemble_get_param: unknown parameter '%s'", name);
     return LPM_ERR_ARG;
 }
 
-// Binds every instance's treecode (current buffers and parameters) to the fused launches; the ensemble's
-// streams are idle.
-static int ens_bind(lpm_ensemble* e) {
-    if (!e->fz) {
-        int rc = tree_fused_create(e->ctx, &e->fz);
-        if (rc) return rc;
+// Fused groups in effect (at most one per lane); the group of instance i is lane_of[i] % groups.
+static int ens_groups(const lpm_ensemble* e) { return std::max(1, std::min(e->groups, (int)e->lanes.size())); }
+
+// Streams, events and tables of every fused group in effect (created outside any capture).
+static int ens_groups_ready(lpm_ensemble* e) {
+    const int G = ens_groups(e);
+    while ((int)e->fz.size() < G) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t a = nullptr, b = nullptr;
+        TreeFused* f = nullptr;
+        cudaError_t err = e->fz.empty() ? cudaSuccess : cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&b, cudaEventDisableTiming);
+        const int rc = err == cudaSuccess ? tree_fused_create(e->ctx, &f) : cuda_status(err, "fused group");
+        if (rc) {
+            if (st) cudaStreamDestroy(st);
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+            return rc;
+        }
+        e->fz.push_back(f);
+        e->gstream.push_back(st);
+        e->gfork.push_back(a);
+        e->gjoin.push_back(b);
     }
-    std::vector<TreeSolver*> ts(e->inst.size());
-    std::vector<double*> us(e->inst.size());
-    for (size_t i = 0; i < e->inst.size(); ++i) {
-        ts[i] = rk4_tree(e->inst[i]);
-        us[i] = rk4_stage_velocity(e->inst[i]);
-    }
-    // the fused launches run on the context's own stream (binding synchronises it)
+    return LPM_OK;
+}
+
+// Binds the treecodes of group g's instances (current buffers and parameters) to the group's fused launches,
+// which run on stream og (binding synchronises it); the group's streams are idle.
+static int ens_bind(lpm_ensemble* e, int g, cudaStream_t og) {
+    const int G = ens_groups(e);
+    std::vector<TreeSolver*> ts;
+    std::vector<double*> us;
+    for (size_t i = 0; i < e->inst.size(); ++i)
+        if (e->lane_of[i] % G == g) {
+            ts.push_back(rk4_tree(e->inst[i]));
+            us.push_back(rk4_stage_velocity(e->inst[i]));
+        }
+    if (ts.empty()) return LPM_OK;
     cudaStream_t user = e->ctx->stream;
-    e->ctx->stream = e->ctx->own_stream;
-    const int rc = tree_fused_bind(e->fz, ts.data(), us.data(), (int)ts.size());
+    e->ctx->stream = og;
+    const int rc = tree_fused_bind(e->fz[g], ts.data(), us.data(), (int)ts.size());
     e->ctx->stream = user;
     return rc;
 }
 
-// One fused step of every instance (four stages: per-instance work on the lanes, the far and near fields of
-// all instances on `origin`).  Uncaptured, the instances are bound again after each stage's lists are built
-// (they may have grown); captured, the caller has bound them.
-static int ens_enqueue_fused(lpm_ensemble* e, double dt, cudaStream_t origin, bool captured) {
-    const size_t L = e->lanes.size();
-    auto fork = [&]() -> cudaError_t {  // the lanes wait for origin's work so far
-        cudaError_t err = cudaEventRecord(e->fork, origin);
-        for (size_t l = 0; l < L && err == cudaSuccess; ++l) err = cudaStreamWaitEvent(e->lanes[l]->stream, e->fork, 0);
+// One fused step of group g's instances (four stages: per-instance work on the group's lanes, the far and near
+// fields of all its instances on og).  Uncaptured, the instances are bound again after each stage's lists are
+// built (they may have grown); captured, the caller has bound them.
+static int ens_group_step(lpm_ensemble* e, int g, double dt, cudaStream_t og, bool captured) {
+    const int G = ens_groups(e);
+    std::vector<size_t> lanes;
+    for (size_t l = 0; l < e->lanes.size(); ++l)
+        if ((int)(l % G) == g) lanes.push_back(l);
+    std::vector<lpm_rk4*> mine;
+    for (size_t i = 0; i < e->inst.size(); ++i)
+        if (e->lane_of[i] % G == g) mine.push_back(e->inst[i]);
+    if (mine.empty()) return LPM_OK;
+    auto fork = [&]() -> cudaError_t {  // the group's lanes wait for og's work so far
+        cudaError_t err = cudaEventRecord(e->gfork[g], og);
+        for (size_t l : lanes)
+            if (err == cudaSuccess) err = cudaStreamWaitEvent(e->lanes[l]->stream, e->gfork[g], 0);
         return err;
     };
-    auto join = [&]() -> cudaError_t {  // origin waits for every lane's work so far
+    auto join = [&]() -> cudaError_t {  // og waits for the group's lanes' work so far
         cudaError_t err = cudaSuccess;
-        for (size_t l = 0; l < L && err == cudaSuccess; ++l) {
-            err = cudaEventRecord(e->join[l], e->lanes[l]->stream);
-            if (err == cudaSuccess) err = cudaStreamWaitEvent(origin, e->join[l], 0);
+        for (size_t l : lanes) {
+            if (err == cudaSuccess) err = cudaEventRecord(e->join[l], e->lanes[l]->stream);
+            if (err == cudaSuccess) err = cudaStreamWaitEvent(og, e->join[l], 0);
         }
         return err;
     };
     for (int stage = 1; stage <= 4; ++stage) {
         LPM_CUDA_TRY(fork());
-        for (lpm_rk4* r : e->inst) {
+        for (lpm_rk4* r : mine) {
             int rc = rk4_stage_begin(r);
             if (rc) return rc;
         }
         LPM_CUDA_TRY(join());
         if (!captured) {
-            LPM_CUDA_TRY(cudaStreamSynchronize(origin));
-            int rc = ens_bind(e);
+            LPM_CUDA_TRY(cudaStreamSynchronize(og));
+            int rc = ens_bind(e, g, og);
             if (rc) return rc;
         }
         cudaStream_t user = e->ctx->stream;
         const bool prof = e->ctx->profiling;
-        e->ctx->stream = origin;
+        e->ctx->stream = og;
         e->ctx->profiling = prof && !captured;  // per-kernel timing never inside a capture
-        int rc = tree_fused_run(e->fz);
+        int rc = tree_fused_run(e->fz[g]);
         e->ctx->stream = user;
         e->ctx->profiling = prof;
         if (rc) return rc;
         LPM_CUDA_TRY(fork());
-        for (lpm_rk4* r : e->inst) {
+        for (lpm_rk4* r : mine) {
             rc = rk4_stage_update(r, stage, dt);
             if (rc) return rc;
         }
         LPM_CUDA_TRY(join());
+    }
+    return LPM_OK;
+}
+
+// One fused step of every instance: the groups fork from origin onto their own streams and join back.
+static int ens_enqueue_fused(lpm_ensemble* e, double dt, cudaStream_t origin, bool captured) {
+    const int G = ens_groups(e);
+    for (int g = 1; g < G; ++g) {
+        LPM_CUDA_TRY(cudaEventRecord(e->gfork[0], origin));
+        LPM_CUDA_TRY(cudaStreamWaitEvent(e->gstream[g], e->gfork[0], 0));
+    }
+    for (int g = 0; g < G; ++g) {
+        int rc = ens_group_step(e, g, dt, g == 0 ? origin : e->gstream[g], captured);
+        if (rc) return rc;
+    }
+    for (int g = 1; g < G; ++g) {
+        LPM_CUDA_TRY(cudaEventRecord(e->gjoin[g], e->gstream[g]));
+        LPM_CUDA_TRY(cudaStreamWaitEvent(origin, e->gjoin[g], 0));
     }
     return LPM_OK;
 }
@@ -323,7 +397,9 @@ static bool ens_fusable(const lpm_ensemble* e) {
 // One step of every instance, each on its lane's current stream.
 static int ens_enqueue(lpm_ensemble* e, double dt) {
     if (ens_fusable(e)) {
-        int rc = ens_enqueue_fused(e, dt, e->ctx->own_stream, false);
+        int rc = ens_groups_ready(e);
+        if (rc) return rc;
+        rc = ens_enqueue_fused(e, dt, e->ctx->own_stream, false);
         if (rc) return rc;
         LPM_CUDA_TRY(cudaStreamSynchronize(e->ctx->own_stream));
         return LPM_OK;
@@ -357,7 +433,8 @@ static int ens_capture(lpm_ensemble* e, double dt) {
     };
     const bool fused = ens_fusable(e);
     if (fused) {  // the fused launches' tables hold the instances' buffers of this capture
-        int rc = ens_bind(e);
+        int rc = ens_groups_ready(e);
+        for (int g = 0; g < ens_groups(e) && !rc; ++g) rc = ens_bind(e, g, g == 0 ? origin : e->gstream[g]);
         if (rc) {
             restore();
             return rc;

@@ -124,18 +124,20 @@ def test_fused_ensemble_equals_lane_mode(ctx):
     per near tile shape) gives bitwise the states of the lane mode, where every instance launches its own far
     and near kernels, on a mixed ensemble: learned-order instances (one with FP64 orders >= 6, whose orders 6..11
     keep their own launches; one with another near tile shape), fixed orders 8 and 12 (order 12 is above the
-    fused FP32 kernels) and an FP32 direct-sum instance."""
+    fused FP32 kernels) and an FP32 direct-sum instance; with the lanes in 1, 2 (the default) or 3 groups that
+    step independently, each with its own fused launches."""
     inst = W.ensemble_instances(levels=(3, 4, 5), per_level=2, seed=11)
     learned = L.tree_solver(L.LPM_PREC_F32, 10, 128, 0.5, learned=True, tolerance=5e-7)
     solvers = [learned, L.tree_solver(L.LPM_PREC_F32, 8, 64, 0.6), learned, L.direct_solver(L.LPM_PREC_F32),
                learned, L.tree_solver(L.LPM_PREC_F32, 12, 128, 0.5)]
     params = L.learned.load()[0]
 
-    def run(fused: bool, use_graph: bool, nsteps: int):
+    def run(fused: bool, use_graph: bool, nsteps: int, groups: int = 2):
         ens = L.Ensemble(ctx, L.biot_savart_kernel(), solvers, [n for _, _, n in inst],
                          [p.shape[0] for _, p, _ in inst], lanes=3)
-        assert ens.get_param("fused") == 1.0  # the default
+        assert ens.get_param("fused") == 1.0 and ens.get_param("fused_groups") == 2.0  # the defaults
         ens.set_param("fused", 1 if fused else 0)
+        ens.set_param("fused_groups", groups)
         assert ens.get_param("fused") == (1.0 if fused else 0.0)
         for i in (0, 2, 4):
             ens.instance(i).set_mlp(params)
@@ -151,11 +153,11 @@ def test_fused_ensemble_equals_lane_mode(ctx):
         return out
 
     lanes = run(False, True, 3)
-    for use_graph, nsteps in ((True, 3), (False, 2)):
-        fused = run(True, use_graph, nsteps)
+    for use_graph, nsteps, groups in ((True, 3, 2), (True, 3, 1), (True, 3, 3), (False, 2, 2)):
+        fused = run(True, use_graph, nsteps, groups)
         ref = lanes if nsteps == 3 else run(False, False, 2)
         for i in range(len(inst)):
-            assert np.array_equal(fused[i], ref[i]), (use_graph, i)
+            assert np.array_equal(fused[i], ref[i]), (use_graph, groups, i)
     with pytest.raises(L.LpmError):
         e = L.Ensemble(ctx, L.biot_savart_kernel(), learned, [inst[0][2]], [inst[0][1].shape[0]], lanes=1)
         try:
