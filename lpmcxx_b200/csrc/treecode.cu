@@ -22,8 +22,9 @@
 //     G0 = sum_j w_j g(y_j),  G_i = sum_j w_j h_ij g(y_j),
 //     sum_j w_j (x cross y_j) 2 g(y_j) = 2 [ (x cross d) G0 + x cross G ].
 // Moments are FP64: ordinary moments sum_j w_j h^k of every leaf from its particles, shifted to parents
-// (M2M) level by level, then converted to the B coefficients.  Orders >= 8 evaluate in FP64, lower
-// orders in FP32, always accumulated in FP64.
+// (M2M) level by level, then converted to the B coefficients.  Orders >= f64_from evaluate in FP64 (every
+// order for LPM_PREC_F64 solvers, none by default for FP32 ones; run-time "f64_from"), the others in FP32,
+// always accumulated in FP64.
 //
 // Near field.  Targets are sorted by Morton key into batches of kBatch; a batch and a source node
 // interact in the far field when rho_node < theta (|x_batch - c| - r_batch), otherwise leaves interact

@@ -23,11 +23,12 @@ REF_HARNESS = HERE / "_ref" / "ref_harness"
 _lib = None
 
 
-def build(ref: bool = False) -> None:
-    """Compile liboracle.so (and, with ref=True, the reference harness under _ref/)."""
+def build(ref: bool = False, ref_dir=None) -> None:
+    """Compile liboracle.so (and, with ref=True, the reference harness under _ref/ from the reference's
+    sources in ref_dir, default the Makefile's REF)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
     if ref:
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", *([f"REF={ref_dir}"] if ref_dir else [])], check=True)
 
 
 def lib() -> C.CDLL:
