@@ -541,6 +541,50 @@ def ensemble_tune(ctx, kern, inst, tol: float = 1e-6) -> dict:
     return tuned
 
 
+ENSEMBLE_EPS_LADDER = (5e-7, 3e-7, 2e-7)  # learned budgets tried per instance, largest first
+
+
+def ensemble_instance_budgets(ctx, kern, inst, tuned, tol: float = 1e-6, safety: float = 0.8) -> list:
+    """Per instance, the largest learned budget of ENSEMBLE_EPS_LADDER, no smaller than its size class's tuned
+    budget, with which the class's other tuned settings meet safety * tol on ENSEMBLE_SAMPLE seeded targets of
+    that instance against the FP64 direct sum (the class's budget, which every member met in tuning, when none
+    of the larger ones does): members whose vortex the class setting over-resolves run with a larger budget."""
+    import torch
+
+    import lpmcxx_b200 as L
+    from lpmcxx_b200 import learned
+
+    params = learned.load()[0]
+    out = []
+    for i, (lvl, p, n_src) in enumerate(inst):
+        t = tuned[lvl]
+        d = torch.tensor(p, device="cuda")
+        rng = np.random.default_rng(500 + i)
+        idx = torch.as_tensor(np.sort(rng.choice(p.shape[0], size=min(ENSEMBLE_SAMPLE, p.shape[0]), replace=False)),
+                              device="cuda")
+        ref = torch.empty((3, idx.numel()), dtype=torch.float64, device="cuda")
+        ctx.direct_sum_dev(kern, L.LPM_PREC_F64, d[:n_src], d[idx].contiguous(), ref)
+        u = torch.empty((3, p.shape[0]), dtype=torch.float64, device="cuda")
+        ts = L.TreeSum(ctx, kern, L.tree_solver(L.LPM_PREC_F32, 10, t["max_per_leaf"], t["theta"], learned=True,
+                                                tolerance=t["eps"]), n_src, p.shape[0])
+        try:
+            ts.set_mlp(params)
+            for name in ("order_bias", "batch_level", "near_targets", "near_tile", "near_split"):
+                ts.set_param(name, t[name])
+            eps = t["eps"]
+            for cand in sorted({e for e in ENSEMBLE_EPS_LADDER if e > t["eps"]}, reverse=True):
+                ts.set_param("eps", cand)
+                ts.eval(d[:n_src], d, u)
+                torch.cuda.synchronize()
+                if float(torch.linalg.norm(u[:, idx] - ref) / torch.linalg.norm(ref)) <= safety * tol:
+                    eps = cand
+                    break
+        finally:
+            ts.close()
+        out.append(eps)
+    return out
+
+
 def ensemble_accuracy(ctx, kern, ens, inst, sample: int = ENSEMBLE_SAMPLE, seed: int = 11) -> list:
     """Relative L2 velocity error of every instance's treecode against the FP64 direct sum, on `sample`
     seeded targets of its current state."""
@@ -586,8 +630,9 @@ def run_gpu_ensemble(args) -> None:
     kern = L.biot_savart_kernel()
     ctx.use_torch_stream()
     tuned = ensemble_tune(ctx, kern, inst)
+    eps_inst = ensemble_instance_budgets(ctx, kern, inst, tuned)
     solvers = [L.tree_solver(L.LPM_PREC_F32, 10, tuned[lvl]["max_per_leaf"], tuned[lvl]["theta"], learned=True,
-                             tolerance=tuned[lvl]["eps"]) for lvl, _, _ in inst]
+                             tolerance=eps_inst[i]) for i, (lvl, _, _) in enumerate(inst)]
     ens = L.Ensemble(ctx, kern, solvers, [n for _, _, n in inst], [p.shape[0] for _, p, _ in inst], lanes=args.lanes)
     ens.set_mlp(learned.load()[0])
     for i, (lvl, p, _) in enumerate(inst):
@@ -642,7 +687,7 @@ def run_gpu_ensemble(args) -> None:
             out_ms.append(e0.elapsed_time(e1))
         return float(np.mean(out_ms))
 
-    one_group_ms = compare_ms("fused_groups", 1)
+    groups_ms = {g: compare_ms("fused_groups", g) for g in (1, 4) if g != groups}
     ens.set_param("fused_groups", groups)
     lane_ms = compare_ms("fused", 0)
     ens.set_param("fused", 1)
@@ -678,8 +723,12 @@ def run_gpu_ensemble(args) -> None:
         "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": f"{len(inst)} instances: icos L{'/L'.join(map(str, levels))} x {args.ens_per_level}, "
                                f"RH m=4 + seeded Gaussian, {n_total:,} particles",
-                   "solver": "learned treecode, per size class the autotuned leaf / theta / budget / batch level "
-                             "(order bias 2)", "tuned": {f"L{k}": v for k, v in tuned.items()},
+                   "solver": "learned treecode, per size class the autotuned leaf / theta / budget / batch level / "
+                             "near tile (order bias 2); per instance the largest budget of "
+                             f"{list(ENSEMBLE_EPS_LADDER)} (no smaller than its class's) that still meets 0.8e-6",
+                   "tuned": {f"L{k}": v for k, v in tuned.items()},
+                   "instance_eps": {f"L{k}": [e for (lvl, _, _), e in zip(inst, eps_inst) if lvl == k]
+                                    for k in tuned},
                    "lanes": args.lanes, "dt": dt,
                    "graph": "one CUDA graph replay per ensemble step; per RK4 stage, the far field of each group "
                             "of instances (the lanes in fused_groups groups stepping independently) is one "
@@ -690,7 +739,8 @@ def run_gpu_ensemble(args) -> None:
                                   "final_max": max(err_final), "final_median": float(np.median(err_final)),
                                   "final_step": args.warmup + args.steps},
         "particle_steps_per_s": value * n_total,
-        "fused_groups": groups, "one_group_ms_per_step": one_group_ms, "lane_mode_ms_per_step": lane_ms,
+        "fused_groups": groups, "other_fused_groups_ms_per_step": {str(g): v for g, v in groups_ms.items()},
+        "lane_mode_ms_per_step": lane_ms,
         "roofline": {"bound": "fp32", "kernel": "whole step (near + far field, all instances)",
                      "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                      "traffic": None, "peak_source": "measured FMA microbenchmark (lpm_fma_peak) on this GPU",
