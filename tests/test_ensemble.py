@@ -164,3 +164,31 @@ def test_fused_ensemble_equals_lane_mode(ctx):
             e.set_param("fused", 2)
         finally:
             e.close()
+
+
+@pytest.mark.gpu
+def test_fused_ensemble_edge_instances(ctx):
+    """Fused steps with instances that take no part in the fused launches: a one-instance ensemble, and an
+    ensemble holding an instance whose particles carry no sources (its velocity is zero, so it stays put up to
+    the re-projection's rounding) next to a treecode instance; both give the lane mode's states bitwise."""
+    inst = W.ensemble_instances(levels=(3, 4), per_level=1, seed=21)
+    solver = L.tree_solver(L.LPM_PREC_F32, 10, 128, 0.5, learned=True, tolerance=5e-7)
+    params = L.learned.load()[0]
+    passive = inst[0][1].copy()
+    cases = [([inst[1]], [inst[1][2]]), ([inst[1], (3, passive, 0)], [inst[1][2], 0])]
+    for members, n_src in cases:
+        got = {}
+        for fused in (1, 0):
+            ens = L.Ensemble(ctx, L.biot_savart_kernel(), solver, n_src, [p.shape[0] for _, p, _ in members],
+                             lanes=2)
+            ens.set_param("fused", fused)
+            ens.set_mlp(params)
+            for i, (_, p, _) in enumerate(members):
+                ens.instance(i).set_state(p)
+            ens.step(0.01, 3, use_graph=True)
+            got[fused] = [ens.instance(i).get_state() for i in range(len(members))]
+            ens.close()
+        for i in range(len(members)):
+            assert np.array_equal(got[1][i], got[0][i]), (len(members), i)
+        if len(members) == 2:  # zero velocity: only the re-projection onto the sphere touches the positions
+            assert np.allclose(got[1][1], passive, rtol=0, atol=1e-14)
