@@ -3154,6 +3154,7 @@ int tree_fused_run(TreeFused* f) {
 }
 
 int tree_check(TreeSolver* t) {
+    if (t->n_src == 0 || t->n_tgt == 0) return LPM_OK;  // its evaluations build no tree and fill no lists
     int32_t f[8], c[8], tc[4];
     lpm_ctx* ctx = t->ctx;
     LPM_CUDA_TRY(cudaMemcpyAsync(f, t->flags, sizeof(f), cudaMemcpyDeviceToHost, ctx->stream));
@@ -3189,6 +3190,10 @@ const Octree& tree_source_octree(const TreeSolver* t, int64_t* n_points) {
 }
 
 int tree_stats(TreeSolver* t, int64_t* out8) {
+    if (t->n_src == 0 || t->n_tgt == 0) {  // no tree, no lists
+        for (int k = 0; k < 10; ++k) out8[k] = 0;
+        return LPM_OK;
+    }
     int32_t f[8], c[8];
     unsigned long long pc[3];
     lpm_ctx* ctx = t->ctx;
