@@ -511,7 +511,7 @@ def run_gpu_direct_cube(args) -> None:
 
 ENSEMBLE_METRIC = "ensemble RK4 steps/s: 64 instances (icos L5/L6/L7/L8 x 16, 27.85M sources), learned treecode"
 ENSEMBLE_TUNE_GRID = ((128, 256, 512), (0.4, 0.5, 0.6), (2e-7, 5e-7))  # leaf sizes, theta, learned budgets
-# seeded targets per instance on which the tuner and the reported errors judge against the FP64 direct sum: the
+# seeded targets per instance on which the tuner and the reported errors compare with the FP64 direct sum: the
 # error concentrates near each vortex core, so the relative L2 over 4096 targets varied up to twofold between
 # samples of the same field
 ENSEMBLE_SAMPLE = 32768
