@@ -406,6 +406,18 @@ int lpm_ensemble_set_param(lpm_ensemble* ens, const char* name, double value);
 int lpm_ensemble_get_param(const lpm_ensemble* ens, const char* name, double* value);
 int lpm_ensemble_step(lpm_ensemble* ens, double dt, int nsteps, int use_graph);
 
+/* ---- checkpoint / resume (no reference counterpart: the reference's VTK / CSV output, src/LpmVtkFileIO.h:17-35,
+ * is write-only).  A binary dump of an RK4 run's state: the particles (x, y, z, w) as FP64 with the particle and
+ * source counts, and the step count, time and time step the caller passes, closed by a 64-bit FNV-1a checksum.
+ * _read restores the state into an RK4 (every instance of an ensemble, in instance order) of the same sizes and
+ * returns the stored step, t and dt (each pointer may be null); a file of other sizes, not written by these calls,
+ * truncated or failing its checksum gives LPM_ERR_ARG and leaves every state as it was.  The steps after a resume
+ * are bitwise those of the run that wrote the file.  Synchronous host file I/O. */
+int lpm_rk4_checkpoint_write(lpm_rk4* rk, const char* path, int64_t step, double t, double dt);
+int lpm_rk4_checkpoint_read(lpm_rk4* rk, const char* path, int64_t* step, double* t, double* dt);
+int lpm_ensemble_checkpoint_write(lpm_ensemble* ens, const char* path, int64_t step, double t, double dt);
+int lpm_ensemble_checkpoint_read(lpm_ensemble* ens, const char* path, int64_t* step, double* t, double* dt);
+
 /* ---- testing (no reference counterpart): failure injection on the host side.  The device allocation made
  * after `after` further successful ones reports failure (LPM_ERR_OOM from the entry point that made it), once;
  * a negative value turns the injection off.  Process-wide. */

@@ -287,6 +287,18 @@ class RK4:
         check(lib().lpm_rk4_get_state(self.h, ptr(o)), "lpm_rk4_get_state")
         return o
 
+    def checkpoint_write(self, path, step: int = 0, t: float = 0.0, dt: float = 0.0) -> None:
+        """lpm_rk4_checkpoint_write: the state, with the caller's step count, time and time step, to a file."""
+        check(lib().lpm_rk4_checkpoint_write(self.h, str(path).encode(), int(step), float(t), float(dt)),
+              "lpm_rk4_checkpoint_write")
+
+    def checkpoint_read(self, path) -> tuple:
+        """lpm_rk4_checkpoint_read: restores the state; returns the stored (step, t, dt)."""
+        s, t, dt = C.c_int64(), C.c_double(), C.c_double()
+        check(lib().lpm_rk4_checkpoint_read(self.h, str(path).encode(), C.byref(s), C.byref(t), C.byref(dt)),
+              "lpm_rk4_checkpoint_read")
+        return s.value, t.value, dt.value
+
     def step(self, dt: float, nsteps: int = 1, use_graph: bool = False) -> None:
         check(lib().lpm_rk4_step(self.h, dt, nsteps, 1 if use_graph else 0), "lpm_rk4_step")
 
@@ -389,6 +401,18 @@ class Ensemble:
 
     def step(self, dt: float, nsteps: int = 1, use_graph: bool = True) -> None:
         check(lib().lpm_ensemble_step(self.h, dt, nsteps, 1 if use_graph else 0), "lpm_ensemble_step")
+
+    def checkpoint_write(self, path, step: int = 0, t: float = 0.0, dt: float = 0.0) -> None:
+        """lpm_ensemble_checkpoint_write: every instance's state in one file."""
+        check(lib().lpm_ensemble_checkpoint_write(self.h, str(path).encode(), int(step), float(t), float(dt)),
+              "lpm_ensemble_checkpoint_write")
+
+    def checkpoint_read(self, path) -> tuple:
+        """lpm_ensemble_checkpoint_read: restores every instance's state; returns the stored (step, t, dt)."""
+        s, t, dt = C.c_int64(), C.c_double(), C.c_double()
+        check(lib().lpm_ensemble_checkpoint_read(self.h, str(path).encode(), C.byref(s), C.byref(t), C.byref(dt)),
+              "lpm_ensemble_checkpoint_read")
+        return s.value, t.value, dt.value
 
 
 class Tree:

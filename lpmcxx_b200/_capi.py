@@ -136,6 +136,10 @@ SIGNATURES = {
     "lpm_ensemble_set_param": (C.c_int, [P, C.c_char_p, C.c_double]),
     "lpm_ensemble_get_param": (C.c_int, [P, C.c_char_p, P]),
     "lpm_ensemble_step": (C.c_int, [P, C.c_double, C.c_int, C.c_int]),
+    "lpm_rk4_checkpoint_write": (C.c_int, [P, C.c_char_p, C.c_int64, C.c_double, C.c_double]),
+    "lpm_rk4_checkpoint_read": (C.c_int, [P, C.c_char_p, P, P, P]),
+    "lpm_ensemble_checkpoint_write": (C.c_int, [P, C.c_char_p, C.c_int64, C.c_double, C.c_double]),
+    "lpm_ensemble_checkpoint_read": (C.c_int, [P, C.c_char_p, P, P, P]),
     "lpm_debug_fail_allocations": (C.c_int, [C.c_int64]),
 }
 

@@ -525,3 +525,24 @@ extern "C" int lpm_ensemble_lane_of(const lpm_ensemble* e, int i, int* lane) {
     *lane = e->lane_of[i];
     return LPM_OK;
 }
+
+namespace lpm {
+int ckpt_write(const char* path, lpm_rk4* const* rks, int n_inst, int64_t step, double t, double dt);
+int ckpt_read(const char* path, lpm_rk4* const* rks, int n_inst, int64_t* step, double* t, double* dt);
+}  // namespace lpm
+
+extern "C" int lpm_ensemble_checkpoint_write(lpm_ensemble* e, const char* path, int64_t step, double t, double dt) {
+    if (!e) {
+        set_error("lpm_ensemble_checkpoint_write: null ensemble");
+        return LPM_ERR_ARG;
+    }
+    return ckpt_write(path, e->inst.data(), (int)e->inst.size(), step, t, dt);
+}
+
+extern "C" int lpm_ensemble_checkpoint_read(lpm_ensemble* e, const char* path, int64_t* step, double* t, double* dt) {
+    if (!e) {
+        set_error("lpm_ensemble_checkpoint_read: null ensemble");
+        return LPM_ERR_ARG;
+    }
+    return ckpt_read(path, e->inst.data(), (int)e->inst.size(), step, t, dt);
+}

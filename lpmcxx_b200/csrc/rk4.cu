@@ -18,7 +18,10 @@
 #include "treecode.h"
 
 #include <cmath>
+#include <cstdio>
+#include <cstring>
 #include <new>
+#include <vector>
 
 struct lpm_rk4 {
     lpm_ctx* ctx = nullptr;
@@ -442,4 +445,151 @@ extern "C" int lpm_rk4_velocity_dev(lpm_rk4* rk, double* out) {
     int rc = refresh_stage(rk);
     if (rc) return rc;
     return rk4_velocity(rk, out);
+}
+
+// ---------------------------------------------------------------------------------- checkpoint / resume
+// File layout (host byte order): "LPMCKPT" + NUL, uint32 version (1), uint32 instance count, int64 step,
+// double t, double dt; per instance int64 particle count, int64 source count and the particles as n x 4
+// doubles (x, y, z, w); then the 64-bit FNV-1a checksum of every byte before it.  The state is all an RK4 step
+// reads (stage positions and accumulators are rebuilt from it), so a resumed run steps bitwise as the one that
+// wrote the file.
+namespace lpm {
+namespace {
+constexpr char kCkptMagic[8] = {'L', 'P', 'M', 'C', 'K', 'P', 'T', '\0'};
+constexpr uint32_t kCkptVersion = 1;
+
+struct CkptFile {
+    FILE* f = nullptr;
+    uint64_t h = 1469598103934665603ull;  // FNV-1a offset basis
+    bool ok = true;
+    ~CkptFile() {
+        if (f) std::fclose(f);
+    }
+    void hash(const void* p, size_t n) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    }
+    void put(const void* p, size_t n) {
+        if (ok && std::fwrite(p, 1, n, f) != n) ok = false;
+        hash(p, n);
+    }
+    void get(void* p, size_t n) {
+        if (ok && std::fread(p, 1, n, f) != n) ok = false;
+        if (ok) hash(p, n);
+    }
+};
+}  // namespace
+
+int ckpt_write(const char* path, lpm_rk4* const* rks, int n_inst, int64_t step, double t, double dt) {
+    if (!path || n_inst < 1) {
+        set_error("checkpoint: bad argument");
+        return LPM_ERR_ARG;
+    }
+    std::vector<std::vector<double>> states((size_t)n_inst);
+    for (int i = 0; i < n_inst; ++i) {  // read every state before the file is touched
+        states[i].resize((size_t)rks[i]->n * 4);
+        int rc = lpm_rk4_get_state(rks[i], states[i].data());
+        if (rc) return rc;
+    }
+    CkptFile c;
+    c.f = std::fopen(path, "wb");
+    if (!c.f) {
+        set_error("checkpoint: cannot open '%s' for writing", path);
+        return LPM_ERR_ARG;
+    }
+    const uint32_t head[2] = {kCkptVersion, (uint32_t)n_inst};
+    c.put(kCkptMagic, sizeof(kCkptMagic));
+    c.put(head, sizeof(head));
+    c.put(&step, sizeof(step));
+    c.put(&t, sizeof(t));
+    c.put(&dt, sizeof(dt));
+    for (int i = 0; i < n_inst; ++i) {
+        const int64_t sizes[2] = {rks[i]->n, rks[i]->n_src};
+        c.put(sizes, sizeof(sizes));
+        c.put(states[i].data(), states[i].size() * sizeof(double));
+    }
+    const uint64_t sum = c.h;
+    c.put(&sum, sizeof(sum));
+    if (!c.ok || std::fflush(c.f) != 0) {
+        set_error("checkpoint: writing '%s' failed", path);
+        return LPM_ERR_ARG;
+    }
+    return LPM_OK;
+}
+
+int ckpt_read(const char* path, lpm_rk4* const* rks, int n_inst, int64_t* step, double* t, double* dt) {
+    if (!path || n_inst < 1) {
+        set_error("checkpoint: bad argument");
+        return LPM_ERR_ARG;
+    }
+    CkptFile c;
+    c.f = std::fopen(path, "rb");
+    if (!c.f) {
+        set_error("checkpoint: cannot open '%s'", path);
+        return LPM_ERR_ARG;
+    }
+    char magic[8];
+    uint32_t head[2];
+    int64_t s = 0;
+    double tt = 0.0, dd = 0.0;
+    c.get(magic, sizeof(magic));
+    c.get(head, sizeof(head));
+    c.get(&s, sizeof(s));
+    c.get(&tt, sizeof(tt));
+    c.get(&dd, sizeof(dd));
+    if (!c.ok || std::memcmp(magic, kCkptMagic, sizeof(magic)) != 0 || head[0] != kCkptVersion) {
+        set_error("checkpoint: '%s' is not an RK4 checkpoint of this library", path);
+        return LPM_ERR_ARG;
+    }
+    if ((int)head[1] != n_inst) {
+        set_error("checkpoint: '%s' holds %u instances, not %d", path, head[1], n_inst);
+        return LPM_ERR_ARG;
+    }
+    std::vector<std::vector<double>> states((size_t)n_inst);
+    for (int i = 0; i < n_inst && c.ok; ++i) {
+        int64_t sizes[2] = {0, 0};
+        c.get(sizes, sizeof(sizes));
+        if (!c.ok) break;
+        if (sizes[0] != rks[i]->n || sizes[1] != rks[i]->n_src) {
+            set_error("checkpoint: instance %d of '%s' has %lld particles / %lld sources, not %lld / %lld", i, path,
+                      (long long)sizes[0], (long long)sizes[1], (long long)rks[i]->n, (long long)rks[i]->n_src);
+            return LPM_ERR_ARG;
+        }
+        states[i].resize((size_t)sizes[0] * 4);
+        c.get(states[i].data(), states[i].size() * sizeof(double));
+    }
+    const uint64_t want = c.h;
+    uint64_t sum = 0;
+    if (c.ok) {
+        if (std::fread(&sum, 1, sizeof(sum), c.f) != sizeof(sum)) c.ok = false;
+    }
+    if (!c.ok || sum != want || std::fgetc(c.f) != EOF) {
+        set_error("checkpoint: '%s' is truncated, corrupted or longer than its contents", path);
+        return LPM_ERR_ARG;
+    }
+    for (int i = 0; i < n_inst; ++i) {  // the states change only once the whole file checked out
+        int rc = lpm_rk4_set_state(rks[i], states[i].data());
+        if (rc) return rc;
+    }
+    if (step) *step = s;
+    if (t) *t = tt;
+    if (dt) *dt = dd;
+    return LPM_OK;
+}
+}  // namespace lpm
+
+extern "C" int lpm_rk4_checkpoint_write(lpm_rk4* rk, const char* path, int64_t step, double t, double dt) {
+    if (!rk) {
+        set_error("lpm_rk4_checkpoint_write: null RK4");
+        return LPM_ERR_ARG;
+    }
+    return ckpt_write(path, &rk, 1, step, t, dt);
+}
+
+extern "C" int lpm_rk4_checkpoint_read(lpm_rk4* rk, const char* path, int64_t* step, double* t, double* dt) {
+    if (!rk) {
+        set_error("lpm_rk4_checkpoint_read: null RK4");
+        return LPM_ERR_ARG;
+    }
+    return ckpt_read(path, &rk, 1, step, t, dt);
 }
