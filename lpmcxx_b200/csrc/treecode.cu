@@ -3023,12 +3023,12 @@ int tree_fused_bind(TreeFused* f, TreeSolver* const* ts, double* const* Us, int 
         fused_free(f);
         const int cap = std::max(n, 1);
         const int64_t icap = std::max<int64_t>(items, 1);
-        cudaError_t e = cudaMalloc(&f->inst, sizeof(FusedInst) * (size_t)cap);
-        if (e == cudaSuccess) e = cudaMalloc(&f->far_tab, sizeof(FarArgs) * kFusedFarSlots * (size_t)cap);
-        if (e == cudaSuccess) e = cudaMalloc(&f->near_tab, sizeof(NearArgs) * kFusedNearGroups * (size_t)cap);
-        if (e == cudaSuccess) e = cudaMalloc(&f->far_items, sizeof(int2) * (size_t)icap);
-        if (e == cudaSuccess) e = cudaMalloc(&f->near_items, sizeof(int2) * (size_t)icap);
-        if (e == cudaSuccess) e = cudaMalloc(&f->aux, sizeof(int32_t) * kFzInts);
+        cudaError_t e = dev_alloc((void**)&f->inst, sizeof(FusedInst) * (size_t)cap);
+        if (e == cudaSuccess) e = dev_alloc((void**)&f->far_tab, sizeof(FarArgs) * kFusedFarSlots * (size_t)cap);
+        if (e == cudaSuccess) e = dev_alloc((void**)&f->near_tab, sizeof(NearArgs) * kFusedNearGroups * (size_t)cap);
+        if (e == cudaSuccess) e = dev_alloc((void**)&f->far_items, sizeof(int2) * (size_t)icap);
+        if (e == cudaSuccess) e = dev_alloc((void**)&f->near_items, sizeof(int2) * (size_t)icap);
+        if (e == cudaSuccess) e = dev_alloc((void**)&f->aux, sizeof(int32_t) * kFzInts);
         if (e != cudaSuccess) {
             fused_free(f);
             return cuda_status(e, "cudaMalloc (fused solvers)");
