@@ -54,6 +54,20 @@ def env_int(name: str, default: int) -> int:
     return int(v) if v not in (None, "") else default
 
 
+def replica_rate(total_ms: float, steps: int, device: str = "cuda") -> tuple:
+    """Replicas (every rank runs its own copy of the workload, no data exchanged): the slowest rank's timed
+    milliseconds (max over ranks) and the whole job's steps/s, world x steps over that time."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    return total_ms, world * steps / (total_ms * 1e-3)
+
+
 # --------------------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
@@ -902,12 +916,9 @@ def run_gpu(args) -> None:
         # the state after the warm-up and timed steps, for the accuracy check at the final state
         state_final = torch.empty_like(state0)
         rk.get_state(state_final)
+        total_ms, value = replica_rate(total_ms, args.steps)
         if world > 1:
-            t = torch.tensor([total_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
             dist.barrier()
-        value = world * args.steps / (total_ms * 1e-3)
 
         # ---- end to end through the host API: pinned host state in, step, state out
         host_in = torch.tensor(p).pin_memory()
