@@ -1409,50 +1409,78 @@ __global__ void __launch_bounds__(kBatch / T) far_scalar_kernel(FarArgs A, int s
     // the batch's last target idles as a whole
     const int64_t q = q0 + 32 * T * (threadIdx.x >> 5) + (threadIdx.x & 31);
     const bool live = q0 + 32 * T * (int64_t)(threadIdx.x >> 5) < qe;  // warp-uniform
+    // T = 2 (FP32): targets and cluster centres as FP32 offsets from the batch's first target o, so that
+    // d = c - x is one FP32 subtraction (the far2 kernel's scheme), and each stage's sums in FP32 folded into
+    // FP64 once per stage; T = 1: FP64 positions, d rounded once from the FP64 difference
+    const double4 o = A.tgt_sorted[q0];
     double4 x[T];
+    float xo[T][3];
 #pragma unroll
-    for (int t = 0; t < T; ++t) x[t] = q + 32 * t < qe ? A.tgt_sorted[q + 32 * t] : make_double4(2, 2, 2, 0);
+    for (int t = 0; t < T; ++t) {
+        x[t] = q + 32 * t < qe ? A.tgt_sorted[q + 32 * t] : make_double4(o.x + 4.0, o.y + 4.0, o.z + 4.0, 0);
+        xo[t][0] = (float)(x[t].x - o.x);
+        xo[t][1] = (float)(x[t].y - o.y);
+        xo[t][2] = (float)(x[t].z - o.z);
+    }
+    float4* ctrf = reinterpret_cast<float4*>(ctr);  // T = 2: 2 x kK FP32 centre offsets in the centres' space
     const F* base = (const F*)(sizeof(F) == 8 ? (const void*)A.B64 : (const void*)A.B32);
-    auto gather = [&](int64_t s0, int n, float4* buf, double4* cs) {
+    auto gather = [&](int64_t s0, int n, float4* buf, int slot) {
         for (int i = threadIdx.x; i < n * kUnits; i += kNT) {
             const int e = i / kUnits, j = i - e * kUnits;
             cp_async16(buf + i, (const char*)(base + (size_t)A.far_list[s0 + e].x * stride) + 16 * j);
         }
-        if ((int)threadIdx.x < n) cs[threadIdx.x] = A.node_ctr[A.far_list[s0 + threadIdx.x].x];
+        if ((int)threadIdx.x < n) {
+            const double4 c = A.node_ctr[A.far_list[s0 + threadIdx.x].x];
+            if constexpr (T == 2)
+                ctrf[slot * kK + threadIdx.x] =
+                    make_float4((float)(c.x - o.x), (float)(c.y - o.y), (float)(c.z - o.z), 0.0f);
+            else
+                ctr[slot * kK + threadIdx.x] = c;
+        }
     };
     double acc[T];
 #pragma unroll
     for (int t = 0; t < T; ++t) acc[t] = 0.0;
-    gather(f0, (int)min((int64_t)kK, f1 - f0), fbuf, ctr);
+    gather(f0, (int)min((int64_t)kK, f1 - f0), fbuf, 0);
     cp_async_commit();
     int sb = 0;
     for (int64_t s0 = f0;; sb ^= 1) {
         const int n = (int)min((int64_t)kK, f1 - s0);
         const int64_t s1 = s0 + n;
-        if (s1 < f1) gather(s1, (int)min((int64_t)kK, f1 - s1), fbuf + (size_t)(sb ^ 1) * kK * kUnits, ctr + (sb ^ 1) * kK);
+        if (s1 < f1) gather(s1, (int)min((int64_t)kK, f1 - s1), fbuf + (size_t)(sb ^ 1) * kK * kUnits, sb ^ 1);
         cp_async_commit();
         cp_async_wait_prev();
         __syncthreads();  // stage sb resident
         if (live) {
             const float4* buf = fbuf + (size_t)sb * kK * kUnits;
-            const double4* cs = ctr + sb * kK;
-            for (int k = 0; k < n; ++k) {
-                F rinv[T], e[T][4];
+            if constexpr (T == 2) {
+                const float4* cs = ctrf + sb * kK;
+                float acc32[2] = {0.0f, 0.0f};
+                for (int k = 0; k < n; ++k) {
+                    const float4 c = cs[k];
+                    float rinv[2], e[2][4];
 #pragma unroll
-                for (int t = 0; t < T; ++t) {
-                    const F dx = (F)(cs[k].x - x[t].x), dy = (F)(cs[k].y - x[t].y), dz = (F)(cs[k].z - x[t].z);
-                    rinv[t] = rsqrt_t(dx * dx + dy * dy + dz * dz);
-                    const F s2 = rinv[t] * rinv[t];
-                    e[t][0] = dx * s2; e[t][1] = dy * s2; e[t][2] = dz * s2; e[t][3] = s2;
-                }
-                const F* row = (const F*)(buf + (size_t)k * kUnits);
-                if constexpr (T == 2) {
+                    for (int t = 0; t < 2; ++t) {
+                        const float dx = c.x - xo[t][0], dy = c.y - xo[t][1], dz = c.z - xo[t][2];
+                        rinv[t] = rsqrt_t(dx * dx + dy * dy + dz * dz);
+                        const float s2 = rinv[t] * rinv[t];
+                        e[t][0] = dx * s2; e[t][1] = dy * s2; e[t][2] = dz * s2; e[t][3] = s2;
+                    }
                     float g[2];
-                    horner1x2<P>(row, e, g);
-                    acc[0] += (double)(rinv[0] * g[0]);
-                    acc[1] += (double)(rinv[1] * g[1]);
-                } else {
-                    acc[0] += (double)(rinv[0] * horner1<P, F>(row, e[0][0], e[0][1], e[0][2], e[0][3]));
+                    horner1x2<P>((const float*)(buf + (size_t)k * kUnits), e, g);
+                    acc32[0] = fmaf(rinv[0], g[0], acc32[0]);
+                    acc32[1] = fmaf(rinv[1], g[1], acc32[1]);
+                }
+                acc[0] += (double)acc32[0];
+                acc[1] += (double)acc32[1];
+            } else {
+                const double4* cs = ctr + sb * kK;
+                for (int k = 0; k < n; ++k) {
+                    const F dx = (F)(cs[k].x - x[0].x), dy = (F)(cs[k].y - x[0].y), dz = (F)(cs[k].z - x[0].z);
+                    const F rinv = rsqrt_t(dx * dx + dy * dy + dz * dz);
+                    const F s2 = rinv * rinv;
+                    const F* row = (const F*)(buf + (size_t)k * kUnits);
+                    acc[0] += (double)(rinv * horner1<P, F>(row, dx * s2, dy * s2, dz * s2, s2));
                 }
             }
         }
