@@ -1300,6 +1300,40 @@ __global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_order2_kerne
         far2_batch<P, PART>(A, b, fbuf);
 }
 
+// The short orders 1..kFarLowMax of the FP32 far field in one persistent launch: a block takes a batch (in
+// decreasing order of its far work) and runs the order-P body for each of these orders in turn, so V receives
+// the orders' sums in the order of separate launches (bitwise the same).  As separate launches these orders
+// were latency-bound (few clusters per batch, waits on the coefficient gathers), each with its own tail.
+constexpr int kFarLowMax = 4;
+struct FarLowArgs {
+    FarArgs a[kFarLowMax];  // a[P - 1]: order P's arguments; far_cnt null: order P is not in this launch
+};
+
+__global__ void __launch_bounds__(kFar2Threads, kFar2MinBlocks) far_low2_kernel(FarLowArgs L,
+                                                                               const int32_t* __restrict__ nbat_p,
+                                                                               const int32_t* __restrict__ order,
+                                                                               int32_t* ticket) {
+    static_assert(kFarLowMax == 4 && kFarLowMax < kFarSplitOrder, "orders 1..4, none split");
+    extern __shared__ float4 fbuf[];
+    __shared__ int slot;
+    const int nbat = *nbat_p;
+    for (int64_t b = next_batch(ticket, order, nbat, &slot); b >= 0; b = next_batch(ticket, order, nbat, &slot)) {
+        if (L.a[0].far_cnt) far2_batch<1>(L.a[0], b, fbuf);
+        __syncthreads();  // the previous order's stage buffers are read before the next order's gathers
+        if (L.a[1].far_cnt) far2_batch<2>(L.a[1], b, fbuf);
+        __syncthreads();
+        if (L.a[2].far_cnt) far2_batch<3>(L.a[2], b, fbuf);
+        __syncthreads();
+        if (L.a[3].far_cnt) far2_batch<4>(L.a[3], b, fbuf);
+    }
+}
+
+// Dynamic shared memory of far_low2_kernel: the largest of its orders' stage buffers.
+size_t far_low_smem() {
+    return std::max(std::max(FarShape<1, float4, kFar2StageUnits>::kSmem, FarShape<2, float4, kFar2StageUnits>::kSmem),
+                    std::max(FarShape<3, float4, kFar2StageUnits>::kSmem, FarShape<4, float4, kFar2StageUnits>::kSmem));
+}
+
 // The Horner scheme of `horner` with scalar coefficients.
 template <int P, typename T>
 __device__ __forceinline__ T horner1(const T* __restrict__ Bc, T e0, T e1, T e2, T s) {
@@ -2265,6 +2299,7 @@ struct TreeSolver {
     int near_split = kNearSplit;      // source groups per batch (run-time "near_split")
     int far_blocks[kPMax + 1][2] = {};  // per order, FP32 / FP64 far kernel
     int far_split_blocks[2] = {};       // the two FP32 launches of order kFarSplitOrder
+    int far_low_blocks = 1;             // far_low2_kernel (FP32 orders 1..kFarLowMax in one launch)
     uint64_t generation = 0;          // reallocations of the lists and per-node arrays (tree_generation)
     std::vector<void*> allocs;
 };
@@ -2603,6 +2638,12 @@ int tree_solver_create(lpm_ctx* ctx, const lpm_kernel_desc& kernel, const lpm_so
             FarKernelFn fn = far_split_select(part, &smem, &threads);
             ea = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
             t->far_split_blocks[part - 1] = (int)std::max<int64_t>(
+                1, std::min<int64_t>(t->n_batches, (int64_t)std::max(per_sm, 1) * ctx->num_sms));
+        }
+        if (ea == cudaSuccess && !scalar) {
+            per_sm = 0;
+            ea = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, far_low2_kernel, kFar2Threads, far_low_smem());
+            t->far_low_blocks = (int)std::max<int64_t>(
                 1, std::min<int64_t>(t->n_batches, (int64_t)std::max(per_sm, 1) * ctx->num_sms));
         }
         if (ea != cudaSuccess) {
@@ -2949,6 +2990,14 @@ int tree_velocity(TreeSolver* t, const double4* src, int64_t n_src, const double
     if (overlap) LPM_CUDA_TRY(cudaEventRecord(t->ev_fork, ctx->stream));
     int p_lo = 0, p_hi = -1;
     far_order_range(t, &p_lo, &p_hi);
+    const int low_hi = std::min(p_hi, kFarLowMax);
+    if (!t->scalar && low_hi > p_lo && low_hi < t->f64_from) {  // FP32 orders p_lo..low_hi in one launch
+        FarLowArgs LA{};
+        for (int P = p_lo; P <= low_hi; ++P) LA.a[P - 1] = far_args(t, P);
+        LPM_LAUNCH(ctx, "far_kernel", far_low2_kernel, (unsigned)t->far_low_blocks, kFar2Threads, far_low_smem(), LA,
+                   t->tcount + 1, t->far_order, t->sched_aux + kAuxFarTicket + p_lo);
+        p_lo = low_hi + 1;
+    }
     for (int P = p_lo; P <= p_hi; ++P) {
         rc = tree_far_order(t, P);
         if (rc) return rc;
