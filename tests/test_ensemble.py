@@ -158,12 +158,16 @@ def test_fused_ensemble_equals_lane_mode(ctx):
         ref = lanes if nsteps == 3 else run(False, False, 2)
         for i in range(len(inst)):
             assert np.array_equal(fused[i], ref[i]), (use_graph, groups, i)
-    with pytest.raises(L.LpmError):
-        e = L.Ensemble(ctx, L.biot_savart_kernel(), learned, [inst[0][2]], [inst[0][1].shape[0]], lanes=1)
-        try:
-            e.set_param("fused", 2)
-        finally:
-            e.close()
+    e = L.Ensemble(ctx, L.biot_savart_kernel(), learned, [inst[0][2]], [inst[0][1].shape[0]], lanes=1)
+    try:
+        for name, value in (("fused", 2), ("fused_groups", 0), ("fused_groups", 65), ("fused_groups", 1.5)):
+            with pytest.raises(L.LpmError):
+                e.set_param(name, value)
+        with pytest.raises(L.LpmError):
+            e.get_param("no_such_parameter")
+        assert e.get_param("fused") == 1.0 and e.get_param("fused_groups") == 2.0  # unchanged by the refusals
+    finally:
+        e.close()
 
 
 @pytest.mark.gpu
